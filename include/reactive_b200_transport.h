@@ -1,0 +1,130 @@
+/* reactive_transport_* : the transport C ABI exported by libreactive_b200.so.
+ *
+ * Every entry point keeps the reference signature, argument meaning, error text
+ * convention and return codes (0 ok, 1 error with text via
+ * reactive_transport_error, 2 concurrent entry rejected, -1 null handle;
+ * src/reactiveTransport/reactiveTransport.cpp:1471-1491). Host arrays are
+ * cell-major and borrowed only for the duration of the synchronous call.
+ * backend must be 1 (CUDA); backend 0 is rejected with an error because this
+ * library has no CPU execution path.
+ *
+ * The *_v3 entry points are additive: they take DEVICE pointers and a CUDA
+ * stream, never synchronise, and never allocate, so a caller can keep the
+ * conserved state resident in HBM and capture a whole step in a CUDA graph.
+ */
+#ifndef REACTIVE_B200_TRANSPORT_H
+#define REACTIVE_B200_TRANSPORT_H
+#include "reactive_b200_types.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/reactiveTransport/reactiveTransport.h:118-121 (impl. reactiveTransport.cpp:1494-1499) */
+void* reactive_transport_create(int backend, const ReactiveTransportConfig* config,
+    const double* volume, const ReactiveTransportFace* faces, const double* fixedQ,
+    const ReactiveTransportState* fixedStates, const double* fixedGasY,
+    const double* fixedGasH, char* error, size_t errorSize);
+/* src/reactiveTransport/reactiveTransport.h:60-63 (impl. reactiveTransport.cpp:1738-1743) */
+void* reactive_transport_create_v2(int backend, const ReactiveTransportConfig* config,
+    const ReactiveTransportOptionsV2* options, const double* volume, const ReactiveTransportFace* faces,
+    const double* fixedQ, const ReactiveTransportState* fixedStates, const double* fixedY, const double* fixedH,
+    char* error, size_t errorSize);
+/* src/reactiveTransport/reactiveTransportV21.h:24-27 (impl. reactiveTransport.cpp:1792-1808) */
+void* reactive_transport_create_v21(int backend, const ReactiveTransportConfig* config,
+    const ReactiveTransportOptionsV21* options, const double* volume, const ReactiveTransportFace* faces,
+    const double* fixedQ, const ReactiveTransportState* fixedStates, const double* fixedY, const double* fixedH,
+    char* error, size_t errorSize);
+/* src/reactiveTransport/reactiveTransport.h:122-125 */
+void reactive_transport_destroy(void* transport);
+const char* reactive_transport_error(void* transport);
+int reactive_transport_is_cuda(void* transport);
+int reactive_transport_stats(void* transport, ReactiveTransportStats* stats);
+/* src/reactiveTransport/reactiveTransport.h:84, :90, :64; reactiveTransportV21.h:28 */
+int reactive_transport_profile(void* transport, ReactiveTransportProfile* profile);
+int reactive_transport_device_profile(void* transport, ReactiveTransportDeviceProfile* profile);
+int reactive_transport_memory_v2(void* transport, ReactiveTransportMemoryV2* result);
+int reactive_transport_profile_v21(void* transport, ReactiveTransportProfileV21* result);
+/* src/reactiveTransport/reactiveTransport.h:126-127 (impl. reactiveTransport.cpp:1506-1512) */
+int reactive_transport_stable_step(void* transport, const double* q,
+    const ReactiveTransportState* state, double cfl, double maximum, double* dt);
+/* src/reactiveTransport/reactiveTransport.h:108-110 (impl. reactiveTransport.cpp:1647-1667) */
+int reactive_transport_stable_step_primitives(void* transport,
+    const ReactiveTransportPrimitive* primitive, const ReactiveTransportState* state,
+    double cfl, double maximum, double* dt);
+/* src/reactiveTransport/reactiveTransport.h:131-133 (impl. reactiveTransport.cpp:1518-1524) */
+int reactive_transport_stage(void* transport, double* q,
+    const ReactiveTransportState* state, const double* gasY, const double* gasH,
+    double dt, int stage, double* boundaryRate);
+/* src/reactiveTransport/reactiveTransport.h:135-137 (impl. reactiveTransport.cpp:1513-1517) */
+int reactive_transport_rhs(void* transport, const double* q,
+    const ReactiveTransportState* state, const double* gasY, const double* gasH,
+    double* rhs, double* boundaryRate);
+/* src/reactiveTransport/reactiveTransport.h:106 (impl. reactiveTransport.cpp:1557-1565) */
+int reactive_transport_upload_conserved(void* transport, const double* q, uint64_t version);
+/* src/reactiveTransport/reactiveTransport.h:113-115 (impl. reactiveTransport.cpp:1710-1720) */
+int reactive_transport_stage_resident(void* transport, const ReactiveTransportState* state,
+    const double* gasY, const double* gasH, double dt, int stage,
+    uint64_t inputVersion, uint64_t outputVersion, double* qOutput, double* boundaryRate);
+/* src/reactiveTransport/reactiveTransport.h:67-72 (impl. reactiveTransport.cpp:1750-1789) */
+int reactive_transport_begin_attempt(void* transport, const char* modelHash, uint64_t attemptId);
+int reactive_transport_end_attempt(void* transport, uint64_t attemptId, int commit);
+int reactive_transport_advance_resident_v2(void* transport, ReactiveTransportToken input,
+    ReactiveTransportToken output, const ReactiveTransportState* state, const ReactiveGasPartition* partition,
+    const double* gasY, const double* gasH, double dt, double* boundaryRate);
+int reactive_transport_download_conserved(void* transport, ReactiveTransportToken token, double* output);
+/* src/reactiveTransport/reactiveTransport.h:58-59 (impl. reactiveTransport.cpp:1636-1646) */
+int reactive_transport_replace_stage_state_v1(void* transport, ReactiveTransportToken before,
+    uint64_t replacementVersion, const double* conserved);
+/* src/reactiveTransport/reactiveTurbulence.h:20-25 (impl. reactiveTransport.cpp:1668-1709) */
+int reactive_transport_set_wale_v1(void* transport, const ReactiveWaleOptionsV1* options);
+int reactive_transport_wale_profile_v1(void* transport, ReactiveWaleProfileV1* profile);
+int reactive_transport_wale_primitives_v1(void* transport, const ReactiveTransportPrimitive* primitive,
+    const ReactiveTransportState* state, double* nut);
+/* Out-of-scope reference entry points kept as stubs that return 1 with a
+ * message, as the reference's own CPU build does for its CUDA-only paths
+ * (src/reactiveTransport/reactiveTransport.cpp:1613-1630):
+ * src/reactiveTransport/reactiveTransport.h:93-102 (NASA-generated gas properties),
+ * :48-54 (capillary), src/reactiveTransport/reactiveTurbulence.h:47-85 (WALE scalars/PR). */
+int reactive_transport_set_gas_thermo(void* transport, const ReactiveGasThermoSpecies* species,
+    size_t count, const ReactiveGasThermoRegion* regions, size_t regionCount,
+    const int64_t* liquidSpecies, size_t liquids);
+int reactive_transport_stage_resident_gas(void* transport, const ReactiveTransportState* state,
+    const ReactiveGasPartition* partition, double dt, int stage,
+    uint64_t inputVersion, uint64_t outputVersion, double* qOutput, double* boundaryRate);
+int reactive_transport_rhs_gas(void* transport, const double* q, const ReactiveTransportState* state,
+    const ReactiveGasPartition* partition, double* rhs, double* boundaryRate);
+int reactive_transport_gas_properties_resident(void* transport, const ReactiveTransportState* state,
+    const ReactiveGasPartition* partition, double* gasY, double* gasH);
+int reactive_transport_set_capillary_v1(void* transport, const void* options);
+int reactive_transport_capillary_geometry_v1(void* transport, const double* cellColor,
+    const double* fixedColor, double* surfaceEnergy, double* curvature, double* normalXYZ);
+int reactive_transport_capillary_profile_v1(void* transport, void* profile);
+int reactive_transport_set_wale_scalars_v1(void* transport, const void* options);
+int reactive_transport_wale_scalar_profile_v1(void* transport, void* profile);
+int reactive_transport_wale_scalar_fields_v1(void* transport, const double* cellCp,
+    const double* cellSpeciesH, const double* fixedCp, const double* fixedSpeciesH);
+
+/* ---- additive device-resident entry points (no reference counterpart; the
+ * reference's resident path is advance_resident_v2 + download_conserved,
+ * src/reactiveTransport/reactiveTransport.cpp:1773-1789, which round-trips q
+ * through the host between RK stages). Conserved arrays are SoA,
+ * q[k*(cells+fixed)+c], with the fixed-state tail filled by
+ * reactive_transport_fill_fixed_v3. */
+int reactive_transport_layout_v3(void* transport, size_t* cells, size_t* fixed, size_t* variables,
+    size_t* species);
+int reactive_transport_fill_fixed_v3(void* transport, double* q, ReactiveTransportState* state, void* stream);
+/* stage 0: qOut = qIn + dt L(qIn). stage 1: qOut = .5 qOut + .5 (qIn + dt L(qIn)),
+ * i.e. qOut holds q^n on entry. boundaryRate (device, variables doubles) may be null. */
+int reactive_transport_stage_device_v3(void* transport, const double* qIn, double* qOut,
+    const ReactiveTransportState* state, double dt, int stage, double* boundaryRate, void* stream);
+/* Writes the CFL step (or -1 when any face is invalid) to dt[0] on the device. */
+int reactive_transport_stable_step_device_v3(void* transport, const double* q,
+    const ReactiveTransportState* state, double cfl, double maximum, double* dt, void* stream);
+/* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading
+ * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
+int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

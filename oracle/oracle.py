@@ -1,0 +1,139 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the CPU oracles and to the
+reference's own CPU builds in oracle/_ref/. Imported by tests/, by
+__graft_entry__.smoke() and by bench.py's CPU-baseline leg, never by the product.
+"""
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = HERE / "_ref"
+ORACLE_LIB = HERE / "liboracle.so"
+REF_TRANSPORT = REF / "libreactiveTransport_ref.so"
+REF_FLASH = REF / "libref_flash.so"
+
+_d = C.POINTER(C.c_double)
+_v = C.c_void_p
+
+
+def build():
+    """Compile liboracle.so and, when the reference sources are present, _ref/."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
+
+
+def _load(path):
+    if not path.exists():
+        build()
+    return C.CDLL(str(path))
+
+
+_oracle = None
+_ref_transport = None
+_ref_flash = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        _oracle = _load(ORACLE_LIB)
+        _oracle.oracle_transport_rhs.argtypes = [_v, _d, _v, _d, _v, _d, _d, C.c_double, _d, _v, _d, _d,
+                                                 _d, _d, _d, _d]
+        _oracle.oracle_transport_rhs.restype = C.c_int
+        _oracle.oracle_transport_stable_dt.argtypes = [_v, _d, _v, _d, _v, C.c_double, _d, _v, C.c_double,
+                                                       C.c_double]
+        _oracle.oracle_transport_stable_dt.restype = C.c_double
+        _oracle.oracle_wale_nut.argtypes = [_d, C.c_double, C.c_double, _d]
+        _oracle.oracle_wale_nut.restype = C.c_int
+        if hasattr(_oracle, "oracle_flash_recover"):
+            _oracle.oracle_flash_recover.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _v, C.POINTER(C.c_int),
+                                                     C.POINTER(C.c_uint64), C.c_int]
+            _oracle.oracle_flash_recover.restype = C.c_int
+    return _oracle
+
+
+def ref_transport_lib():
+    """The reference's transport compiled for CPU (backend 0, serial)."""
+    global _ref_transport
+    if _ref_transport is None:
+        if not REF_TRANSPORT.exists():
+            build()
+        _ref_transport = C.CDLL(str(REF_TRANSPORT))
+    return _ref_transport
+
+
+def ref_flash_lib():
+    """The reference's device flash compiled for the host."""
+    global _ref_flash
+    if _ref_flash is None:
+        if not REF_FLASH.exists():
+            build()
+        lib = C.CDLL(str(REF_FLASH))
+        lib.ref_flash_recover.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _v, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_uint64), C.c_int, C.c_int]
+        lib.ref_flash_recover.restype = C.c_int
+        lib.ref_pr_evaluate_tp.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _d,
+                                           C.POINTER(C.c_int)]
+        lib.ref_pr_evaluate_trho.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, _d,
+                                             C.POINTER(C.c_int)]
+        _ref_flash = lib
+    return _ref_flash
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_d)
+
+
+def transport_rhs(case, q, states, gy=None, gh=None, wale_cw=-1.0, want_nut=False, want_denominator=False):
+    """Oracle RHS (cell-major), boundary ledger, nu_t, CFL denominators, status."""
+    cfg = case["config"]
+    nc, nv = cfg.cells, cfg.variables
+    rhs = np.zeros((nc, nv))
+    boundary = np.zeros(nv)
+    nut = np.zeros(nc) if want_nut else None
+    den = np.zeros(nc) if want_denominator else None
+    status = oracle_lib().oracle_transport_rhs(
+        C.byref(cfg), _p(case["volume"]), case["faces"], _p(case["fixed_q"]), case["fixed_states_ptr"],
+        _p(case.get("fixed_y")), _p(case.get("fixed_h")), wale_cw, _p(np.ascontiguousarray(q)),
+        C.cast(states, _v), _p(gy), _p(gh), _p(rhs), _p(boundary), _p(nut), _p(den))
+    return rhs, boundary, nut, den, status
+
+
+def wale_nut(g, delta, cw):
+    g = np.ascontiguousarray(g, dtype=np.float64).reshape(9)
+    out = C.c_double()
+    ok = oracle_lib().oracle_wale_nut(_p(g), delta, cw, C.byref(out))
+    return out.value if ok else None
+
+
+def transport_stable_dt(case, q, states, cfl, maximum, wale_cw=-1.0):
+    cfg = case["config"]
+    return oracle_lib().oracle_transport_stable_dt(
+        C.byref(cfg), _p(case["volume"]), case["faces"], _p(case["fixed_q"]), case["fixed_states_ptr"], wale_cw,
+        _p(np.ascontiguousarray(q)), C.cast(states, _v), cfl, maximum)
+
+
+def ref_flash_recover(model_image, q, energy, guess, threads=1, use_cache=True):
+    """Reference flash on the host: (states, success, counters[count,7])."""
+    from_dtype = guess.dtype
+    count = len(energy)
+    out = np.zeros(count, dtype=from_dtype)
+    success = np.zeros(count, dtype=np.int32)
+    counters = np.zeros((count, 7), dtype=np.uint64)
+    rc = ref_flash_lib().ref_flash_recover(
+        model_image, count, _p(np.ascontiguousarray(q, dtype=np.float64)),
+        _p(np.ascontiguousarray(energy, dtype=np.float64)), guess.ctypes.data_as(_v), out.ctypes.data_as(_v),
+        success.ctypes.data_as(C.POINTER(C.c_int)), counters.ctypes.data_as(C.POINTER(C.c_uint64)),
+        int(use_cache), int(threads))
+    if rc:
+        raise RuntimeError("reference flash rejected the model image")
+    return out, success, counters
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1

@@ -1,0 +1,449 @@
+// reactive_transport_* C ABI on B200: host object, residency/version contract,
+// and launch sequencing for the face-graph and structured Cartesian kernels.
+//
+// The contract (argument meaning, validation messages, return codes 0/1/2/-1,
+// version tokens, RK stage rules, residency invalidation on failure) follows
+// src/reactiveTransport/reactiveTransport.cpp:381-1815 and
+// src/reactiveTransport/reactiveTransport.h:48-141. Execution is CUDA only:
+// backend 0 (the reference's serial CPU loop) is rejected, never emulated.
+#include "transport_kernels.cuh"
+#include "../../include/reactive_b200_transport.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace rb200 {
+namespace {
+
+size_t product(size_t a, size_t b) {
+    require(!b || a <= std::numeric_limits<size_t>::max() / b, "Transport allocation size overflow");
+    return a * b;
+}
+
+struct DeviceArena {
+    std::vector<void*> blocks;
+    uint64_t bytes = 0, peak = 0;
+    double limit = 0;
+    template <class T> T* get(size_t n) {
+        if (!n) return nullptr;
+        const size_t b = product(n, sizeof(T));
+        require(double(bytes) + double(b) <= limit, "Transport exceeds maxDeviceMemoryGB/workspace budget");
+        void* p = nullptr;
+        check(cudaMalloc(&p, b), "cudaMalloc");
+        blocks.push_back(p);
+        bytes += b;
+        peak = std::max(peak, bytes);
+        return static_cast<T*>(p);
+    }
+    ~DeviceArena() { for (void* p : blocks) cudaFree(p); }
+};
+
+struct Transport {
+    std::mutex entry;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    ReactiveTransportConfig cfg{};
+    GraphView v{};
+    DeviceArena arena;
+    double* q = nullptr;        // SoA nv x all (the resident RK input)
+    double* initial = nullptr;  // SoA nv x all (the other RK buffer)
+    double* rhs = nullptr;      // SoA nv x cells (materialised diagnostic)
+    double* staging = nullptr;  // cell-major bridge, max(cells, fixed) x max(nv, 9... )
+    size_t stagingDoubles = 0;
+    double* reduceScratch = nullptr;
+    size_t reduceBlocks = 0;
+    double* boundaryRate = nullptr;
+    ReactiveTransportState* stateDevice = nullptr;
+    unsigned* flags = nullptr;  // [0] WALE failure
+    ReactiveTransportStats stats{};
+    ReactiveTransportProfile profile{};
+    ReactiveTransportDeviceProfile deviceProfile{};
+    ReactiveTransportProfileV21 cost{};
+    ReactiveWaleProfileV1 waleProfile{1, sizeof(ReactiveWaleProfileV1), 0, 0, 0, 0};
+    std::string physicalHash;
+    uint64_t attemptId = 0, lastAttempt = 0, tokenStage = 0;
+    bool attemptOpen = false;
+    uint64_t residentVersion = 0, highestVersion = 0;
+    bool haveResident = false, haveInitial = false;
+    double stageDt = 0;
+    uint64_t deviceCopies = 0, synchronizations = 0, memcpyCalls = 0;
+    char error[1024] = {0};
+
+    Transport(int backend, const ReactiveTransportConfig& c, const double* volumes,
+              const ReactiveTransportFace* faces, const double* fixedQ, const ReactiveTransportState* fixedStates,
+              const double* fixedY, const double* fixedH, const ReactiveTransportOptionsV2* options,
+              const ReactiveTransportOptionsV21* options21) {
+        require(backend == 0 || backend == 1, "Unknown transport backend");
+        require(backend == 1, "This library executes on CUDA only; backend 0 (serial CPU) is not provided");
+        int count = 0;
+        check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+        require(count > 0, "No CUDA device");
+        check(cudaGetDevice(&device), "cudaGetDevice");
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        cfg = c;
+        arena.limit = cfg.maxBytes;
+        if (options) {
+            require(options->abiVersion == 1 && options->structBytes == sizeof(*options) && options->bridgeCells > 0,
+                    "Invalid transport options ABI");
+            require(options->physicalModelHash[64] == 0 && std::strlen(options->physicalModelHash) == 64,
+                    "Invalid transport model hash");
+            physicalHash = options->physicalModelHash;
+            require(!options->recomputeGas, "Generated NASA gas properties are not part of this build");
+        }
+        if (options21) cost.blockThreads = options21->blockThreads;
+        cost.slots = 1;
+        require(cfg.cells && cfg.species && cfg.faces, "Empty transport mesh/model");
+        require(cfg.cells <= size_t(INT64_MAX) && cfg.faces < size_t(INT64_MAX) && cfg.fixed <= size_t(INT64_MAX),
+                "Transport index overflow");
+        require(cfg.mechanical ? cfg.variables == cfg.species + 6
+                               : (cfg.variables >= cfg.species + 4 && cfg.variables <= cfg.species + 6),
+                "Wrong transport conserved-variable count");
+        require(std::isfinite(cfg.maxBytes) && cfg.maxBytes > 0, "Invalid transport memory budget");
+        require(std::isfinite(cfg.waveFactor) && cfg.waveFactor >= 1, "Invalid transport wave factor");
+        require(std::isfinite(cfg.viscosity) && std::isfinite(cfg.conductivity) && std::isfinite(cfg.diffusivity)
+                    && cfg.viscosity >= 0 && cfg.conductivity >= 0 && cfg.diffusivity >= 0,
+                "Invalid transport coefficients");
+        require(!cfg.mechanical || (cfg.viscosity == 0 && cfg.conductivity == 0 && cfg.diffusivity == 0),
+                "Mechanical transport requires inviscid, non-diffusive model");
+        require(volumes && faces, "Null transport geometry");
+        require(cfg.cells <= std::numeric_limits<size_t>::max() - cfg.fixed, "Fixed-state index overflow");
+        const size_t all = cfg.cells + cfg.fixed;
+        std::vector<int64_t> row(cfg.cells + 1, 0), boundary;
+        for (size_t i = 0; i < cfg.cells; ++i)
+            require(std::isfinite(volumes[i]) && volumes[i] > 0, "Invalid transport volume");
+        for (size_t i = 0; i < cfg.faces; ++i) {
+            const auto& f = faces[i];
+            require(f.owner >= 0 && size_t(f.owner) < cfg.cells && f.neighbour >= -1
+                        && (f.neighbour < 0 || size_t(f.neighbour) < cfg.cells),
+                    "Invalid transport face cell");
+            require(f.kind >= 0 && f.kind <= 3 && (f.kind == 0) == (f.neighbour >= 0), "Invalid transport face kind");
+            require(f.kind != 3 || (f.fixed >= 0 && size_t(f.fixed) < cfg.fixed && !cfg.mechanical),
+                    "Invalid fixed boundary state index");
+            double norm = 0;
+            for (double x : f.normal) norm += x * x;
+            require(std::isfinite(norm) && std::abs(norm - 1) < 1e-8, "Invalid transport unit normal");
+            require(std::isfinite(f.area) && std::isfinite(f.distance) && std::isfinite(f.ownerWeight) && f.area > 0
+                        && f.distance > 0 && f.ownerWeight >= 0 && f.ownerWeight <= 1,
+                    "Invalid transport face geometry");
+            ++row[f.owner + 1];
+            if (f.neighbour >= 0) ++row[f.neighbour + 1];
+            else boundary.push_back(int64_t(i));
+        }
+        for (size_t i = 0; i < cfg.cells; ++i) row[i + 1] += row[i];
+        std::vector<int64_t> incidence(size_t(row.back()));
+        auto next = row;
+        for (size_t i = 0; i < cfg.faces; ++i) {
+            incidence[size_t(next[faces[i].owner]++)] = -int64_t(i) - 1;
+            if (faces[i].neighbour >= 0) incidence[size_t(next[faces[i].neighbour]++)] = int64_t(i) + 1;
+        }
+        std::vector<double> inverse(cfg.cells);
+        for (size_t i = 0; i < cfg.cells; ++i) {
+            inverse[i] = 1 / volumes[i];
+            require(std::isfinite(inverse[i]), "Invalid inverse volume");
+        }
+        validateStates(fixedStates, cfg.fixed);
+        std::vector<ReactiveTransportPrimitive> fixedPrimitive(cfg.fixed);
+        for (size_t i = 0; i < cfg.fixed; ++i) {
+            auto& p = fixedPrimitive[i];
+            for (size_t k = 0; k < cfg.species; ++k) p.rho += fixedQ[i * cfg.variables + k];
+            require(std::isfinite(p.rho) && p.rho > 0, "Invalid fixed density");
+            for (int d = 0; d < 3; ++d) {
+                p.u[d] = fixedQ[i * cfg.variables + cfg.species + d] / p.rho;
+                require(std::isfinite(p.u[d]), "Invalid fixed velocity");
+            }
+        }
+        auto* faceDevice = arena.get<ReactiveTransportFace>(cfg.faces);
+        auto* rowDevice = arena.get<int64_t>(row.size());
+        auto* incidenceDevice = arena.get<int64_t>(incidence.size());
+        auto* boundaryDevice = arena.get<int64_t>(boundary.size());
+        auto* invDevice = arena.get<double>(cfg.cells);
+        stateDevice = arena.get<ReactiveTransportState>(all);
+        q = arena.get<double>(product(all, cfg.variables));
+        initial = arena.get<double>(product(all, cfg.variables));
+        auto* primitive = arena.get<ReactiveTransportPrimitive>(all);
+        auto* work = arena.get<double>(product(cfg.faces, FW_FIELDS));
+        auto* carrier = arena.get<int>(cfg.faces);
+        auto* faceSpeed = arena.get<double>(cfg.faces);
+        auto* step = arena.get<double>(cfg.cells);
+        boundaryRate = arena.get<double>(cfg.variables);
+        flags = arena.get<unsigned>(4);
+        reduceBlocks = std::min<size_t>(1024, (cfg.cells + 255) / 256);
+        reduceScratch = arena.get<double>(reduceBlocks + 1);
+        double* gasY = nullptr;
+        double* gasH = nullptr;
+        if (cfg.diffusivity > 0) {
+            gasY = arena.get<double>(product(all, cfg.species));
+            gasH = arena.get<double>(product(all, cfg.species));
+        }
+        double* grad = cfg.viscosity > 0 ? arena.get<double>(product(cfg.cells, 9)) : nullptr;
+        stagingDoubles = std::max(product(std::max(cfg.cells, cfg.fixed), cfg.variables),
+                                  product(std::max(cfg.cells, cfg.fixed), cfg.species));
+        staging = arena.get<double>(stagingDoubles);
+        deviceProfile.faceWorkspaceBytes = product(cfg.faces, FW_FIELDS * sizeof(double) + sizeof(int) + sizeof(double));
+        profile.boundaryPartitions = 1;
+
+        upload(faceDevice, faces, cfg.faces);
+        upload(rowDevice, row.data(), row.size());
+        upload(incidenceDevice, incidence.data(), incidence.size());
+        upload(boundaryDevice, boundary.data(), boundary.size());
+        upload(invDevice, inverse.data(), cfg.cells);
+        upload(stateDevice + cfg.cells, fixedStates, cfg.fixed);
+        upload(primitive + cfg.cells, fixedPrimitive.data(), cfg.fixed);
+        check(cudaMemsetAsync(flags, 0, 4 * sizeof(unsigned), stream), "cudaMemsetAsync");
+
+        v.cells = cfg.cells; v.fixed = cfg.fixed; v.all = all; v.ns = cfg.species; v.nv = cfg.variables;
+        v.faces = cfg.faces; v.nBoundary = boundary.size(); v.mechanical = cfg.mechanical;
+        v.viscosity = cfg.viscosity; v.conductivity = cfg.conductivity; v.diffusivity = cfg.diffusivity;
+        v.waveFactor = cfg.waveFactor;
+        v.face = faceDevice; v.row = rowDevice; v.incidence = incidenceDevice; v.boundary = boundaryDevice;
+        v.invV = invDevice; v.state = stateDevice; v.q = q; v.primitive = primitive; v.grad = grad;
+        v.gasY = gasY; v.gasH = gasH; v.work = work; v.carrier = carrier; v.faceSpeed = faceSpeed; v.step = step;
+        v.waleError = flags;
+
+        packInto(q, fixedQ, cfg.fixed, cfg.variables, all, cfg.cells);
+        packInto(initial, fixedQ, cfg.fixed, cfg.variables, all, cfg.cells);
+        if (cfg.diffusivity > 0) {
+            packInto(gasY, fixedY, cfg.fixed, cfg.species, all, cfg.cells);
+            packInto(gasH, fixedH, cfg.fixed, cfg.species, all, cfg.cells);
+        }
+        finish();
+    }
+    ~Transport() {
+        if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+    }
+
+    // ---------------------------------------------------------------- transfers
+    template <class T> void upload(T* dst, const T* src, size_t n) {
+        if (!n) return;
+        require(src && dst, "Null transport input buffer");
+        check(cudaMemcpyAsync(dst, src, product(n, sizeof(T)), cudaMemcpyHostToDevice, stream), "H2D");
+        stats.uploadedBytes += product(n, sizeof(T));
+        ++memcpyCalls;
+    }
+    template <class T> void download(T* dst, const T* src, size_t n) {
+        if (!n) return;
+        require(src && dst, "Null transport output buffer");
+        check(cudaMemcpyAsync(dst, src, product(n, sizeof(T)), cudaMemcpyDeviceToHost, stream), "D2H");
+        stats.downloadedBytes += product(n, sizeof(T));
+        ++memcpyCalls;
+    }
+    void finish() {
+        ++synchronizations;
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    }
+    void launched() {
+        check(cudaGetLastError(), "kernel launch");
+        ++stats.kernelLaunches;
+    }
+    // Host cell-major rows -> SoA columns [offset, offset+count) of stride `stride`.
+    void packInto(double* dst, const double* src, size_t count, size_t width, size_t stride, size_t offset) {
+        if (!count) return;
+        require(src, "Null packed source");
+        upload(staging, src, count * width);
+        packSoA<<<gridFor(count * width, 256), 256, 0, stream>>>(staging, dst, count, width, stride, offset);
+        launched();
+        ++cost.layoutLaunches;
+        ++cost.layoutTiles;
+    }
+    void unpackFrom(double* dst, const double* src, size_t count, size_t width, size_t stride, size_t offset) {
+        require(dst, "Null unpack output");
+        unpackSoA<<<gridFor(count * width, 256), 256, 0, stream>>>(src, staging, count, width, stride, offset);
+        launched();
+        ++cost.layoutLaunches;
+        ++cost.layoutTiles;
+        download(dst, staging, count * width);
+    }
+    static void validateStates(const ReactiveTransportState* states, size_t count) {
+        require(!count || states, "Null transport state");
+        for (size_t c = 0; c < count; ++c) {
+            const auto& s = states[c];
+            require(std::isfinite(s.p) && s.p > 0 && std::isfinite(s.T) && s.T > 0 && std::isfinite(s.rho) && s.rho > 0
+                        && std::isfinite(s.sound) && s.sound > 0 && std::isfinite(s.cv) && s.cv > 0
+                        && std::isfinite(s.gasMass) && s.gasMass >= 0 && std::isfinite(s.dilatation),
+                    "Invalid recovered transport state");
+        }
+    }
+    void uploadQ(const double* hostQ) {
+        packInto(q, hostQ, cfg.cells, cfg.variables, v.all, 0);
+        ++profile.conservedUploads;
+        profile.conservedUploadBytes += cfg.cells * cfg.variables * sizeof(double);
+    }
+    void uploadState(const ReactiveTransportState* states) {
+        require(!cfg.cells || states, "Null transport state");
+        validateStates(states, cfg.cells);
+        upload(stateDevice, states, cfg.cells);
+        profile.stateUploadBytes += cfg.cells * sizeof(ReactiveTransportState);
+    }
+    void unpackQ(double* hostQ) {
+        unpackFrom(hostQ, q, cfg.cells, cfg.variables, v.all, 0);
+        profile.conservedDownloadBytes += cfg.cells * cfg.variables * sizeof(double);
+    }
+
+    // ---------------------------------------------------------------- kernels
+    void launchPrimitives(const double* qSoA, cudaStream_t s) {
+        GraphView g = v;
+        g.q = qSoA;
+        cellPrimitives<<<gridFor(v.all, 256), 256, 0, s>>>(g, 0, v.all);
+        launched();
+    }
+    void launchWale(cudaStream_t s, const ReactiveTransportState* state) {
+        GraphView g = v;
+        g.state = state;
+        cellGradients<<<gridFor(v.cells, 256), 256, 0, s>>>(g);
+        launched();
+        cellWale<<<gridFor(v.cells, 256), 256, 0, s>>>(g);
+        launched();
+        ++waleProfile.gradientBuilds;
+        ++waleProfile.viscosityBuilds;
+        waleProfile.cellsEvaluated += v.cells;
+    }
+    void buildWaleChecked() {
+        if (!v.wale) return;
+        check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
+        launchWale(stream, stateDevice);
+        unsigned status = 0;
+        download(&status, flags, 1);
+        finish();
+        require(!status, "Invalid WALE gradient/filter width/eddy viscosity");
+    }
+    // Face work (+ gradients) for one flux evaluation on device data.
+    void launchFaces(const double* qSoA, const ReactiveTransportState* state, cudaStream_t s) {
+        GraphView g = v;
+        g.q = qSoA;
+        g.state = state;
+        if (v.wale) launchWale(s, state);
+        else if (cfg.viscosity > 0) {
+            cellGradients<<<gridFor(v.cells, 256), 256, 0, s>>>(g);
+            launched();
+        }
+        faceWork<<<gridFor(v.faces, 128), 128, 0, s>>>(g);
+        launched();
+        ++deviceProfile.transportFaceLaunches;
+    }
+    void launchRates(const double* qSoA, const ReactiveTransportState* state, double* out, size_t stride,
+                     int mode, double dt, cudaStream_t s) {
+        GraphView g = v;
+        g.q = qSoA;
+        g.state = state;
+        cellRates<8><<<gridFor(v.cells, 128), 128, 0, s>>>(g, out, stride, mode, dt);
+        launched();
+    }
+    void launchLedger(const double* qSoA, const ReactiveTransportState* state, double* rate, cudaStream_t s) {
+        GraphView g = v;
+        g.q = qSoA;
+        g.state = state;
+        boundaryLedger<<<unsigned(cfg.variables), 256, 0, s>>>(g, rate);
+        launched();
+    }
+    void launchSpeeds(const ReactiveTransportState* state, cudaStream_t s) {
+        GraphView g = v;
+        g.state = state;
+        faceSpeeds<<<gridFor(v.faces, 256), 256, 0, s>>>(g);
+        launched();
+        ++deviceProfile.cflFaceLaunches;
+    }
+    void launchStep(double cfl, double maximumStep, double* result, cudaStream_t s) {
+        cellSteps<<<gridFor(v.cells, 256), 256, 0, s>>>(v, cfl, maximumStep);
+        launched();
+        const unsigned blocks = unsigned(reduceBlocks);
+        minimumReduce<<<blocks, 256, 0, s>>>(v.step, v.cells, reduceScratch);
+        launched();
+        minimumReduce<<<1, 1024, 0, s>>>(reduceScratch, blocks, result);
+        launched();
+    }
+
+    // ------------------------------------------------------- reference contract
+    void prepareResident(const ReactiveTransportState* states, const double* gasY, const double* gasH, bool transport) {
+        uploadState(states);
+        if (transport && cfg.diffusivity > 0) {
+            packInto(const_cast<double*>(v.gasY), gasY, cfg.cells, cfg.species, v.all, 0);
+            packInto(const_cast<double*>(v.gasH), gasH, cfg.cells, cfg.species, v.all, 0);
+            profile.gasUploadBytes += 2 * cfg.cells * cfg.species * sizeof(double);
+        }
+        launchPrimitives(q, stream);
+        if (v.wale) buildWaleChecked();
+        if (transport) {
+            GraphView g = v;
+            if (!v.wale && cfg.viscosity > 0) {
+                cellGradients<<<gridFor(v.cells, 256), 256, 0, stream>>>(g);
+                launched();
+            }
+            faceWork<<<gridFor(v.faces, 128), 128, 0, stream>>>(g);
+            launched();
+            ++deviceProfile.transportFaceLaunches;
+            if (v.wale) {
+                unsigned status = 0;
+                download(&status, flags, 1);
+                finish();
+                require(!status, "Nonfinite WALE traction/energy flux; stage remains uncommitted");
+            }
+        } else launchSpeeds(stateDevice, stream);
+    }
+    void prepare(const double* hostQ, const ReactiveTransportState* states, const double* gasY, const double* gasH,
+                 bool transport) {
+        haveResident = false;
+        uploadQ(hostQ);
+        prepareResident(states, gasY, gasH, transport);
+    }
+    void gather(bool materialize) {
+        if (materialize) {
+            if (!rhs) rhs = arena.get<double>(product(cfg.cells, cfg.variables));
+            launchRates(q, stateDevice, rhs, cfg.cells, 0, 0, stream);
+        }
+        launchLedger(q, stateDevice, boundaryRate, stream);
+    }
+    void stableStep(double cfl, double maximumStep, double* dt) {
+        require(dt && std::isfinite(cfl) && cfl > 0 && cfl <= .5 && std::isfinite(maximumStep) && maximumStep > 0,
+                "Invalid transport CFL controls");
+        launchStep(cfl, maximumStep, reduceScratch + reduceBlocks, stream);
+        download(dt, reduceScratch + reduceBlocks, 1);
+        finish();
+        require(std::isfinite(*dt) && *dt > 0, "Invalid wave/diffusion timestep");
+        ++stats.stepQueries;
+    }
+    void advance(double dt, int stage, double* hostQ, double* boundary) {
+        launchRates(q, stateDevice, initial, v.all, stage == 0 ? 1 : 2, dt, stream);
+        std::swap(q, initial);
+        v.q = q;
+        if (hostQ) unpackQ(hostQ);
+        download(boundary, boundaryRate, cfg.variables);
+        finish();
+        haveInitial = stage == 0;
+        stageDt = dt;
+        ++stats.stages;
+    }
+    void installWale(const ReactiveWaleOptionsV1& options) {
+        require(options.abiVersion == 1 && options.structBytes == sizeof(options), "Invalid WALE options ABI");
+        require(!v.wale && !highestVersion && !stats.stages && !stats.stepQueries && profile.conservedUploads == 0
+                    && profile.stateUploadBytes == 0,
+                "WALE is immutable and must be installed before stepping");
+        require(!cfg.mechanical, "WALE mechanical-environment closure is not implemented");
+        require(std::isfinite(options.Cw) && options.Cw >= 0, "Invalid WALE coefficient");
+        const size_t before = arena.bytes;
+        if (!v.grad) v.grad = arena.get<double>(product(cfg.cells, 9));
+        v.nut = arena.get<double>(cfg.cells);
+        v.cw = options.Cw;
+        v.wale = true;
+        waleProfile.workspaceBytes = arena.bytes - before + sizeof(uint32_t);
+    }
+    void uploadPrimitives(const ReactiveTransportPrimitive* primitive, const ReactiveTransportState* state) {
+        require(primitive, "Null transport primitives");
+        for (size_t c = 0; c < cfg.cells; ++c) {
+            require(std::isfinite(primitive[c].rho) && primitive[c].rho > 0, "Invalid primitive density");
+            for (double u : primitive[c].u) require(std::isfinite(u), "Invalid primitive velocity");
+        }
+        uploadState(state);
+        upload(v.primitive, primitive, cfg.cells);
+        profile.primitiveUploadBytes += cfg.cells * sizeof(ReactiveTransportPrimitive);
+    }
+};
+
+}  // namespace
+}  // namespace rb200
+
+#include "transport_abi.inc"

@@ -1,0 +1,399 @@
+// Face-graph transport kernels (any polyhedral face list), sm_100a, FP64.
+//
+// Operator semantics are those of the reference functors in
+// src/reactiveTransport/reactiveTransportKernels.h:
+//   cellPrimitives   <- Cells            :193-199
+//   cellGradients    <- Gradients        :290-301
+//   cellWale         <- WaleViscosities  :303-313
+//   faceSpeeds       <- FaceSpeeds       :315-341
+//   faceWork         <- Faces            :343-500 (HLL core, viscous/WALE traction,
+//                                                  conduction, Fick diffusion)
+//   cellRates        <- Rhs / Advance    :502-528, :551-560
+//   cellSteps        <- Step             :529-549
+// The data layout is this project's: conserved and gas fields are SoA with
+// stride cells+fixed; face work is SoA (one array per field) so every load in
+// the gather is coalesced over faces; one thread owns one cell and applies each
+// face's work record to up to eight variables from registers, so a face record
+// is read once per (cell, incidence, 8 variables) instead of once per variable.
+#pragma once
+#include "common.cuh"
+#include "wale.cuh"
+#include "../../include/reactive_b200_types.h"
+
+namespace rb200 {
+
+enum FaceWorkField {
+    FW_VELOCITY = 0, FW_ADV_L, FW_ADV_R, FW_P_MOM, FW_P_ENERGY, FW_TRACTION_X, FW_TRACTION_Y,
+    FW_TRACTION_Z, FW_ENERGY, FW_DIFFUSION, FW_SUM_J, FW_CARRIER_FLUX, FW_FIELDS
+};
+
+struct GraphView {
+    size_t cells = 0, fixed = 0, all = 0, ns = 0, nv = 0, faces = 0, nBoundary = 0;
+    int mechanical = 0;
+    double viscosity = 0, conductivity = 0, diffusivity = 0, waveFactor = 1;
+    const ReactiveTransportFace* face = nullptr;
+    const int64_t* row = nullptr;        // cells+1 offsets into incidence
+    const int64_t* incidence = nullptr;  // -(f+1): cell owns f; +(f+1): cell is f's neighbour
+    const int64_t* boundary = nullptr;   // boundary face ids
+    const double* invV = nullptr;
+    const ReactiveTransportState* state = nullptr;  // all
+    const double* q = nullptr;                       // SoA nv x all
+    ReactiveTransportPrimitive* primitive = nullptr; // all
+    double* grad = nullptr;                          // SoA 9 x cells
+    double* nut = nullptr;                           // cells
+    bool wale = false;
+    double cw = 0;
+    const double* gasY = nullptr;                    // SoA ns x all
+    const double* gasH = nullptr;
+    double* work = nullptr;                          // SoA FW_FIELDS x faces
+    int* carrier = nullptr;                          // faces
+    double* faceSpeed = nullptr;                     // faces
+    double* step = nullptr;                          // cells
+    unsigned* waleError = nullptr;
+};
+
+__device__ __forceinline__ size_t rightCell(const GraphView& v, const ReactiveTransportFace& f) {
+    return f.neighbour >= 0 ? size_t(f.neighbour)
+                            : (f.kind == 3 ? v.cells + size_t(f.fixed) : size_t(f.owner));
+}
+
+// Right-side velocities with the slip-wall mirror u - 2(u.n)n.
+__device__ __forceinline__ void sideVelocities(const GraphView& v, const ReactiveTransportFace& f,
+                                               double ul[3], double ur[3]) {
+    const ReactiveTransportPrimitive l = v.primitive[f.owner];
+    const ReactiveTransportPrimitive r = v.primitive[rightCell(v, f)];
+    double dot = 0;
+    for (int d = 0; d < 3; ++d) { ul[d] = l.u[d]; ur[d] = r.u[d]; dot += r.u[d] * f.normal[d]; }
+    if (f.kind == 1)
+        for (int d = 0; d < 3; ++d) ur[d] -= 2 * dot * f.normal[d];
+}
+
+__device__ __forceinline__ double faceNut(const GraphView& v, const ReactiveTransportFace& f, bool right) {
+    if (!v.wale) return 0;
+    return v.nut[right && f.neighbour >= 0 ? size_t(f.neighbour) : size_t(f.owner)];
+}
+
+__global__ void cellPrimitives(GraphView v, size_t begin, size_t end) {
+    for (size_t c = begin + blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < end;
+         c += size_t(blockDim.x) * gridDim.x) {
+        ReactiveTransportPrimitive p{};
+        for (size_t k = 0; k < v.ns; ++k) p.rho += v.q[k * v.all + c];
+        for (int d = 0; d < 3; ++d) p.u[d] = v.q[(v.ns + d) * v.all + c] / p.rho;
+        v.primitive[c] = p;
+    }
+}
+
+__global__ void cellGradients(GraphView v) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells;
+         c += size_t(blockDim.x) * gridDim.x) {
+        double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const double iv = v.invV[c];
+        for (int64_t j = v.row[c]; j < v.row[c + 1]; ++j) {
+            const int64_t e = v.incidence[j];
+            const ReactiveTransportFace f = v.face[e < 0 ? -e - 1 : e - 1];
+            double ul[3], ur[3];
+            sideVelocities(v, f, ul, ur);
+            const double scale = (e < 0 ? 1.0 : -1.0) * f.area * iv;
+            for (int i = 0; i < 3; ++i) {
+                const double uf = f.ownerWeight * ul[i] + (1 - f.ownerWeight) * ur[i];
+                for (int d = 0; d < 3; ++d) g[3 * i + d] += uf * f.normal[d] * scale;
+            }
+        }
+        for (int j = 0; j < 9; ++j) v.grad[j * v.cells + c] = g[j];
+    }
+}
+
+__global__ void cellWale(GraphView v) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells;
+         c += size_t(blockDim.x) * gridDim.x) {
+        double g[9];
+        for (int j = 0; j < 9; ++j) g[j] = v.grad[j * v.cells + c];
+        const double volume = 1 / v.invV[c];
+        double delta = 0, nut = 0;
+        bool ok = isfinite(volume) && volume > 0;
+        if (ok) { delta = cbrt(volume); ok = isfinite(delta) && delta > 0; }
+        ok = ok && waleEddyViscosity(g, delta, v.cw, nut);
+        if (!ok || !isfinite(nut) || nut < 0 || !isfinite(v.state[c].rho * nut)) {
+            atomicOr(v.waleError, 1u);
+            continue;
+        }
+        v.nut[c] = nut;
+    }
+}
+
+__global__ void faceSpeeds(GraphView v) {
+    for (size_t fi = blockIdx.x * size_t(blockDim.x) + threadIdx.x; fi < v.faces;
+         fi += size_t(blockDim.x) * gridDim.x) {
+        const ReactiveTransportFace f = v.face[fi];
+        const ReactiveTransportState sl = v.state[f.owner], sr = v.state[rightCell(v, f)];
+        double ul[3], ur[3], unL = 0, unR = 0;
+        sideVelocities(v, f, ul, ur);
+        for (int d = 0; d < 3; ++d) { unL += ul[d] * f.normal[d]; unR += ur[d] * f.normal[d]; }
+        const double aL = v.waveFactor * sl.sound, aR = v.waveFactor * sr.sound;
+        const double left = dmin(0, dmin(unL - aL, unR - aR)), right = dmax(0, dmax(unL + aL, unR + aR));
+        const double invWave = 1 / (right - left);
+        const double rhoNut = v.wale ? f.ownerWeight * sl.rho * faceNut(v, f, false)
+                                           + (1 - f.ownerWeight) * sr.rho * faceNut(v, f, true)
+                                     : 0;
+        const double mu = v.viscosity + rhoNut;
+        const double D = v.diffusivity
+            + dmax(dmax(4 * mu / (3 * sl.rho), 4 * mu / (3 * sr.rho)),
+                   dmax(v.conductivity / (sl.rho * sl.cv), v.conductivity / (sr.rho * sr.cv)));
+        double speed = dmax(fabs(unL) + aL, fabs(unR) + aR) + 2 * D / f.distance;
+        if (!isfinite(unL) || !isfinite(unR) || !isfinite(speed) || !isfinite(invWave) || right <= left)
+            speed = -1;
+        v.faceSpeed[fi] = speed;
+    }
+}
+
+__global__ void faceWork(GraphView v) {
+    for (size_t fi = blockIdx.x * size_t(blockDim.x) + threadIdx.x; fi < v.faces;
+         fi += size_t(blockDim.x) * gridDim.x) {
+        const ReactiveTransportFace f = v.face[fi];
+        const size_t l = size_t(f.owner), r = rightCell(v, f);
+        const ReactiveTransportState sl = v.state[l], sr = v.state[r];
+        const double w = f.ownerWeight;
+        double ul[3], ur[3], unL = 0, unR = 0;
+        sideVelocities(v, f, ul, ur);
+        for (int d = 0; d < 3; ++d) { unL += ul[d] * f.normal[d]; unR += ur[d] * f.normal[d]; }
+        const double aL = v.waveFactor * sl.sound, aR = v.waveFactor * sr.sound;
+        const double left = dmin(0, dmin(unL - aL, unR - aR)), right = dmax(0, dmax(unL + aL, unR + aR));
+        const double invWave = 1 / (right - left);
+        double out[FW_FIELDS] = {};
+        out[FW_VELOCITY] = (right * unL - left * unR) * invWave;
+        out[FW_ADV_L] = right * (unL - left) * invWave;
+        out[FW_ADV_R] = left * (right - unR) * invWave;
+        out[FW_P_MOM] = (right * sl.p - left * sr.p) * invWave;
+        out[FW_P_ENERGY] = (right * sl.p * unL - left * sr.p * unR) * invWave;
+        double traction[3] = {0, 0, 0}, energy = 0;
+        if (v.viscosity > 0 || v.wale) {
+            double g[9];
+            for (int j = 0; j < 9; ++j) {
+                g[j] = v.grad[j * v.cells + l];
+                if (f.neighbour >= 0) g[j] = w * g[j] + (1 - w) * v.grad[j * v.cells + r];
+            }
+            for (int i = 0; i < 3; ++i) {
+                double normal = 0;
+                for (int d = 0; d < 3; ++d) normal += g[i * 3 + d] * f.normal[d];
+                const double target = (ur[i] - ul[i]) / ((f.kind == 1 ? 2 : 1) * f.distance);
+                for (int d = 0; d < 3; ++d) g[i * 3 + d] += f.normal[d] * (target - normal);
+            }
+            const double div = g[0] + g[4] + g[8];
+            const double mu = v.viscosity
+                + (v.wale ? w * sl.rho * faceNut(v, f, false) + (1 - w) * sr.rho * faceNut(v, f, true) : 0);
+            for (int i = 0; i < 3; ++i)
+                for (int d = 0; d < 3; ++d)
+                    traction[i] += mu * (g[3 * i + d] + g[3 * d + i] - (i == d ? 2 * div / 3 : 0)) * f.normal[d];
+            if (f.kind == 1) {
+                double dot = 0;
+                for (int d = 0; d < 3; ++d) dot += traction[d] * f.normal[d];
+                for (int d = 0; d < 3; ++d) traction[d] = dot * f.normal[d];
+            }
+            for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * ul[d] + (1 - w) * ur[d]);
+        }
+        if (v.conductivity > 0 && f.kind != 1) energy -= v.conductivity * (sr.T - sl.T) / f.distance;
+        int carrier = 0;
+        if (v.diffusivity > 0 && sl.gasMass > 0 && sr.gasMass > 0 && f.kind != 1) {
+            const double mass = f.neighbour >= 0
+                ? sl.gasMass * sr.gasMass / ((1 - w) * sr.gasMass + w * sl.gasMass) : sl.gasMass;
+            const double diffusion = -mass * v.diffusivity / f.distance;
+            double sumJ = 0, largest = -1;
+            for (size_t k = 0; k < v.ns; ++k) {
+                const double yl = v.gasY[k * v.all + l], yr = v.gasY[k * v.all + r];
+                sumJ += diffusion * (yr - yl);
+                const double y = w * yl + (1 - w) * yr;
+                if (y > largest) { largest = y; carrier = int(k); }
+            }
+            const double hc = w * v.gasH[size_t(carrier) * v.all + l] + (1 - w) * v.gasH[size_t(carrier) * v.all + r];
+            double carrierFlux = 0;
+            for (size_t k = 0; k < v.ns; ++k) {
+                if (int(k) == carrier) continue;
+                const double yl = v.gasY[k * v.all + l], yr = v.gasY[k * v.all + r];
+                const double J = diffusion * (yr - yl) - (w * yl + (1 - w) * yr) * sumJ;
+                carrierFlux -= J;
+                const double hk = w * v.gasH[k * v.all + l] + (1 - w) * v.gasH[k * v.all + r];
+                energy += J * (hk - hc);
+            }
+            out[FW_DIFFUSION] = diffusion;
+            out[FW_SUM_J] = sumJ;
+            out[FW_CARRIER_FLUX] = carrierFlux;
+        }
+        if (v.wale) {
+            bool bad = !isfinite(energy);
+            for (int d = 0; d < 3; ++d) bad |= !isfinite(traction[d]);
+            if (bad) atomicOr(v.waleError, 1u);
+        }
+        out[FW_TRACTION_X] = traction[0];
+        out[FW_TRACTION_Y] = traction[1];
+        out[FW_TRACTION_Z] = traction[2];
+        out[FW_ENERGY] = energy;
+        for (int j = 0; j < FW_FIELDS; ++j) v.work[size_t(j) * v.faces + fi] = out[j];
+        v.carrier[fi] = carrier;
+    }
+}
+
+// Flux of variable k through face fi, times the face area (the reference's
+// View::faceFlux, src/reactiveTransport/reactiveTransportKernels.h:180-191).
+__device__ __forceinline__ double faceFluxK(const GraphView& v, const ReactiveTransportFace& f, size_t fi,
+                                            size_t r, size_t k, const double* wk, int carrier) {
+    const size_t l = size_t(f.owner);
+    const double ql = v.q[k * v.all + l];
+    double qr = v.q[k * v.all + r];
+    const size_t ns = v.ns;
+    if (f.kind == 1 && k >= ns && k < ns + 3) {
+        double normal = 0;
+        for (int d = 0; d < 3; ++d) normal += v.q[(ns + d) * v.all + r] * f.normal[d];
+        qr -= 2 * normal * f.normal[k - ns];
+    }
+    double flux = wk[FW_ADV_L] * ql + wk[FW_ADV_R] * qr;
+    if (k >= ns && k < ns + 3) flux += wk[FW_P_MOM] * f.normal[k - ns];
+    if (k == ns + 3) flux += wk[FW_P_ENERGY];
+    if (k < ns) {
+        if (wk[FW_DIFFUSION] != 0) {
+            if (int(k) == carrier) flux += wk[FW_CARRIER_FLUX];
+            else {
+                const double yl = v.gasY[k * v.all + l], yr = v.gasY[k * v.all + r];
+                flux += wk[FW_DIFFUSION] * (yr - yl) - (f.ownerWeight * yl + (1 - f.ownerWeight) * yr) * wk[FW_SUM_J];
+            }
+        }
+    } else if (k < ns + 3) flux -= wk[FW_TRACTION_X + (k - ns)];
+    else if (k == ns + 3) flux += wk[FW_ENERGY];
+    return flux * f.area;
+}
+
+// mode 0: rate -> out (SoA nv x cells, the materialised RHS)
+// mode 1: SSPRK2 stage 0, out = q + dt*rate
+// mode 2: SSPRK2 stage 1, out = .5*out + .5*(q + dt*rate)   (out holds q^n)
+// out has stride `outStride` (cells for the RHS, all for the RK buffers).
+template <int CHUNK>
+__global__ void cellRates(GraphView v, double* out, size_t outStride, int mode, double dt) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells;
+         c += size_t(blockDim.x) * gridDim.x) {
+        const double iv = v.invV[c];
+        const int64_t begin = v.row[c], end = v.row[c + 1];
+        double div = 0;
+        if (v.mechanical) {
+            for (int64_t j = begin; j < end; ++j) {
+                const int64_t e = v.incidence[j];
+                const size_t fi = size_t(e < 0 ? -e - 1 : e - 1);
+                const double sign = e < 0 ? -1 : 1;
+                div -= sign * v.work[FW_VELOCITY * v.faces + fi] * v.face[fi].area * iv;
+            }
+        }
+        for (size_t k0 = 0; k0 < v.nv; k0 += CHUNK) {
+            double acc[CHUNK];
+#pragma unroll
+            for (int kk = 0; kk < CHUNK; ++kk) acc[kk] = 0;
+            for (int64_t j = begin; j < end; ++j) {
+                const int64_t e = v.incidence[j];
+                const size_t fi = size_t(e < 0 ? -e - 1 : e - 1);
+                const double sign = e < 0 ? -1 : 1;
+                const ReactiveTransportFace f = v.face[fi];
+                const size_t r = rightCell(v, f);
+                double wk[FW_FIELDS];
+#pragma unroll
+                for (int t = 0; t < FW_FIELDS; ++t) wk[t] = v.work[size_t(t) * v.faces + fi];
+                const int carrier = v.carrier[fi];
+#pragma unroll
+                for (int kk = 0; kk < CHUNK; ++kk) {
+                    const size_t k = k0 + kk;
+                    if (k < v.nv) acc[kk] += sign * faceFluxK(v, f, fi, r, k, wk, carrier) * iv;
+                }
+            }
+#pragma unroll
+            for (int kk = 0; kk < CHUNK; ++kk) {
+                const size_t k = k0 + kk;
+                if (k >= v.nv) break;
+                double rate = acc[kk];
+                if (v.mechanical && k >= v.ns + 4)
+                    rate += (v.q[k * v.all + c] + (k == v.ns + 4 ? 1 : -1) * v.state[c].dilatation) * div;
+                const size_t o = k * outStride + c;
+                if (mode == 0) out[o] = rate;
+                else if (mode == 1) out[o] = v.q[k * v.all + c] + dt * rate;
+                else out[o] = .5 * out[o] + .5 * (v.q[k * v.all + c] + dt * rate);
+            }
+        }
+    }
+}
+
+__global__ void cellSteps(GraphView v, double cfl, double maximumStep) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells;
+         c += size_t(blockDim.x) * gridDim.x) {
+        double denominator = 0;
+        bool bad = false;
+        for (int64_t j = v.row[c]; j < v.row[c + 1]; ++j) {
+            const int64_t e = v.incidence[j];
+            const size_t fi = size_t(e < 0 ? -e - 1 : e - 1);
+            const double speed = v.faceSpeed[fi];
+            if (!isfinite(speed) || speed < 0) { bad = true; break; }
+            denominator += v.face[fi].area * speed;
+        }
+        double step = denominator > 0 ? dmin(maximumStep, cfl / (v.invV[c] * denominator)) : maximumStep;
+        if (bad || !isfinite(denominator) || denominator < 0) step = -1;
+        v.step[c] = step;
+    }
+}
+
+// Global minimum with invalid (non-finite or non-positive) entries absorbing as
+// -1 (the reference's Minimum, src/reactiveTransport/reactiveTransport.cpp:222-232).
+// Pass 1 writes one value per block, pass 2 (one block) folds them.
+__global__ void minimumReduce(const double* in, size_t n, double* out) {
+    __shared__ double warpValues[32];
+    double m = HUGE_VAL;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(blockDim.x) * gridDim.x) {
+        const double x = in[i];
+        m = fmin(m, isfinite(x) && x > 0 ? x : -1.0);
+    }
+    m = warpMin(m);
+    if ((threadIdx.x & 31) == 0) warpValues[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? warpValues[threadIdx.x] : HUGE_VAL;
+        m = warpMin(m);
+        if (threadIdx.x == 0) out[blockIdx.x] = m;
+    }
+}
+
+// Boundary ledger: sum over boundary faces of faceFlux(f,k), one block per
+// variable, deterministic order (block-strided accumulation then tree).
+__global__ void boundaryLedger(GraphView v, double* rate) {
+    __shared__ double warpValues[32];
+    const size_t k = blockIdx.x;
+    double s = 0;
+    for (size_t j = threadIdx.x; j < v.nBoundary; j += blockDim.x) {
+        const size_t fi = size_t(v.boundary[j]);
+        const ReactiveTransportFace f = v.face[fi];
+        double wk[FW_FIELDS];
+        for (int t = 0; t < FW_FIELDS; ++t) wk[t] = v.work[size_t(t) * v.faces + fi];
+        s += faceFluxK(v, f, fi, rightCell(v, f), k, wk, v.carrier[fi]);
+    }
+    s = warpSum(s);
+    if ((threadIdx.x & 31) == 0) warpValues[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? warpValues[threadIdx.x] : 0.0;
+        s = warpSum(s);
+        if (threadIdx.x == 0) rate[k] = s;
+    }
+}
+
+// Cell-major (c*width + k) <-> SoA (k*stride + offset + c) transposition used at
+// the host boundary; the host ABI stays cell-major.
+__global__ void packSoA(const double* __restrict__ in, double* __restrict__ out, size_t count,
+                        size_t width, size_t stride, size_t offset) {
+    const size_t n = count * width;
+    for (size_t j = blockIdx.x * size_t(blockDim.x) + threadIdx.x; j < n; j += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = j / width, k = j % width;
+        out[k * stride + offset + c] = in[j];
+    }
+}
+__global__ void unpackSoA(const double* __restrict__ in, double* __restrict__ out, size_t count,
+                          size_t width, size_t stride, size_t offset) {
+    const size_t n = count * width;
+    for (size_t j = blockIdx.x * size_t(blockDim.x) + threadIdx.x; j < n; j += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = j / width, k = j % width;
+        out[j] = in[k * stride + offset + c];
+    }
+}
+
+}  // namespace rb200
