@@ -1,0 +1,67 @@
+/* reactive_gpu_hem_* : the HEM UV-flash C ABI exported by libreactive_b200.so.
+ *
+ * Model images, batch arrays, success flags and profile structs are those of the
+ * reference ABI (src/reactiveThermo/reactiveGpuHem.h:40-84). This build flashes
+ * one condensable species with its own pure liquid (ns = 1, nl = 1, no solid,
+ * boundaryRecovery = 0, the pure-N2O configuration); create rejects other
+ * images with an error message. Device or API errors never fall back to a CPU
+ * flash. A failed cell leaves the caller's state unchanged and reports
+ * success = 0.
+ */
+#ifndef REACTIVE_B200_HEM_H
+#define REACTIVE_B200_HEM_H
+#include "reactive_b200_types.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/reactiveThermo/reactiveGpuHem.h:40 (policy strings :31-37) */
+const char* reactive_gpu_hem_numerical_policy_v1(void);
+/* src/reactiveThermo/reactiveGpuHem.h:41 (impl. src/reactiveTransport/reactiveGpuHem.cuh:190-219) */
+void* reactive_gpu_hem_create_v1(const void* model, size_t modelBytes, size_t capacity, char* error, size_t errorSize);
+/* src/reactiveThermo/reactiveGpuHem.h:44 */
+void* reactive_gpu_hem_create_resident_v1(const void* model, size_t modelBytes, size_t capacity, char* error,
+    size_t errorSize);
+/* src/reactiveThermo/reactiveGpuHem.h:46-47 */
+size_t reactive_gpu_hem_device_bytes_v1(void* hem);
+void reactive_gpu_hem_destroy_v1(void* hem);
+/* src/reactiveThermo/reactiveGpuHem.h:51-52 (impl. reactiveGpuHem.cuh:227-353): q holds ns masses per
+ * cell, energy the internal energy density, state the seed in / the result out. */
+int reactive_gpu_hem_run_v1(void* hem, const double* q, const double* energy, size_t count,
+    ReactiveThermoState* state, int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);
+/* src/reactiveThermo/reactiveGpuHem.h:63-72, :81-84: capillary and primitive-initialisation
+ * paths; outside this build's scope, they return 1 with a message. */
+int reactive_gpu_hem_run_v2(void* hem, const double* q, const double* energy,
+    const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* state, int* success,
+    ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);
+int reactive_gpu_hem_initialize_tp_v1(void* hem, double* q, double* energy,
+    const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* state, int* success,
+    ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);
+int reactive_gpu_hem_run_resident_v1(void* hem, const double* q, const double* energy,
+    const ReactiveThermoState* seed, const ReactiveGpuHemCapillaryInputV2* capillary, const uint32_t* order,
+    size_t count, ReactiveGpuHemOutputV1* output, ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);
+
+/* ---- additive device-resident entry point (no reference counterpart; the
+ * reference's resident HEM takes host-prepared q/energy arrays,
+ * src/reactiveTransport/reactiveGpuHem.cuh:360-403). All pointers are DEVICE
+ * memory. `conserved` is the transport's SoA conserved array (row k at
+ * conserved + k*stride; species rows, three momentum rows, total energy), the
+ * internal energy is formed on the device. seed/state are full thermo states;
+ * transport (optional) receives the compact transport state. success (optional)
+ * receives per-cell flags; failed cells copy their seed. Never synchronises or
+ * allocates; safe to capture in a CUDA graph.
+ * flags bit 0: count the batch's work counters (read with run_counters_v3). */
+int reactive_gpu_hem_run_device_v3(void* hem, const double* conserved, size_t stride, size_t count,
+    size_t variables, const ReactiveThermoState* seed, ReactiveThermoState* state,
+    ReactiveTransportState* transport, int* success, void* reserved, int flags, void* stream,
+    char* error, size_t errorSize);
+/* Synchronises `stream` and reports the counters accumulated since the last call
+ * (phase/residual evaluations, candidates, stable candidates, failures in
+ * deviceFailures, Jacobians); resets them. */
+int reactive_gpu_hem_run_counters_v3(void* hem, ReactiveGpuHemProfileV1* profile, void* stream, char* error,
+    size_t errorSize);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -28,4 +28,14 @@ double oracle_transport_stable_dt(const ReactiveTransportConfig* cfg, const doub
 /* WALE nu_t for one velocity gradient g[3i+j] = du_i/dx_j; returns 0 on invalid input. */
 int oracle_wale_nut(const double* g, double delta, double cw, double* nut);
 
+/* Pure-component (ns = 1, nl = 1) HEM UV flash over `count` cells; q holds one
+ * mass density per cell, energy the internal energy density, guess the seed
+ * states. counters: 7 per cell (phases, residuals, candidates, stable, failures,
+ * analytic Jacobians, finite-difference Jacobians), may be null. Returns 1 for a
+ * model outside the pure-component scope. */
+int oracle_flash_recover(const char* image, size_t count, const double* q, const double* energy,
+    const ReactiveThermoState* guess, ReactiveThermoState* out, int* success, uint64_t* counters, int threads);
+int oracle_pr_evaluate_tp(const char* image, int table, double T, double p, int choice, int chem,
+    double* out, int* phase);
+
 #endif

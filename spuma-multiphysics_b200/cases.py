@@ -1,0 +1,159 @@
+"""Synthetic case construction on the host (seeded, reproducible).
+
+* flash_batch: the standalone HEM workload, states generated forward from a
+  seed: a share of saturated two-phase cells (T uniform, vapour quality uniform
+  in [0, 1]) and single-phase cells (p log-uniform, T uniform) converted to
+  (rho, e) by Peng-Robinson on the default (largest-volume) root.
+* impingement: the N2O impingement cube. Uniform Cartesian face list in the
+  ordering of the reference's mesh tool (tools/impinging_cartesian_mesh.py:54-127:
+  internal faces sorted by (owner, neighbour), then boundary patches), two
+  circular ports on x=0 and y=0 selected by face centre inside the circle
+  (:12-36), boundary weights and distances as the solver assigns them
+  (src/reactiveFoam/ReactiveFoam.C:1193-1204: fixed-state 0, extrapolate 1,
+  internal 1 - ownerDistance/distance).
+"""
+import numpy as np
+
+from . import _abi as A
+from .eos import PureFluid
+from .thermo_data import N2O
+
+
+def flash_batch(n, seed=20260303, two_phase_share=0.6, fluid=None, seed_policy="exact"):
+    """(q, e, guess states, generating labels) for n pure-fluid cells.
+
+    seed_policy "exact": the generating (p, T, liquid mass) is the flash seed;
+    "fixed": every seed is 40 bar / 293.15 K gas.
+    """
+    fluid = fluid or PureFluid(N2O)
+    rng = np.random.default_rng(seed)
+    n2 = int(round(two_phase_share * n))
+    n1 = n - n2
+    T2 = rng.uniform(220.0, 305.0, n2)
+    x = rng.uniform(0.0, 1.0, n2)
+    psat, gas, liq = fluid.saturation(T2)
+    v2 = x / gas["rho"] + (1 - x) / liq["rho"]
+    rho2 = 1 / v2
+    e2 = rho2 * (x * gas["e"] + (1 - x) * liq["e"])
+    ml2 = (1 - x) * rho2
+    p1 = np.exp(rng.uniform(np.log(1e5), np.log(80e5), n1))
+    T1 = rng.uniform(200.0, 320.0, n1)
+    one = fluid.tp(T1, p1, "auto")
+    rho = np.concatenate([rho2, one["rho"]])
+    e = np.concatenate([e2, one["rho"] * one["e"]])
+    T = np.concatenate([T2, T1])
+    p = np.concatenate([psat, p1])
+    ml = np.concatenate([ml2, np.zeros(n1)])
+    order = rng.permutation(n)
+    rho, e, T, p, ml = rho[order], e[order], T[order], p[order], ml[order]
+    guess = np.zeros(n, dtype=A.THERMO_DTYPE)
+    if seed_policy == "exact":
+        guess["p"], guess["T"] = p, T
+        guess["liquidMass"][:, 0] = ml
+        guess["activeLiquids"] = (ml > 0).astype(np.int32)
+    else:
+        guess["p"], guess["T"] = 40e5, 293.15
+    guess["rho"] = rho
+    return np.ascontiguousarray(rho), np.ascontiguousarray(e), guess
+
+
+def phase_label(states):
+    """0 gas only, 1 liquid only, 2 two-phase (from gasMass > 0 and activeLiquids)."""
+    gas = states["gasMass"] > 0
+    liq = states["activeLiquids"] != 0
+    return np.where(gas & liq, 2, np.where(liq, 1, 0)).astype(np.int8)
+
+
+def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset=0.006, boundary_kind=2):
+    """Face array (numpy FACE_DTYPE) and cell volumes of an n^3 cube.
+
+    Port faces on x=0 (centre y=port_offset, z=port_z) and y=0 (centre
+    x=port_offset, z=port_z) are fixed-state faces (fixed index 0); every other
+    boundary face has kind `boundary_kind` (2 extrapolate: transmissive).
+    """
+    h = edge / n
+    area, volume = h * h, h ** 3
+    cell = lambda i, j, k: i + n * (j + n * k)
+    internal = []
+    # owner, neighbour for x, y, z faces
+    k, j, i = np.indices((n, n, n - 1))
+    internal.append((cell(i, j, k).ravel(), cell(i + 1, j, k).ravel(), 0))
+    k, j, i = np.indices((n, n - 1, n))
+    internal.append((cell(i, j, k).ravel(), cell(i, j + 1, k).ravel(), 1))
+    k, j, i = np.indices((n - 1, n, n))
+    internal.append((cell(i, j, k).ravel(), cell(i, j, k + 1).ravel(), 2))
+    owners = np.concatenate([a[0] for a in internal])
+    neighbours = np.concatenate([a[1] for a in internal])
+    axes = np.concatenate([np.full(a[0].size, a[2]) for a in internal])
+    order = np.lexsort((neighbours, owners))
+    owners, neighbours, axes = owners[order], neighbours[order], axes[order]
+    nint = owners.size
+    r2 = (port_diameter / 2) ** 2
+    bnd = []  # (owner, axis, sign, kind)
+    for axis in range(3):
+        for upper in (False, True):
+            a, b = np.indices((n, n))  # the two lateral indices (slow, fast)
+            coords = [None, None, None]
+            lat = [d for d in range(3) if d != axis]
+            coords[lat[1]], coords[lat[0]] = a.ravel(), b.ravel()
+            coords[axis] = np.full(n * n, n - 1 if upper else 0)
+            owner = cell(*coords)
+            kind = np.full(n * n, boundary_kind)
+            if not upper and axis < 2:
+                lateral = 1 - axis
+                xc = (coords[lateral] + .5) * h
+                zc = (coords[2] + .5) * h
+                port = (xc - port_offset) ** 2 + (zc - port_z) ** 2 < r2
+                kind[port] = 3
+            bnd.append((owner, np.full(n * n, axis), np.full(n * n, 1.0 if upper else -1.0), kind))
+    b_owner = np.concatenate([x[0] for x in bnd])
+    b_axis = np.concatenate([x[1] for x in bnd])
+    b_sign = np.concatenate([x[2] for x in bnd])
+    b_kind = np.concatenate([x[3] for x in bnd])
+    faces = np.zeros(nint + b_owner.size, dtype=A.FACE_DTYPE)
+    faces["owner"][:nint] = owners
+    faces["neighbour"][:nint] = neighbours
+    faces["fixed"][:nint] = -1
+    faces["normal"][np.arange(nint), axes] = 1.0
+    faces["area"][:nint] = area
+    faces["distance"][:nint] = h
+    faces["ownerWeight"][:nint] = 0.5
+    faces["kind"][:nint] = 0
+    sl = slice(nint, None)
+    faces["owner"][sl] = b_owner
+    faces["neighbour"][sl] = -1
+    faces["fixed"][sl] = np.where(b_kind == 3, 0, -1)
+    normals = np.zeros((b_owner.size, 3))
+    normals[np.arange(b_owner.size), b_axis] = b_sign
+    faces["normal"][sl] = normals
+    faces["area"][sl] = area
+    faces["distance"][sl] = h / 2
+    faces["ownerWeight"][sl] = np.where(b_kind == 3, 0.0, np.where(b_kind == 2, 1.0, 0.5))
+    faces["kind"][sl] = b_kind
+    return faces, np.full(n ** 3, volume)
+
+
+def impingement(n, fluid=None, seed=1234, ambient_p=40e5, ambient_T=293.15, inlet_p=56.01325e5, inlet_T=293.15,
+                perturbation=0.01):
+    """Initial conserved state (cell-major n^3 x 5), seed thermo states and the
+    liquid inlet (fixed q and thermo) of the N2O impingement case."""
+    fluid = fluid or PureFluid(N2O)
+    rng = np.random.default_rng(seed)
+    N = n ** 3
+    gas = fluid.tp(np.array([ambient_T]), np.array([ambient_p]), "gas")
+    rho0 = gas["rho"][0]
+    rho = rho0 * (1 + perturbation * rng.uniform(-1, 1, N))
+    T = np.full(N, ambient_T)
+    props = fluid.trho(T, rho)
+    q = np.zeros((N, 5))
+    q[:, 0] = rho
+    q[:, 4] = rho * props["e"]
+    guess = np.zeros(N, dtype=A.THERMO_DTYPE)
+    guess["p"], guess["T"], guess["rho"] = props["p"], T, rho
+    liq = fluid.tp(np.array([inlet_T]), np.array([inlet_p]), "liquid")
+    fixed_q = np.array([[liq["rho"][0], 0, 0, 0, liq["rho"][0] * liq["e"][0]]])
+    fixed_guess = np.zeros(1, dtype=A.THERMO_DTYPE)
+    fixed_guess["p"], fixed_guess["T"], fixed_guess["rho"] = inlet_p, inlet_T, liq["rho"][0]
+    fixed_guess["liquidMass"][:, 0] = liq["rho"][0]
+    fixed_guess["activeLiquids"] = 1
+    return dict(q=q, guess=guess, fixed_q=fixed_q, fixed_guess=fixed_guess)

@@ -1,1 +1,706 @@
-// placeholder until the HEM sources land
+// reactive_gpu_hem_* C ABI on B200: candidate-parallel pure-fluid UV flash.
+//
+// Launch sequence per batch (all on one stream, no host synchronisation, no
+// allocation; capturable in a CUDA graph):
+//   1 inputs     per cell: (rho, e, seed p/T/liquid mass)
+//   2 pass A     persistent work queue over (cell, {all-gas, all-liquid})
+//   3 compact    cells that still need the two-phase seeds (all cells unless
+//                the model's stableGasPrune option skips them after a stable gas)
+//   4 pass B     persistent work queue over (listed cell, 5 beta seeds)
+//   5 select     first maximum entropy among stable candidates, in reference
+//                order; cells without one are queued for the restart search
+//   6 pass C     persistent queue over (queued cell, 4 restart temperatures),
+//                each running the 5 seeds and keeping its first best
+//   7 select     over the 4 restarts; cells still without a candidate fail
+// Candidate records live in HBM (192 B each); every loop in the solvers is
+// bounded and no thread waits on another, so every launch terminates.
+#include "hem_flash.cuh"
+#include "common.cuh"
+#include "../../include/reactive_b200_hem.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace rb200 {
+namespace {
+
+struct CandRecord {
+    ReactiveThermoState st;
+    double entropyD;
+    int status;  // 0 not converged, 1 converged but unstable, 2 converged and stable
+    int pad;
+};
+static_assert(sizeof(CandRecord) == 192, "candidate record layout");
+
+enum Counter { Q_A = 0, Q_B, LIST, Q_C, FALLBACK, FAILED, NCOUNTERS = 8 };
+enum Total { T_PHASES = 0, T_RESIDUALS, T_CANDIDATES, T_STABLE, T_FAILURES, T_ANALYTIC, T_FD, NTOTALS = 8 };
+
+constexpr int kPassThreads = 128;
+__constant__ double kSeeds[5] = {-1, .5, .95, .1, .9999};
+__constant__ double kRestart[4] = {0.02, 0.25, 0.5, 0.75};
+
+__device__ __forceinline__ void flushCounts(const Counts& n, unsigned long long* totals) {
+    unsigned long long v[7] = {n.phases, n.residuals, n.candidates, n.stable, n.failures, n.analytic, n.fd};
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        unsigned long long x = v[i];
+        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(totals + i, x);
+    }
+}
+
+// Warp-wide dynamic fetch of 32 consecutive items from a device counter.
+__device__ __forceinline__ unsigned fetchItems(unsigned* counter) {
+    unsigned base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+__global__ void inputsFromHost(const double* q, const double* energy, const ReactiveThermoState* guess, size_t count,
+                               int ns, CellInput* in) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
+        double rho = 0;
+        for (int k = 0; k < ns; ++k) rho += q[c * ns + k];
+        const ReactiveThermoState g = guess[c];
+        in[c] = CellInput{rho, energy[c], g.p, g.T, g.liquidMass[0]};
+    }
+}
+
+// Internal energy density E - |m|^2/(2 rho) from the SoA conserved rows.
+__global__ void inputsFromConserved(const double* cons, size_t stride, size_t count, int ns,
+                                    const ReactiveThermoState* seed, CellInput* in) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
+        double rho = 0;
+        for (int k = 0; k < ns; ++k) rho += cons[size_t(k) * stride + c];
+        const double mx = cons[size_t(ns) * stride + c], my = cons[size_t(ns + 1) * stride + c],
+                     mz = cons[size_t(ns + 2) * stride + c], E = cons[size_t(ns + 3) * stride + c];
+        const double e = E - .5 * (mx * mx + my * my + mz * mz) / rho;
+        in[c] = CellInput{rho, e, seed[c].p, seed[c].T, seed[c].liquidMass[0]};
+    }
+}
+
+__device__ inline void finishCandidate(const HemConst& C, const CellInput& in, bool ok, const Eval& v,
+                                       const CandidateOut& o, CandRecord* rec, Counts& n) {
+    int status = 0;
+    if (ok) {
+        stateFromEval(v, in.q, o, rec->st);
+        rec->entropyD = v.entropyD;
+        const double mass = v.liqMass, p = v.p, T = v.T;
+        status = stableAt(C, in.q, mass, p, T, n) ? 2 : 1;
+    }
+    if (status == 2) ++n.stable; else ++n.failures;
+    rec->status = status;
+}
+
+// Pass A: items (kind in {gas, liquid}) x cells, kind-major so a warp runs one
+// candidate kind over consecutive cells.
+__global__ void __launch_bounds__(kPassThreads) passPartitions(const HemConst* __restrict__ Cp,
+                                                               const CellInput* __restrict__ in, size_t count,
+                                                               CandRecord* rec, unsigned* counters,
+                                                               unsigned long long* totals) {
+    const HemConst& C = *Cp;
+    Counts n;
+    const unsigned total = unsigned(2 * count);
+    for (;;) {
+        const unsigned base = fetchItems(counters + Q_A);
+        if (base >= total) break;
+        const unsigned item = base + (threadIdx.x & 31);
+        if (item < total) {
+            const unsigned kind = item / unsigned(count), c = item % unsigned(count);
+            const CellInput x = in[c];
+            Eval v;
+            CandidateOut o{};
+            bool ok;
+            if (kind == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n);
+            else ok = frozenSolve(C, x, x.q, 0, v, o, n);
+            finishCandidate(C, x, ok, v, o, rec + size_t(kind) * count + c, n);
+        }
+    }
+    flushCounts(n, totals);
+}
+
+__device__ __forceinline__ bool gasDecides(const HemConst& C, const CandRecord& gas) {
+    return C.stableGasPrune && gas.status == 2 && gas.st.gasMass > 0;
+}
+
+__global__ void compactSeedCells(const HemConst* __restrict__ Cp, const CandRecord* rec, size_t count,
+                                 unsigned* list, unsigned* counters) {
+    const HemConst& C = *Cp;
+    for (size_t base = blockIdx.x * size_t(blockDim.x); base < count; base += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = base + threadIdx.x;
+        const bool need = c < count && !gasDecides(C, rec[c]);
+        const unsigned mask = __ballot_sync(0xffffffffu, need);
+        unsigned slot = 0;
+        if ((threadIdx.x & 31) == 0 && mask) slot = atomicAdd(counters + LIST, unsigned(__popc(mask)));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (need) list[slot + __popc(mask & ((1u << (threadIdx.x & 31)) - 1))] = unsigned(c);
+    }
+}
+
+// Pass B: items (seed) x listed cells, seed-major.
+__global__ void __launch_bounds__(kPassThreads) passSeeds(const HemConst* __restrict__ Cp,
+                                                          const CellInput* __restrict__ in, size_t count,
+                                                          const unsigned* __restrict__ list, CandRecord* rec,
+                                                          unsigned* counters, unsigned long long* totals) {
+    const HemConst& C = *Cp;
+    Counts n;
+    const unsigned listed = counters[LIST];
+    const unsigned total = 5u * listed;
+    for (;;) {
+        const unsigned base = fetchItems(counters + Q_B);
+        if (base >= total) break;
+        const unsigned item = base + (threadIdx.x & 31);
+        if (item < total) {
+            const unsigned seed = item / listed, c = list[item % listed];
+            const CellInput x = in[c];
+            Eval v;
+            CandidateOut o{};
+            const bool ok = twoPhaseSolve(C, x, kSeeds[seed], -1.0, v, o, n);
+            finishCandidate(C, x, ok, v, o, rec + size_t(2 + seed) * count + c, n);
+        }
+    }
+    flushCounts(n, totals);
+}
+
+__device__ inline void writeOutputs(const ReactiveThermoState& s, size_t c, ReactiveThermoState* state,
+                                    ReactiveTransportState* transport) {
+    if (state) state[c] = s;
+    if (transport) transport[c] = ReactiveTransportState{s.p, s.T, s.rho, s.cv, s.soundFrozen, s.gasMass, 0.0};
+}
+
+__global__ void selectCandidates(const HemConst* __restrict__ Cp, const CandRecord* rec, size_t count,
+                                 ReactiveThermoState* state, ReactiveTransportState* transport, int* success,
+                                 unsigned* fallback, unsigned* counters) {
+    const HemConst& C = *Cp;
+    for (size_t base = blockIdx.x * size_t(blockDim.x); base < count; base += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = base + threadIdx.x;
+        int best = -1;
+        double bestEntropy = 0;
+        if (c < count) {
+            const int kinds = gasDecides(C, rec[c]) ? 2 : 7;
+            for (int k = 0; k < kinds; ++k) {
+                const CandRecord& r = rec[size_t(k) * count + c];
+                if (r.status == 2 && (best < 0 || r.entropyD > bestEntropy)) { best = k; bestEntropy = r.entropyD; }
+            }
+            if (best >= 0) {
+                writeOutputs(rec[size_t(best) * count + c].st, c, state, transport);
+                if (success) success[c] = 1;
+            }
+        }
+        const bool need = c < count && best < 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, need);
+        unsigned slot = 0;
+        if ((threadIdx.x & 31) == 0 && mask) slot = atomicAdd(counters + FALLBACK, unsigned(__popc(mask)));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (need) fallback[slot + __popc(mask & ((1u << (threadIdx.x & 31)) - 1))] = unsigned(c);
+    }
+}
+
+// Pass C: restart temperatures x queued cells; each item runs the five seeds.
+__global__ void __launch_bounds__(kPassThreads) passRestarts(const HemConst* __restrict__ Cp,
+                                                             const CellInput* __restrict__ in,
+                                                             const unsigned* __restrict__ fallback, CandRecord* fb,
+                                                             size_t capacity, unsigned* counters,
+                                                             unsigned long long* totals) {
+    const HemConst& C = *Cp;
+    Counts n;
+    const unsigned queued = counters[FALLBACK];
+    const unsigned total = 4u * queued;
+    const double lower = fmax(C.Tmin, C.liquidTmin), upper = fmin(C.Tmax, C.liquidTc * (1 - 1e-10));
+    for (;;) {
+        const unsigned base = fetchItems(counters + Q_C);
+        if (base >= total) break;
+        const unsigned item = base + (threadIdx.x & 31);
+        if (item < total) {
+            const unsigned t = item / queued, slot = item % queued;
+            const CellInput x = in[fallback[slot]];
+            CandRecord* out = fb + size_t(t) * capacity + slot;
+            out->status = 0;
+            if (upper > lower) {
+                const double restartT = lower + (upper - lower) * kRestart[t];
+                bool have = false;
+                double bestEntropy = 0;
+                for (int s = 0; s < 5; ++s) {
+                    Eval v;
+                    CandidateOut o{};
+                    const bool ok = twoPhaseSolve(C, x, kSeeds[s], restartT, v, o, n);
+                    if (!ok) { ++n.failures; continue; }
+                    const bool stable = stableAt(C, x.q, v.liqMass, v.p, v.T, n);
+                    if (!stable) { ++n.failures; continue; }
+                    ++n.stable;
+                    if (!have || v.entropyD > bestEntropy) {
+                        have = true;
+                        bestEntropy = v.entropyD;
+                        stateFromEval(v, x.q, o, out->st);
+                        out->entropyD = v.entropyD;
+                        out->status = 2;
+                    }
+                }
+            }
+        }
+    }
+    flushCounts(n, totals);
+}
+
+__global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsigned* fallback,
+                               const ReactiveThermoState* seed, ReactiveThermoState* state,
+                               ReactiveTransportState* transport, int* success, unsigned* counters) {
+    const unsigned queued = counters[FALLBACK];
+    for (unsigned slot = blockIdx.x * blockDim.x + threadIdx.x; slot < queued; slot += blockDim.x * gridDim.x) {
+        const size_t c = fallback[slot];
+        int best = -1;
+        double bestEntropy = 0;
+        for (int t = 0; t < 4; ++t) {
+            const CandRecord& r = fb[size_t(t) * capacity + slot];
+            if (r.status == 2 && (best < 0 || r.entropyD > bestEntropy)) { best = t; bestEntropy = r.entropyD; }
+        }
+        if (best >= 0) {
+            writeOutputs(fb[size_t(best) * capacity + slot].st, c, state, transport);
+            if (success) success[c] = 1;
+        } else {
+            if (seed && state) writeOutputs(seed[c], c, state, nullptr);
+            if (transport && seed) writeOutputs(seed[c], c, nullptr, transport);
+            if (success) success[c] = 0;
+            atomicAdd(counters + FAILED, 1u);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host
+std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C);
+
+struct HemDevice {
+    std::mutex entry;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t capacity = 0;
+    bool hostPath = false;
+    HemConst hostConst{};
+    HemConst* cst = nullptr;
+    CellInput* in = nullptr;
+    CandRecord* rec = nullptr;  // 7 x capacity
+    CandRecord* fb = nullptr;   // 4 x capacity
+    unsigned* list = nullptr;
+    unsigned* fallback = nullptr;
+    unsigned* counters = nullptr;
+    unsigned long long* totals = nullptr;
+    // host-path staging
+    double* dq = nullptr;
+    double* de = nullptr;
+    ReactiveThermoState* dguess = nullptr;
+    ReactiveThermoState* dout = nullptr;
+    int* dsuccess = nullptr;
+    int passBlocks = 0;
+    size_t bytes = 0;
+    std::vector<void*> blocks;
+
+    template <class T> T* alloc(size_t n) {
+        void* p = nullptr;
+        check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
+        blocks.push_back(p);
+        bytes += n * sizeof(T);
+        return static_cast<T*>(p);
+    }
+    ~HemDevice() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : blocks) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void ensureHostPath() {
+        if (hostPath) return;
+        dq = alloc<double>(capacity);
+        de = alloc<double>(capacity);
+        dguess = alloc<ReactiveThermoState>(capacity);
+        dout = alloc<ReactiveThermoState>(capacity);
+        dsuccess = alloc<int>(capacity);
+        hostPath = true;
+    }
+    // Launches steps 2-7 for `count` prepared inputs.
+    void launchSearch(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
+                      ReactiveTransportState* transport, int* success, cudaStream_t s) {
+        check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "memset counters");
+        passPartitions<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, rec, counters, totals);
+        check(cudaGetLastError(), "passPartitions");
+        compactSeedCells<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, list, counters);
+        check(cudaGetLastError(), "compactSeedCells");
+        passSeeds<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, rec, counters, totals);
+        check(cudaGetLastError(), "passSeeds");
+        selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, state, transport, success, fallback,
+                                                             counters);
+        check(cudaGetLastError(), "selectCandidates");
+        passRestarts<<<passBlocks, kPassThreads, 0, s>>>(cst, in, fallback, fb, capacity, counters, totals);
+        check(cudaGetLastError(), "passRestarts");
+        selectRestarts<<<gridFor(count, 256), 256, 0, s>>>(fb, capacity, fallback, seed, state, transport, success,
+                                                           counters);
+        check(cudaGetLastError(), "selectRestarts");
+    }
+};
+
+void* create(const void* raw, size_t bytes, size_t capacity, bool hostPath, char* error, size_t size) {
+    try {
+        require(raw && bytes == sizeof(ReactiveB200HemModel) && capacity && capacity <= UINT32_MAX / 8,
+                "Invalid CUDA HEM model/capacity");
+        ReactiveB200HemModel m;
+        std::memcpy(&m, raw, sizeof(m));
+        std::unique_ptr<HemDevice> d(new HemDevice);
+        const std::string why = validateAndDerive(m, d->hostConst);
+        require(why.empty(), why.c_str());
+        int count = 0;
+        check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+        require(count > 0, "No CUDA device");
+        check(cudaGetDevice(&d->device), "cudaGetDevice");
+        check(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        d->capacity = capacity;
+        d->cst = d->alloc<HemConst>(1);
+        d->in = d->alloc<CellInput>(capacity);
+        d->rec = d->alloc<CandRecord>(7 * capacity);
+        d->fb = d->alloc<CandRecord>(4 * capacity);
+        d->list = d->alloc<unsigned>(capacity);
+        d->fallback = d->alloc<unsigned>(capacity);
+        d->counters = d->alloc<unsigned>(NCOUNTERS);
+        d->totals = d->alloc<unsigned long long>(NTOTALS);
+        check(cudaMemcpyAsync(d->cst, &d->hostConst, sizeof(HemConst), cudaMemcpyHostToDevice, d->stream), "H2D");
+        check(cudaMemsetAsync(d->totals, 0, NTOTALS * sizeof(unsigned long long), d->stream), "memset");
+        int perSm = 0, sms = 0;
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, passSeeds, kPassThreads, 0), "occupancy");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "attribute");
+        d->passBlocks = std::max(1, perSm) * std::max(1, sms);
+        if (hostPath) d->ensureHostPath();
+        check(cudaStreamSynchronize(d->stream), "sync");
+        return d.release();
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return nullptr;
+    }
+}
+
+// Model validation (the reference's validModel, src/reactiveThermo/reactiveDeviceFlash.h:80-108,
+// for the tables this build evaluates) and the derived device constants.
+bool finiteD(double x) { return std::isfinite(x); }
+
+std::string species(const ReactiveB200Table& t, PureSpecies& sp) {
+    if (t.ns != 1) return "HEM table must hold one species";
+    const ReactiveB200Species& s = t.species[0];
+    if (!finiteD(t.refPressure) || t.refPressure <= 0) return "Invalid HEM table reference pressure";
+    if (!finiteD(s.molecularWeight) || s.molecularWeight <= 0 || !finiteD(s.a) || s.a <= 0 || !finiteD(s.b)
+        || s.b <= 0 || !finiteD(s.kappa) || s.regionCount <= 0 || s.regionCount > kMaxRegions)
+        return "Invalid HEM species data";
+    if (t.aBinary[0][0] != s.a) return "Invalid HEM binary a";
+    sp.a = s.a; sp.b = s.b; sp.kappa = s.kappa; sp.W = s.molecularWeight; sp.refP = t.refPressure;
+    sp.Tc = s.a * kOmegaB / (s.b * kOmegaA * kGas);
+    sp.regionCount = s.regionCount;
+    for (int r = 0; r < s.regionCount; ++r) {
+        const auto& g = s.regions[r];
+        if ((g.polynomial != 7 && g.polynomial != 9) || !finiteD(g.minimumTemperature)
+            || !finiteD(g.maximumTemperature) || g.minimumTemperature <= 0
+            || g.maximumTemperature <= g.minimumTemperature
+            || (r && g.minimumTemperature < s.regions[r - 1].minimumTemperature))
+            return "Invalid HEM NASA region";
+        for (int j = 0; j < g.polynomial; ++j) if (!finiteD(g.coefficient[j])) return "Invalid HEM NASA coefficient";
+        sp.polynomial[r] = g.polynomial;
+        sp.regionMin[r] = g.minimumTemperature;
+        for (int j = 0; j < 9; ++j) sp.coeff[r][j] = g.coefficient[j];
+    }
+    sp.regionMaxLast = s.regions[s.regionCount - 1].maximumTemperature;
+    return "";
+}
+
+// Host copy of the pure-fluid cubic used only to place the reported-phase line
+// (same relations as the device code, evaluated once per table).
+struct HostRoots { double lo; int signedCount; bool ok; };
+HostRoots hostRoots(const PureSpecies& sp, double T, double p) {
+    HostRoots out{0, 0, false};
+    const double sq = std::sqrt(T / sp.Tc), f = 1.0 + sp.kappa * (1.0 - sq);
+    if (std::fabs(f) <= 1e-14) return out;
+    const double q0 = std::fabs(f), aa = sp.a * q0 * q0;
+    const double b = sp.b, b2 = b * b, RTp = kGas * T / p, aap = aa / p, bn = b - RTp;
+    const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
+    const double center = -bn / 3.0, delta2 = (bn * bn - 3.0 * cn) / 9.0;
+    const double q = 2.0 * bn * bn * bn / 27.0 - bn * cn / 3.0 + dn;
+    const double delta = delta2 > 0 ? std::sqrt(delta2) : 0, h = 2.0 * delta * delta2;
+    double disc = q * q - h * h;
+    if (std::fabs(std::fabs(h) - std::fabs(q)) < 1e-10) {
+        if (disc > 1e-10) return out;
+        disc = 0;
+    }
+    auto cubic = [&](double V) { return ((V + bn) * V + cn) * V + dn; };
+    auto polish = [&](double x) {
+        for (int n = 0; n < 12; ++n) {
+            const double r = cubic(x), d = (3.0 * x + 2.0 * bn) * x + cn;
+            if (std::fabs(d) <= 1e-300) break;
+            const double step = r / d;
+            x -= step;
+            if (std::fabs(step) <= 4e-15 * std::max(1.0, std::fabs(x))) break;
+        }
+        return x;
+    };
+    std::vector<double> raw;
+    int side = 0;
+    if (std::fabs(disc) < 1e-14) {
+        if (!(delta2 > 0) || q == 0) return out;
+        const bool gasSide = q < 0;
+        const double pair = center + (gasSide ? -1.0 : 1.0) * delta;
+        double x = center + (gasSide ? 2.0 : -2.0) * delta;
+        bool conv = false;
+        for (int n = 0; n < 24; ++n) {
+            const double fx = cubic(x), dfx = (3.0 * x + 2.0 * bn) * x + cn;
+            if (!std::isfinite(fx) || !std::isfinite(dfx) || std::fabs(dfx) <= 1e-300) return out;
+            const double step = fx / dfx;
+            x -= step;
+            if (std::fabs(step) <= 4e-15 * std::max(1.0, std::fabs(x))) { conv = true; break; }
+        }
+        if (!conv || !(x > b) || !(std::fabs(x - pair) > 1e-3 * std::max(std::fabs(x), std::fabs(pair)))) return out;
+        raw.push_back(x);
+        side = gasSide ? 1 : -1;
+    } else if (disc > 1e-14 || !(delta2 > 0)) {
+        const double sd = .5 * std::sqrt(std::max(0.0, disc));
+        raw.push_back(polish(center + std::cbrt(-.5 * q + sd) + std::cbrt(-.5 * q - sd)));
+    } else {
+        const double arg = std::min(1.0, std::max(-1.0, -.5 * q / (delta * delta * delta)));
+        const double theta = std::acos(arg) / 3.0;
+        for (int i = 0; i < 3; ++i) raw.push_back(polish(center + 2.0 * delta * std::cos(theta + i * 2.0 * kPi / 3.0)));
+    }
+    std::sort(raw.begin(), raw.end());
+    std::vector<double> phys;
+    for (double v : raw) if (std::isfinite(v) && v > b) phys.push_back(v);
+    if (phys.empty()) return out;
+    out.lo = phys[0];
+    out.ok = true;
+    if (side) out.signedCount = side;
+    else if (phys.size() >= 2) out.signedCount = int(phys.size());
+    else {
+        const double Tcm = sp.Tc, pc = kOmegaB * kGas * Tcm / b, vc = kOmegaVc * kGas * Tcm / pc;
+        out.signedCount = (T > Tcm ? phys[0] < vc : phys[0] < center) ? -1 : 1;
+    }
+    return out;
+}
+
+std::string phaseLine(PureSpecies& sp) {
+    const double tc = sp.a * kOmegaB / (sp.b * kOmegaA * kGas), pc = kOmegaB * kGas * tc / sp.b;
+    const double vc = kOmegaVc * kGas * tc / pc;
+    double tmid = tc - 100.0;
+    if (tmid < 0) tmid = .5 * tc;
+    const double ratio = tc / tmid;
+    double pp = pc * std::exp(-.8734 * ratio * ratio - 3.4522 * ratio + 4.2918), liquidVolume = -1;
+    bool found = false;
+    for (int it = 0; it < 100; ++it) {
+        const HostRoots r = hostRoots(sp, tmid, pp);
+        if (!r.ok) return "HEM reported-phase construction failed";
+        if (r.signedCount == 1 || r.signedCount == 2) {
+            found = pp > pc;
+            liquidVolume = r.lo;
+            pp *= 1.04;
+            if (found) break;
+        } else {
+            liquidVolume = r.lo;
+            found = true;
+            break;
+        }
+    }
+    if (!found || !(liquidVolume > 0)) return "HEM reported-phase construction failed";
+    const double rc = sp.W / vc, rl = sp.W / liquidVolume, rg = sp.W / (kGas * tmid / pp);
+    sp.tcLine = tc;
+    sp.rhoC = rc;
+    sp.dRho = rc - .5 * (rl + rg);
+    sp.dT = tc - tmid;
+    return std::isfinite(sp.dRho) && sp.dT > 0 ? "" : "HEM reported-phase construction failed";
+}
+
+std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C) {
+    if (m.ns != 1 || m.nl != 1 || m.condensable[0] != 0 || m.condensedKind[0] != 0 || m.condensedKind[1] != 0
+        || m.boundaryRecovery != 0)
+        return "HEM model outside this build's scope: one condensable species with its own pure liquid "
+               "(ns=1, nl=1, no solid, boundaryRecovery=0)";
+    if ((m.scalarRecovery != 0 && m.scalarRecovery != 1) || (m.analyticJacobian != 0 && m.analyticJacobian != 1)
+        || (m.stableGasPrune != 0 && m.stableGasPrune != 1)
+        || (m.enforceSpeciesTemperatureBounds != 0 && m.enforceSpeciesTemperatureBounds != 1))
+        return "Invalid CUDA HEM model flags";
+    if (!finiteD(m.Tmin) || !finiteD(m.Tmax) || !(m.Tmin > 0 && m.Tmax > m.Tmin) || !finiteD(m.pmin)
+        || !finiteD(m.pmax) || !(m.pmin > 0 && m.pmax > m.pmin) || !(m.vtol > 0 && m.etol > 0 && m.mutol > 0)
+        || !finiteD(m.vtol) || !finiteD(m.etol) || !finiteD(m.mutol))
+        return "Invalid CUDA HEM model tables or domain";
+    std::string why = species(m.phase[0], C.gas);
+    if (why.empty()) why = species(m.phase[1], C.liq);
+    if (!why.empty()) return why;
+    if (m.weights[0] != m.phase[0].species[0].molecularWeight
+        || m.phase[1].species[0].molecularWeight != m.weights[0])
+        return "Invalid CUDA HEM species weights";
+    if (!finiteD(m.liquidTmin[0]) || !finiteD(m.liquidTc[0]) || !(m.liquidTmin[0] > 0 && m.liquidTc[0] > m.liquidTmin[0]))
+        return "Invalid CUDA HEM liquid range";
+    why = phaseLine(C.gas);
+    if (why.empty()) why = phaseLine(C.liq);
+    if (!why.empty()) return why;
+    C.Tmin = m.Tmin; C.Tmax = m.Tmax; C.pmin = m.pmin; C.pmax = m.pmax;
+    C.vtol = m.vtol; C.etol = m.etol; C.mutol = m.mutol;
+    C.liquidTmin = m.liquidTmin[0]; C.liquidTc = m.liquidTc[0];
+    C.gasTmin = m.phase[0].species[0].regions[0].minimumTemperature;
+    C.gasTmax = C.gas.regionMaxLast;
+    C.enforceBounds = m.enforceSpeciesTemperatureBounds;
+    C.scalarRecovery = m.scalarRecovery;
+    C.analyticJacobian = m.analyticJacobian;
+    C.stableGasPrune = m.stableGasPrune;
+    return "";
+}
+
+void readTotals(HemDevice& d, ReactiveGpuHemProfileV1& p, cudaStream_t s) {
+    unsigned long long t[NTOTALS] = {};
+    unsigned ctr[NCOUNTERS] = {};
+    check(cudaMemcpyAsync(t, d.totals, sizeof(t), cudaMemcpyDeviceToHost, s), "D2H totals");
+    check(cudaMemcpyAsync(ctr, d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, s), "D2H counters");
+    check(cudaStreamSynchronize(s), "sync");
+    check(cudaMemsetAsync(d.totals, 0, sizeof(t), s), "memset totals");
+    p.phaseEvaluations = t[T_PHASES];
+    p.residualEvaluations = t[T_RESIDUALS];
+    p.flashCandidates = t[T_CANDIDATES];
+    p.stableCandidates = t[T_STABLE];
+    p.analyticJacobians = t[T_ANALYTIC];
+    p.finiteDifferenceJacobians = t[T_FD];
+    p.deviceFailures = ctr[FAILED];
+}
+
+}  // namespace
+}  // namespace rb200
+
+using rb200::HemDevice;
+
+extern "C" {
+
+const char* reactive_gpu_hem_numerical_policy_v1(void) {
+    return "fp64-fma-rn-candidate-parallel-v1:prec-div=true:prec-sqrt=true:fast-math=false";
+}
+void* reactive_gpu_hem_create_v1(const void* model, size_t bytes, size_t capacity, char* error, size_t size) {
+    return rb200::create(model, bytes, capacity, true, error, size);
+}
+void* reactive_gpu_hem_create_resident_v1(const void* model, size_t bytes, size_t capacity, char* error,
+                                          size_t size) {
+    return rb200::create(model, bytes, capacity, false, error, size);
+}
+size_t reactive_gpu_hem_device_bytes_v1(void* raw) { return raw ? static_cast<HemDevice*>(raw)->bytes : 0; }
+void reactive_gpu_hem_destroy_v1(void* raw) { delete static_cast<HemDevice*>(raw); }
+
+int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, size_t count, ReactiveThermoState* states,
+                            int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t size) {
+    try {
+        rb200::require(raw && q && energy && states && success && profile && profile->abiVersion == 1
+                           && profile->structBytes == sizeof(*profile),
+                       "Invalid CUDA HEM batch arguments");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        rb200::require(count && count <= d.capacity, "CUDA HEM batch exceeds capacity");
+        rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+        d.ensureHostPath();
+        const auto begin = std::chrono::steady_clock::now();
+        cudaEvent_t ev[4];
+        for (auto& e : ev) rb200::check(cudaEventCreate(&e), "event");
+        cudaStream_t s = d.stream;
+        rb200::check(cudaEventRecord(ev[0], s), "event");
+        rb200::check(cudaMemcpyAsync(d.dq, q, count * sizeof(double), cudaMemcpyHostToDevice, s), "H2D q");
+        rb200::check(cudaMemcpyAsync(d.de, energy, count * sizeof(double), cudaMemcpyHostToDevice, s), "H2D e");
+        rb200::check(cudaMemcpyAsync(d.dguess, states, count * sizeof(ReactiveThermoState), cudaMemcpyHostToDevice, s),
+                     "H2D seed");
+        rb200::check(cudaMemsetAsync(d.dsuccess, 0, count * sizeof(int), s), "memset");
+        rb200::check(cudaEventRecord(ev[1], s), "event");
+        rb200::inputsFromHost<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.dq, d.de, d.dguess, count, 1, d.in);
+        rb200::check(cudaGetLastError(), "inputs");
+        d.launchSearch(count, d.dguess, d.dout, nullptr, d.dsuccess, s);
+        rb200::check(cudaEventRecord(ev[2], s), "event");
+        std::vector<ReactiveThermoState> out(count);
+        rb200::check(cudaMemcpyAsync(out.data(), d.dout, count * sizeof(ReactiveThermoState), cudaMemcpyDeviceToHost, s),
+                     "D2H states");
+        rb200::check(cudaMemcpyAsync(success, d.dsuccess, count * sizeof(int), cudaMemcpyDeviceToHost, s),
+                     "D2H success");
+        rb200::check(cudaEventRecord(ev[3], s), "event");
+        ReactiveGpuHemProfileV1 p{};
+        p.abiVersion = 1;
+        p.structBytes = sizeof(p);
+        rb200::readTotals(d, p, s);
+        float upload = 0, kernel = 0, download = 0;
+        cudaEventElapsedTime(&upload, ev[0], ev[1]);
+        cudaEventElapsedTime(&kernel, ev[1], ev[2]);
+        cudaEventElapsedTime(&download, ev[2], ev[3]);
+        for (auto& e : ev) cudaEventDestroy(e);
+        p.batches = 1;
+        p.submitted = count;
+        for (size_t c = 0; c < count; ++c)
+            if (success[c]) { states[c] = out[c]; ++p.succeeded; }
+        p.deviceFailures = count - p.succeeded;
+        p.transferBytes = count * (2 * sizeof(double) + 2 * sizeof(ReactiveThermoState) + sizeof(int));
+        p.deviceBytes = d.bytes;
+        p.hostBytes = count * sizeof(ReactiveThermoState);
+        p.kernelSeconds = kernel / 1000.;
+        p.copySeconds = (upload + download) / 1000.;
+        p.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+        *profile = p;
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
+
+int reactive_gpu_hem_run_v2(void*, const double*, const double*, const ReactiveGpuHemCapillaryInputV2*, size_t,
+                            ReactiveThermoState*, int*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
+    if (error && size) std::snprintf(error, size, "Capillary HEM is not part of this B200 build");
+    return 1;
+}
+int reactive_gpu_hem_initialize_tp_v1(void*, double*, double*, const ReactiveGpuHemCapillaryInputV2*, size_t,
+                                      ReactiveThermoState*, int*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
+    if (error && size) std::snprintf(error, size, "Capillary primitive initialisation is not part of this B200 build");
+    return 1;
+}
+int reactive_gpu_hem_run_resident_v1(void*, const double*, const double*, const ReactiveThermoState*,
+                                     const ReactiveGpuHemCapillaryInputV2*, const uint32_t*, size_t,
+                                     ReactiveGpuHemOutputV1*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
+    if (error && size)
+        std::snprintf(error, size, "The capillary resident HEM is not part of this B200 build; use run_device_v3");
+    return 1;
+}
+
+int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t stride, size_t count, size_t variables,
+                                   const ReactiveThermoState* seed, ReactiveThermoState* state,
+                                   ReactiveTransportState* transport, int* success, void*, int, void* stream,
+                                   char* error, size_t size) {
+    try {
+        rb200::require(raw && conserved && seed && (state || transport) && count && stride >= count
+                           && variables >= 5,
+                       "Invalid device HEM batch arguments");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        rb200::require(count <= d.capacity, "Device HEM batch exceeds capacity");
+        auto s = static_cast<cudaStream_t>(stream);
+        rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1, seed, d.in);
+        rb200::check(cudaGetLastError(), "inputs");
+        d.launchSearch(count, seed, state, transport, success, s);
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
+
+int reactive_gpu_hem_run_counters_v3(void* raw, ReactiveGpuHemProfileV1* profile, void* stream, char* error,
+                                     size_t size) {
+    try {
+        rb200::require(raw && profile, "Invalid HEM counter query");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        ReactiveGpuHemProfileV1 p{};
+        p.abiVersion = 1;
+        p.structBytes = sizeof(p);
+        rb200::readTotals(d, p, static_cast<cudaStream_t>(stream));
+        p.deviceBytes = d.bytes;
+        *profile = p;
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,293 @@
+// Peng-Robinson equation of state of one pure species on the device (FP64).
+//
+// Thermodynamic relations (Cantera 3.2 conventions, as restated by the
+// reference in src/reactiveThermo/reactiveDevicePR.h): NASA7/9 ideal-gas part
+// (:127-155, region choice :198-212), alpha(T) and its T-derivatives (:214-247),
+// cubic Z roots with the absolute near-repeated-root band and the isolated third
+// root (:280-307, :333-422), residual (T, rho) properties and chemical potential
+// (:474-562), root choice at (T, p) and the pressure postcondition (:575-609),
+// and the reported-phase line through (Tc, rho_c) (:429-471) precomputed once
+// per table (src/reactiveThermo/reactiveDevicePRPurePhaseCache.h:29-85).
+//
+// The root solve and root selection stay FP64: the discriminant thresholds are
+// absolute and the near-repeated band decides phase availability.
+#pragma once
+#include <cuda_runtime.h>
+#include <cfloat>
+
+namespace rb200 {
+
+constexpr double kGas = 8314.46261815324;  // J/(kmol K)
+constexpr double kSqrt2 = 1.41421356237309504880168872420969808;
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kOmegaA = 4.5723552892138218e-1;
+constexpr double kOmegaB = 7.77960739038885e-2;
+constexpr double kOmegaVc = 3.07401308698703833e-1;
+
+enum EosStatus : int {
+    EOS_OK = 0, EOS_INVALID_TABLE, EOS_INVALID_INPUT, EOS_INVALID_COMPOSITION, EOS_NO_ROOT,
+    EOS_UNAVAILABLE, EOS_UNSTABLE, EOS_NONFINITE
+};
+enum RootChoice : int { ROOT_AUTO = 0, ROOT_GAS = 1, ROOT_LIQUID = 2 };
+
+constexpr int kMaxRegions = 8;
+
+// Immutable per-species constants, derived on the host from the model image.
+struct PureSpecies {
+    double a, b, kappa, W, Tc, refP;
+    double tcLine, rhoC, dRho, dT;  // reported-phase line
+    int regionCount;
+    int polynomial[kMaxRegions];
+    double regionMin[kMaxRegions];
+    double regionMaxLast;
+    double coeff[kMaxRegions][9];
+};
+
+struct PhaseProps {
+    double p, rho, e, s, cp, cv, alpha, kappaT, V, h, mu;  // per mass except V (molar), mu (molar)
+};
+
+__device__ __forceinline__ bool fin(double x) { return isfinite(x); }
+
+__device__ __forceinline__ int nasaRegion(const PureSpecies& sp, double T) {
+    int r = 0;
+    for (int j = 1; j < sp.regionCount; ++j) {
+        const double b = sp.regionMin[j];
+        const bool high = sp.polynomial[j] == 9 ? T >= b : T > b;
+        if (!high) break;
+        r = j;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void nasaEval(const PureSpecies& sp, double T, double& cpR, double& hRT, double& sR) {
+    const int r = nasaRegion(sp, T);
+    const double* a = sp.coeff[r];
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, iT = 1.0 / T, lT = log(T);
+    if (sp.polynomial[r] == 7) {
+        cpR = a[0] + a[1] * T + a[2] * T2 + a[3] * T3 + a[4] * T4;
+        hRT = a[0] + .5 * a[1] * T + a[2] * T2 / 3.0 + .25 * a[3] * T3 + .2 * a[4] * T4 + a[5] * iT;
+        sR = a[0] * lT + a[1] * T + .5 * a[2] * T2 + a[3] * T3 / 3.0 + .25 * a[4] * T4 + a[6];
+    } else {
+        const double c0 = a[0] * iT * iT, c1 = a[1] * iT, c2 = a[2], c3 = a[3] * T, c4 = a[4] * T2,
+                     c5 = a[5] * T3, c6 = a[6] * T4;
+        cpR = c0 + c1 + c2 + c3 + c4 + c5 + c6;
+        hRT = -c0 + lT * c1 + c2 + .5 * c3 + c4 / 3.0 + .25 * c5 + .2 * c6 + a[7] * iT;
+        sR = -.5 * c0 - c1 + lT * c2 + c3 + .5 * c4 + c5 / 3.0 + .25 * c6 + a[8];
+    }
+}
+
+// a*alpha(T) and its first two T-derivatives.
+__device__ __forceinline__ int alphaTerms(const PureSpecies& sp, double T, double& aa, double& da, double& d2a) {
+    const double sq = sqrt(T / sp.Tc), f = 1.0 + sp.kappa * (1.0 - sq);
+    if (fabs(f) <= 1e-14) return EOS_NONFINITE;
+    const double sign = f > 0 ? 1.0 : -1.0, q = fabs(f);
+    const double dq = -sign * sp.kappa / (2.0 * sp.Tc * sq);
+    const double d2q = sign * sp.kappa / (4.0 * sp.Tc * sp.Tc * sq * sq * sq);
+    aa = sp.a * q * q;
+    da = sp.a * (dq * q + q * dq);
+    d2a = sp.a * (d2q * q + 2.0 * dq * dq + q * d2q);
+    return fin(aa) && fin(da) && fin(d2a) && aa > 0 ? EOS_OK : EOS_NONFINITE;
+}
+
+__device__ __forceinline__ double cubicAt(double V, double bn, double cn, double dn) {
+    return ((V + bn) * V + cn) * V + dn;
+}
+
+// Physical roots (finite, above the covolume), smallest and largest.
+struct Roots {
+    double lo, hi;
+    int count;
+    bool gas, liquid;
+};
+
+__device__ inline bool isolatedRoot(double center, double delta, double delta2, double q, double bn, double cn,
+                                    double dn, double b, double RTp, double aap, double& root, bool& gasSide) {
+    if (!(delta2 > 0) || !fin(delta) || !fin(q) || q == 0) return false;
+    gasSide = q < 0;
+    const double pair = center + (gasSide ? -1.0 : 1.0) * delta;
+    double x = center + (gasSide ? 2.0 : -2.0) * delta;
+    bool converged = false;
+    for (int n = 0; n < 24; ++n) {
+        const double f = cubicAt(x, bn, cn, dn), df = (3.0 * x + 2.0 * bn) * x + cn;
+        if (!fin(f) || !fin(df) || fabs(df) <= 1e-300) return false;
+        const double step = f / df;
+        x -= step;
+        if (fabs(step) <= 4e-15 * fmax(1.0, fabs(x))) { converged = true; break; }
+    }
+    if (!converged || !fin(x) || !(x > b)) return false;
+    const double f = cubicAt(x, bn, cn, dn);
+    const double scale = fabs(x * x * x) + fabs(bn * x * x) + fabs(cn * x) + fabs(dn);
+    if (!(fabs(f) <= 64.0 * DBL_EPSILON * scale)) return false;
+    if (!(fabs(x - pair) > 1e-3 * fmax(fabs(x), fabs(pair)))) return false;
+    if (gasSide ? !(x > pair) : !(x < pair)) return false;
+    const double vb = x - b, den = x * x + 2.0 * b * x - b * b;
+    if (!(vb > 0) || !(den > 0)) return false;
+    if (!(-RTp / (vb * vb) + 2.0 * aap * (x + b) / (den * den) < 0)) return false;
+    root = x;
+    return true;
+}
+
+__device__ __forceinline__ double signedCbrt(double x) { return cbrt(x); }
+
+// Twelve Newton polishing steps on the cubic (stops early on a tiny step).
+__device__ __forceinline__ double polishRoot(double x, double bn, double cn, double dn) {
+    for (int n = 0; n < 12; ++n) {
+        const double res = cubicAt(x, bn, cn, dn), d = (3.0 * x + 2.0 * bn) * x + cn;
+        if (fabs(d) <= 1e-300) break;
+        const double step = res / d;
+        x -= step;
+        if (fabs(step) <= 4e-15 * fmax(1.0, fabs(x))) break;
+    }
+    return x;
+}
+
+__device__ inline int cubicRoots(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
+    const double b = sp.b, b2 = b * b, RTp = kGas * T / p, aap = aa / p, bn = b - RTp;
+    const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
+    const double center = -bn / 3.0, delta2 = (bn * bn - 3.0 * cn) / 9.0;
+    const double q = 2.0 * bn * bn * bn / 27.0 - bn * cn / 3.0 + dn;
+    const double delta = delta2 > 0 ? sqrt(delta2) : 0.0, h = 2.0 * delta * delta2;
+    double disc = q * q - h * h;
+    if (fabs(fabs(h) - fabs(q)) < 1e-10) {
+        if (disc > 1e-10) return EOS_NONFINITE;
+        disc = 0;
+    }
+    double raw0 = 0, raw1 = 0, raw2 = 0;
+    int rawCount;
+    int side = 0;
+    if (fabs(disc) < 1e-14) {
+        bool gasSide = false;
+        if (!isolatedRoot(center, delta, delta2, q, bn, cn, dn, b, RTp, aap, raw0, gasSide)) return EOS_NO_ROOT;
+        rawCount = 1;
+        side = gasSide ? 1 : -1;
+    } else if (disc > 1e-14 || !(delta2 > 0)) {
+        const double sd = .5 * sqrt(fmax(0.0, disc));
+        raw0 = center + signedCbrt(-.5 * q + sd) + signedCbrt(-.5 * q - sd);
+        rawCount = 1;
+    } else if (disc < -1e-14) {
+        const double arg = fmin(1.0, fmax(-1.0, -.5 * q / (delta * delta * delta)));
+        const double theta = acos(arg) / 3.0;
+        raw0 = center + 2.0 * delta * cos(theta);
+        raw1 = center + 2.0 * delta * cos(theta + 2.0 * kPi / 3.0);
+        raw2 = center + 2.0 * delta * cos(theta + 4.0 * kPi / 3.0);
+        rawCount = 3;
+    } else return EOS_NO_ROOT;
+    if (!side) {
+        raw0 = polishRoot(raw0, bn, cn, dn);
+        if (rawCount == 3) {
+            raw1 = polishRoot(raw1, bn, cn, dn);
+            raw2 = polishRoot(raw2, bn, cn, dn);
+            double t;
+            if (raw0 > raw1) { t = raw0; raw0 = raw1; raw1 = t; }
+            if (raw1 > raw2) { t = raw1; raw1 = raw2; raw2 = t; }
+            if (raw0 > raw1) { t = raw0; raw0 = raw1; raw1 = t; }
+        }
+    }
+    const bool ok0 = fin(raw0) && raw0 > b;
+    const bool ok1 = rawCount == 3 && fin(raw1) && raw1 > b;
+    const bool ok2 = rawCount == 3 && fin(raw2) && raw2 > b;
+    const int n = int(ok0) + int(ok1) + int(ok2);
+    if (!n) return EOS_NO_ROOT;
+    r.count = n;
+    r.lo = ok0 ? raw0 : (ok1 ? raw1 : raw2);
+    r.hi = ok2 ? raw2 : (ok1 ? raw1 : raw0);
+    if (side) {
+        r.gas = side > 0;
+        r.liquid = side < 0;
+    } else if (n >= 2) {
+        r.gas = r.liquid = true;
+    } else {
+        const double Tcm = sp.a * kOmegaB / (b * kOmegaA * kGas);
+        const double pc = kOmegaB * kGas * Tcm / b, vc = kOmegaVc * kGas * Tcm / pc;
+        const bool liquidSign = T > Tcm ? r.lo < vc : r.lo < center;
+        r.liquid = liquidSign;
+        r.gas = !liquidSign || T > Tcm;
+    }
+    return EOS_OK;
+}
+
+// Properties at (T, rho). chem: also the molar chemical potential. phaseOut:
+// -2 supercritical, -1 gas, 0 liquid by the reported-phase line.
+__device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool chem, PhaseProps& s, int& phaseOut) {
+    if (!fin(T) || !fin(rho) || T <= 0 || rho <= 0) return EOS_INVALID_INPUT;
+    double aa, da, d2a;
+    const int st = alphaTerms(sp, T, aa, da, d2a);
+    if (st != EOS_OK) return st;
+    const double b = sp.b, W = sp.W, V = W / rho;
+    if (!(V > b)) return EOS_NO_ROOT;
+    const double den = V * V + 2.0 * V * b - b * b, vmb = V - b;
+    if (!(den > 0) || !(vmb > 0)) return EOS_NO_ROOT;
+    const double p = kGas * T / vmb - aa / den;
+    if (!fin(p) || p <= 0) return EOS_NO_ROOT;
+    const double dpdV = -kGas * T / (vmb * vmb) + 2.0 * aa * (V + b) / (den * den);
+    const double dpdT = kGas / vmb - da / den;
+    if (!fin(dpdV) || !fin(dpdT) || dpdV >= 0) return EOS_UNSTABLE;
+    const double logRatio = log((V + (1.0 + kSqrt2) * b) / (V + (1.0 - kSqrt2) * b));
+    const double L = logRatio / (2.0 * kSqrt2 * b);
+    double cpR, hRT, sR;
+    nasaEval(sp, T, cpR, hRT, sR);
+    const double z = p * V / (kGas * T);
+    const double hM = kGas * T * hRT + (kGas * T * (z - 1.0) + L * (T * da - aa));
+    const double sM = (kGas * sR - kGas * log(p / sp.refP)) + (kGas * log(z * (1.0 - b / V)) + L * da);
+    const double dHdT = kGas * cpR + V * dpdT - kGas + L * T * d2a;
+    const double cpM = dHdT - (V + T * dpdT / dpdV) * dpdT;
+    const double cvM = cpM + T * dpdT * dpdT / dpdV;
+    s.p = p;
+    s.rho = rho;
+    s.V = V;
+    s.h = hM / W;
+    s.e = (hM - p * V) / W;
+    s.s = sM / W;
+    s.cp = cpM / W;
+    s.cv = cvM / W;
+    s.alpha = -dpdT / (V * dpdV);
+    s.kappaT = -1.0 / (V * dpdV);
+    const double sound2 = V * V * (-cpM / cvM * dpdV / W);
+    if (!(s.cp > 0) || !(s.cv > 0) || !(s.kappaT > 0) || !(sound2 > 0)) return EOS_UNSTABLE;
+    if (chem) {
+        const double RT = kGas * T, f = 1.0 + sp.kappa * (1.0 - sqrt(T / sp.Tc));
+        const double pp = sp.a * fabs(f * f), num = 2.0 * b * pp - aa * b;
+        s.mu = RT * (hRT - sR) + RT * log(p / sp.refP) - RT * log(p * V / RT) + RT * log(V / vmb) + RT * b / vmb
+             - num / (2.0 * kSqrt2 * b * b) * logRatio - aa * b * V / (b * den);
+        if (!fin(s.mu)) return EOS_NONFINITE;
+    }
+    if (T >= sp.tcLine) phaseOut = -2;
+    else {
+        const double rhoMid = sp.rhoC + (T - sp.tcLine) * sp.dRho / sp.dT;
+        if (!fin(rhoMid)) return EOS_NONFINITE;
+        phaseOut = rho < rhoMid ? -1 : 0;
+    }
+    if (!fin(s.e) || !fin(s.h) || !fin(s.s) || !fin(s.cp) || !fin(s.cv) || !fin(s.alpha) || !fin(s.kappaT)
+        || !fin(sqrt(sound2)) || !fin(dpdT) || !fin(dpdV))
+        return EOS_NONFINITE;
+    return EOS_OK;
+}
+
+// Properties at (T, p) on the chosen root, with the host postcondition
+// |p(T, rho) - p| <= 1e-7 max(1, p) and the reported-phase consistency check.
+__device__ inline int prTP(const PureSpecies& sp, double T, double p, int choice, bool chem, PhaseProps& s) {
+    if (!fin(T) || !fin(p) || T <= 0 || p <= 0) return EOS_INVALID_INPUT;
+    double aa, da, d2a;
+    int st = alphaTerms(sp, T, aa, da, d2a);
+    if (st != EOS_OK) return st;
+    Roots r;
+    st = cubicRoots(sp, T, p, aa, r);
+    if (st != EOS_OK) return st;
+    int sel = r.count - 1;
+    if (choice == ROOT_LIQUID) {
+        if (!r.liquid) return EOS_UNAVAILABLE;
+        sel = 0;
+    } else if (choice == ROOT_GAS && !r.gas) return EOS_UNAVAILABLE;
+    const double V = sel == 0 ? r.lo : r.hi;
+    int phase = 0;
+    st = prTrho(sp, T, sp.W / V, chem, s, phase);
+    if (st != EOS_OK) return st;
+    if (fabs(s.p - p) > 1e-7 * fmax(1.0, p)) return EOS_NONFINITE;
+    s.p = p;
+    if (choice == ROOT_GAS && phase >= 0) return EOS_UNAVAILABLE;
+    if (choice == ROOT_LIQUID && phase < 0) return EOS_UNAVAILABLE;
+    return EOS_OK;
+}
+
+}  // namespace rb200

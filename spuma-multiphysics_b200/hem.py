@@ -1,0 +1,75 @@
+"""Python host wrapper of the reactive_gpu_hem_* ABI (the reference's GPU HEM
+interface, src/reactiveThermo/reactiveGpuHem.h:40-84), driven with numpy host
+arrays or torch device tensors."""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A, _lib
+from .thermo_data import model_bytes, pure_model
+
+
+class HemError(RuntimeError):
+    pass
+
+
+class GpuHem:
+    """One HEM handle: a model image uploaded once and scratch for `capacity` cells."""
+
+    def __init__(self, model=None, capacity=1, resident=False):
+        self.lib = _lib.load()
+        self.model = model if model is not None else pure_model()
+        self.image = model_bytes(self.model) if not isinstance(self.model, (bytes, bytearray)) else bytes(self.model)
+        err = C.create_string_buffer(1024)
+        create = self.lib.reactive_gpu_hem_create_resident_v1 if resident else self.lib.reactive_gpu_hem_create_v1
+        h = create(self.image, len(self.image), capacity, err, len(err))
+        if not h:
+            raise HemError(err.value.decode())
+        self.handle = C.c_void_p(h)
+        self.capacity = capacity
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.reactive_gpu_hem_destroy_v1(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    @property
+    def device_bytes(self):
+        return self.lib.reactive_gpu_hem_device_bytes_v1(self.handle)
+
+    def run(self, q, energy, states):
+        """Flash host arrays in place: states (THERMO_DTYPE) are seeds in, results
+        out for successful cells. Returns (success int32 array, profile)."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        energy = np.ascontiguousarray(energy, dtype=np.float64)
+        assert states.dtype == A.THERMO_DTYPE and states.flags.c_contiguous
+        n = len(energy)
+        success = np.zeros(n, dtype=np.int32)
+        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+        err = C.create_string_buffer(1024)
+        rc = self.lib.reactive_gpu_hem_run_v1(self.handle, A.dptr(q), A.dptr(energy), n,
+                                              states.ctypes.data_as(C.c_void_p),
+                                              success.ctypes.data_as(C.POINTER(C.c_int)), C.byref(prof), err, len(err))
+        if rc:
+            raise HemError(err.value.decode())
+        return success, prof
+
+    def run_device(self, conserved, stride, count, variables, seed, state=None, transport=None, success=None,
+                   stream=0):
+        """Device batch: all arguments are device pointers (ints) or torch tensors."""
+        ptr = lambda t: 0 if t is None else (t if isinstance(t, int) else t.data_ptr())
+        err = C.create_string_buffer(1024)
+        rc = self.lib.reactive_gpu_hem_run_device_v3(self.handle, ptr(conserved), stride, count, variables,
+                                                     ptr(seed), ptr(state), ptr(transport), ptr(success), None, 0,
+                                                     stream, err, len(err))
+        if rc:
+            raise HemError(err.value.decode())
+
+    def counters(self, stream=0):
+        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+        err = C.create_string_buffer(1024)
+        if self.lib.reactive_gpu_hem_run_counters_v3(self.handle, C.byref(prof), stream, err, len(err)):
+            raise HemError(err.value.decode())
+        return prof

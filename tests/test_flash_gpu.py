@@ -1,0 +1,103 @@
+"""GPU parity of the CUDA HEM flash (reactive_gpu_hem_* in libreactive_b200.so)
+against the flash oracle and the reference flash (oracle/_ref): phase labels
+bit-exact, success flags equal, p and T within 1e-9 relative; the device-resident
+entry point against the host-array entry point."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from spuma_multiphysics_b200 import _abi as A, cases
+from spuma_multiphysics_b200.hem import GpuHem, HemError
+import flash_cases as F
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("policy,n", [("exact", 4000), ("fixed", 1000)])
+def test_cuda_flash_matches_oracle_and_reference(policy, n):
+    image = F.model_image()
+    q, e, guess = cases.flash_batch(n, seed=1000 + n, seed_policy=policy)
+    hem = GpuHem(capacity=n)
+    got = guess.copy()
+    ok, prof = hem.run(q, e, got)
+    ref, ref_ok, _ = oracle.ref_flash_recover(image, q, e, guess)
+    orc, orc_ok, _ = F.oracle_flash(oracle, image, q, e, guess)
+    for other, other_ok in ((ref, ref_ok), (orc, orc_ok)):
+        s = F.compare(got, ok, other, other_ok)
+        assert s["success_equal"], s
+        assert s["label_mismatch"] == 0, s
+        assert s["p_rel"] <= F.P_T_TOL and s["T_rel"] <= F.P_T_TOL, s
+        assert s["ml_rel"] <= F.STATE_TOL and s["c_rel"] <= F.STATE_TOL, s
+    assert prof.submitted == n and prof.succeeded == int(ok.sum())
+    assert prof.flashCandidates > 0 and prof.residualEvaluations > 0
+    # failed cells keep their seed
+    assert np.array_equal(got[ok == 0], guess[ok == 0])
+
+
+def test_cuda_flash_edge_inputs():
+    q, e, guess = cases.flash_batch(64, seed=9)
+    q[0] = 0.0
+    e[1] = np.nan
+    q[2] = -1.0
+    e[3] = -1e12
+    hem = GpuHem(capacity=64)
+    got = guess.copy()
+    ok, _ = hem.run(q, e, got)
+    ref, ref_ok, _ = oracle.ref_flash_recover(F.model_image(), q, e, guess)
+    assert np.array_equal(ok != 0, ref_ok != 0)
+    assert not ok[:4].any()
+
+
+def test_cuda_flash_rejects_out_of_scope_models():
+    m = A.HemModel()
+    img = bytes(C.string_at(C.addressof(m), C.sizeof(m)))
+    with pytest.raises(HemError):
+        GpuHem(model=img, capacity=4)
+    with pytest.raises(HemError):
+        GpuHem(capacity=8).run(*cases.flash_batch(16, seed=3))
+
+
+def test_cuda_flash_prune_policy():
+    """stableGasPrune=1 (the reference's opt-in policy) skips the two-phase seeds
+    after a stable all-gas candidate; checked against the reference flash with
+    the same model flag."""
+    model = F.model_image(stable_gas_prune=1)
+    q, e, guess = cases.flash_batch(3000, seed=4242)
+    from spuma_multiphysics_b200 import thermo_data as td
+    hem = GpuHem(model=td.pure_model(stable_gas_prune=1), capacity=3000)
+    got = guess.copy()
+    ok, prof = hem.run(q, e, got)
+    ref, ref_ok, _ = oracle.ref_flash_recover(model, q, e, guess)
+    s = F.compare(got, ok, ref, ref_ok)
+    assert s["success_equal"] and s["label_mismatch"] == 0, s
+    assert s["p_rel"] <= F.P_T_TOL and s["T_rel"] <= F.P_T_TOL, s
+
+
+def test_cuda_flash_device_resident_matches_host_path():
+    import torch
+    n = 5000
+    q, e, guess = cases.flash_batch(n, seed=31337)
+    hem = GpuHem(capacity=n)
+    host = guess.copy()
+    ok, _ = hem.run(q, e, host)
+    # conserved SoA rows: rho, m (zero velocity), E = e at rest
+    cons = torch.zeros((5, n + 3), dtype=torch.float64, device="cuda")
+    cons[0, :n] = torch.from_numpy(q).cuda()
+    cons[4, :n] = torch.from_numpy(e).cuda()
+    seed = torch.from_numpy(guess.view(np.uint8).copy()).cuda()
+    state = torch.zeros_like(seed)
+    transport = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
+    success = torch.zeros(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    hem.run_device(cons, n + 3, n, 5, seed, state, transport, success, stream)
+    torch.cuda.synchronize()
+    dev = state.cpu().numpy().view(A.THERMO_DTYPE)
+    assert np.array_equal(success.cpu().numpy(), ok)
+    both = ok != 0
+    assert np.array_equal(dev[both].view(np.uint8), host[both].view(np.uint8))  # bitwise identical
+    tr = transport.cpu().numpy()
+    assert np.array_equal(tr[both, 0], host["p"][both]) and np.array_equal(tr[both, 4], host["soundFrozen"][both])
+    prof = hem.counters(stream)
+    assert prof.flashCandidates > 0

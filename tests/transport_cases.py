@@ -194,7 +194,8 @@ def contract_walk(lib, backend, case, oracle):
         expected, expected_br = oracle_rhs(q, states, y, h)
         summary["rhs_error"] = err = scaled_error(rhs, expected)
         assert err <= RHS_TOL, f"operator mismatch {err}"
-        assert scaled_error(br[None, :], expected_br[None, :]) <= RHS_TOL
+        berr = scaled_error(br[None, :], expected_br[None, :])
+        assert berr <= RHS_TOL, f"boundary ledger mismatch {berr}: {br} vs {expected_br}"
         dt = C.c_double()
         check(lib.reactive_transport_stable_step(handle, dp(q), states_ptr(states), .23, .1, C.byref(dt)))
         expected_dt = oracle_dt(q, states)
