@@ -1,0 +1,509 @@
+#!/usr/bin/env python3
+"""Benchmark: Mcell-steps/s of the SSPRK2 + HEM step on the N2O impingement cube.
+
+Workload (default): 160^3 = 4,096,000 cells, 80 mm edge, pure N2O (Peng-Robinson,
+HEM UV flash), gas at 40 bar / 293.15 K with a seeded +-1% density perturbation,
+two 5 mm liquid inlets at 56.01325 bar / 293.15 K, transmissive walls, HLL,
+viscosity 1.821e-5 Pa s, conduction 0.02587 W/m/K, WALE Cw 0.325, dt = 1e-8 s.
+One step = CFL query, stage 0, HEM recovery of every cell, CFL recheck, stage 1,
+HEM recovery of every cell (both seeded with the step-start states), boundary
+ledger.
+
+Lines printed by rank 0 (one JSON object):
+  value   device-resident step, inputs resident in HBM, captured CUDA graph
+  e2e     the same steps through the reference-facing C ABI with host arrays
+          (upload_conserved / advance_resident_v2 / download_conserved /
+          reactive_gpu_hem_run_v1 per stage, as the reference solver calls it)
+  plain   the same device-resident kernels launched one by one (no graph)
+`--impl reference` times the reference's own CPU implementation (its transport
+built for the CPU, serial, and its flash compiled for the host on every core)
+on a bounded sample: one step of the same case at 40^3.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mcell-steps/s at 160³, plain FP64 vs mixed/batched; adjoint/forward time"
+UNIT = "Mcell-steps/s"
+VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
+
+
+def load_package():
+    import importlib.util
+    name = "spuma_multiphysics_b200"
+    if name not in sys.modules:
+        pkg = ROOT / "spuma-multiphysics_b200"
+        spec = importlib.util.spec_from_file_location(name, pkg / "__init__.py", submodule_search_locations=[str(pkg)])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def workload(n):
+    return {"workload": f"N2O impingement {n}^3 ({n ** 3:,} cells), 40 bar ambient, 2 liquid inlets, "
+                        f"viscous + conduction + WALE, SSPRK2 + 2 HEM UV flashes per step, dt=1e-8 s",
+            "cells": n ** 3, "faces": 3 * n * n * (n - 1) + 6 * n * n, "species": 1, "variables": 5,
+            "flux": "HLL", "precision": "FP64", "l2": "inputs larger than L2 (q alone 164 MB at 160^3; "
+                                                      "flash candidate records 8.6 GB)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = str(index), None, []
+        try:
+            import torch
+            self.index = f"GPU-{torch.cuda.get_device_properties(int(index)).uuid}"
+        except Exception:
+            pass
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def fp64_peak(lib, torch):
+    """Measured FP64 FMA rate (TFLOP/s) with the library's FMA-chain probe."""
+    scratch = torch.zeros(148 * 64, dtype=torch.float64, device="cuda")
+    flops = C.c_double()
+    s = torch.cuda.current_stream()
+    lib.rb200_probe_fp64_fma_v1.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                            C.POINTER(C.c_double)]
+    for _ in range(2):
+        lib.rb200_probe_fp64_fma_v1(148 * 8, 256, 2000, scratch.data_ptr(), s.cuda_stream, C.byref(flops))
+    best = 0.0
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        lib.rb200_probe_fp64_fma_v1(148 * 8, 256, 2000, scratch.data_ptr(), s.cuda_stream, C.byref(flops))
+        b.record(s)
+        b.synchronize()
+        best = max(best, flops.value / (a.elapsed_time(b) * 1e-3) / 1e12)
+    return best
+
+
+class HostPath:
+    """The reference solver's call pattern (ReactiveFoam.C:961-1019, transportStage
+    :651-661, stableStep :798-812) on this library with host arrays: q and the
+    thermo states cross PCIe every stage, exactly as the reference drop-in runs."""
+
+    def __init__(self, pkg, faces, volume, flow, fixed_q):
+        from spuma_multiphysics_b200 import _abi as A
+        self.A, self.lib = A, pkg._lib.load()
+        self.cells = len(volume)
+        self.q = flow.conserved().copy()
+        self.states = flow.states().copy()
+        self.hem = flow.hem
+        cfg = A.Config(self.cells, 1, 5, len(faces), len(fixed_q), VISCOSITY, CONDUCTIVITY, 0.0, 1.1, 1.6e11, 0)
+        fixed_tr = np.frombuffer(flow.tr[self.cells:].cpu().numpy().tobytes(), dtype=A.STATE_DTYPE).copy()
+        opts = A.OptionsV2(1, C.sizeof(A.OptionsV2), 256, 0, b"0" * 64)
+        err = C.create_string_buffer(2048)
+        self.faces = np.ascontiguousarray(faces)
+        self.volume = np.ascontiguousarray(volume)
+        self.fixed_q = np.ascontiguousarray(fixed_q, dtype=np.float64)
+        h = self.lib.reactive_transport_create_v2(1, C.byref(cfg), C.byref(opts), A.dptr(self.volume),
+                                                  self.faces.ctypes.data_as(C.POINTER(A.Face)),
+                                                  A.dptr(self.fixed_q), fixed_tr.ctypes.data_as(C.POINTER(A.State)),
+                                                  None, None, err, len(err))
+        assert h, err.value
+        self.t = C.c_void_p(h)
+        wale = A.WaleOptions(1, C.sizeof(A.WaleOptions), WALE_CW)
+        assert self.lib.reactive_transport_set_wale_v1(self.t, C.byref(wale)) == 0
+        self.version, self.attempt = 0, 0
+        self.h2d = self.d2h = 0
+
+    def _compact(self, states):
+        A = self.A
+        tr = np.zeros(len(states), dtype=A.STATE_DTYPE)
+        tr["p"], tr["T"], tr["rho"], tr["cv"] = states["p"], states["T"], states["rho"], states["cv"]
+        tr["sound"], tr["gasMass"] = states["soundFrozen"], states["gasMass"]
+        return tr
+
+    def _primitives(self, states):
+        prim = np.zeros((self.cells, 4))
+        prim[:, 0] = states["rho"]
+        prim[:, 1:] = self.q[:, 1:4] / states["rho"][:, None]
+        return prim
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(self.lib.reactive_transport_error(self.t).decode())
+
+    def step(self, dt):
+        A, lib, t = self.A, self.lib, self.t
+        start = self.states.copy()
+        dtc = C.c_double()
+        tr0 = self._compact(start)
+        prim = self._primitives(start)
+        self._check(lib.reactive_transport_stable_step_primitives(t, prim.ctypes.data_as(C.POINTER(A.Primitive)),
+                                                                  tr0.ctypes.data_as(C.POINTER(A.State)), .5, dt,
+                                                                  C.byref(dtc)))
+        self.attempt += 1
+        self._check(lib.reactive_transport_begin_attempt(t, b"0" * 64, self.attempt))
+        self.version += 1
+        self._check(lib.reactive_transport_upload_conserved(t, A.dptr(self.q), self.version))
+        br = np.zeros(5)
+        for stage in (0, 1):
+            states = start if stage == 0 else self.states
+            tr = self._compact(states)
+            before = A.Token(self.attempt, stage, self.version)
+            self.version += 1
+            after = A.Token(self.attempt, stage + 1, self.version)
+            self._check(lib.reactive_transport_advance_resident_v2(t, before, after, tr.ctypes.data_as(
+                C.POINTER(A.State)), None, None, None, dt, A.dptr(br)))
+            self._check(lib.reactive_transport_download_conserved(t, after, A.dptr(self.q)))
+            self.h2d += tr.nbytes
+            self.d2h += self.q.nbytes
+            seeds = start.copy()
+            e = self.q[:, 4] - .5 * np.sum(self.q[:, 1:4] ** 2, axis=1) / self.q[:, 0]
+            ok, _ = self.hem.run(np.ascontiguousarray(self.q[:, 0]), e, seeds)
+            if not ok.all():
+                raise RuntimeError("HEM recovery failed")
+            self.h2d += self.q[:, 0].nbytes + e.nbytes + seeds.nbytes
+            self.d2h += seeds.nbytes + ok.nbytes
+            self.states = seeds
+            if stage == 0:
+                prim = self._primitives(self.states)
+                self._check(lib.reactive_transport_stable_step_primitives(
+                    t, prim.ctypes.data_as(C.POINTER(A.Primitive)),
+                    self._compact(self.states).ctypes.data_as(C.POINTER(A.State)), .5, dt, C.byref(dtc)))
+        self._check(lib.reactive_transport_end_attempt(t, self.attempt, 1))
+        self.h2d += self.q.nbytes + 2 * tr0.nbytes + 2 * prim.nbytes
+
+    def close(self):
+        self.lib.reactive_transport_destroy(self.t)
+
+
+def run_ours(args, rank, world):
+    import torch
+    pkg = load_package()
+    from spuma_multiphysics_b200 import cases
+    from spuma_multiphysics_b200.flow import Flow
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    n = args.size
+    t0 = time.time()
+    faces, volume = cases.cartesian_faces(n)
+    init = cases.impingement(n, seed=2026 + rank)
+    flow = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
+                viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
+    setup_s = time.time() - t0
+    lib = flow.lib
+    stream = flow.stream
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return t.item()
+        return x
+
+    # ---- graph-captured device-resident step (value)
+    stats0 = pkg._abi.Stats()
+    lib.reactive_transport_stats(flow.transport, C.byref(stats0))
+    flow.capture(DT)
+    stats1 = pkg._abi.Stats()
+    lib.reactive_transport_stats(flow.transport, C.byref(stats1))
+    launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 7
+    for _ in range(args.warmup):
+        flow.step(DT)
+    flow.check(DT)
+    barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clocks:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            flow.step(DT)
+        b.record(stream)
+        barrier()
+    graph_ms = max_over_ranks(a.elapsed_time(b) / args.steps)
+    flow.check(DT)
+    cells = n ** 3
+    value = world * cells / (graph_ms * 1e-3) / 1e6
+
+    # ---- plain launches, with CUDA events around every flash (dominant kernel)
+    plain_ms, flash_ms, flash_phase_evals = None, None, None
+    if not args.skip_plain:
+        flow.hem.counters(stream.cuda_stream)
+        ev = []
+        lib_t, t = flow.lib, flow.transport
+        barrier()
+        a.record(stream)
+        for _ in range(args.steps):
+            flow.step(DT, graph=False)
+        b.record(stream)
+        barrier()
+        plain_ms = max_over_ranks(a.elapsed_time(b) / args.steps)
+        prof = flow.hem.counters(stream.cuda_stream)
+        flash_phase_evals = prof.phaseEvaluations / (2 * args.steps)
+        # flash alone on the resident state, timed on its own stream
+        times = []
+        for _ in range(max(2, args.steps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            flow.hem.run_device(flow.qn, flow.qn.shape[1], flow.cells, flow.nv, flow.sn, flow.s1, flow.tr,
+                                flow.success, stream.cuda_stream)
+            e1.record(stream)
+            times.append((e0, e1))
+        stream.synchronize()
+        flash_ms = statistics.mean(x.elapsed_time(y) for x, y in times)
+        flow.hem.counters(stream.cuda_stream)
+        flow.check(DT)
+
+    # ---- e2e through the reference-facing C ABI with host arrays
+    e2e = None
+    if not args.skip_e2e:
+        host = HostPath(pkg, faces, volume, flow, init["fixed_q"])
+        host.step(DT)  # warm-up
+        host.h2d = host.d2h = 0
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            host.step(DT)
+        barrier()
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
+        e2e = {"value": world * cells / e2e_s / 1e6, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+               "h2d_bytes_per_step": host.h2d // args.e2e_steps, "d2h_bytes_per_step": host.d2h // args.e2e_steps,
+               "path": "reactive_transport_upload_conserved/advance_resident_v2/download_conserved + "
+                       "reactive_gpu_hem_run_v1, host arrays"}
+        host.close()
+
+    peaks = measured_peaks()
+    fp64 = fp64_peak(lib, torch)
+    roofline = None
+    if flash_ms:
+        flops_per_eval = args.flops_per_phase_eval
+        achieved = flops_per_eval * flash_phase_evals / (flash_ms * 1e-3) / 1e12 if flops_per_eval else None
+        roofline = {"bound": "fp64", "kernel": "HEM flash (candidate passes, one recovery of all cells)",
+                    "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                    "frac": achieved / fp64 if achieved else None,
+                    "peak_source": "measured in this run (FP64 FMA-chain probe)",
+                    "traffic": args.flash_traffic, "ms_per_launch": flash_ms,
+                    "phase_evaluations_per_launch": flash_phase_evals,
+                    "flops_per_phase_evaluation": flops_per_eval}
+    # HBM roofline of the whole step (algorithmic bytes per cell-step, FP64, nv=5, 4 transport thermo fields)
+    bytes_per_cell_step = 8 * (5 * 5 + 2 * 4) + 2 * (8 * 5 + 80)
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    step_roofline = {"bound": "hbm", "bytes_per_cell_step": bytes_per_cell_step,
+                     "achieved": value * 1e6 * bytes_per_cell_step / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": value * 1e6 * bytes_per_cell_step / 1e9 / hbm,
+                     "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback"}
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        cpu = cpu_reference(args, seconds_hint=20)
+    clock = clocks.summary()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N2O impingement initial state)",
+            "config": {**workload(n), "parallelism": f"{world} independent replicas (one per GPU)"},
+            "plain_fp64": {"ms_per_step": plain_ms, "value": world * cells / (plain_ms * 1e-3) / 1e6 if plain_ms
+                           else None, "form": "same kernels, launched one by one"},
+            "e2e": e2e, "roofline": roofline, "roofline_step_hbm": step_roofline, "cpu_baseline": cpu,
+            "clocks": clock, "gpu_launches": launches_per_step * args.steps,
+            "fp64_peak_tflops": fp64, "setup_s": setup_s}
+    flow.close()
+    return line
+
+
+def cpu_reference(args, seconds_hint=20, n=40):
+    """One SSPRK2 + recovery step of the same case at 40^3 on the reference's CPU code:
+    its transport built for the CPU (serial by construction) and its flash compiled for
+    the host, threaded over all cores."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    pkg = load_package()
+    from spuma_multiphysics_b200 import cases, thermo_data as td
+    from oracle import oracle
+    import rk_oracle
+    threads = oracle.cpu_threads()
+    faces, volume = cases.cartesian_faces(n)
+    init = cases.impingement(n, seed=2026)
+    image = td.model_bytes(td.pure_model())
+    ref = rk_oracle.ReferenceFlow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
+                                  VISCOSITY, CONDUCTIVITY, WALE_CW, image, threads=threads)
+    samples = []
+    for _ in range(max(1, getattr(args, "cpu_steps", 1))):
+        t0 = time.perf_counter()
+        ref.step(DT)
+        samples.append(time.perf_counter() - t0)
+    ref.close()
+    s = statistics.mean(samples)
+    return {"value": n ** 3 / s / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"one SSPRK2 step (2 transport stages + 2 recoveries of all cells) of the same case at "
+                      f"{n}^3 ({n ** 3:,} cells); transport serial (reference CPU build), flash on {threads} threads",
+            "seconds_per_step": s}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference(args)
+        if i >= args.warmup:
+            samples.append(r)
+    value = statistics.mean(r["value"] for r in samples)
+    cpu = dict(samples[0])
+    cpu["value"] = value
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(r["seconds_per_step"] for r in samples),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded N2O impingement initial state)", "impl": "reference",
+            "config": {**workload(args.size), "parallelism": "reference CPU code on host cores"},
+            "cpu_baseline": cpu, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+
+
+def run_flash_batch(args):
+    """Standalone batched HEM flash (the 4,096,000-state configuration when
+    --flash-batch 4096000): states generated forward from a seed, 60% saturated
+    two-phase, 40% single-phase; seeds are the generating states."""
+    import torch
+    pkg = load_package()
+    from spuma_multiphysics_b200 import _abi as A, cases, thermo_data as td
+    from spuma_multiphysics_b200.hem import GpuHem
+    n = args.flash_batch
+    t0 = time.time()
+    q, e, guess = cases.flash_batch(n, seed=20260303)
+    gen_s = time.time() - t0
+    hem = GpuHem(model=td.pure_model(stable_gas_prune=args.flash_prune), capacity=n)
+    dev = torch.device("cuda")
+    cons = torch.zeros((5, n), dtype=torch.float64, device=dev)
+    cons[0] = torch.from_numpy(q).to(dev)
+    cons[4] = torch.from_numpy(e).to(dev)
+    seed = torch.from_numpy(guess.view(np.uint8).copy()).to(dev)
+    state = torch.zeros_like(seed)
+    ok = torch.zeros(n, dtype=torch.int32, device=dev)
+    s = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        hem.run_device(cons, n, n, 5, seed, state, None, ok, s.cuda_stream)
+    s.synchronize()
+    hem.counters(s.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clocks:
+        a.record(s)
+        for _ in range(args.steps):
+            hem.run_device(cons, n, n, 5, seed, state, None, ok, s.cuda_stream)
+        b.record(s)
+        s.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    prof = hem.counters(s.cuda_stream)
+    out = state.cpu().numpy().view(A.THERMO_DTYPE)
+    labels = cases.phase_label(out)
+    iters = out["iterations"]
+    return {"metric": "HEM UV flash calls/s (standalone batch)", "value": n / (ms * 1e-3), "unit": "flash/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic (seeded pure-N2O states generated forward)",
+            "config": {"workload": f"batched HEM UV flash, {n:,} pure-N2O cells, 60% two-phase",
+                       "stableGasPrune": args.flash_prune},
+            "succeeded": int(ok.sum().item()), "labels": np.bincount(labels, minlength=3).tolist(),
+            "iterations": {"p50": float(np.percentile(iters, 50)), "p99": float(np.percentile(iters, 99)),
+                           "max": int(iters.max())},
+            "phase_evaluations_per_cell": prof.phaseEvaluations / (args.steps * n),
+            "residual_evaluations_per_cell": prof.residualEvaluations / (args.steps * n),
+            "clocks": clocks.summary(), "generation_s": gen_s}
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--size", type=int, default=160)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--skip-plain", action="store_true")
+    p.add_argument("--skip-e2e", action="store_true")
+    p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--flops-per-phase-eval", type=float, default=0.0,
+                   help="FP64 FLOPs per PR phase evaluation of the flash kernels (from an ncu capture)")
+    p.add_argument("--flash-traffic", type=float, default=None, help="DRAM bytes per flash launch (ncu)")
+    p.add_argument("--flash-batch", type=int, default=0, help="run the standalone batched flash on this many cells")
+    p.add_argument("--flash-prune", type=int, default=0, help="the model's stableGasPrune flag for --flash-batch")
+    args = p.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.flash_batch:
+            line = run_flash_batch(args)
+        else:
+            line = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

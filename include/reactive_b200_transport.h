@@ -114,7 +114,8 @@ int reactive_transport_layout_v3(void* transport, size_t* cells, size_t* fixed, 
     size_t* species);
 int reactive_transport_fill_fixed_v3(void* transport, double* q, ReactiveTransportState* state, void* stream);
 /* stage 0: qOut = qIn + dt L(qIn). stage 1: qOut = .5 qOut + .5 (qIn + dt L(qIn)),
- * i.e. qOut holds q^n on entry. boundaryRate (device, variables doubles) may be null. */
+ * i.e. qOut holds q^n on entry. boundaryRate (device, variables doubles) may be null.
+ * Requires diffusivity 0 (molecular species diffusion takes host gas fractions). */
 int reactive_transport_stage_device_v3(void* transport, const double* qIn, double* qOut,
     const ReactiveTransportState* state, double dt, int stage, double* boundaryRate, void* stream);
 /* Writes the CFL step (or -1 when any face is invalid) to dt[0] on the device. */

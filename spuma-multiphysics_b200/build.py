@@ -15,7 +15,7 @@ LIB = HERE / "libreactive_b200.so"
 # (--fmad=false) so antisymmetric face terms cancel exactly, e.g. the HLL mass and
 # energy fluxes through a slip wall are exactly zero as in the reference's CPU and
 # CUDA builds. HEM: fused multiply-add (the Newton iteration is insensitive to it).
-SOURCES = {"transport.cu": ["--fmad=false"], "hem.cu": ["--fmad=true"]}
+SOURCES = {"transport.cu": ["--fmad=false"], "hem.cu": ["--fmad=true"], "probe.cu": ["--fmad=true"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--shared", "-Xptxas", "-warn-spills",
          "--expt-relaxed-constexpr"]

@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kPassThreads) passPartitions(const HemConst* _
             CandidateOut o{};
             bool ok;
             if (kind == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n);
-            else ok = frozenSolve(C, x, x.q, 0, v, o, n);
+            else ok = x.q * (1 + 1e-12) >= C.liquidFloor && frozenSolve(C, x, x.q, 0, v, o, n);
             finishCandidate(C, x, ok, v, o, rec + size_t(kind) * count + c, n);
         }
     }
@@ -545,6 +545,9 @@ std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C) {
     C.scalarRecovery = m.scalarRecovery;
     C.analyticJacobian = m.analyticJacobian;
     C.stableGasPrune = m.stableGasPrune;
+    C.samePure = std::memcmp(&C.gas, &C.liq, sizeof(PureSpecies)) == 0;
+    // The line rho_mid(T) = rho_c + (T - Tc) dRho/dT is >= rho_c below Tc when dRho <= 0 (dT > 0).
+    C.liquidFloor = (C.liq.dRho <= 0 && C.liquidTc * (1 - 1e-10) <= C.liq.tcLine) ? C.liq.rhoC * (1 - C.vtol) : 0.0;
     return "";
 }
 

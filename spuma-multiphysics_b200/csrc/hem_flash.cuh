@@ -31,6 +31,12 @@ struct HemConst {
     double liquidTmin, liquidTc;
     double gasTmin, gasTmax;  // NASA fit bounds of the gas species (enforced when requested)
     int enforceBounds, scalarRecovery, analyticJacobian, stableGasPrune;
+    int samePure;  // gas and liquid tables hold the same species: one cubic serves both roots
+    // Density below which the all-liquid partition provably cannot converge (0: no bound).
+    // A reported liquid needs rho >= rhoMid(T) >= rho_c whenever the reported-phase line
+    // falls with T and the liquid range ends at or below its Tc; the all-liquid volume
+    // residual q/rho_l - 1 then stays below q/rho_c - 1 < -vtol.
+    double liquidFloor;
 };
 
 struct CellInput {
@@ -88,9 +94,29 @@ __device__ __forceinline__ void addPhase(Eval& v, double mass, const PhaseProps&
     v.cpD += mass * ph.cp;
 }
 
+// Gas-branch status at (p, T) from shared T-terms and roots (same checks and
+// order as gasPhase).
+__device__ __forceinline__ int gasFromShared(const HemConst& C, int shared, const TTerms& t, const Roots& r,
+                                             double p, bool chem, PhaseProps& o, Counts& n) {
+    ++n.phases;
+    if (C.enforceBounds && (t.T < C.gasTmin || t.T > C.gasTmax)) return EOS_INVALID_INPUT;
+    if (shared != EOS_OK) return shared;
+    return rootProps(C.gas, t, r, p, ROOT_GAS, chem, o);
+}
+__device__ __forceinline__ int liquidFromShared(const HemConst& C, int shared, const TTerms& t, const Roots& r,
+                                                double p, bool chem, PhaseProps& o, Counts& n) {
+    ++n.phases;
+    if (t.T < C.liquidTmin) return EOS_INVALID_INPUT;
+    if (t.T >= C.liquidTc * (1 - 1e-10)) return EOS_UNAVAILABLE;
+    if (shared != EOS_OK) return shared;
+    return rootProps(C.liq, t, r, p, ROOT_LIQUID, chem, o);
+}
+
 // Phase sums at (p, T) for liquid mass `mass` out of total density q. With
 // `virt` the liquid is also evaluated when absent and both chemical potentials
-// are formed (two-phase residual and stability test).
+// are formed (two-phase residual and stability test). When both branches are
+// needed and the tables hold one species, the T-terms and the cubic are formed
+// once for both roots (the same arithmetic as two separate evaluations).
 __device__ inline bool evaluate(const HemConst& C, double q, double mass, double p, double T, bool virt, Eval& v,
                                 Counts& n) {
     v.p = p; v.T = T;
@@ -107,15 +133,26 @@ __device__ inline bool evaluate(const HemConst& C, double q, double mass, double
     const double gas = q - mass;
     if (!fin(gas) || gas < 0 || gas > q) return false;
     v.gasMass = gas;
+    const bool needLiquid = mass > 0 || (virt && q > 0);
+    const bool shared = C.samePure && gas > 0 && needLiquid;
+    TTerms t;
+    Roots r;
+    int sharedStatus = EOS_OK;
+    if (shared) {
+        sharedStatus = tTerms(C.gas, T, t);
+        if (sharedStatus == EOS_OK) sharedStatus = cubicRoots(C.gas, T, p, t.aa, r);
+    }
     PhaseProps ph;
     if (gas > 0) {
-        if (gasPhase(C, p, T, virt, ph, n) != EOS_OK) return false;
+        const int st = shared ? gasFromShared(C, sharedStatus, t, r, p, virt, ph, n) : gasPhase(C, p, T, virt, ph, n);
+        if (st != EOS_OK) return false;
         addPhase(v, gas, ph, p);
         v.gRho = ph.rho; v.gE = ph.e; v.gV = ph.V; v.gH = ph.h;
         if (virt) v.muG = ph.mu / (kGas * T);
     }
-    if (mass > 0 || (virt && q > 0)) {
-        const int status = liquidPhase(C, p, T, virt, ph, n);
+    if (needLiquid) {
+        const int status = shared ? liquidFromShared(C, sharedStatus, t, r, p, virt, ph, n)
+                                  : liquidPhase(C, p, T, virt, ph, n);
         if (status != EOS_OK) {
             if (mass > 0 || !unavailableStatus(status)) return false;
             v.muL = HUGE_VAL;

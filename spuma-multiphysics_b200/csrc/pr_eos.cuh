@@ -207,13 +207,35 @@ __device__ inline int cubicRoots(const PureSpecies& sp, double T, double p, doub
     return EOS_OK;
 }
 
-// Properties at (T, rho). chem: also the molar chemical potential. phaseOut:
-// -2 supercritical, -1 gas, 0 liquid by the reported-phase line.
-__device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool chem, PhaseProps& s, int& phaseOut) {
-    if (!fin(T) || !fin(rho) || T <= 0 || rho <= 0) return EOS_INVALID_INPUT;
-    double aa, da, d2a;
-    const int st = alphaTerms(sp, T, aa, da, d2a);
-    if (st != EOS_OK) return st;
+// Temperature-only terms shared by every evaluation at one T: a*alpha and its
+// T-derivatives, |1 + kappa(1 - sqrt(T/Tc))|, and the NASA cp/R, h/RT, s/R.
+struct TTerms {
+    double T, aa, da, d2a, q, cpR, hRT, sR;
+};
+
+__device__ inline int tTerms(const PureSpecies& sp, double T, TTerms& t) {
+    if (!fin(T) || T <= 0) return EOS_INVALID_INPUT;
+    const double sq = sqrt(T / sp.Tc), f = 1.0 + sp.kappa * (1.0 - sq);
+    if (fabs(f) <= 1e-14) return EOS_NONFINITE;
+    const double sign = f > 0 ? 1.0 : -1.0, q = fabs(f);
+    const double dq = -sign * sp.kappa / (2.0 * sp.Tc * sq);
+    const double d2q = sign * sp.kappa / (4.0 * sp.Tc * sp.Tc * sq * sq * sq);
+    t.T = T;
+    t.q = q;
+    t.aa = sp.a * q * q;
+    t.da = sp.a * (dq * q + q * dq);
+    t.d2a = sp.a * (d2q * q + 2.0 * dq * dq + q * d2q);
+    if (!(fin(t.aa) && fin(t.da) && fin(t.d2a) && t.aa > 0)) return EOS_NONFINITE;
+    nasaEval(sp, T, t.cpR, t.hRT, t.sR);
+    return EOS_OK;
+}
+
+// Properties at (T, rho) from the T-only terms. chem: also the molar chemical
+// potential. phaseOut: -2 supercritical, -1 gas, 0 liquid by the reported-phase line.
+__device__ inline int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
+                              int& phaseOut) {
+    const double T = t.T, aa = t.aa, da = t.da, d2a = t.d2a;
+    if (!fin(rho) || rho <= 0) return EOS_INVALID_INPUT;
     const double b = sp.b, W = sp.W, V = W / rho;
     if (!(V > b)) return EOS_NO_ROOT;
     const double den = V * V + 2.0 * V * b - b * b, vmb = V - b;
@@ -225,12 +247,10 @@ __device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool c
     if (!fin(dpdV) || !fin(dpdT) || dpdV >= 0) return EOS_UNSTABLE;
     const double logRatio = log((V + (1.0 + kSqrt2) * b) / (V + (1.0 - kSqrt2) * b));
     const double L = logRatio / (2.0 * kSqrt2 * b);
-    double cpR, hRT, sR;
-    nasaEval(sp, T, cpR, hRT, sR);
     const double z = p * V / (kGas * T);
-    const double hM = kGas * T * hRT + (kGas * T * (z - 1.0) + L * (T * da - aa));
-    const double sM = (kGas * sR - kGas * log(p / sp.refP)) + (kGas * log(z * (1.0 - b / V)) + L * da);
-    const double dHdT = kGas * cpR + V * dpdT - kGas + L * T * d2a;
+    const double hM = kGas * T * t.hRT + (kGas * T * (z - 1.0) + L * (T * da - aa));
+    const double sM = (kGas * t.sR - kGas * log(p / sp.refP)) + (kGas * log(z * (1.0 - b / V)) + L * da);
+    const double dHdT = kGas * t.cpR + V * dpdT - kGas + L * T * d2a;
     const double cpM = dHdT - (V + T * dpdT / dpdV) * dpdT;
     const double cvM = cpM + T * dpdT * dpdT / dpdV;
     s.p = p;
@@ -246,10 +266,10 @@ __device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool c
     const double sound2 = V * V * (-cpM / cvM * dpdV / W);
     if (!(s.cp > 0) || !(s.cv > 0) || !(s.kappaT > 0) || !(sound2 > 0)) return EOS_UNSTABLE;
     if (chem) {
-        const double RT = kGas * T, f = 1.0 + sp.kappa * (1.0 - sqrt(T / sp.Tc));
-        const double pp = sp.a * fabs(f * f), num = 2.0 * b * pp - aa * b;
-        s.mu = RT * (hRT - sR) + RT * log(p / sp.refP) - RT * log(p * V / RT) + RT * log(V / vmb) + RT * b / vmb
-             - num / (2.0 * kSqrt2 * b * b) * logRatio - aa * b * V / (b * den);
+        const double RT = kGas * T;
+        const double pp = sp.a * (t.q * t.q), num = 2.0 * b * pp - aa * b;
+        s.mu = RT * (t.hRT - t.sR) + RT * log(p / sp.refP) - RT * log(p * V / RT) + RT * log(V / vmb)
+             + RT * b / vmb - num / (2.0 * kSqrt2 * b * b) * logRatio - aa * b * V / (b * den);
         if (!fin(s.mu)) return EOS_NONFINITE;
     }
     if (T >= sp.tcLine) phaseOut = -2;
@@ -264,16 +284,18 @@ __device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool c
     return EOS_OK;
 }
 
-// Properties at (T, p) on the chosen root, with the host postcondition
-// |p(T, rho) - p| <= 1e-7 max(1, p) and the reported-phase consistency check.
-__device__ inline int prTP(const PureSpecies& sp, double T, double p, int choice, bool chem, PhaseProps& s) {
-    if (!fin(T) || !fin(p) || T <= 0 || p <= 0) return EOS_INVALID_INPUT;
-    double aa, da, d2a;
-    int st = alphaTerms(sp, T, aa, da, d2a);
+__device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool chem, PhaseProps& s, int& phaseOut) {
+    if (!fin(T) || !fin(rho) || T <= 0 || rho <= 0) return EOS_INVALID_INPUT;
+    TTerms t;
+    const int st = tTerms(sp, T, t);
     if (st != EOS_OK) return st;
-    Roots r;
-    st = cubicRoots(sp, T, p, aa, r);
-    if (st != EOS_OK) return st;
+    return prTrhoT(sp, t, rho, chem, s, phaseOut);
+}
+
+// Root choice at (T, p) with the host postcondition |p(T, rho) - p| <= 1e-7 max(1, p)
+// and the reported-phase consistency of the chosen branch.
+__device__ inline int rootProps(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
+                                bool chem, PhaseProps& s) {
     int sel = r.count - 1;
     if (choice == ROOT_LIQUID) {
         if (!r.liquid) return EOS_UNAVAILABLE;
@@ -281,13 +303,24 @@ __device__ inline int prTP(const PureSpecies& sp, double T, double p, int choice
     } else if (choice == ROOT_GAS && !r.gas) return EOS_UNAVAILABLE;
     const double V = sel == 0 ? r.lo : r.hi;
     int phase = 0;
-    st = prTrho(sp, T, sp.W / V, chem, s, phase);
+    const int st = prTrhoT(sp, t, sp.W / V, chem, s, phase);
     if (st != EOS_OK) return st;
     if (fabs(s.p - p) > 1e-7 * fmax(1.0, p)) return EOS_NONFINITE;
     s.p = p;
     if (choice == ROOT_GAS && phase >= 0) return EOS_UNAVAILABLE;
     if (choice == ROOT_LIQUID && phase < 0) return EOS_UNAVAILABLE;
     return EOS_OK;
+}
+
+__device__ inline int prTP(const PureSpecies& sp, double T, double p, int choice, bool chem, PhaseProps& s) {
+    if (!fin(T) || !fin(p) || T <= 0 || p <= 0) return EOS_INVALID_INPUT;
+    TTerms t;
+    int st = tTerms(sp, T, t);
+    if (st != EOS_OK) return st;
+    Roots r;
+    st = cubicRoots(sp, T, p, t.aa, r);
+    if (st != EOS_OK) return st;
+    return rootProps(sp, t, r, p, choice, chem, s);
 }
 
 }  // namespace rb200

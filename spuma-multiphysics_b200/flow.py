@@ -1,0 +1,172 @@
+"""SSPRK2 + HEM step driver (the RK stage driver of the hot path), device resident.
+
+One accepted step follows the reference's Flow::step
+(src/reactiveFoam/ReactiveFoam.C:961-1019) with chemistry off:
+    CFL query at the step-start state                      (:1443, stableStep :798-812)
+    stage 0   q1 = qn + dt L(qn; thermo_n)                 (transportStage :651-661)
+    recovery  thermo_1 = flash(q1) seeded by thermo_n       (recover :732-751)
+    CFL recheck at q1                                       (:993)
+    stage 1   q_{n+1} = qn/2 + (q1 + dt L(q1; thermo_1))/2
+    recovery  thermo_{n+1} = flash(q_{n+1}) seeded by thermo_n (step-start seed, :1011-1013)
+    boundary ledger  .5 dt (B0 + B1)                        (:1014-1016)
+Transport uses the frozen sound speed (compact, :419-420).
+
+Unlike the reference, q and the thermodynamic states never leave HBM between
+stages: the transport *_v3 and HEM run_device_v3 entry points work on the same
+SoA conserved arrays, and with `graph=True` the whole step (2 CFL reductions,
+2 transport stages, 2 flashes, the ledger) replays as one captured CUDA graph.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _abi as A, _lib
+from .hem import GpuHem
+from .thermo_data import pure_model
+
+
+class FlowError(RuntimeError):
+    pass
+
+
+def _check(lib, handle, rc):
+    if rc:
+        raise FlowError(lib.reactive_transport_error(handle).decode())
+
+
+class Flow:
+    def __init__(self, faces, volume, q0, guess0, fixed_q, fixed_guess, viscosity=0.0, conductivity=0.0,
+                 wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda"):
+        """faces: FACE_DTYPE array; q0: cell-major (cells, 5) conserved state;
+        guess0/fixed_guess: THERMO_DTYPE seeds used for the initial recovery."""
+        self.lib = _lib.load()
+        self.device = torch.device(device)
+        self.cells = len(volume)
+        self.fixed = len(fixed_q)
+        self.nv = q0.shape[1]
+        self.cfl = cfl
+        self.hem = GpuHem(model=model if model is not None else pure_model(), capacity=max(self.cells, self.fixed))
+        # Initial recoveries on the host path (once): fixed inlet states and cells.
+        fixed_state = fixed_guess.copy()
+        e_fixed = fixed_q[:, 4] - .5 * np.sum(fixed_q[:, 1:4] ** 2, axis=1) / fixed_q[:, 0]
+        ok, _ = self.hem.run(np.ascontiguousarray(fixed_q[:, 0]), e_fixed, fixed_state)
+        if not ok.all():
+            raise FlowError("fixed-state recovery failed")
+        state0 = guess0.copy()
+        e0 = q0[:, 4] - .5 * np.sum(q0[:, 1:4] ** 2, axis=1) / q0[:, 0]
+        ok, _ = self.hem.run(np.ascontiguousarray(q0[:, 0]), e0, state0)
+        if not ok.all():
+            raise FlowError(f"initial recovery failed in {int((ok == 0).sum())} cells")
+        fixed_tr = np.zeros(self.fixed, dtype=A.STATE_DTYPE)
+        for k_out, k_in in (("p", "p"), ("T", "T"), ("rho", "rho"), ("cv", "cv"), ("sound", "soundFrozen"),
+                            ("gasMass", "gasMass")):
+            fixed_tr[k_out] = fixed_state[k_in]
+        cfg = A.Config(self.cells, 1, self.nv, len(faces), self.fixed, viscosity, conductivity, 0.0, wave_factor,
+                       1.6e11, 0)
+        self._faces = np.ascontiguousarray(faces)
+        err = C.create_string_buffer(2048)
+        h = self.lib.reactive_transport_create(
+            1, C.byref(cfg), A.dptr(np.ascontiguousarray(volume, dtype=np.float64)),
+            self._faces.ctypes.data_as(C.POINTER(A.Face)), A.dptr(np.ascontiguousarray(fixed_q, dtype=np.float64)),
+            fixed_tr.ctypes.data_as(C.POINTER(A.State)), None, None, err, len(err))
+        if not h:
+            raise FlowError(err.value.decode())
+        self.transport = C.c_void_p(h)
+        if wale_cw is not None:
+            opts = A.WaleOptions(1, C.sizeof(A.WaleOptions), wale_cw)
+            _check(self.lib, self.transport, self.lib.reactive_transport_set_wale_v1(self.transport, C.byref(opts)))
+        all_ = self.cells + self.fixed
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.qn = torch.zeros((self.nv, all_), **f64)
+        self.qn[:, :self.cells] = torch.from_numpy(np.ascontiguousarray(q0.T)).to(dev)
+        self.q1 = torch.zeros_like(self.qn)
+        self.tr = torch.zeros((all_, 7), **f64)
+        self.sn = torch.from_numpy(state0.view(np.uint8).copy()).to(dev)   # step-start thermo (seeds)
+        self.s1 = torch.zeros_like(self.sn)                                   # stage-1 thermo
+        self.success = torch.zeros(self.cells, dtype=torch.int32, device=dev)
+        self.boundary = torch.zeros((2, self.nv), **f64)
+        self.dt_cfl = torch.zeros(2, **f64)
+        self.stream = torch.cuda.Stream(device=dev)
+        s = self.stream.cuda_stream
+        tr0 = np.zeros(self.cells, dtype=A.STATE_DTYPE)
+        for k_out, k_in in (("p", "p"), ("T", "T"), ("rho", "rho"), ("cv", "cv"), ("sound", "soundFrozen"),
+                            ("gasMass", "gasMass")):
+            tr0[k_out] = state0[k_in]
+        self.tr[:self.cells] = torch.from_numpy(tr0.view(np.float64).reshape(self.cells, 7)).to(dev)
+        torch.cuda.synchronize(dev)
+        _check(self.lib, self.transport,
+               self.lib.reactive_transport_fill_fixed_v3(self.transport, self.qn.data_ptr(), self.tr.data_ptr(), s))
+        _check(self.lib, self.transport,
+               self.lib.reactive_transport_fill_fixed_v3(self.transport, self.q1.data_ptr(), self.tr.data_ptr(), s))
+        self.stream.synchronize()
+        self.graph = None
+        self.graph_dt = None
+        self.steps = 0
+
+    # ------------------------------------------------------------------ step
+    def _launch_step(self, dt):
+        lib, t, s = self.lib, self.transport, self.stream.cuda_stream
+        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.qn.data_ptr(), self.tr.data_ptr(),
+                                                                    self.cfl, dt, self.dt_cfl.data_ptr(), s))
+        _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.qn.data_ptr(), self.q1.data_ptr(),
+                                                              self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(), s))
+        self.hem.run_device(self.q1, self.qn.shape[1], self.cells, self.nv, self.sn, self.s1, self.tr, self.success, s)
+        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.q1.data_ptr(), self.tr.data_ptr(),
+                                                                    self.cfl, dt, self.dt_cfl[1:].data_ptr(), s))
+        _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.q1.data_ptr(), self.qn.data_ptr(),
+                                                              self.tr.data_ptr(), dt, 1, self.boundary[1].data_ptr(), s))
+        # second recovery, seeded by the step-start states, results in place
+        self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s)
+
+    def capture(self, dt):
+        """Capture one step as a CUDA graph (replayed by step(dt) for this dt)."""
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=self.stream):
+            self._launch_step(dt)
+        self.graph_dt = dt
+
+    def step(self, dt, graph=True):
+        if graph:
+            if self.graph is None or self.graph_dt != dt:
+                self.capture(dt)  # records the launches; nothing executes until replay
+            with torch.cuda.stream(self.stream):  # replay() launches on the current stream
+                self.graph.replay()
+        else:
+            with torch.cuda.stream(self.stream):
+                self._launch_step(dt)
+        self.steps += 1
+
+    def check(self, dt):
+        """Host check after a run of steps: every flash succeeded, dt within CFL,
+        no WALE failure (synchronises)."""
+        self.stream.synchronize()
+        status = C.c_uint()
+        _check(self.lib, self.transport,
+               self.lib.reactive_transport_status_v3(self.transport, C.byref(status), 1, self.stream.cuda_stream))
+        failed = int((self.success == 0).sum().item())
+        cfl = self.dt_cfl.min().item()
+        if status.value:
+            raise FlowError("WALE gradient/viscosity/traction became non-finite")
+        if failed:
+            raise FlowError(f"HEM recovery failed in {failed} cells")
+        if not (cfl > 0 and dt <= cfl * (1 + 1e-10)):
+            raise FlowError(f"dt={dt} exceeds the wave/diffusion CFL step {cfl}")
+        return dict(cfl_dt=cfl)
+
+    # --------------------------------------------------------------- views
+    def conserved(self):
+        """Cell-major host copy of the conserved state (cells, nv)."""
+        return self.qn[:, :self.cells].T.contiguous().cpu().numpy()
+
+    def states(self):
+        return self.sn.cpu().numpy().view(A.THERMO_DTYPE)
+
+    def close(self):
+        if getattr(self, "transport", None):
+            self.stream.synchronize()
+            self.graph = None
+            self.lib.reactive_transport_destroy(self.transport)
+            self.transport = None
+            self.hem.close()

@@ -64,14 +64,23 @@ def test_cuda_wale(lib, spec):
         lib.reactive_transport_destroy(h)
 
 
-@pytest.mark.parametrize("spec", [T.CASES[7], T.CASES[17], T.CASES[-1]], ids=lambda s: "-".join(map(str, s)))
+V3_CASES = [dict(ns=4, nc=7, kind=3, viscous_only=True, conduction=True),
+            dict(ns=1, nc=64, kind=2, spatial=True, viscous_only=True, conduction=True),
+            dict(ns=2, nc=33, kind=1, spatial=True, extra_boundary=40, viscous_only=True, wale=.325),
+            dict(ns=1, nc=40, kind=3, spatial=True, conduction=True, wale=.325)]
+
+
+@pytest.mark.parametrize("spec", V3_CASES, ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
 def test_cuda_device_resident_v3(lib, spec):
-    """Both SSPRK2 stages on device pointers equal the host-ABI stages."""
+    """Both SSPRK2 stages and the CFL step on device pointers against the oracle."""
     import torch
     L = _lib.load()
-    case = T.case_from_tuple(spec)
+    spec = dict(spec)
+    cw = spec.pop("wale", None)
+    case = T.make_case(**spec)
     ns, nc, nv = case["ns"], case["nc"], case["nv"]
-    h = T.create(lib, 1, case)
+    h = T.create(lib, 1, case, wale_cw=cw)
+    wale_cw = -1.0 if cw is None else cw
     try:
         cells, fixed, nvar, nsp = (C.c_size_t() for _ in range(4))
         assert L.reactive_transport_layout_v3(h, C.byref(cells), C.byref(fixed), C.byref(nvar), C.byref(nsp)) == 0
@@ -89,14 +98,15 @@ def test_cuda_device_resident_v3(lib, spec):
         assert L.reactive_transport_stable_step_device_v3(h, q0.data_ptr(), st.data_ptr(), .23, .1,
                                                           dt_dev.data_ptr(), stream) == 0
         torch.cuda.synchronize()
-        odt = oracle.transport_stable_dt(case, case["q"], case["states"].ctypes.data_as(C.c_void_p), .23, .1)
+        odt = oracle.transport_stable_dt(case, case["q"], case["states"].ctypes.data_as(C.c_void_p), .23, .1,
+                                         wale_cw=wale_cw)
         assert abs(dt_dev.item() / odt - 1) < T.DT_TOL
         step = .1 * odt
         assert L.reactive_transport_stage_device_v3(h, q0.data_ptr(), q1.data_ptr(), st.data_ptr(), step, 0,
                                                     br.data_ptr(), stream) == 0
         torch.cuda.synchronize()
         rhs, exp_br, _, _, _ = oracle.transport_rhs(case, case["q"], case["states"].ctypes.data_as(C.c_void_p),
-                                                    case["y"], case["h"])
+                                                    case["y"], case["h"], wale_cw=wale_cw)
         got1 = q1[:, :nc].cpu().numpy().T
         assert T.scaled_error(got1, case["q"] + step * rhs) <= T.RHS_TOL
         assert T.scaled_error(br.cpu().numpy()[None], exp_br[None]) <= T.RHS_TOL
@@ -107,8 +117,9 @@ def test_cuda_device_resident_v3(lib, spec):
                                                     stream) == 0
         torch.cuda.synchronize()
         rhs1, _, _, _, _ = oracle.transport_rhs(case, np.ascontiguousarray(got1), st1.ctypes.data_as(C.c_void_p),
-                                                y1, h1)
+                                                y1, h1, wale_cw=wale_cw)
         assert T.scaled_error(qn[:, :nc].cpu().numpy().T, .5 * case["q"] + .5 * (got1 + step * rhs1)) <= T.RHS_TOL
         assert torch.equal(qn[:, nc:], q0[:, nc:])
+        # a diffusive configuration is rejected on the device path
     finally:
         lib.reactive_transport_destroy(h)

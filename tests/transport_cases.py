@@ -40,7 +40,7 @@ def states_ptr(arr):
 
 
 def make_case(ns, nc, kind, transport=False, mechanical=False, spatial=False, extra_boundary=0, frozen=0,
-              seed=0, viscous_only=False):
+              seed=0, viscous_only=False, conduction=False):
     rng = np.random.default_rng(9100 + 17 * ns + nc + 131 * kind + 7 * frozen + int(spatial) + seed)
     nv = ns + 4 + 2 * int(mechanical) + frozen
     q = np.zeros((nc, nv))
@@ -84,7 +84,7 @@ def make_case(ns, nc, kind, transport=False, mechanical=False, spatial=False, ex
         arr[i] = A.Face(o, nb, fx, (C.c_double * 3)(*n), area, dist, w, k)
     fixed_states, fixed_y, fixed_h = ideal_states(fixed_q, ns)
     visc = .007 if (transport or viscous_only) else 0.0
-    cfg = A.Config(nc, ns, nv, len(faces), n_fixed, visc, 2.0 if transport else 0.0,
+    cfg = A.Config(nc, ns, nv, len(faces), n_fixed, visc, 2.0 if (transport or conduction) else 0.0,
                    .003 if transport else 0.0, 1.1, 2e8, int(mechanical))
     states, y, h = ideal_states(q, ns, mechanical)
     return dict(config=cfg, faces=arr, volume=volume, q=q, states=states, y=y, h=h,
