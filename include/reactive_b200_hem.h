@@ -50,7 +50,9 @@ int reactive_gpu_hem_run_resident_v1(void* hem, const double* q, const double* e
  * transport (optional) receives the compact transport state. success (optional)
  * receives per-cell flags; failed cells copy their seed. Never synchronises or
  * allocates; safe to capture in a CUDA graph.
- * flags bit 0: count the batch's work counters (read with run_counters_v3). */
+ * flags bit 1: run the plain form instead (one thread per cell running the whole
+ * candidate search in order, no work queue, no pruning).
+ * Work counters accumulate in either form (read with run_counters_v3). */
 int reactive_gpu_hem_run_device_v3(void* hem, const double* conserved, size_t stride, size_t count,
     size_t variables, const ReactiveThermoState* seed, ReactiveThermoState* state,
     ReactiveTransportState* transport, int* success, void* reserved, int flags, void* stream,

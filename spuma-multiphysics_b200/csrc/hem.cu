@@ -272,6 +272,68 @@ __global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsi
     }
 }
 
+// One thread per cell running the whole search in order (the layout of the
+// reference's hemKernel, src/reactiveTransport/reactiveGpuHem.cuh:64-80): the
+// plain form the candidate-parallel passes are measured against. No pruning.
+__global__ void __launch_bounds__(kPassThreads) flashPerCell(const HemConst* __restrict__ Cp,
+                                                             const CellInput* __restrict__ in, size_t count,
+                                                             const ReactiveThermoState* seed,
+                                                             ReactiveThermoState* state,
+                                                             ReactiveTransportState* transport, int* success,
+                                                             unsigned* counters, unsigned long long* totals) {
+    const HemConst& C = *Cp;
+    Counts n;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
+        const CellInput x = in[c];
+        ReactiveThermoState best{};
+        double bestEntropy = 0;
+        bool have = false, gasStable = false;
+        for (int k = 0; k < 7; ++k) {
+            if (k >= 2 && C.stableGasPrune && gasStable) break;
+            Eval v;
+            CandidateOut o{};
+            bool ok;
+            if (k == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n);
+            else if (k == 1) ok = frozenSolve(C, x, x.q, 0, v, o, n);
+            else ok = twoPhaseSolve(C, x, kSeeds[k - 2], -1.0, v, o, n);
+            if (!ok) { ++n.failures; continue; }
+            if (!stableAt(C, x.q, v.liqMass, v.p, v.T, n)) { ++n.failures; continue; }
+            ++n.stable;
+            if (k == 0) gasStable = v.gasMass > 0;
+            if (!have || v.entropyD > bestEntropy) {
+                have = true;
+                bestEntropy = v.entropyD;
+                stateFromEval(v, x.q, o, best);
+            }
+        }
+        if (!have) {
+            const double lower = fmax(C.Tmin, C.liquidTmin), upper = fmin(C.Tmax, C.liquidTc * (1 - 1e-10));
+            for (int t = 0; t < 4 && upper > lower; ++t)
+                for (int s = 0; s < 5; ++s) {
+                    Eval v;
+                    CandidateOut o{};
+                    if (!twoPhaseSolve(C, x, kSeeds[s], lower + (upper - lower) * kRestart[t], v, o, n)
+                        || !stableAt(C, x.q, v.liqMass, v.p, v.T, n)) { ++n.failures; continue; }
+                    ++n.stable;
+                    if (!have || v.entropyD > bestEntropy) {
+                        have = true;
+                        bestEntropy = v.entropyD;
+                        stateFromEval(v, x.q, o, best);
+                    }
+                }
+        }
+        if (have) {
+            writeOutputs(best, c, state, transport);
+        } else {
+            if (state) state[c] = seed[c];
+            if (transport) writeOutputs(seed[c], c, nullptr, transport);
+            atomicAdd(counters + FAILED, 1u);
+        }
+        if (success) success[c] = have ? 1 : 0;
+    }
+    flushCounts(n, totals);
+}
+
 // ------------------------------------------------------------------ host
 std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C);
 
@@ -320,6 +382,13 @@ struct HemDevice {
         dout = alloc<ReactiveThermoState>(capacity);
         dsuccess = alloc<int>(capacity);
         hostPath = true;
+    }
+    void launchPerCell(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
+                       ReactiveTransportState* transport, int* success, cudaStream_t s) {
+        check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "memset counters");
+        flashPerCell<<<unsigned((count + kPassThreads - 1) / kPassThreads), kPassThreads, 0, s>>>(
+            cst, in, count, seed, state, transport, success, counters, totals);
+        check(cudaGetLastError(), "flashPerCell");
     }
     // Launches steps 2-7 for `count` prepared inputs.
     void launchSearch(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
@@ -667,7 +736,7 @@ int reactive_gpu_hem_run_resident_v1(void*, const double*, const double*, const 
 
 int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t stride, size_t count, size_t variables,
                                    const ReactiveThermoState* seed, ReactiveThermoState* state,
-                                   ReactiveTransportState* transport, int* success, void*, int, void* stream,
+                                   ReactiveTransportState* transport, int* success, void*, int flags, void* stream,
                                    char* error, size_t size) {
     try {
         rb200::require(raw && conserved && seed && (state || transport) && count && stride >= count
@@ -679,7 +748,8 @@ int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t st
         auto s = static_cast<cudaStream_t>(stream);
         rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1, seed, d.in);
         rb200::check(cudaGetLastError(), "inputs");
-        d.launchSearch(count, seed, state, transport, success, s);
+        if (flags & 2) d.launchPerCell(count, seed, state, transport, success, s);
+        else d.launchSearch(count, seed, state, transport, success, s);
         return 0;
     } catch (const std::exception& e) {
         if (error && size) std::snprintf(error, size, "%s", e.what());

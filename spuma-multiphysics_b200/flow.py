@@ -106,19 +106,21 @@ class Flow:
         self.steps = 0
 
     # ------------------------------------------------------------------ step
-    def _launch_step(self, dt):
+    def _launch_step(self, dt, per_cell=False):
         lib, t, s = self.lib, self.transport, self.stream.cuda_stream
         _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.qn.data_ptr(), self.tr.data_ptr(),
                                                                     self.cfl, dt, self.dt_cfl.data_ptr(), s))
         _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.qn.data_ptr(), self.q1.data_ptr(),
                                                               self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(), s))
-        self.hem.run_device(self.q1, self.qn.shape[1], self.cells, self.nv, self.sn, self.s1, self.tr, self.success, s)
+        self.hem.run_device(self.q1, self.qn.shape[1], self.cells, self.nv, self.sn, self.s1, self.tr, self.success, s,
+                            per_cell)
         _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.q1.data_ptr(), self.tr.data_ptr(),
                                                                     self.cfl, dt, self.dt_cfl[1:].data_ptr(), s))
         _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.q1.data_ptr(), self.qn.data_ptr(),
                                                               self.tr.data_ptr(), dt, 1, self.boundary[1].data_ptr(), s))
         # second recovery, seeded by the step-start states, results in place
-        self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s)
+        self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s,
+                            per_cell)
 
     def capture(self, dt):
         """Capture one step as a CUDA graph (replayed by step(dt) for this dt)."""
@@ -127,15 +129,17 @@ class Flow:
             self._launch_step(dt)
         self.graph_dt = dt
 
-    def step(self, dt, graph=True):
-        if graph:
+    def step(self, dt, graph=True, per_cell=False):
+        """One step. graph: replay the captured graph (work-queue flash); per_cell:
+        launch one by one with the plain one-thread-per-cell flash."""
+        if graph and not per_cell:
             if self.graph is None or self.graph_dt != dt:
                 self.capture(dt)  # records the launches; nothing executes until replay
             with torch.cuda.stream(self.stream):  # replay() launches on the current stream
                 self.graph.replay()
         else:
             with torch.cuda.stream(self.stream):
-                self._launch_step(dt)
+                self._launch_step(dt, per_cell)
         self.steps += 1
 
     def check(self, dt):

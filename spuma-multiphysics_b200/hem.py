@@ -57,13 +57,14 @@ class GpuHem:
         return success, prof
 
     def run_device(self, conserved, stride, count, variables, seed, state=None, transport=None, success=None,
-                   stream=0):
-        """Device batch: all arguments are device pointers (ints) or torch tensors."""
+                   stream=0, per_cell=False):
+        """Device batch: all arguments are device pointers (ints) or torch tensors.
+        per_cell: the plain one-thread-per-cell form instead of the work-queue passes."""
         ptr = lambda t: 0 if t is None else (t if isinstance(t, int) else t.data_ptr())
         err = C.create_string_buffer(1024)
         rc = self.lib.reactive_gpu_hem_run_device_v3(self.handle, ptr(conserved), stride, count, variables,
-                                                     ptr(seed), ptr(state), ptr(transport), ptr(success), None, 0,
-                                                     stream, err, len(err))
+                                                     ptr(seed), ptr(state), ptr(transport), ptr(success), None,
+                                                     2 if per_cell else 0, stream, err, len(err))
         if rc:
             raise HemError(err.value.decode())
 

@@ -75,6 +75,30 @@ def test_cuda_flash_prune_policy():
     assert s["p_rel"] <= F.P_T_TOL and s["T_rel"] <= F.P_T_TOL, s
 
 
+@pytest.mark.parametrize("prune", [0, 1])
+def test_cuda_flash_per_cell_form_matches_queue_form(prune):
+    """The plain one-thread-per-cell form and the work-queue form give bitwise
+    identical states (same solvers, same candidate order)."""
+    import torch
+    from spuma_multiphysics_b200 import thermo_data as td
+    n = 3000
+    q, e, guess = cases.flash_batch(n, seed=777 + prune)
+    hem = GpuHem(model=td.pure_model(stable_gas_prune=prune), capacity=n)
+    cons = torch.zeros((5, n), dtype=torch.float64, device="cuda")
+    cons[0] = torch.from_numpy(q).cuda()
+    cons[4] = torch.from_numpy(e).cuda()
+    seed = torch.from_numpy(guess.view(np.uint8).copy()).cuda()
+    outs = []
+    for per_cell in (False, True):
+        state = torch.zeros_like(seed)
+        ok = torch.zeros(n, dtype=torch.int32, device="cuda")
+        hem.run_device(cons, n, n, 5, seed, state, None, ok, torch.cuda.current_stream().cuda_stream, per_cell)
+        torch.cuda.synchronize()
+        outs.append((state.cpu().numpy(), ok.cpu().numpy()))
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][0], outs[1][0])
+
+
 def test_cuda_flash_device_resident_matches_host_path():
     import torch
     n = 5000
