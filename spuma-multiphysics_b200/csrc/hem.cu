@@ -3,10 +3,11 @@
 // Launch sequence per batch (all on one stream, no host synchronisation, no
 // allocation; capturable in a CUDA graph):
 //   1 inputs     per cell: (rho, e, seed p/T/liquid mass)
-//   2 pass A     persistent work queue over (cell, {all-gas, all-liquid})
-//   3 compact    cells that still need the two-phase seeds (all cells unless
-//                the model's stableGasPrune option skips them after a stable gas)
-//   4 pass B     persistent work queue over (listed cell, 5 beta seeds)
+//   2 queue      persistent lane-level work queue over (candidate, cell) items:
+//                all seven candidates of every cell; with the model's
+//                stableGasPrune option, the all-gas/all-liquid items first, then
+//   3 compact    the cells the all-gas candidate does not decide, and
+//   4 queue      their five two-phase seeds
 //   5 select     first maximum entropy among stable candidates, in reference
 //                order; cells without one are queued for the restart search
 //   6 pass C     persistent queue over (queued cell, 4 restart temperatures),
@@ -15,6 +16,7 @@
 // Candidate records live in HBM (192 B each); every loop in the solvers is
 // bounded and no thread waits on another, so every launch terminates.
 #include "hem_flash.cuh"
+#include "hem_queue.cuh"
 #include "common.cuh"
 #include "../../include/reactive_b200_hem.h"
 
@@ -98,28 +100,73 @@ __device__ inline void finishCandidate(const HemConst& C, const CellInput& in, b
     rec->status = status;
 }
 
-// Pass A: items (kind in {gas, liquid}) x cells, kind-major so a warp runs one
-// candidate kind over consecutive cells.
-__global__ void __launch_bounds__(kPassThreads) passPartitions(const HemConst* __restrict__ Cp,
-                                                               const CellInput* __restrict__ in, size_t count,
-                                                               CandRecord* rec, unsigned* counters,
-                                                               unsigned long long* totals) {
+struct MainRecords {
+    CandRecord* rec;
+    size_t count;
+    __device__ CandRecord& at(const QueueLane& L) const { return rec[size_t(L.kind) * count + L.cell]; }
+    __device__ void state(const QueueLane& L, const Eval& v) const {
+        CandRecord& r = at(L);
+        stateFromEval(v, L.x.q, L.o, r.st);
+        r.entropyD = v.entropyD;
+    }
+    __device__ void status(const QueueLane& L, int code) const { at(L).status = code; }
+};
+
+// Persistent lane-level queue over items (kind, cell): kinds [kindBase,
+// kindBase+kinds), cells 0..count-1 or list[0..counters[LIST]) when list != null.
+// Items are kind-major, so consecutive items share a candidate kind.
+__global__ void __launch_bounds__(kPassThreads) passQueue(const HemConst* __restrict__ Cp,
+                                                          const CellInput* __restrict__ in, size_t count,
+                                                          const unsigned* __restrict__ list, int kindBase, int kinds,
+                                                          CandRecord* rec, unsigned* counters, int queueSlot,
+                                                          unsigned long long* totals) {
     const HemConst& C = *Cp;
     Counts n;
-    const unsigned total = unsigned(2 * count);
+    const unsigned cells = list ? counters[LIST] : unsigned(count);
+    const unsigned total = unsigned(kinds) * cells;
+    const MainRecords records{rec, count};
+    const int stallLimitGas = C.stableGasPrune ? 4 : 0;
+    const unsigned lane = threadIdx.x & 31u;
+    QueueLane L;
+    L.st = Q_FREE;
+    L.req = REQ_NONE;
+    Eval v;
+    bool pending = false, exhausted = cells == 0;
     for (;;) {
-        const unsigned base = fetchItems(counters + Q_A);
-        if (base >= total) break;
-        const unsigned item = base + (threadIdx.x & 31);
-        if (item < total) {
-            const unsigned kind = item / unsigned(count), c = item % unsigned(count);
-            const CellInput x = in[c];
-            Eval v;
-            CandidateOut o{};
-            bool ok;
-            if (kind == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n);
-            else ok = x.q * (1 + 1e-12) >= C.liquidFloor && frozenSolve(C, x, x.q, 0, v, o, n);
-            finishCandidate(C, x, ok, v, o, rec + size_t(kind) * count + c, n);
+        for (int round = 0; round < 2; ++round) {
+            const bool need = L.st == Q_FREE && !exhausted;
+            const unsigned mask = __ballot_sync(0xffffffffu, need);
+            if (mask) {
+                unsigned base = 0;
+                if (lane == unsigned(__ffs(mask) - 1)) base = atomicAdd(counters + queueSlot, unsigned(__popc(mask)));
+                base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+                if (need) {
+                    const unsigned item = base + __popc(mask & ((1u << lane) - 1));
+                    if (item < total) {
+                        const unsigned kind = unsigned(kindBase) + item / cells, slot = item % cells;
+                        L.kind = int(kind);
+                        L.cell = list ? list[slot] : slot;
+                        L.x = in[L.cell];
+                        L.o = CandidateOut{};
+                        L.mass = kind == 1 ? L.x.q : 0.0;
+                        L.st = kind >= 2 ? Q_TP_START : Q_FZ_START;
+                        L.req = REQ_NONE;
+                    } else exhausted = true;
+                }
+            }
+            if (L.st != Q_FREE && !pending) pending = plan(C, L, v, records, n, stallLimitGas);
+        }
+        const bool any = __any_sync(0xffffffffu, pending);
+        if (!any) {
+            if (__all_sync(0xffffffffu, L.st == Q_FREE && exhausted)) break;
+            continue;
+        }
+        if (pending) {
+            if (L.req == REQ_POINT) L.ok = evaluate(C, L.x.q, L.rm, L.rp, L.rT, L.rv, v, n);
+            else if (L.req == REQ_PROBE) L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, n);
+            else L.ok = tangentStable(C, L.rp, L.rT, n);
+            L.req = REQ_NONE;
+            pending = false;
         }
     }
     flushCounts(n, totals);
@@ -141,31 +188,6 @@ __global__ void compactSeedCells(const HemConst* __restrict__ Cp, const CandReco
         slot = __shfl_sync(0xffffffffu, slot, 0);
         if (need) list[slot + __popc(mask & ((1u << (threadIdx.x & 31)) - 1))] = unsigned(c);
     }
-}
-
-// Pass B: items (seed) x listed cells, seed-major.
-__global__ void __launch_bounds__(kPassThreads) passSeeds(const HemConst* __restrict__ Cp,
-                                                          const CellInput* __restrict__ in, size_t count,
-                                                          const unsigned* __restrict__ list, CandRecord* rec,
-                                                          unsigned* counters, unsigned long long* totals) {
-    const HemConst& C = *Cp;
-    Counts n;
-    const unsigned listed = counters[LIST];
-    const unsigned total = 5u * listed;
-    for (;;) {
-        const unsigned base = fetchItems(counters + Q_B);
-        if (base >= total) break;
-        const unsigned item = base + (threadIdx.x & 31);
-        if (item < total) {
-            const unsigned seed = item / listed, c = list[item % listed];
-            const CellInput x = in[c];
-            Eval v;
-            CandidateOut o{};
-            const bool ok = twoPhaseSolve(C, x, kSeeds[seed], -1.0, v, o, n);
-            finishCandidate(C, x, ok, v, o, rec + size_t(2 + seed) * count + c, n);
-        }
-    }
-    flushCounts(n, totals);
 }
 
 __device__ inline void writeOutputs(const ReactiveThermoState& s, size_t c, ReactiveThermoState* state,
@@ -394,12 +416,18 @@ struct HemDevice {
     void launchSearch(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
                       ReactiveTransportState* transport, int* success, cudaStream_t s) {
         check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "memset counters");
-        passPartitions<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, rec, counters, totals);
-        check(cudaGetLastError(), "passPartitions");
-        compactSeedCells<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, list, counters);
-        check(cudaGetLastError(), "compactSeedCells");
-        passSeeds<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, rec, counters, totals);
-        check(cudaGetLastError(), "passSeeds");
+        if (hostConst.stableGasPrune) {
+            // all-gas and all-liquid first; the seeds only for cells the gas does not decide
+            passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 2, rec, counters, Q_A, totals);
+            check(cudaGetLastError(), "passQueue");
+            compactSeedCells<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, list, counters);
+            check(cudaGetLastError(), "compactSeedCells");
+            passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, 2, 5, rec, counters, Q_B, totals);
+            check(cudaGetLastError(), "passQueue");
+        } else {
+            passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 7, rec, counters, Q_A, totals);
+            check(cudaGetLastError(), "passQueue");
+        }
         selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, state, transport, success, fallback,
                                                              counters);
         check(cudaGetLastError(), "selectCandidates");
@@ -437,7 +465,7 @@ void* create(const void* raw, size_t bytes, size_t capacity, bool hostPath, char
         check(cudaMemcpyAsync(d->cst, &d->hostConst, sizeof(HemConst), cudaMemcpyHostToDevice, d->stream), "H2D");
         check(cudaMemsetAsync(d->totals, 0, NTOTALS * sizeof(unsigned long long), d->stream), "memset");
         int perSm = 0, sms = 0;
-        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, passSeeds, kPassThreads, 0), "occupancy");
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, passQueue, kPassThreads, 0), "occupancy");
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "attribute");
         d->passBlocks = std::max(1, perSm) * std::max(1, sms);
         if (hostPath) d->ensureHostPath();
