@@ -63,6 +63,20 @@ int reactive_gpu_hem_run_device_v3(void* hem, const double* conserved, size_t st
 int reactive_gpu_hem_run_counters_v3(void* hem, ReactiveGpuHemProfileV1* profile, void* stream, char* error,
     size_t errorSize);
 
+/* Flash without any allocation. No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc when they need a flash, for example a solver
+ * whose own memory pool owns the whole device and forbids other allocations. It
+ * takes the model image and DEVICE
+ * arrays like reactive_gpu_hem_run_device_v3 but needs no handle: its scratch is
+ * one file-scope device array (about 9 MB, held by every GPU that loads this
+ * library until the process exits) for at most 4,096 cells per call; larger
+ * batches are rejected with an error. The first call on each device looks up the
+ * array's address and should come before any stream capture. Calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
+int reactive_gpu_hem_run_static_v3(const void* model, size_t modelBytes, const double* conserved, size_t stride,
+    size_t count, size_t variables, const ReactiveThermoState* seed, ReactiveThermoState* state,
+    ReactiveTransportState* transport, int* success, void* stream, char* error, size_t errorSize);
+
 #ifdef __cplusplus
 }
 #endif

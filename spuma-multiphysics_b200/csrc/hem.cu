@@ -805,3 +805,121 @@ int reactive_gpu_hem_run_counters_v3(void* raw, ReactiveGpuHemProfileV1* profile
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Flash without any allocation, for callers that cannot call cudaMalloc.
+//
+// Some callers of the HEM cannot allocate device memory when they need a flash:
+// a solver that owns the whole device through its own memory pool and forbids
+// other allocations. For them this entry point runs the
+// same work-queue flash as reactive_gpu_hem_run_device_v3 with no handle: its
+// scratch (the derived model constants, per-cell inputs, candidate records,
+// lists and queue counters) lives in one file-scope __device__ array sized for
+// at most kStaticHemCells cells (about 9 MB). Every GPU that loads this library
+// holds that array until the process exits.
+//
+// The array's device address is looked up with cudaGetSymbolAddress once per
+// device, on the first call made with that device current; make that first call
+// before capturing any stream. Every call uses the same array and finds the
+// previous call's contents there; the queue counters and work totals are cleared
+// at the start of each call. Calls that overlap on the GPU (two streams, two
+// host threads) race on the array: serialise them.
+namespace rb200 {
+namespace {
+constexpr size_t kStaticHemCells = 4096;
+constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kStaticConst = 0;
+constexpr size_t kStaticIn = align256(kStaticConst + sizeof(HemConst));
+constexpr size_t kStaticRec = align256(kStaticIn + kStaticHemCells * sizeof(CellInput));
+constexpr size_t kStaticFb = align256(kStaticRec + 7 * kStaticHemCells * sizeof(CandRecord));
+constexpr size_t kStaticList = align256(kStaticFb + 4 * kStaticHemCells * sizeof(CandRecord));
+constexpr size_t kStaticFallback = align256(kStaticList + kStaticHemCells * sizeof(unsigned));
+constexpr size_t kStaticCounters = align256(kStaticFallback + kStaticHemCells * sizeof(unsigned));
+constexpr size_t kStaticTotals = align256(kStaticCounters + NCOUNTERS * sizeof(unsigned));
+constexpr size_t kStaticBytes = align256(kStaticTotals + NTOTALS * sizeof(unsigned long long));
+
+static __device__ __align__(256) unsigned char staticHemScratch[kStaticBytes];
+
+std::mutex staticHemMutex;
+void* staticHemAddress[64] = {};
+
+// Device address of the scratch array for the current device (looked up once).
+unsigned char* staticScratch() {
+    int device = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    require(device >= 0 && device < 64, "Device ordinal out of range for the static HEM scratch");
+    std::lock_guard<std::mutex> lock(staticHemMutex);
+    if (!staticHemAddress[device]) {
+        void* ptr = nullptr;
+        check(cudaGetSymbolAddress(&ptr, staticHemScratch), "cudaGetSymbolAddress(static HEM scratch)");
+        require(ptr != nullptr, "Static HEM scratch has no device address");
+        staticHemAddress[device] = ptr;
+    }
+    return static_cast<unsigned char*>(staticHemAddress[device]);
+}
+
+__global__ void storeConstants(HemConst c, HemConst* dst) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dst = c;
+}
+}  // namespace
+}  // namespace rb200
+
+extern "C" int reactive_gpu_hem_run_static_v3(const void* model, size_t modelBytes, const double* conserved,
+                                              size_t stride, size_t count, size_t variables,
+                                              const ReactiveThermoState* seed, ReactiveThermoState* state,
+                                              ReactiveTransportState* transport, int* success, void* stream,
+                                              char* error, size_t size) {
+    using namespace rb200;
+    try {
+        require(model && modelBytes == sizeof(ReactiveB200HemModel), "Invalid HEM model image");
+        require(conserved && seed && (state || transport) && count && stride >= count && variables >= 5,
+                "Invalid static HEM batch arguments");
+        if (count > kStaticHemCells)
+            throw std::runtime_error("Static HEM batch of " + std::to_string(count) + " cells exceeds the maximum of "
+                                     + std::to_string(kStaticHemCells) + "; split the batch or use a handle");
+        ReactiveB200HemModel m;
+        std::memcpy(&m, model, sizeof(m));
+        HemConst hostConst{};
+        const std::string why = validateAndDerive(m, hostConst);
+        require(why.empty(), why.c_str());
+        unsigned char* base = staticScratch();
+        auto* cst = reinterpret_cast<HemConst*>(base + kStaticConst);
+        auto* in = reinterpret_cast<CellInput*>(base + kStaticIn);
+        auto* rec = reinterpret_cast<CandRecord*>(base + kStaticRec);
+        auto* fb = reinterpret_cast<CandRecord*>(base + kStaticFb);
+        auto* list = reinterpret_cast<unsigned*>(base + kStaticList);
+        auto* fallback = reinterpret_cast<unsigned*>(base + kStaticFallback);
+        auto* counters = reinterpret_cast<unsigned*>(base + kStaticCounters);
+        auto* totals = reinterpret_cast<unsigned long long*>(base + kStaticTotals);
+        auto s = static_cast<cudaStream_t>(stream);
+        int perSm = 0, sms = 0, device = 0;
+        check(cudaGetDevice(&device), "cudaGetDevice");
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, passQueue, kPassThreads, 0), "occupancy");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attribute");
+        const int blocks = std::max(1, perSm) * std::max(1, sms);
+        storeConstants<<<1, 1, 0, s>>>(hostConst, cst);
+        check(cudaGetLastError(), "storeConstants");
+        check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "clear counters");
+        check(cudaMemsetAsync(totals, 0, NTOTALS * sizeof(unsigned long long), s), "clear totals");
+        inputsFromConserved<<<gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1, seed, in);
+        check(cudaGetLastError(), "inputs");
+        if (hostConst.stableGasPrune) {
+            passQueue<<<blocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 2, rec, counters, Q_A, totals);
+            compactSeedCells<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, list, counters);
+            passQueue<<<blocks, kPassThreads, 0, s>>>(cst, in, count, list, 2, 5, rec, counters, Q_B, totals);
+        } else {
+            passQueue<<<blocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 7, rec, counters, Q_A, totals);
+        }
+        check(cudaGetLastError(), "passQueue");
+        selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, state, transport, success, fallback,
+                                                             counters);
+        passRestarts<<<blocks, kPassThreads, 0, s>>>(cst, in, fallback, fb, kStaticHemCells, counters, totals);
+        selectRestarts<<<gridFor(count, 256), 256, 0, s>>>(fb, kStaticHemCells, fallback, seed, state, transport,
+                                                           success, counters);
+        check(cudaGetLastError(), "select");
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
