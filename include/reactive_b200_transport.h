@@ -121,6 +121,17 @@ int reactive_transport_stage_device_v3(void* transport, const double* qIn, doubl
 /* Writes the CFL step (or -1 when any face is invalid) to dt[0] on the device. */
 int reactive_transport_stable_step_device_v3(void* transport, const double* q,
     const ReactiveTransportState* state, double cfl, double maximum, double* dt, void* stream);
+/* Structured Cartesian fast path of the device-resident entries (no reference
+ * counterpart: the reference's Cartesian descriptor,
+ * reactive_transport_install_cartesian_v1 in
+ * src/reactiveTransport/reactiveCartesianTransport.h:34, serves its capillary
+ * geometry, not the flux). At create the face list is checked for a uniform box in the
+ * canonical ordering; when it is one, stage_device_v3 and
+ * stable_step_device_v3 use cell-stencil kernels that read no face-work array
+ * and give bitwise the same stage results as the face graph. request -1 only
+ * queries, 0 selects the face graph, 1 the structured path (an error when the
+ * face list is not such a box); *active (may be NULL) receives the selection. */
+int reactive_transport_structured_v3(void* transport, int request, int* active);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);

@@ -64,23 +64,27 @@ def phase_label(states):
     return np.where(gas & liq, 2, np.where(liq, 1, 0)).astype(np.int8)
 
 
-def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset=0.006, boundary_kind=2):
-    """Face array (numpy FACE_DTYPE) and cell volumes of an n^3 cube.
+def box_faces(dims, h, side_kinds=(2, 2, 2, 2, 2, 2)):
+    """Face array (numpy FACE_DTYPE) and cell volumes of a uniform nx x ny x nz
+    box of cubic cells of edge h, in the mesh tool's canonical ordering
+    (tools/impinging_cartesian_mesh.py:54-127): cells x-fastest; internal faces
+    sorted by (owner, neighbour) with the lower cell as owner and normal +e_axis;
+    then the boundary faces side by side (-x, +x, -y, +y, -z, +z), each side in
+    lateral order (fast, slow) = (y, z), (x, z), (x, y).
 
-    Port faces on x=0 (centre y=port_offset, z=port_z) and y=0 (centre
-    x=port_offset, z=port_z) are fixed-state faces (fixed index 0); every other
-    boundary face has kind `boundary_kind` (2 extrapolate: transmissive).
-    """
-    h = edge / n
+    side_kinds[s] is one boundary kind for the whole side or an array of kinds
+    in that side's lateral order (1 slip wall, 2 extrapolate, 3 fixed state with
+    fixed index 0). Boundary ownerWeight: 0 fixed state, 1 extrapolate, .5 slip;
+    distance h/2."""
+    nx, ny, nz = dims
     area, volume = h * h, h ** 3
-    cell = lambda i, j, k: i + n * (j + n * k)
+    cell = lambda i, j, k: i + nx * (j + ny * k)
     internal = []
-    # owner, neighbour for x, y, z faces
-    k, j, i = np.indices((n, n, n - 1))
+    k, j, i = np.indices((nz, ny, nx - 1))
     internal.append((cell(i, j, k).ravel(), cell(i + 1, j, k).ravel(), 0))
-    k, j, i = np.indices((n, n - 1, n))
+    k, j, i = np.indices((nz, ny - 1, nx))
     internal.append((cell(i, j, k).ravel(), cell(i, j + 1, k).ravel(), 1))
-    k, j, i = np.indices((n - 1, n, n))
+    k, j, i = np.indices((nz - 1, ny, nx))
     internal.append((cell(i, j, k).ravel(), cell(i, j, k + 1).ravel(), 2))
     owners = np.concatenate([a[0] for a in internal])
     neighbours = np.concatenate([a[1] for a in internal])
@@ -88,28 +92,19 @@ def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset
     order = np.lexsort((neighbours, owners))
     owners, neighbours, axes = owners[order], neighbours[order], axes[order]
     nint = owners.size
-    r2 = (port_diameter / 2) ** 2
-    bnd = []  # (owner, axis, sign, kind)
-    for axis in range(3):
-        for upper in (False, True):
-            a, b = np.indices((n, n))  # the two lateral indices (slow, fast)
-            coords = [None, None, None]
-            lat = [d for d in range(3) if d != axis]
-            coords[lat[1]], coords[lat[0]] = a.ravel(), b.ravel()
-            coords[axis] = np.full(n * n, n - 1 if upper else 0)
-            owner = cell(*coords)
-            kind = np.full(n * n, boundary_kind)
-            if not upper and axis < 2:
-                lateral = 1 - axis
-                xc = (coords[lateral] + .5) * h
-                zc = (coords[2] + .5) * h
-                port = (xc - port_offset) ** 2 + (zc - port_z) ** 2 < r2
-                kind[port] = 3
-            bnd.append((owner, np.full(n * n, axis), np.full(n * n, 1.0 if upper else -1.0), kind))
-    b_owner = np.concatenate([x[0] for x in bnd])
-    b_axis = np.concatenate([x[1] for x in bnd])
-    b_sign = np.concatenate([x[2] for x in bnd])
-    b_kind = np.concatenate([x[3] for x in bnd])
+    b_owner, b_axis, b_sign, b_kind = [], [], [], []
+    for side in range(6):
+        axis, upper = side >> 1, bool(side & 1)
+        lat = [d for d in range(3) if d != axis]
+        slow, fast = np.indices((dims[lat[1]], dims[lat[0]]))
+        coords = [None, None, None]
+        coords[lat[0]], coords[lat[1]] = fast.ravel(), slow.ravel()
+        coords[axis] = np.full(fast.size, dims[axis] - 1 if upper else 0)
+        b_owner.append(cell(*coords))
+        b_axis.append(np.full(fast.size, axis))
+        b_sign.append(np.full(fast.size, 1.0 if upper else -1.0))
+        b_kind.append(np.broadcast_to(np.asarray(side_kinds[side]), (fast.size,)))
+    b_owner, b_axis, b_sign, b_kind = (np.concatenate(x) for x in (b_owner, b_axis, b_sign, b_kind))
     faces = np.zeros(nint + b_owner.size, dtype=A.FACE_DTYPE)
     faces["owner"][:nint] = owners
     faces["neighbour"][:nint] = neighbours
@@ -130,7 +125,32 @@ def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset
     faces["distance"][sl] = h / 2
     faces["ownerWeight"][sl] = np.where(b_kind == 3, 0.0, np.where(b_kind == 2, 1.0, 0.5))
     faces["kind"][sl] = b_kind
-    return faces, np.full(n ** 3, volume)
+    return faces, np.full(nx * ny * nz, volume)
+
+
+def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset=0.006, boundary_kind=2):
+    """Face array (numpy FACE_DTYPE) and cell volumes of an n^3 cube of edge
+    `edge` (box_faces ordering).
+
+    Port faces on x=0 (centre y=port_offset, z=port_z) and y=0 (centre
+    x=port_offset, z=port_z) are fixed-state faces (fixed index 0); every other
+    boundary face has kind `boundary_kind` (2 extrapolate: transmissive). A face
+    belongs to a port when its centre lies inside the port circle
+    (tools/impinging_cartesian_mesh.py:12-36,89-99).
+    """
+    h = edge / n
+    r2 = (port_diameter / 2) ** 2
+    kinds = []
+    for side in range(6):
+        axis, upper = side >> 1, bool(side & 1)
+        kind = np.full(n * n, boundary_kind)
+        if not upper and axis < 2:
+            slow, fast = np.indices((n, n))   # z slow; the lateral axis (y on x=0, x on y=0) fast
+            lateral_c = (fast.ravel() + .5) * h
+            zc = (slow.ravel() + .5) * h
+            kind[(lateral_c - port_offset) ** 2 + (zc - port_z) ** 2 < r2] = 3
+        kinds.append(kind)
+    return box_faces((n, n, n), h, kinds)
 
 
 def impingement(n, fluid=None, seed=1234, ambient_p=40e5, ambient_T=293.15, inlet_p=56.01325e5, inlet_T=293.15,

@@ -1,0 +1,460 @@
+// Structured fast path of the transport for a uniform Cartesian box.
+//
+// When the face list is a uniform nx x ny x nz box in natural cell order
+// (c = i + nx (j + ny k); internal faces (c, c+1), (c, c+nx), (c, c+nx ny) with
+// normals +x, +y, +z; boundary faces on the six box sides), the operator is
+// evaluated by cell stencils instead of a face graph: no face-work array and no
+// CSR incidence are read. One kernel forms the Green-Gauss velocity gradient and
+// the WALE viscosity of a cell from its six neighbours; a second computes the six
+// face fluxes of a cell (HLL, viscous/WALE traction, conduction), sums them and
+// applies the SSPRK2 update, so the flux of an internal face is computed by both
+// of its cells instead of being stored and re-read. Boundary sides keep their own
+// face records (kind, fixed index, weight, distance, area); in the canonical
+// ordering the boundary faces of each box side form one contiguous block.
+//
+// The face physics is that of transport_kernels.cuh
+// (src/reactiveTransport/reactiveTransportKernels.h:290-560). With an
+// axis-aligned unit normal every projection reduces to one component; the
+// terms a face graph multiplies by a zero normal component are still formed
+// and added here (they are signed zeros for finite data), and a cell's faces are
+// summed in its face-graph incidence order, so for finite data both paths give
+// bitwise identical stage results.
+#pragma once
+#include "transport_kernels.cuh"
+
+namespace rb200 {
+
+constexpr int kCartMaxNs = 4;
+
+struct CartView {
+    int nx, ny, nz;
+    size_t cells, fixed, all;
+    double area[3], dist[3];      // internal faces per axis (ownerWeight 0.5)
+    const double* invV;
+    const ReactiveTransportFace* face;
+    size_t sideBase[6];           // -x,+x,-y,+y,-z,+z: first face of the side block
+    size_t boundaryBase, nBoundary;
+    const ReactiveTransportPrimitive* primitive;  // cells + fixed (velocities, as the face-graph kernels use)
+    double viscosity, conductivity, waveFactor;
+    bool wale;
+    double cw;
+};
+
+struct CellData {
+    double q[kCartMaxNs + 4];
+    double u[3];
+    double p, T, rho, cv, c;
+};
+
+template <int NS>
+__device__ __forceinline__ void loadCell(const CartView& v, const double* __restrict__ q,
+                                         const ReactiveTransportState* __restrict__ st, size_t c, CellData& d,
+                                         bool needQ) {
+    if (needQ) {
+#pragma unroll
+        for (int k = 0; k < NS + 4; ++k) d.q[k] = q[size_t(k) * v.all + c];
+    }
+    const ReactiveTransportPrimitive pr = v.primitive[c];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) d.u[a] = pr.u[a];
+    const ReactiveTransportState s = st[c];
+    d.p = s.p; d.T = s.T; d.rho = s.rho; d.cv = s.cv; d.c = s.sound;
+}
+
+// Right state of a boundary face of kind 1 (slip: velocity and momentum
+// mirrored), 2 (extrapolate: owner), 3 (fixed state).
+template <int NS>
+__device__ __forceinline__ void boundaryRight(const CartView& v, const double* __restrict__ q,
+                                              const ReactiveTransportState* __restrict__ st,
+                                              const ReactiveTransportFace& f, int axis, const CellData& L,
+                                              CellData& R, bool needQ) {
+    if (f.kind == 3) {
+        loadCell<NS>(v, q, st, v.cells + size_t(f.fixed), R, needQ);
+        return;
+    }
+    R = L;
+    if (f.kind == 1) {
+        // u - 2 (u.n) n with n = +-e_axis: the component along the axis changes sign
+        R.u[axis] = L.u[axis] - 2 * L.u[axis];
+        if (needQ) R.q[NS + axis] = L.q[NS + axis] - 2 * L.q[NS + axis];
+    }
+}
+
+// Unit normal component d of a face with normal sgn*e_axis.
+__device__ __forceinline__ double nrm(int d, int axis, double sgn) { return d == axis ? sgn : 0.0; }
+
+// Flux of all variables through a face with unit normal sgn*e_axis, times the
+// area, seen from the owner (left) side (faceWork + faceFluxK of the face graph).
+// gL/gR: gradients (9 components; gR only used for internal faces); nutL/nutR
+// the WALE viscosities of the owner and right sides.
+template <int NS>
+__device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double sgn, double area, double dist,
+                                             double w, int kind, bool internal, const CellData& L, const CellData& R,
+                                             const double* gL, const double* gR, double nutL, double nutR,
+                                             double* F, bool& bad) {
+    const double unL = L.u[axis] * sgn, unR = R.u[axis] * sgn;
+    const double aL = v.waveFactor * L.c, aR = v.waveFactor * R.c;
+    const double left = dmin(0, dmin(unL - aL, unR - aR)), right = dmax(0, dmax(unL + aL, unR + aR));
+    const double inv = 1 / (right - left);
+    const double advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
+    const double pM = (right * L.p - left * R.p) * inv, pE = (right * L.p * unL - left * R.p * unR) * inv;
+    double traction[3] = {0, 0, 0}, energy = 0;
+    if (v.viscosity > 0 || v.wale) {
+        double g[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) g[j] = internal ? w * gL[j] + (1 - w) * gR[j] : gL[j];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double normal = 0;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) normal += g[i * 3 + d] * nrm(d, axis, sgn);
+            const double target = (R.u[i] - L.u[i]) / ((kind == 1 ? 2 : 1) * dist);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) g[i * 3 + d] += nrm(d, axis, sgn) * (target - normal);
+        }
+        const double div = g[0] + g[4] + g[8];
+        const double mu = v.viscosity + (v.wale ? w * L.rho * nutL + (1 - w) * R.rho * nutR : 0);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                traction[i] += mu * (g[3 * i + d] + g[3 * d + i] - (i == d ? 2 * div / 3 : 0)) * nrm(d, axis, sgn);
+        if (kind == 1) {
+            double dot = 0;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) dot += traction[d] * nrm(d, axis, sgn);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) traction[d] = dot * nrm(d, axis, sgn);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * L.u[d] + (1 - w) * R.u[d]);
+    }
+    if (v.conductivity > 0 && kind != 1) energy -= v.conductivity * (R.T - L.T) / dist;
+    if (v.wale) {
+        bad |= !isfinite(energy);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) bad |= !isfinite(traction[d]);
+    }
+#pragma unroll
+    for (int k = 0; k < NS + 4; ++k) {
+        double flux = advL * L.q[k] + advR * R.q[k];
+        if (k >= NS && k < NS + 3) flux += pM * nrm(k - NS, axis, sgn);
+        if (k == NS + 3) flux += pE;
+        if (k >= NS && k < NS + 3) flux -= traction[k - NS];
+        else if (k == NS + 3) flux += energy;
+        F[k] = flux * area;
+    }
+}
+
+__device__ __forceinline__ void cellCoords(const CartView& v, size_t c, int& i, int& j, int& k) {
+    i = int(c % size_t(v.nx));
+    const size_t r = c / size_t(v.nx);
+    j = int(r % size_t(v.ny));
+    k = int(r / size_t(v.ny));
+}
+
+// Face record of box side s (-x,+x,-y,+y,-z,+z) at cell (i, j, k).
+__device__ __forceinline__ const ReactiveTransportFace& sideFace(const CartView& v, int s, int i, int j, int k) {
+    const size_t lateral = s < 2 ? size_t(j) + size_t(v.ny) * k
+                                 : (s < 4 ? size_t(i) + size_t(v.nx) * k : size_t(i) + size_t(v.nx) * j);
+    return v.face[v.sideBase[s] + lateral];
+}
+
+// The n-th side of a cell in its face-graph incidence order for the canonical
+// ordering: internal faces are sorted by (owner, neighbour), so a cell meets the
+// faces it neighbours (-z, -y, -x) before those it owns (+x, +y, +z); the
+// boundary faces follow in side-block order (-x, +x, -y, +y, -z, +z). n < 6
+// walks the internal sides, n >= 6 the boundary sides.
+__device__ __forceinline__ int sideOf(int n) {
+    constexpr int order[6] = {4, 2, 0, 1, 3, 5};
+    return n < 6 ? order[n] : n - 6;
+}
+
+__device__ __forceinline__ bool hasNeighbour(const CartView& v, int s, int i, int j, int k) {
+    const int coord = s < 2 ? i : (s < 4 ? j : k);
+    const int dim = s < 2 ? v.nx : (s < 4 ? v.ny : v.nz);
+    return (s & 1) ? coord + 1 < dim : coord > 0;
+}
+
+__device__ __forceinline__ size_t neighbourOf(const CartView& v, int s, size_t c) {
+    const size_t step = s < 2 ? 1 : (s < 4 ? size_t(v.nx) : size_t(v.nx) * v.ny);
+    return (s & 1) ? c + step : c - step;
+}
+
+// Green-Gauss gradient (and the WALE viscosity) of every cell.
+template <int NS>
+__global__ void __launch_bounds__(256) cartGradients(CartView v, const ReactiveTransportState* __restrict__ st,
+                                                     double* __restrict__ grad, double* __restrict__ nut,
+                                                     unsigned* error) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        CellData C;
+        loadCell<NS>(v, nullptr, st, c, C, false);
+        double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const double iv = v.invV[c];
+#pragma unroll
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            const int axis = s >> 1;
+            double uf[3], scale, sgn;
+            if (interior) {
+                // internal face: owner is the lower cell, normal +e_axis; this cell's
+                // incidence sign is +1 on its upper side (owner), -1 on its lower side
+                const ReactiveTransportPrimitive pn = v.primitive[neighbourOf(v, s, c)];
+                const bool owner = s & 1;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    uf[a] = owner ? .5 * C.u[a] + (1 - .5) * pn.u[a] : .5 * pn.u[a] + (1 - .5) * C.u[a];
+                scale = (owner ? 1.0 : -1.0) * v.area[axis] * iv;
+                sgn = 1;
+            } else {
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                CellData R;
+                boundaryRight<NS>(v, nullptr, st, f, axis, C, R, false);
+                const double w = f.ownerWeight;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) uf[a] = w * C.u[a] + (1 - w) * R.u[a];
+                scale = 1.0 * f.area * iv;
+                sgn = (s & 1) ? 1.0 : -1.0;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) g[3 * a + d] += uf[a] * nrm(d, axis, sgn) * scale;
+        }
+#pragma unroll
+        for (int jj = 0; jj < 9; ++jj) grad[size_t(jj) * v.cells + c] = g[jj];
+        if (v.wale) {
+            const double volume = 1 / iv;
+            double delta = 0, nu = 0;
+            bool ok = isfinite(volume) && volume > 0;
+            if (ok) { delta = cbrt(volume); ok = isfinite(delta) && delta > 0; }
+            ok = ok && waleEddyViscosity(g, delta, v.cw, nu);
+            if (!ok || !isfinite(nu) || nu < 0 || !isfinite(C.rho * nu)) atomicOr(error, 1u);
+            else nut[c] = nu;
+        }
+    }
+}
+
+// The flux of side s of cell c and this cell's incidence sign for it.
+template <int NS>
+__device__ __forceinline__ void sideFlux(const CartView& v, const double* __restrict__ q,
+                                         const ReactiveTransportState* __restrict__ st,
+                                         const double* __restrict__ grad, const double* __restrict__ nut, size_t c,
+                                         int s, bool interior, int i, int j, int k, const CellData& C,
+                                         const double* gC, double nutC, double* F, double& sign, bool& bad) {
+    const int axis = s >> 1;
+    const bool viscous = v.viscosity > 0 || v.wale;
+    if (interior) {
+        const size_t nb = neighbourOf(v, s, c);
+        CellData N;
+        loadCell<NS>(v, q, st, nb, N, true);
+        double gN[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (viscous) {
+#pragma unroll
+            for (int jj = 0; jj < 9; ++jj) gN[jj] = grad[size_t(jj) * v.cells + nb];
+        }
+        const double nutN = v.wale ? nut[nb] : 0;
+        if (s & 1) {  // this cell owns the face
+            faceFluxCart<NS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, C, N, gC, gN, nutC, nutN, F,
+                             bad);
+            sign = -1;
+        } else {
+            faceFluxCart<NS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, N, C, gN, gC, nutN, nutC, F,
+                             bad);
+            sign = 1;
+        }
+    } else {
+        const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+        CellData R;
+        boundaryRight<NS>(v, q, st, f, axis, C, R, true);
+        // a boundary face's right-side WALE viscosity is the owner's
+        faceFluxCart<NS>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false, C, R, gC,
+                         gC, nutC, nutC, F, bad);
+        sign = -1;
+    }
+}
+
+// Sum of the six face fluxes of every cell and the SSPRK2 update:
+// mode 0 rate -> out (stride outStride), 1 out = q + dt rate,
+// 2 out = .5 out + .5 (q + dt rate) (out holds q^n).
+template <int NS>
+__global__ void __launch_bounds__(128) cartRates(CartView v, const double* __restrict__ q,
+                                                 const ReactiveTransportState* __restrict__ st,
+                                                 const double* __restrict__ grad, const double* __restrict__ nut,
+                                                 double* out, size_t outStride, int mode, double dt,
+                                                 unsigned* error) {
+    const bool viscous = v.viscosity > 0 || v.wale;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        CellData C;
+        loadCell<NS>(v, q, st, c, C, true);
+        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (viscous) {
+#pragma unroll
+            for (int jj = 0; jj < 9; ++jj) gC[jj] = grad[size_t(jj) * v.cells + c];
+        }
+        const double nutC = v.wale ? nut[c] : 0;
+        const double iv = v.invV[c];
+        double rate[NS + 4];
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) rate[kk] = 0;
+        bool bad = false;
+#pragma unroll
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            double F[NS + 4], sign;
+            sideFlux<NS>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad);
+#pragma unroll
+            for (int kk = 0; kk < NS + 4; ++kk) rate[kk] += sign * F[kk] * iv;
+        }
+        if (bad) atomicOr(error, 1u);
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) {
+            const size_t o = size_t(kk) * outStride + c;
+            if (mode == 0) out[o] = rate[kk];
+            else if (mode == 1) out[o] = C.q[kk] + dt * rate[kk];
+            else out[o] = .5 * out[o] + .5 * (C.q[kk] + dt * rate[kk]);
+        }
+    }
+}
+
+// Wave/diffusion speed of one face (faceSpeeds of the face graph); -1 when invalid.
+__device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, double sgn, double dist, double w,
+                                                const CellData& L, const CellData& R, double nutL, double nutR) {
+    const double unL = L.u[axis] * sgn, unR = R.u[axis] * sgn;
+    const double aL = v.waveFactor * L.c, aR = v.waveFactor * R.c;
+    const double left = dmin(0, dmin(unL - aL, unR - aR)), right = dmax(0, dmax(unL + aL, unR + aR));
+    const double invWave = 1 / (right - left);
+    const double rhoNut = v.wale ? w * L.rho * nutL + (1 - w) * R.rho * nutR : 0;
+    const double mu = v.viscosity + rhoNut;
+    const double D = 0.0 + dmax(dmax(4 * mu / (3 * L.rho), 4 * mu / (3 * R.rho)),
+                                dmax(v.conductivity / (L.rho * L.cv), v.conductivity / (R.rho * R.cv)));
+    double speed = dmax(fabs(unL) + aL, fabs(unR) + aR) + 2 * D / dist;
+    if (!isfinite(unL) || !isfinite(unR) || !isfinite(speed) || !isfinite(invWave) || right <= left) speed = -1;
+    return speed;
+}
+
+// CFL step of every cell from its six face speeds (cellSteps), folded to one
+// partial minimum per block with invalid steps absorbing as -1 (minimumReduce).
+template <int NS>
+__global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTransportState* __restrict__ st,
+                                                 const double* __restrict__ nut, double cfl, double maximumStep,
+                                                 double* partial) {
+    __shared__ double warpValues[32];
+    double m = HUGE_VAL;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        CellData C;
+        loadCell<NS>(v, nullptr, st, c, C, false);
+        const double nutC = v.wale ? nut[c] : 0;
+        double denominator = 0;
+        bool bad = false;
+#pragma unroll
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            const int axis = s >> 1;
+            double speed, area;
+            if (interior) {
+                const size_t nb = neighbourOf(v, s, c);
+                CellData N;
+                loadCell<NS>(v, nullptr, st, nb, N, false);
+                const double nutN = v.wale ? nut[nb] : 0;
+                speed = (s & 1) ? faceSpeedCart(v, axis, 1.0, v.dist[axis], .5, C, N, nutC, nutN)
+                                : faceSpeedCart(v, axis, 1.0, v.dist[axis], .5, N, C, nutN, nutC);
+                area = v.area[axis];
+            } else {
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                CellData R;
+                boundaryRight<NS>(v, nullptr, st, f, axis, C, R, false);
+                speed = faceSpeedCart(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight, C, R, nutC, nutC);
+                area = f.area;
+            }
+            if (!isfinite(speed) || speed < 0) { bad = true; break; }
+            denominator += area * speed;
+        }
+        double step = denominator > 0 ? dmin(maximumStep, cfl / (v.invV[c] * denominator)) : maximumStep;
+        if (bad || !isfinite(denominator) || denominator < 0) step = -1;
+        m = fmin(m, isfinite(step) && step > 0 ? step : -1.0);
+    }
+    m = warpMin(m);
+    if ((threadIdx.x & 31) == 0) warpValues[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? warpValues[threadIdx.x] : HUGE_VAL;
+        m = warpMin(m);
+        if (threadIdx.x == 0) partial[blockIdx.x] = m;
+    }
+}
+
+// Boundary ledger: the sum over boundary faces of each variable's face flux.
+// Pass 1 (this kernel) writes one partial per (block, variable) in a fixed
+// partition, pass 2 (foldPartials) adds them in block order: deterministic.
+template <int NS>
+__global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __restrict__ q,
+                                                  const ReactiveTransportState* __restrict__ st,
+                                                  const double* __restrict__ grad, const double* __restrict__ nut,
+                                                  double* partial) {
+    __shared__ double warpValues[kCartMaxNs + 4][32];
+    double sum[NS + 4];
+#pragma unroll
+    for (int kk = 0; kk < NS + 4; ++kk) sum[kk] = 0;
+    const bool viscous = v.viscosity > 0 || v.wale;
+    bool bad = false;
+    for (size_t b = blockIdx.x * size_t(blockDim.x) + threadIdx.x; b < v.nBoundary;
+         b += size_t(blockDim.x) * gridDim.x) {
+        const ReactiveTransportFace f = v.face[v.boundaryBase + b];
+        const size_t c = size_t(f.owner);
+        const int axis = f.normal[0] != 0 ? 0 : (f.normal[1] != 0 ? 1 : 2);
+        const double sgn = f.normal[axis] > 0 ? 1.0 : -1.0;
+        CellData C, R;
+        loadCell<NS>(v, q, st, c, C, true);
+        boundaryRight<NS>(v, q, st, f, axis, C, R, true);
+        double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (viscous) {
+#pragma unroll
+            for (int jj = 0; jj < 9; ++jj) g[jj] = grad[size_t(jj) * v.cells + c];
+        }
+        const double nutC = v.wale ? nut[c] : 0;
+        double F[NS + 4];
+        faceFluxCart<NS>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, C, R, g, g, nutC, nutC, F,
+                         bad);
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) sum[kk] += F[kk];
+    }
+#pragma unroll
+    for (int kk = 0; kk < NS + 4; ++kk) {
+        const double s = warpSum(sum[kk]);
+        if ((threadIdx.x & 31) == 0) warpValues[kk][threadIdx.x >> 5] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) {
+            double s = threadIdx.x < (blockDim.x >> 5) ? warpValues[kk][threadIdx.x] : 0.0;
+            s = warpSum(s);
+            if (threadIdx.x == 0) partial[size_t(blockIdx.x) * (NS + 4) + kk] = s;
+        }
+    }
+}
+
+// out[k] = sum over blocks of partial[b*nv + k], one warp per variable, fixed order.
+__global__ void foldPartials(const double* __restrict__ partial, int blocks, int nv, double* out) {
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k >= nv) return;
+    double s = 0;
+    for (int b = lane; b < blocks; b += 32) s += partial[size_t(b) * nv + k];
+    s = warpSum(s);
+    if (lane == 0) out[k] = s;
+}
+
+}  // namespace rb200

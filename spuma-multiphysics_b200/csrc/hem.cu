@@ -43,7 +43,14 @@ static_assert(sizeof(CandRecord) == 192, "candidate record layout");
 enum Counter { Q_A = 0, Q_B, LIST, Q_C, FALLBACK, FAILED, NCOUNTERS = 8 };
 enum Total { T_PHASES = 0, T_RESIDUALS, T_CANDIDATES, T_STABLE, T_FAILURES, T_ANALYTIC, T_FD, NTOTALS = 8 };
 
+// Work-queue kernels: 128 threads, at least four blocks per SM (<= 128
+// registers a thread). With the EOS routines out of line, sixteen resident warps
+// per SM hide the latency of the FP64 chains better than eight warps at 255
+// registers, and spill nothing that matters.
 constexpr int kPassThreads = 128;
+#ifndef RB200_PASS_MINBLOCKS
+#define RB200_PASS_MINBLOCKS 4
+#endif
 __constant__ double kSeeds[5] = {-1, .5, .95, .1, .9999};
 __constant__ double kRestart[4] = {0.02, 0.25, 0.5, 0.75};
 
@@ -115,7 +122,7 @@ struct MainRecords {
 // Persistent lane-level queue over items (kind, cell): kinds [kindBase,
 // kindBase+kinds), cells 0..count-1 or list[0..counters[LIST]) when list != null.
 // Items are kind-major, so consecutive items share a candidate kind.
-__global__ void __launch_bounds__(kPassThreads) passQueue(const HemConst* __restrict__ Cp,
+__global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(const HemConst* __restrict__ Cp,
                                                           const CellInput* __restrict__ in, size_t count,
                                                           const unsigned* __restrict__ list, int kindBase, int kinds,
                                                           CandRecord* rec, unsigned* counters, int queueSlot,
@@ -225,7 +232,7 @@ __global__ void selectCandidates(const HemConst* __restrict__ Cp, const CandReco
 }
 
 // Pass C: restart temperatures x queued cells; each item runs the five seeds.
-__global__ void __launch_bounds__(kPassThreads) passRestarts(const HemConst* __restrict__ Cp,
+__global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passRestarts(const HemConst* __restrict__ Cp,
                                                              const CellInput* __restrict__ in,
                                                              const unsigned* __restrict__ fallback, CandRecord* fb,
                                                              size_t capacity, unsigned* counters,
@@ -297,7 +304,7 @@ __global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsi
 // One thread per cell running the whole search in order (the layout of the
 // reference's hemKernel, src/reactiveTransport/reactiveGpuHem.cuh:64-80): the
 // plain form the candidate-parallel passes are measured against. No pruning.
-__global__ void __launch_bounds__(kPassThreads) flashPerCell(const HemConst* __restrict__ Cp,
+__global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) flashPerCell(const HemConst* __restrict__ Cp,
                                                              const CellInput* __restrict__ in, size_t count,
                                                              const ReactiveThermoState* seed,
                                                              ReactiveThermoState* state,

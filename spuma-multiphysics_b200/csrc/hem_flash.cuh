@@ -23,6 +23,11 @@
 #include "pr_eos.cuh"
 #include "../../include/reactive_b200_types.h"
 
+// Linkage of the flash-level routines (see RB200_EOS_FN).
+#ifndef RB200_FLASH_FN
+#define RB200_FLASH_FN __noinline__
+#endif
+
 namespace rb200 {
 
 struct HemConst {
@@ -65,14 +70,14 @@ __device__ __forceinline__ bool inBounds(const HemConst& C, double p, double T) 
     return fin(p) && fin(T) && p >= C.pmin && p <= C.pmax && T >= C.Tmin && T <= C.Tmax;
 }
 
-__device__ inline int gasPhase(const HemConst& C, double p, double T, bool chem, PhaseProps& o, Counts& n) {
+__device__ RB200_FLASH_FN int gasPhase(const HemConst& C, double p, double T, bool chem, PhaseProps& o, Counts& n) {
     ++n.phases;
     if (!inBounds(C, p, T)) return EOS_INVALID_INPUT;
     if (C.enforceBounds && (T < C.gasTmin || T > C.gasTmax)) return EOS_INVALID_INPUT;
     return prTP(C.gas, T, p, ROOT_GAS, chem, o);
 }
 
-__device__ inline int liquidPhase(const HemConst& C, double p, double T, bool chem, PhaseProps& o, Counts& n) {
+__device__ RB200_FLASH_FN int liquidPhase(const HemConst& C, double p, double T, bool chem, PhaseProps& o, Counts& n) {
     ++n.phases;
     if (!inBounds(C, p, T)) return EOS_INVALID_INPUT;
     if (T < C.liquidTmin) return EOS_INVALID_INPUT;
@@ -117,7 +122,7 @@ __device__ __forceinline__ int liquidFromShared(const HemConst& C, int shared, c
 // are formed (two-phase residual and stability test). When both branches are
 // needed and the tables hold one species, the T-terms and the cubic are formed
 // once for both roots (the same arithmetic as two separate evaluations).
-__device__ inline bool evaluate(const HemConst& C, double q, double mass, double p, double T, bool virt, Eval& v,
+__device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass, double p, double T, bool virt, Eval& v,
                                 Counts& n) {
     v.p = p; v.T = T;
     v.volume = v.energy = v.entropyD = v.Vp = v.VT = v.Ep = v.ET = v.cpD = 0;
@@ -176,7 +181,7 @@ __device__ inline bool evaluate(const HemConst& C, double q, double mass, double
 __device__ __forceinline__ double energyScale(const Eval& v, double q) { return fmax(1e5 * q, v.cpD * v.T); }
 
 // Full-pivot elimination for n <= 3 with the rank test pivot > largest*n*eps.
-__device__ inline bool solveSmall(double a[3][3], double b[3], int n, double x[3]) {
+__device__ RB200_FLASH_FN bool solveSmall(double a[3][3], double b[3], int n, double x[3]) {
     int column[3] = {0, 1, 2};
     double largest = 0;
 #pragma unroll
@@ -241,7 +246,7 @@ __device__ inline bool solveSmall(double a[3][3], double b[3], int n, double x[3
 }
 
 // Energy residual of the all-gas state at (T, rho) and the gas-root check.
-__device__ inline bool gasProbe(const HemConst& C, double q, double eIn, double T, double& F, double& cv, double& p,
+__device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn, double T, double& F, double& cv, double& p,
                                 double& cp, Counts& n) {
     PhaseProps prop, gas;
     int phase;
@@ -261,7 +266,7 @@ struct CandidateOut {
     int iterations;
 };
 
-__device__ inline bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, Counts& n) {
+__device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, Counts& n) {
     const double q = in.q;
     double T = clampd(in.gT, C.Tmin, C.Tmax), F, cv, p, cp;
     if (!gasProbe(C, q, in.e, T, F, cv, p, cp, n)) return false;
@@ -314,7 +319,7 @@ __device__ inline bool scalarGas(const HemConst& C, const CellInput& in, Eval& v
 }
 
 // Newton on (ln p, ln T) with the liquid partition held fixed.
-__device__ inline bool frozenSolve(const HemConst& C, const CellInput& in, double mass, int stallLimit, Eval& v,
+__device__ RB200_FLASH_FN bool frozenSolve(const HemConst& C, const CellInput& in, double mass, int stallLimit, Eval& v,
                                    CandidateOut& o, Counts& n) {
     if (!fin(in.e)) return false;
     if (C.scalarRecovery && mass == 0 && scalarGas(C, in, v, o, n)) return true;
@@ -353,7 +358,7 @@ __device__ inline bool frozenSolve(const HemConst& C, const CellInput& in, doubl
     return false;
 }
 
-__device__ inline bool twoPhaseResidual(const HemConst& C, const CellInput& in, double lp, double lT, double beta,
+__device__ RB200_FLASH_FN bool twoPhaseResidual(const HemConst& C, const CellInput& in, double lp, double lT, double beta,
                                         double scale, double f[3], Eval& v, Counts& n) {
     ++n.residuals;
     if (!(beta >= 0 && beta < 1)) return false;
@@ -379,7 +384,7 @@ __device__ inline bool analyticJacobian(const Eval& v, double q, double W, doubl
     return true;
 }
 
-__device__ inline bool jacobian(const HemConst& C, const CellInput& in, const double x[3], double scale,
+__device__ RB200_FLASH_FN bool jacobian(const HemConst& C, const CellInput& in, const double x[3], double scale,
                                 const double f[3], const Eval& v, double J[3][3], Counts& n) {
     if (C.analyticJacobian && analyticJacobian(v, in.q, C.liq.W, scale, J)) { ++n.analytic; return true; }
     ++n.fd;
@@ -411,7 +416,7 @@ __device__ inline bool jacobian(const HemConst& C, const CellInput& in, const do
 
 // Two-phase Newton from a beta seed (seed < 0: the previous state's liquid
 // fraction clamped to [1e-8, 1-1e-8]); restartT >= 0 replaces the seed T.
-__device__ inline bool twoPhaseSolve(const HemConst& C, const CellInput& in, double seed, double restartT, Eval& v,
+__device__ RB200_FLASH_FN bool twoPhaseSolve(const HemConst& C, const CellInput& in, double seed, double restartT, Eval& v,
                                      CandidateOut& o, Counts& n) {
     ++n.candidates;
     const double q = in.q;
@@ -461,7 +466,7 @@ __device__ inline bool twoPhaseSolve(const HemConst& C, const CellInput& in, dou
 }
 
 // Stability of a converged candidate at (p, T) with liquid mass `mass`.
-__device__ inline bool stableAt(const HemConst& C, double q, double mass, double p, double T, Counts& n) {
+__device__ RB200_FLASH_FN bool stableAt(const HemConst& C, double q, double mass, double p, double T, Counts& n) {
     if (q - mass > 0) {
         Eval cmp;
         if (!evaluate(C, q, mass, p, T, true, cmp, n)) return false;

@@ -66,7 +66,7 @@ __device__ __forceinline__ void recordState(const Eval& v, const QueueLane& L, R
 
 // Stability of an all-liquid candidate at (p, T): the gas tangent plane at the
 // liquid's chemical potential (no gas branch counts as stable).
-__device__ inline bool tangentStable(const HemConst& C, double p, double T, Counts& n) {
+__device__ RB200_FLASH_FN bool tangentStable(const HemConst& C, double p, double T, Counts& n) {
     PhaseProps liq, gas;
     if (liquidPhase(C, p, T, true, liq, n) != EOS_OK) return false;
     const double muL = liq.mu / (kGas * T);

@@ -15,6 +15,14 @@
 #include <cuda_runtime.h>
 #include <cfloat>
 
+// Linkage of the large EOS routines. Out of line (one copy each in the binary)
+// keeps the instruction footprint of the flash kernels small: their warps run
+// different solver states side by side, and with every call site expanded the
+// code no longer fits the instruction cache.
+#ifndef RB200_EOS_FN
+#define RB200_EOS_FN __noinline__
+#endif
+
 namespace rb200 {
 
 constexpr double kGas = 8314.46261815324;  // J/(kmol K)
@@ -142,7 +150,7 @@ __device__ __forceinline__ double polishRoot(double x, double bn, double cn, dou
     return x;
 }
 
-__device__ inline int cubicRoots(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
+__device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
     const double b = sp.b, b2 = b * b, RTp = kGas * T / p, aap = aa / p, bn = b - RTp;
     const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
     const double center = -bn / 3.0, delta2 = (bn * bn - 3.0 * cn) / 9.0;
@@ -213,7 +221,7 @@ struct TTerms {
     double T, aa, da, d2a, q, cpR, hRT, sR;
 };
 
-__device__ inline int tTerms(const PureSpecies& sp, double T, TTerms& t) {
+__device__ RB200_EOS_FN int tTerms(const PureSpecies& sp, double T, TTerms& t) {
     if (!fin(T) || T <= 0) return EOS_INVALID_INPUT;
     const double sq = sqrt(T / sp.Tc), f = 1.0 + sp.kappa * (1.0 - sq);
     if (fabs(f) <= 1e-14) return EOS_NONFINITE;
@@ -232,7 +240,7 @@ __device__ inline int tTerms(const PureSpecies& sp, double T, TTerms& t) {
 
 // Properties at (T, rho) from the T-only terms. chem: also the molar chemical
 // potential. phaseOut: -2 supercritical, -1 gas, 0 liquid by the reported-phase line.
-__device__ inline int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
+__device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
                               int& phaseOut) {
     const double T = t.T, aa = t.aa, da = t.da, d2a = t.d2a;
     if (!fin(rho) || rho <= 0) return EOS_INVALID_INPUT;
@@ -284,7 +292,7 @@ __device__ inline int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho
     return EOS_OK;
 }
 
-__device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool chem, PhaseProps& s, int& phaseOut) {
+__device__ RB200_EOS_FN int prTrho(const PureSpecies& sp, double T, double rho, bool chem, PhaseProps& s, int& phaseOut) {
     if (!fin(T) || !fin(rho) || T <= 0 || rho <= 0) return EOS_INVALID_INPUT;
     TTerms t;
     const int st = tTerms(sp, T, t);
@@ -294,7 +302,7 @@ __device__ inline int prTrho(const PureSpecies& sp, double T, double rho, bool c
 
 // Root choice at (T, p) with the host postcondition |p(T, rho) - p| <= 1e-7 max(1, p)
 // and the reported-phase consistency of the chosen branch.
-__device__ inline int rootProps(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
+__device__ RB200_EOS_FN int rootProps(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
                                 bool chem, PhaseProps& s) {
     int sel = r.count - 1;
     if (choice == ROOT_LIQUID) {
@@ -312,7 +320,7 @@ __device__ inline int rootProps(const PureSpecies& sp, const TTerms& t, const Ro
     return EOS_OK;
 }
 
-__device__ inline int prTP(const PureSpecies& sp, double T, double p, int choice, bool chem, PhaseProps& s) {
+__device__ RB200_EOS_FN int prTP(const PureSpecies& sp, double T, double p, int choice, bool chem, PhaseProps& s) {
     if (!fin(T) || !fin(p) || T <= 0 || p <= 0) return EOS_INVALID_INPUT;
     TTerms t;
     int st = tTerms(sp, T, t);

@@ -6,7 +6,7 @@
 // src/reactiveTransport/reactiveTransport.cpp:381-1815 and
 // src/reactiveTransport/reactiveTransport.h:48-141. Execution is CUDA only:
 // backend 0 (the reference's serial CPU loop) is rejected, never emulated.
-#include "transport_kernels.cuh"
+#include "cartesian_kernels.cuh"
 #include "../../include/reactive_b200_transport.h"
 
 #include <algorithm>
@@ -15,6 +15,7 @@
 #include <limits>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace rb200 {
@@ -60,6 +61,11 @@ struct Transport {
     double* boundaryRate = nullptr;
     ReactiveTransportState* stateDevice = nullptr;
     unsigned* flags = nullptr;  // [0] WALE failure
+    // structured Cartesian fast path (device-resident entries only)
+    bool boxDetected = false, structured = false;
+    CartView box{};
+    double* ledgerPartial = nullptr;
+    unsigned ledgerBlocks = 0;
     ReactiveTransportStats stats{};
     ReactiveTransportProfile profile{};
     ReactiveTransportDeviceProfile deviceProfile{};
@@ -204,6 +210,12 @@ struct Transport {
         v.invV = invDevice; v.state = stateDevice; v.q = q; v.primitive = primitive; v.grad = grad;
         v.gasY = gasY; v.gasH = gasH; v.work = work; v.carrier = carrier; v.faceSpeed = faceSpeed; v.step = step;
         v.waleError = flags;
+        boxDetected = detectBox(faces, cfg.faces - boundary.size(), invDevice, primitive);
+        structured = boxDetected;
+        if (boxDetected) {
+            ledgerBlocks = unsigned(std::min<size_t>(296, (box.nBoundary + 255) / 256));
+            ledgerPartial = arena.get<double>(product(ledgerBlocks, cfg.variables));
+        }
 
         packInto(q, fixedQ, cfg.fixed, cfg.variables, all, cfg.cells);
         packInto(initial, fixedQ, cfg.fixed, cfg.variables, all, cfg.cells);
@@ -353,6 +365,153 @@ struct Transport {
         const unsigned blocks = unsigned(reduceBlocks);
         minimumReduce<<<blocks, 256, 0, s>>>(v.step, v.cells, reduceScratch);
         launched();
+        minimumReduce<<<1, 1024, 0, s>>>(reduceScratch, blocks, result);
+        launched();
+    }
+
+    // ------------------------------------------------ structured Cartesian box
+    // The face list is a uniform nx x ny x nz box in the canonical ordering:
+    // cells in natural order c = i + nx (j + ny k); internal faces sorted by
+    // (owner, neighbour) with owner the lower cell, normal exactly +e_axis,
+    // ownerWeight 0.5 and one area and distance per axis; then the boundary
+    // faces in six contiguous side blocks (-x, +x, -y, +y, -z, +z), each in
+    // lateral order (fast, slow) = (j, k), (i, k), (i, j), normal exactly
+    // -+e_axis. Any other face list, species diffusion, the mechanical
+    // variables, or more than four species use the face graph.
+    bool detectBox(const ReactiveTransportFace* faces, size_t nInternal, const double* invDevice,
+                   const ReactiveTransportPrimitive* primitive) {
+        if (cfg.mechanical || cfg.diffusivity != 0 || cfg.variables != cfg.species + 4 || cfg.species < 1
+            || cfg.species > size_t(kCartMaxNs) || nInternal < 3 || cfg.cells < 8)
+            return false;
+        if (faces[1].neighbour <= 0 || faces[2].neighbour <= 0 || size_t(faces[2].neighbour) >= cfg.cells)
+            return false;
+        const size_t nx = size_t(faces[1].neighbour), nxy = size_t(faces[2].neighbour);
+        if (faces[0].owner != 0 || faces[0].neighbour != 1 || faces[1].owner != 0 || faces[2].owner != 0 || nx < 2
+            || nxy < 2 * nx || nxy % nx || cfg.cells % nxy)
+            return false;
+        const size_t ny = nxy / nx, nz = cfg.cells / nxy;
+        if (ny < 2 || nz < 2 || nx > INT32_MAX || ny > INT32_MAX || nz > INT32_MAX) return false;
+        const size_t internal = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1);
+        const size_t bnd = 2 * (ny * nz + nx * nz + nx * ny);
+        if (internal != nInternal || internal + bnd != cfg.faces) return false;
+        double area[3] = {faces[0].area, faces[1].area, faces[2].area};
+        double dist[3] = {faces[0].distance, faces[1].distance, faces[2].distance};
+        auto axisNormal = [](const ReactiveTransportFace& f, int axis, double sgn) {
+            for (int d = 0; d < 3; ++d)
+                if (f.normal[d] != (d == axis ? sgn : 0.0)) return false;
+            return true;
+        };
+        size_t fi = 0;
+        for (size_t c = 0; c < cfg.cells; ++c) {
+            const size_t i = c % nx, j = (c / nx) % ny, k = c / nxy;
+            const bool has[3] = {i + 1 < nx, j + 1 < ny, k + 1 < nz};
+            const size_t step[3] = {1, nx, nxy};
+            for (int a = 0; a < 3; ++a) {
+                if (!has[a]) continue;
+                const auto& f = faces[fi++];
+                if (size_t(f.owner) != c || f.neighbour < 0 || size_t(f.neighbour) != c + step[a] || f.kind != 0
+                    || !axisNormal(f, a, 1.0) || f.area != area[a] || f.distance != dist[a] || f.ownerWeight != .5)
+                    return false;
+            }
+        }
+        size_t base[6];
+        for (int side = 0; side < 6; ++side) {
+            const int a = side >> 1;
+            const bool upper = side & 1;
+            const size_t fast = a == 0 ? ny : nx, slow = a == 2 ? ny : nz;
+            base[side] = fi;
+            for (size_t t = 0; t < slow; ++t)
+                for (size_t u = 0; u < fast; ++u) {
+                    size_t i = 0, j = 0, k = 0;
+                    if (a == 0) { i = upper ? nx - 1 : 0; j = u; k = t; }
+                    else if (a == 1) { j = upper ? ny - 1 : 0; i = u; k = t; }
+                    else { k = upper ? nz - 1 : 0; i = u; j = t; }
+                    const auto& f = faces[fi++];
+                    if (size_t(f.owner) != i + nx * (j + ny * k) || f.neighbour != -1 || f.kind < 1 || f.kind > 3
+                        || !axisNormal(f, a, upper ? 1.0 : -1.0))
+                        return false;
+                }
+        }
+        box.nx = int(nx); box.ny = int(ny); box.nz = int(nz);
+        box.cells = cfg.cells; box.fixed = cfg.fixed; box.all = cfg.cells + cfg.fixed;
+        for (int a = 0; a < 3; ++a) { box.area[a] = area[a]; box.dist[a] = dist[a]; }
+        box.invV = invDevice;
+        box.face = v.face;
+        for (int side = 0; side < 6; ++side) box.sideBase[side] = base[side];
+        box.boundaryBase = nInternal;
+        box.nBoundary = bnd;
+        box.primitive = primitive;
+        box.viscosity = cfg.viscosity; box.conductivity = cfg.conductivity; box.waveFactor = cfg.waveFactor;
+        return true;
+    }
+    CartView boxView() const {
+        CartView b = box;
+        b.wale = v.wale;
+        b.cw = v.cw;
+        return b;
+    }
+    template <template <int> class K, class... Args> void bySpecies(Args&&... args) {
+        switch (cfg.species) {
+        case 1: K<1>::run(std::forward<Args>(args)...); break;
+        case 2: K<2>::run(std::forward<Args>(args)...); break;
+        case 3: K<3>::run(std::forward<Args>(args)...); break;
+        default: K<4>::run(std::forward<Args>(args)...); break;
+        }
+        launched();
+    }
+    template <int NS> struct GradientsK {
+        static void run(const CartView& b, const ReactiveTransportState* st, double* grad, double* nut,
+                        unsigned* error, cudaStream_t s) {
+            cartGradients<NS><<<gridFor(b.cells, 256), 256, 0, s>>>(b, st, grad, nut, error);
+        }
+    };
+    template <int NS> struct RatesK {
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
+                        const double* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
+                        cudaStream_t s) {
+            cartRates<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error);
+        }
+    };
+    template <int NS> struct StepsK {
+        static void run(const CartView& b, const ReactiveTransportState* st, const double* nut, double cfl,
+                        double maximumStep, double* partial, unsigned blocks, cudaStream_t s) {
+            cartSteps<NS><<<blocks, 256, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
+        }
+    };
+    template <int NS> struct LedgerK {
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
+                        const double* nut, double* partial, unsigned blocks, cudaStream_t s) {
+            cartLedger<NS><<<blocks, 256, 0, s>>>(b, q, st, grad, nut, partial);
+        }
+    };
+    // Gradient (+ WALE viscosity) of the structured box, when the operator needs it.
+    void launchBoxGradients(const ReactiveTransportState* state, cudaStream_t s) {
+        if (!(v.wale || cfg.viscosity > 0)) return;
+        bySpecies<GradientsK>(boxView(), state, v.grad, v.nut, flags, s);
+        if (v.wale) {
+            ++waleProfile.gradientBuilds;
+            ++waleProfile.viscosityBuilds;
+            waleProfile.cellsEvaluated += v.cells;
+        }
+    }
+    void launchBoxStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt, int stage,
+                        double* rate, cudaStream_t s) {
+        launchBoxGradients(state, s);
+        if (rate) {
+            bySpecies<LedgerK>(boxView(), qIn, state, v.grad, v.nut, ledgerPartial, ledgerBlocks, s);
+            foldPartials<<<1, 32 * unsigned(cfg.variables), 0, s>>>(ledgerPartial, int(ledgerBlocks),
+                                                                    int(cfg.variables), rate);
+            launched();
+        }
+        bySpecies<RatesK>(boxView(), qIn, state, v.grad, v.nut, qOut, v.all, stage == 0 ? 1 : 2, dt, flags, s);
+        ++deviceProfile.transportFaceLaunches;
+    }
+    void launchBoxStep(const ReactiveTransportState* state, double cfl, double maximumStep, double* result,
+                       cudaStream_t s) {
+        if (v.wale) launchBoxGradients(state, s);
+        const unsigned blocks = unsigned(reduceBlocks);
+        bySpecies<StepsK>(boxView(), state, v.nut, cfl, maximumStep, reduceScratch, blocks, s);
+        ++deviceProfile.cflFaceLaunches;
         minimumReduce<<<1, 1024, 0, s>>>(reduceScratch, blocks, result);
         launched();
     }

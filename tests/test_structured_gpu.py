@@ -1,0 +1,162 @@
+"""GPU: the structured Cartesian path of the device-resident transport entries.
+
+A uniform box in the mesh tool's canonical face ordering is detected at create;
+reactive_transport_stage_device_v3 and reactive_transport_stable_step_device_v3
+then run cell-stencil kernels instead of the face graph. Both SSPRK2 stages and
+the CFL step must be bitwise identical to the face-graph path on the same handle
+and inputs, and match the oracle within the reference validation tolerances
+(tools/validate_reactive_transport.py:191-208). The boundary ledger is summed in
+a different order, so it is compared within the operator tolerance.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from spuma_multiphysics_b200 import _abi as A, _lib, cases
+import transport_cases as T
+
+pytestmark = pytest.mark.gpu
+
+H = 2e-3
+
+
+def box_case(dims, ns, side_kinds, viscous=False, conduction=False, seed=0):
+    faces_np, volume = cases.box_faces(dims, H, side_kinds)
+    nc = volume.size
+    rng = np.random.default_rng(4100 + 31 * ns + nc + seed)
+    nv = ns + 4
+    q = np.zeros((nc, nv))
+    q[:, :ns] = rng.uniform(.002, 1, (nc, ns))
+    q[:, :ns] /= q[:, :ns].sum(axis=1)[:, None]
+    q[:, :ns] *= rng.uniform(.75, 1.35, (nc, 1))
+    rho = q[:, :ns].sum(axis=1)
+    vel = rng.normal(0, 11, (nc, 3))
+    q[:, ns:ns + 3] = rho[:, None] * vel
+    q[:, ns + 3] = rng.uniform(7.5e4, 1.25e5, nc) / .4 + .5 * rho * np.sum(vel ** 2, axis=1)
+    n_fixed = int(np.any(faces_np["kind"] == 3))
+    fixed_q = np.ascontiguousarray(q[:1] * 1.013)
+    fixed_states, fixed_y, fixed_h = T.ideal_states(fixed_q, ns)
+    states, y, h = T.ideal_states(q, ns)
+    arr = (A.Face * len(faces_np)).from_buffer_copy(faces_np.tobytes())
+    cfg = A.Config(nc, ns, nv, len(faces_np), n_fixed, .007 if viscous else 0.0, 2.0 if conduction else 0.0, 0.0,
+                   1.1, 2e8, 0)
+    return dict(config=cfg, faces=arr, volume=volume, q=q, states=states, y=y, h=h,
+                fixed_q=fixed_q if n_fixed else np.zeros((1, nv)), fixed_states=fixed_states,
+                fixed_states_ptr=C.cast(T.states_ptr(fixed_states), C.c_void_p), fixed_y=fixed_y, fixed_h=fixed_h,
+                ns=ns, nc=nc, nv=nv, mechanical=False)
+
+
+def mixed_kinds(dims, seed):
+    """Per-face boundary kinds: every side mixes slip, extrapolate and fixed state."""
+    rng = np.random.default_rng(seed)
+    sizes = [dims[1] * dims[2]] * 2 + [dims[0] * dims[2]] * 2 + [dims[0] * dims[1]] * 2
+    return [rng.choice([1, 2, 3], size=n) for n in sizes]
+
+
+BOXES = [
+    dict(dims=(5, 4, 3), ns=1, kinds=(2, 2, 2, 2, 2, 2)),
+    dict(dims=(6, 5, 4), ns=2, kinds=(1, 2, 3, 1, 2, 1), viscous=True, conduction=True),
+    dict(dims=(4, 4, 4), ns=1, kinds="mixed", viscous=True, conduction=True, wale=.325),
+    dict(dims=(7, 3, 5), ns=4, kinds="mixed", wale=.5),
+    dict(dims=(9, 8, 10), ns=3, kinds=(3, 1, 1, 2, 2, 3), conduction=True, wale=.325),
+]
+
+
+def _stage_pair(L, h, case, stream, torch):
+    """CFL step, stage 0 and stage 1 on the handle's current path."""
+    nc, nv, ns = case["nc"], case["nv"], case["ns"]
+    cells, fixed, nvar, nsp = (C.c_size_t() for _ in range(4))
+    assert L.reactive_transport_layout_v3(h, C.byref(cells), C.byref(fixed), C.byref(nvar), C.byref(nsp)) == 0
+    all_ = nc + fixed.value
+    q0 = torch.zeros((nv, all_), dtype=torch.float64, device="cuda")
+    q0[:, :nc] = torch.from_numpy(case["q"].T.copy()).cuda()
+    st = torch.zeros((all_, 7), dtype=torch.float64, device="cuda")
+    st[:nc] = torch.from_numpy(case["states"].view(np.float64).reshape(nc, 7)).cuda()
+    assert L.reactive_transport_fill_fixed_v3(h, q0.data_ptr(), st.data_ptr(), stream) == 0
+    dt = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert L.reactive_transport_stable_step_device_v3(h, q0.data_ptr(), st.data_ptr(), .23, .1, dt.data_ptr(),
+                                                      stream) == 0
+    torch.cuda.synchronize()
+    step = .1 * dt.item()
+    q1 = q0.clone()
+    br0 = torch.zeros(nv, dtype=torch.float64, device="cuda")
+    assert L.reactive_transport_stage_device_v3(h, q0.data_ptr(), q1.data_ptr(), st.data_ptr(), step, 0,
+                                                br0.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    got1 = np.ascontiguousarray(q1[:, :nc].cpu().numpy().T)
+    st1, _, _ = T.ideal_states(got1, ns)
+    st[:nc] = torch.from_numpy(st1.view(np.float64).reshape(nc, 7)).cuda()
+    qn = q0.clone()
+    br1 = torch.zeros(nv, dtype=torch.float64, device="cuda")
+    assert L.reactive_transport_stage_device_v3(h, q1.data_ptr(), qn.data_ptr(), st.data_ptr(), step, 1,
+                                                br1.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    status = C.c_uint()
+    assert L.reactive_transport_status_v3(h, C.byref(status), 1, stream) == 0
+    return dict(dt=dt.item(), step=step, q1=got1, qn=qn[:, :nc].cpu().numpy().T, br0=br0.cpu().numpy(),
+                br1=br1.cpu().numpy(), st1=st1, status=status.value, tail=bool(torch.equal(qn[:, nc:], q0[:, nc:])))
+
+
+@pytest.mark.parametrize("spec", BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_structured_path_matches_face_graph_and_oracle(spec):
+    import torch
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    cw = spec.get("wale")
+    h = T.create(lib, 1, case, wale_cw=cw)
+    try:
+        active = C.c_int(-1)
+        assert L.reactive_transport_structured_v3(h, -1, C.byref(active)) == 0
+        assert active.value == 1, "canonical box not detected"
+        stream = torch.cuda.current_stream().cuda_stream
+        box = _stage_pair(L, h, case, stream, torch)
+        assert L.reactive_transport_structured_v3(h, 0, C.byref(active)) == 0 and active.value == 0
+        graph = _stage_pair(L, h, case, stream, torch)
+        assert box["status"] == 0 and graph["status"] == 0
+        assert box["tail"] and graph["tail"]
+        # same arithmetic in the same order: bitwise identical stage results
+        assert box["dt"] == graph["dt"]
+        assert np.array_equal(box["q1"], graph["q1"])
+        assert np.array_equal(box["qn"], graph["qn"])
+        for k in ("br0", "br1"):
+            assert T.scaled_error(box[k][None], graph[k][None]) <= T.RHS_TOL
+        # against the oracle (itself pinned to the reference's CPU build)
+        wale_cw = -1.0 if cw is None else cw
+        states_p = case["states"].ctypes.data_as(C.c_void_p)
+        odt = oracle.transport_stable_dt(case, case["q"], states_p, .23, .1, wale_cw=wale_cw)
+        assert abs(box["dt"] / odt - 1) < T.DT_TOL
+        rhs, exp_br, _, _, status = oracle.transport_rhs(case, case["q"], states_p, wale_cw=wale_cw)
+        assert status == 0
+        step = box["step"]
+        assert T.scaled_error(box["q1"], case["q"] + step * rhs) <= T.RHS_TOL
+        assert T.scaled_error(box["br0"][None], exp_br[None]) <= T.RHS_TOL
+        rhs1, exp_br1, _, _, _ = oracle.transport_rhs(case, box["q1"], box["st1"].ctypes.data_as(C.c_void_p),
+                                                      wale_cw=wale_cw)
+        assert T.scaled_error(box["qn"], .5 * case["q"] + .5 * (box["q1"] + step * rhs1)) <= T.RHS_TOL
+        assert T.scaled_error(box["br1"][None], exp_br1[None]) <= T.RHS_TOL
+    finally:
+        lib.reactive_transport_destroy(h)
+
+
+def test_non_canonical_face_order_uses_the_face_graph():
+    L = _lib.load()
+    lib = T.bind(L)
+    case = box_case((4, 3, 3), 1, (2, 2, 2, 2, 2, 2))
+    faces = case["faces"]
+    # swap two internal faces: still a valid face graph, no longer canonical
+    a, b = A.Face(), A.Face()
+    C.memmove(C.byref(a), C.byref(faces[3]), C.sizeof(A.Face))
+    C.memmove(C.byref(b), C.byref(faces[4]), C.sizeof(A.Face))
+    faces[3], faces[4] = b, a
+    h = T.create(lib, 1, case)
+    try:
+        active = C.c_int(-1)
+        assert L.reactive_transport_structured_v3(h, -1, C.byref(active)) == 0 and active.value == 0
+        assert L.reactive_transport_structured_v3(h, 1, C.byref(active)) == 1
+        assert b"not a structured Cartesian box" in lib.reactive_transport_error(h)
+    finally:
+        lib.reactive_transport_destroy(h)
