@@ -15,7 +15,11 @@ LIB = HERE / "libreactive_b200.so"
 # (--fmad=false) so antisymmetric face terms cancel exactly, e.g. the HLL mass and
 # energy fluxes through a slip wall are exactly zero as in the reference's CPU and
 # CUDA builds. HEM: fused multiply-add (the Newton iteration is insensitive to it).
-SOURCES = {"transport.cu": ["--fmad=false"], "hem.cu": ["--fmad=true"], "probe.cu": ["--fmad=true"]}
+# The plain per-cell flash (hem_plain.cu) inlines every EOS/flash routine, the
+# work-queue flash (hem.cu) keeps them out of line: each form built as it runs best.
+SOURCES = {"transport.cu": ["--fmad=false"], "hem.cu": ["--fmad=true"],
+           "hem_plain.cu": ["--fmad=true", "-DRB200_EOS_FN=inline", "-DRB200_FLASH_FN=inline"],
+           "probe.cu": ["--fmad=true"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--shared", "-Xptxas", "-warn-spills",
          "--expt-relaxed-constexpr"]
@@ -48,7 +52,7 @@ def build(force=False, verbose=False, extra=()):
         cmd = [nvcc(), *ARCH, *compile_flags, *policy, *extra, "-c", str(CSRC / name), "-o", str(obj)]
         _run(cmd, verbose)
         objects.append(str(obj))
-    _run([nvcc(), *ARCH, "--shared", *objects, "-o", str(LIB), "-lcudart"], verbose)
+    _run([nvcc(), *ARCH, "--shared", *objects, "-o", str(LIB), "-lcudart", "-lpthread"], verbose)
     return LIB
 
 

@@ -3,8 +3,11 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <thread>
+#include <vector>
 
 namespace rb200 {
 
@@ -14,6 +17,31 @@ inline void check(cudaError_t status, const char* what) {
 }
 inline void require(bool ok, const char* message) {
     if (!ok) throw std::runtime_error(message);
+}
+
+// Index of the first element in [0, count) for which ok(i) is false, or count.
+// Large host arrays (the per-cell validation of caller buffers) are scanned by
+// all hardware threads in contiguous chunks; the result is the same index a
+// serial scan finds.
+template <class Pred> size_t firstFailure(size_t count, Pred ok) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t threads = count < (size_t(1) << 18) ? 1 : std::min<size_t>(hw, 64);
+    if (threads == 1) {
+        for (size_t i = 0; i < count; ++i)
+            if (!ok(i)) return i;
+        return count;
+    }
+    std::vector<size_t> first(threads, count);
+    std::vector<std::thread> pool;
+    const size_t chunk = (count + threads - 1) / threads;
+    for (size_t t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] {
+            const size_t end = std::min(count, (t + 1) * chunk);
+            for (size_t i = t * chunk; i < end; ++i)
+                if (!ok(i)) { first[t] = i; return; }
+        });
+    for (auto& th : pool) th.join();
+    return *std::min_element(first.begin(), first.end());
 }
 
 // 148 SMs on B200; grids for grid-stride kernels are sized in whole waves of

@@ -16,6 +16,7 @@
 // Candidate records live in HBM (192 B each); every loop in the solvers is
 // bounded and no thread waits on another, so every launch terminates.
 #include "hem_flash.cuh"
+#include "hem_common.cuh"
 #include "hem_queue.cuh"
 #include "common.cuh"
 #include "../../include/reactive_b200_hem.h"
@@ -30,6 +31,10 @@
 #include <vector>
 
 namespace rb200 {
+// The plain one-thread-per-cell form (hem_plain.cu).
+void launchPlainFlash(const HemConst* cst, const CellInput* in, size_t count, const ReactiveThermoState* seed,
+                      ReactiveThermoState* state, ReactiveTransportState* transport, int* success,
+                      unsigned* counters, unsigned long long* totals, cudaStream_t s);
 namespace {
 
 struct CandRecord {
@@ -39,30 +44,6 @@ struct CandRecord {
     int pad;
 };
 static_assert(sizeof(CandRecord) == 192, "candidate record layout");
-
-enum Counter { Q_A = 0, Q_B, LIST, Q_C, FALLBACK, FAILED, NCOUNTERS = 8 };
-enum Total { T_PHASES = 0, T_RESIDUALS, T_CANDIDATES, T_STABLE, T_FAILURES, T_ANALYTIC, T_FD, NTOTALS = 8 };
-
-// Work-queue kernels: 128 threads, at least four blocks per SM (<= 128
-// registers a thread). With the EOS routines out of line, sixteen resident warps
-// per SM hide the latency of the FP64 chains better than eight warps at 255
-// registers, and spill nothing that matters.
-constexpr int kPassThreads = 128;
-#ifndef RB200_PASS_MINBLOCKS
-#define RB200_PASS_MINBLOCKS 4
-#endif
-__constant__ double kSeeds[5] = {-1, .5, .95, .1, .9999};
-__constant__ double kRestart[4] = {0.02, 0.25, 0.5, 0.75};
-
-__device__ __forceinline__ void flushCounts(const Counts& n, unsigned long long* totals) {
-    unsigned long long v[7] = {n.phases, n.residuals, n.candidates, n.stable, n.failures, n.analytic, n.fd};
-#pragma unroll
-    for (int i = 0; i < 7; ++i) {
-        unsigned long long x = v[i];
-        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if ((threadIdx.x & 31) == 0 && x) atomicAdd(totals + i, x);
-    }
-}
 
 // Warp-wide dynamic fetch of 32 consecutive items from a device counter.
 __device__ __forceinline__ unsigned fetchItems(unsigned* counter) {
@@ -197,12 +178,6 @@ __global__ void compactSeedCells(const HemConst* __restrict__ Cp, const CandReco
     }
 }
 
-__device__ inline void writeOutputs(const ReactiveThermoState& s, size_t c, ReactiveThermoState* state,
-                                    ReactiveTransportState* transport) {
-    if (state) state[c] = s;
-    if (transport) transport[c] = ReactiveTransportState{s.p, s.T, s.rho, s.cv, s.soundFrozen, s.gasMass, 0.0};
-}
-
 __global__ void selectCandidates(const HemConst* __restrict__ Cp, const CandRecord* rec, size_t count,
                                  ReactiveThermoState* state, ReactiveTransportState* transport, int* success,
                                  unsigned* fallback, unsigned* counters) {
@@ -277,6 +252,14 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passRestar
     flushCounts(n, totals);
 }
 
+// Failed cells get their seed state back, so one contiguous copy of the
+// results leaves them unchanged in the caller's array.
+__global__ void keepFailed(const ReactiveThermoState* __restrict__ seed, const int* __restrict__ success,
+                           size_t count, ReactiveThermoState* __restrict__ out) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x)
+        if (!success[c]) out[c] = seed[c];
+}
+
 __global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsigned* fallback,
                                const ReactiveThermoState* seed, ReactiveThermoState* state,
                                ReactiveTransportState* transport, int* success, unsigned* counters) {
@@ -304,64 +287,6 @@ __global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsi
 // One thread per cell running the whole search in order (the layout of the
 // reference's hemKernel, src/reactiveTransport/reactiveGpuHem.cuh:64-80): the
 // plain form the candidate-parallel passes are measured against. No pruning.
-__global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) flashPerCell(const HemConst* __restrict__ Cp,
-                                                             const CellInput* __restrict__ in, size_t count,
-                                                             const ReactiveThermoState* seed,
-                                                             ReactiveThermoState* state,
-                                                             ReactiveTransportState* transport, int* success,
-                                                             unsigned* counters, unsigned long long* totals) {
-    const HemConst& C = *Cp;
-    Counts n;
-    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
-        const CellInput x = in[c];
-        ReactiveThermoState best{};
-        double bestEntropy = 0;
-        bool have = false, gasStable = false;
-        for (int k = 0; k < 7; ++k) {
-            if (k >= 2 && C.stableGasPrune && gasStable) break;
-            Eval v;
-            CandidateOut o{};
-            bool ok;
-            if (k == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n);
-            else if (k == 1) ok = frozenSolve(C, x, x.q, 0, v, o, n);
-            else ok = twoPhaseSolve(C, x, kSeeds[k - 2], -1.0, v, o, n);
-            if (!ok) { ++n.failures; continue; }
-            if (!stableAt(C, x.q, v.liqMass, v.p, v.T, n)) { ++n.failures; continue; }
-            ++n.stable;
-            if (k == 0) gasStable = v.gasMass > 0;
-            if (!have || v.entropyD > bestEntropy) {
-                have = true;
-                bestEntropy = v.entropyD;
-                stateFromEval(v, x.q, o, best);
-            }
-        }
-        if (!have) {
-            const double lower = fmax(C.Tmin, C.liquidTmin), upper = fmin(C.Tmax, C.liquidTc * (1 - 1e-10));
-            for (int t = 0; t < 4 && upper > lower; ++t)
-                for (int s = 0; s < 5; ++s) {
-                    Eval v;
-                    CandidateOut o{};
-                    if (!twoPhaseSolve(C, x, kSeeds[s], lower + (upper - lower) * kRestart[t], v, o, n)
-                        || !stableAt(C, x.q, v.liqMass, v.p, v.T, n)) { ++n.failures; continue; }
-                    ++n.stable;
-                    if (!have || v.entropyD > bestEntropy) {
-                        have = true;
-                        bestEntropy = v.entropyD;
-                        stateFromEval(v, x.q, o, best);
-                    }
-                }
-        }
-        if (have) {
-            writeOutputs(best, c, state, transport);
-        } else {
-            if (state) state[c] = seed[c];
-            if (transport) writeOutputs(seed[c], c, nullptr, transport);
-            atomicAdd(counters + FAILED, 1u);
-        }
-        if (success) success[c] = have ? 1 : 0;
-    }
-    flushCounts(n, totals);
-}
 
 // ------------------------------------------------------------------ host
 std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C);
@@ -415,9 +340,7 @@ struct HemDevice {
     void launchPerCell(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
                        ReactiveTransportState* transport, int* success, cudaStream_t s) {
         check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "memset counters");
-        flashPerCell<<<unsigned((count + kPassThreads - 1) / kPassThreads), kPassThreads, 0, s>>>(
-            cst, in, count, seed, state, transport, success, counters, totals);
-        check(cudaGetLastError(), "flashPerCell");
+        launchPlainFlash(cst, in, count, seed, state, transport, success, counters, totals, s);
     }
     // Launches steps 2-7 for `count` prepared inputs.
     void launchSearch(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
@@ -716,9 +639,11 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
         rb200::inputsFromHost<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.dq, d.de, d.dguess, count, 1, d.in);
         rb200::check(cudaGetLastError(), "inputs");
         d.launchSearch(count, d.dguess, d.dout, nullptr, d.dsuccess, s);
+        // a failed cell leaves the caller's state unchanged: its seed goes back
+        rb200::keepFailed<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.dguess, d.dsuccess, count, d.dout);
+        rb200::check(cudaGetLastError(), "keepFailed");
         rb200::check(cudaEventRecord(ev[2], s), "event");
-        std::vector<ReactiveThermoState> out(count);
-        rb200::check(cudaMemcpyAsync(out.data(), d.dout, count * sizeof(ReactiveThermoState), cudaMemcpyDeviceToHost, s),
+        rb200::check(cudaMemcpyAsync(states, d.dout, count * sizeof(ReactiveThermoState), cudaMemcpyDeviceToHost, s),
                      "D2H states");
         rb200::check(cudaMemcpyAsync(success, d.dsuccess, count * sizeof(int), cudaMemcpyDeviceToHost, s),
                      "D2H success");
@@ -734,8 +659,7 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
         for (auto& e : ev) cudaEventDestroy(e);
         p.batches = 1;
         p.submitted = count;
-        for (size_t c = 0; c < count; ++c)
-            if (success[c]) { states[c] = out[c]; ++p.succeeded; }
+        for (size_t c = 0; c < count; ++c) p.succeeded += success[c] != 0;
         p.deviceFailures = count - p.succeeded;
         p.transferBytes = count * (2 * sizeof(double) + 2 * sizeof(ReactiveThermoState) + sizeof(int));
         p.deviceBytes = d.bytes;

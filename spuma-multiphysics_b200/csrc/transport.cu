@@ -272,13 +272,13 @@ struct Transport {
     }
     static void validateStates(const ReactiveTransportState* states, size_t count) {
         require(!count || states, "Null transport state");
-        for (size_t c = 0; c < count; ++c) {
+        const size_t bad = firstFailure(count, [&](size_t c) {
             const auto& s = states[c];
-            require(std::isfinite(s.p) && s.p > 0 && std::isfinite(s.T) && s.T > 0 && std::isfinite(s.rho) && s.rho > 0
-                        && std::isfinite(s.sound) && s.sound > 0 && std::isfinite(s.cv) && s.cv > 0
-                        && std::isfinite(s.gasMass) && s.gasMass >= 0 && std::isfinite(s.dilatation),
-                    "Invalid recovered transport state");
-        }
+            return std::isfinite(s.p) && s.p > 0 && std::isfinite(s.T) && s.T > 0 && std::isfinite(s.rho) && s.rho > 0
+                && std::isfinite(s.sound) && s.sound > 0 && std::isfinite(s.cv) && s.cv > 0
+                && std::isfinite(s.gasMass) && s.gasMass >= 0 && std::isfinite(s.dilatation);
+        });
+        require(bad == count, "Invalid recovered transport state");
     }
     void uploadQ(const double* hostQ) {
         packInto(q, hostQ, cfg.cells, cfg.variables, v.all, 0);
@@ -592,9 +592,13 @@ struct Transport {
     }
     void uploadPrimitives(const ReactiveTransportPrimitive* primitive, const ReactiveTransportState* state) {
         require(primitive, "Null transport primitives");
-        for (size_t c = 0; c < cfg.cells; ++c) {
-            require(std::isfinite(primitive[c].rho) && primitive[c].rho > 0, "Invalid primitive density");
-            for (double u : primitive[c].u) require(std::isfinite(u), "Invalid primitive velocity");
+        const size_t bad = firstFailure(cfg.cells, [&](size_t c) {
+            return std::isfinite(primitive[c].rho) && primitive[c].rho > 0 && std::isfinite(primitive[c].u[0])
+                && std::isfinite(primitive[c].u[1]) && std::isfinite(primitive[c].u[2]);
+        });
+        if (bad < cfg.cells) {
+            require(std::isfinite(primitive[bad].rho) && primitive[bad].rho > 0, "Invalid primitive density");
+            require(false, "Invalid primitive velocity");
         }
         uploadState(state);
         upload(v.primitive, primitive, cfg.cells);
