@@ -37,6 +37,14 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Mcell-steps/s at 160³, plain FP64 vs mixed/batched; adjoint/forward time"
 UNIT = "Mcell-steps/s"
+# Per-unit figures of the dominant kernel (the work-queue flash, passQueue), from
+# an ncu capture of the 40^3 impingement flash (the command is in
+# profiles/passQueue_flops_impingement40.md): FP64 FLOPs = 2 DFMA + DADD + DMUL
+# thread instructions, and DRAM read+write bytes, each per PR phase evaluation
+# (the device counter the flash reports). Both scale with phase evaluations, not
+# cells: the DRAM traffic is the solver's local-memory (stack) traffic.
+FLOPS_PER_PHASE_EVAL = 418.85
+DRAM_BYTES_PER_PHASE_EVAL = 74.8
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
 
 
@@ -397,8 +405,10 @@ def run_ours(args, rank, world):
                     "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                     "frac": achieved / fp64 if achieved else None,
                     "peak_source": "measured in this run (FP64 FMA-chain probe)",
-                    "traffic": args.flash_traffic, "ms_per_launch": flash_ms,
-                    "phase_evaluations_per_launch": flash_phase_evals,
+                    "traffic": args.dram_bytes_per_phase_eval * flash_phase_evals,
+                    "traffic_note": "DRAM bytes per launch, ncu per-phase-evaluation figure x this launch's "
+                                    "phase evaluations",
+                    "ms_per_launch": flash_ms, "phase_evaluations_per_launch": flash_phase_evals,
                     "flops_per_phase_evaluation": flops_per_eval}
     # HBM roofline of the whole step (algorithmic bytes per cell-step, FP64, nv=5, 4 transport thermo fields)
     bytes_per_cell_step = 8 * (5 * 5 + 2 * 4) + 2 * (8 * 5 + 80)
@@ -534,9 +544,10 @@ def main():
     p.add_argument("--skip-plain", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
-    p.add_argument("--flops-per-phase-eval", type=float, default=0.0,
+    p.add_argument("--flops-per-phase-eval", type=float, default=FLOPS_PER_PHASE_EVAL,
                    help="FP64 FLOPs per PR phase evaluation of the flash kernels (from an ncu capture)")
-    p.add_argument("--flash-traffic", type=float, default=None, help="DRAM bytes per flash launch (ncu)")
+    p.add_argument("--dram-bytes-per-phase-eval", type=float, default=DRAM_BYTES_PER_PHASE_EVAL,
+                   help="DRAM bytes per PR phase evaluation of the flash kernels (from an ncu capture)")
     p.add_argument("--flash-batch", type=int, default=0, help="run the standalone batched flash on this many cells")
     p.add_argument("--flash-prune", type=int, default=0, help="the model's stableGasPrune flag for --flash-batch")
     args = p.parse_args()
