@@ -20,6 +20,7 @@ built for the CPU, serial, and its flash compiled for the host on every core)
 on a bounded sample: one step of the same case at 40^3.
 """
 import argparse
+import contextlib
 import ctypes as C
 import json
 import os
@@ -60,12 +61,12 @@ def load_package():
     return sys.modules[name]
 
 
-def workload(n):
+def workload(n, precision="mixed (FP32 transport arithmetic, FP64 state and flash)"):
     return {"workload": f"N2O impingement {n}^3 ({n ** 3:,} cells), 40 bar ambient, 2 liquid inlets, "
                         f"viscous + conduction + WALE, SSPRK2 + 2 HEM UV flashes per step, dt=1e-8 s",
             "cells": n ** 3, "faces": 3 * n * n * (n - 1) + 6 * n * n, "species": 1, "variables": 5,
-            "flux": "HLL", "precision": "FP64", "l2": "inputs larger than L2 (q alone 164 MB at 160^3; "
-                                                      "flash candidate records 8.6 GB)"}
+            "flux": "HLL", "precision": precision, "l2": "inputs larger than L2 (q alone 164 MB at 160^3; "
+                                                         "flash candidate records 8.6 GB)"}
 
 
 class ClockSampler:
@@ -300,17 +301,21 @@ def run_ours(args, rank, world):
     import torch
     pkg = load_package()
     from spuma_multiphysics_b200 import cases
-    from spuma_multiphysics_b200.flow import Flow
+    from spuma_multiphysics_b200.flow import Flow, field_errors
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     n = args.size
     t0 = time.time()
     faces, volume = cases.cartesian_faces(n)
     init = cases.impingement(n, seed=2026 + rank)
-    flow = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
-                viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
+    kw = dict(viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
+    # the headline form: mixed-precision structured transport + work-queue flash, one CUDA graph per step
+    mixed = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], precision="mixed",
+                 **kw)
+    # the same step in FP64 (graph-captured), and below its plain launch-by-launch form
+    flow = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], **kw)
     setup_s = time.time() - t0
     lib = flow.lib
-    stream = flow.stream
+    rank_dev = int(os.environ.get("LOCAL_RANK", 0))
 
     def barrier():
         if world > 1:
@@ -321,28 +326,41 @@ def run_ours(args, rank, world):
     def max_over_ranks_(x):
         return max_over_ranks(x, world, "cuda")
 
-    # ---- graph-captured device-resident step (value)
-    stats0 = pkg._abi.Stats()
-    lib.reactive_transport_stats(flow.transport, C.byref(stats0))
-    flow.capture(DT)
-    stats1 = pkg._abi.Stats()
-    lib.reactive_transport_stats(flow.transport, C.byref(stats1))
-    launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 7
-    for _ in range(args.warmup):
-        flow.step(DT)
-    flow.check(DT)
-    barrier()
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clocks:
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.nvtx.range_push("timed_step")
-        a.record(stream)
-        for _ in range(args.steps):
-            flow.step(DT)
-        b.record(stream)
+    def timed_graph_steps(f, sample_clocks):
+        """W warm-up then K timed graph replays of flow f (CUDA events on its stream)."""
+        f.capture(DT)
+        for _ in range(args.warmup):
+            f.step(DT)
+        f.check(DT)
         barrier()
-        torch.cuda.nvtx.range_pop()
-    graph_ms = max_over_ranks_(a.elapsed_time(b) / args.steps)
-    flow.check(DT)
+        sampler = ClockSampler(rank_dev) if sample_clocks else contextlib.nullcontext()
+        with sampler as clocks_:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push("timed_step")
+            a.record(f.stream)
+            for _ in range(args.steps):
+                f.step(DT)
+            b.record(f.stream)
+            barrier()
+            torch.cuda.nvtx.range_pop()
+        f.check(DT)
+        return max_over_ranks_(a.elapsed_time(b) / args.steps), clocks_
+
+    # kernels launched per step: transport launches counted by the handle, plus
+    # five per flash (inputs, queue, select, restart queue, restart select)
+    stats0 = pkg._abi.Stats()
+    lib.reactive_transport_stats(mixed.transport, C.byref(stats0))
+    mixed.capture(DT)
+    stats1 = pkg._abi.Stats()
+    lib.reactive_transport_stats(mixed.transport, C.byref(stats1))
+    launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
+    graph_ms, clocks = timed_graph_steps(mixed, True)
+    fp64_ms, _ = timed_graph_steps(flow, False)
+    # both runs took the same W + K steps from the same state
+    mixed_errors = field_errors(mixed.conserved(), mixed.states(), flow.conserved(), flow.states())
+    mixed.close()
+    stream = flow.stream
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cells = n ** 3
     value = world * cells / (graph_ms * 1e-3) / 1e6
 
@@ -423,8 +441,12 @@ def run_ours(args, rank, world):
     clock = clocks.summary()
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N2O impingement initial state)",
+            "vs_baseline": None, "dtype": "f64 state, f32 flux", "data": "synthetic (seeded N2O impingement initial state)",
             "config": {**workload(n), "parallelism": f"{world} independent replicas (one per GPU)"},
+            "form": "mixed precision (FP32 gradients/WALE/face fluxes, compensated sums into the FP64 state), "
+                    "structured transport, work-queue FP64 flash, one CUDA graph per step",
+            "mixed_field_error_vs_fp64": {"steps": args.warmup + args.steps, **mixed_errors},
+            "fp64_graph": {"ms_per_step": fp64_ms, "value": world * cells / (fp64_ms * 1e-3) / 1e6},
             "plain_fp64": {"ms_per_step": plain_ms, "value": world * cells / (plain_ms * 1e-3) / 1e6 if plain_ms
                            else None, "form": "FP64, kernels launched one by one, flash one thread per cell "
                                                "running the whole candidate search (no work queue, no pruning)"},
@@ -533,6 +555,43 @@ def run_flash_batch(args):
             "clocks": clocks.summary(), "generation_s": gen_s}
 
 
+def run_precision_study(args):
+    """The 80^3 impingement case (viscosity, conduction, WALE) run in FP64 and in
+    the mixed form side by side for --study-steps steps from the same state; the
+    per-field error of the mixed run against the FP64 run (the FP64 device path is
+    the one matched to the reference's CPU RK driver in the tests)."""
+    import torch
+    load_package()
+    from spuma_multiphysics_b200 import cases
+    from spuma_multiphysics_b200.flow import Flow, field_errors
+    n, steps = args.precision_study, args.study_steps
+    faces, volume = cases.cartesian_faces(n)
+    init = cases.impingement(n, seed=2026)
+    kw = dict(viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
+    out = {}
+    flows = {}
+    for name in ("fp64", "mixed"):
+        f = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], precision=name, **kw)
+        f.capture(DT)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(f.stream)
+        for _ in range(steps):
+            f.step(DT)
+        b.record(f.stream)
+        f.check(DT)
+        out[name] = {"ms_per_step": a.elapsed_time(b) / steps}
+        flows[name] = f
+    errors = field_errors(flows["mixed"].conserved(), flows["mixed"].states(), flows["fp64"].conserved(),
+                          flows["fp64"].states())
+    for f in flows.values():
+        f.close()
+    return {"metric": "per-field error of the mixed form against FP64 after the run", "unit": "relative",
+            "config": {**workload(n, "FP64 and mixed side by side"), "steps": steps},
+            "errors": errors, "error_definition": "max over cells of |mixed - fp64| / |fp64| (rho, rhoE, p, T); "
+                                                  "momentum: max |mixed - fp64| / max |fp64|",
+            "timing": out, "data": "synthetic (seeded N2O impingement initial state)"}
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__)
     p.add_argument("--gpus", type=int, default=1)
@@ -550,6 +609,9 @@ def main():
                    help="DRAM bytes per PR phase evaluation of the flash kernels (from an ncu capture)")
     p.add_argument("--flash-batch", type=int, default=0, help="run the standalone batched flash on this many cells")
     p.add_argument("--flash-prune", type=int, default=0, help="the model's stableGasPrune flag for --flash-batch")
+    p.add_argument("--precision-study", type=int, default=0,
+                   help="run FP64 and mixed side by side on this cube size and report per-field errors")
+    p.add_argument("--study-steps", type=int, default=20)
     args = p.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -562,6 +624,8 @@ def main():
     try:
         if args.flash_batch:
             line = run_flash_batch(args)
+        elif args.precision_study:
+            line = run_precision_study(args)
         else:
             line = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
     finally:

@@ -132,6 +132,15 @@ int reactive_transport_stable_step_device_v3(void* transport, const double* q,
  * queries, 0 selects the face graph, 1 the structured path (an error when the
  * face list is not such a box); *active (may be NULL) receives the selection. */
 int reactive_transport_structured_v3(void* transport, int request, int* active);
+/* Arithmetic of the structured path (no reference counterpart; the reference
+ * transport is FP64 only). request -1 only queries, 0 selects FP64, 1 the mixed
+ * form: velocity gradients, WALE eddy viscosity and face fluxes (HLL, traction,
+ * conduction) in FP32, each cell's six face contributions summed with
+ * compensation (Neumaier two-sum) and the stage update applied to the FP64
+ * conserved state in FP64. The CFL step stays FP64. Mixed requires the
+ * structured path; selecting the face graph returns to FP64. *active (may be
+ * NULL) receives 1 for mixed. */
+int reactive_transport_precision_v3(void* transport, int request, int* active);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);

@@ -81,55 +81,72 @@ __device__ __forceinline__ void boundaryRight(const CartView& v, const double* _
 }
 
 // Unit normal component d of a face with normal sgn*e_axis.
-__device__ __forceinline__ double nrm(int d, int axis, double sgn) { return d == axis ? sgn : 0.0; }
+template <class R> __device__ __forceinline__ R nrm(int d, int axis, R sgn) { return d == axis ? sgn : R(0); }
+template <class R> __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
+template <class R> __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
+
+// Neumaier's compensated sum: s + c carries the sum of all added x to about
+// twice the working precision.
+__device__ __forceinline__ void twoSum(float& s, float& c, float x) {
+    const float t = s + x;
+    c += fabsf(s) >= fabsf(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+}
 
 // Flux of all variables through a face with unit normal sgn*e_axis, times the
 // area, seen from the owner (left) side (faceWork + faceFluxK of the face graph).
 // gL/gR: gradients (9 components; gR only used for internal faces); nutL/nutR
-// the WALE viscosities of the owner and right sides.
-template <int NS>
-__device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double sgn, double area, double dist,
-                                             double w, int kind, bool internal, const CellData& L, const CellData& R,
-                                             const double* gL, const double* gR, double nutL, double nutR,
-                                             double* F, bool& bad) {
-    const double unL = L.u[axis] * sgn, unR = R.u[axis] * sgn;
-    const double aL = v.waveFactor * L.c, aR = v.waveFactor * R.c;
-    const double left = dmin(0, dmin(unL - aL, unR - aR)), right = dmax(0, dmax(unL + aL, unR + aR));
-    const double inv = 1 / (right - left);
-    const double advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
-    const double pM = (right * L.p - left * R.p) * inv, pE = (right * L.p * unL - left * R.p * unR) * inv;
-    double traction[3] = {0, 0, 0}, energy = 0;
+// the WALE viscosities of the owner and right sides. R is the arithmetic type:
+// double on the FP64 path (the face graph's exact operation sequence), float
+// on the mixed path (inputs rounded to FP32 once, every operation in FP32).
+template <int NS, class R>
+__device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double sgnD, double areaD, double distD,
+                                             double wD, int kind, bool internal, const CellData& L, const CellData& Rt,
+                                             const R* gL, const R* gR, R nutL, R nutR, R* F, bool& bad) {
+    const R sgn = R(sgnD), w = R(wD), dist = R(distD), area = R(areaD);
+    const R unL = R(L.u[axis]) * sgn, unR = R(Rt.u[axis]) * sgn;
+    const R aL = R(v.waveFactor) * R(L.c), aR = R(v.waveFactor) * R(Rt.c);
+    const R left = rmin(R(0), rmin(unL - aL, unR - aR)), right = rmax(R(0), rmax(unL + aL, unR + aR));
+    const R inv = R(1) / (right - left);
+    const R advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
+    const R pL = R(L.p), pR = R(Rt.p);
+    const R pM = (right * pL - left * pR) * inv, pE = (right * pL * unL - left * pR * unR) * inv;
+    R traction[3] = {R(0), R(0), R(0)}, energy = R(0);
     if (v.viscosity > 0 || v.wale) {
-        double g[9];
+        R uL[3], uR[3];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) g[j] = internal ? w * gL[j] + (1 - w) * gR[j] : gL[j];
+        for (int d = 0; d < 3; ++d) { uL[d] = R(L.u[d]); uR[d] = R(Rt.u[d]); }
+        R g[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) g[j] = internal ? w * gL[j] + (R(1) - w) * gR[j] : gL[j];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            double normal = 0;
+            R normal = R(0);
 #pragma unroll
             for (int d = 0; d < 3; ++d) normal += g[i * 3 + d] * nrm(d, axis, sgn);
-            const double target = (R.u[i] - L.u[i]) / ((kind == 1 ? 2 : 1) * dist);
+            const R target = (uR[i] - uL[i]) / (R(kind == 1 ? 2 : 1) * dist);
 #pragma unroll
             for (int d = 0; d < 3; ++d) g[i * 3 + d] += nrm(d, axis, sgn) * (target - normal);
         }
-        const double div = g[0] + g[4] + g[8];
-        const double mu = v.viscosity + (v.wale ? w * L.rho * nutL + (1 - w) * R.rho * nutR : 0);
+        const R div = g[0] + g[4] + g[8];
+        const R mu = R(v.viscosity) + (v.wale ? w * R(L.rho) * nutL + (R(1) - w) * R(Rt.rho) * nutR : R(0));
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                traction[i] += mu * (g[3 * i + d] + g[3 * d + i] - (i == d ? 2 * div / 3 : 0)) * nrm(d, axis, sgn);
+                traction[i] += mu * (g[3 * i + d] + g[3 * d + i] - (i == d ? R(2) * div / R(3) : R(0)))
+                    * nrm(d, axis, sgn);
         if (kind == 1) {
-            double dot = 0;
+            R dot = R(0);
 #pragma unroll
             for (int d = 0; d < 3; ++d) dot += traction[d] * nrm(d, axis, sgn);
 #pragma unroll
             for (int d = 0; d < 3; ++d) traction[d] = dot * nrm(d, axis, sgn);
         }
 #pragma unroll
-        for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * L.u[d] + (1 - w) * R.u[d]);
+        for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * uL[d] + (R(1) - w) * uR[d]);
     }
-    if (v.conductivity > 0 && kind != 1) energy -= v.conductivity * (R.T - L.T) / dist;
+    if (v.conductivity > 0 && kind != 1) energy -= R(v.conductivity) * (R(Rt.T) - R(L.T)) / dist;
     if (v.wale) {
         bad |= !isfinite(energy);
 #pragma unroll
@@ -137,7 +154,7 @@ __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double
     }
 #pragma unroll
     for (int k = 0; k < NS + 4; ++k) {
-        double flux = advL * L.q[k] + advR * R.q[k];
+        R flux = advL * R(L.q[k]) + advR * R(Rt.q[k]);
         if (k >= NS && k < NS + 3) flux += pM * nrm(k - NS, axis, sgn);
         if (k == NS + 3) flux += pE;
         if (k >= NS && k < NS + 3) flux -= traction[k - NS];
@@ -181,25 +198,25 @@ __device__ __forceinline__ size_t neighbourOf(const CartView& v, int s, size_t c
     return (s & 1) ? c + step : c - step;
 }
 
-// Green-Gauss gradient (and the WALE viscosity) of every cell.
-template <int NS>
+// Green-Gauss gradient (and the WALE viscosity) of every cell, in arithmetic
+// type R (stored as R: 9 gradient components and nu_t per cell).
+template <int NS, class R>
 __global__ void __launch_bounds__(256) cartGradients(CartView v, const ReactiveTransportState* __restrict__ st,
-                                                     double* __restrict__ grad, double* __restrict__ nut,
-                                                     unsigned* error) {
+                                                     R* __restrict__ grad, R* __restrict__ nut, unsigned* error) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
         loadCell<NS>(v, nullptr, st, c, C, false);
-        double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        const double iv = v.invV[c];
+        R g[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+        const R iv = R(v.invV[c]);
 #pragma unroll
         for (int n = 0; n < 12; ++n) {
             const int s = sideOf(n);
             const bool interior = hasNeighbour(v, s, i, j, k);
             if (interior != (n < 6)) continue;
             const int axis = s >> 1;
-            double uf[3], scale, sgn;
+            R uf[3], scale, sgn;
             if (interior) {
                 // internal face: owner is the lower cell, normal +e_axis; this cell's
                 // incidence sign is +1 on its upper side (owner), -1 on its lower side
@@ -207,18 +224,19 @@ __global__ void __launch_bounds__(256) cartGradients(CartView v, const ReactiveT
                 const bool owner = s & 1;
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
-                    uf[a] = owner ? .5 * C.u[a] + (1 - .5) * pn.u[a] : .5 * pn.u[a] + (1 - .5) * C.u[a];
-                scale = (owner ? 1.0 : -1.0) * v.area[axis] * iv;
-                sgn = 1;
+                    uf[a] = owner ? R(.5) * R(C.u[a]) + (R(1) - R(.5)) * R(pn.u[a])
+                                  : R(.5) * R(pn.u[a]) + (R(1) - R(.5)) * R(C.u[a]);
+                scale = R(owner ? 1.0 : -1.0) * R(v.area[axis]) * iv;
+                sgn = R(1);
             } else {
                 const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
-                CellData R;
-                boundaryRight<NS>(v, nullptr, st, f, axis, C, R, false);
-                const double w = f.ownerWeight;
+                CellData Rt;
+                boundaryRight<NS>(v, nullptr, st, f, axis, C, Rt, false);
+                const R w = R(f.ownerWeight);
 #pragma unroll
-                for (int a = 0; a < 3; ++a) uf[a] = w * C.u[a] + (1 - w) * R.u[a];
-                scale = 1.0 * f.area * iv;
-                sgn = (s & 1) ? 1.0 : -1.0;
+                for (int a = 0; a < 3; ++a) uf[a] = w * R(C.u[a]) + (R(1) - w) * R(Rt.u[a]);
+                scale = R(1.0) * R(f.area) * iv;
+                sgn = (s & 1) ? R(1) : R(-1);
             }
 #pragma unroll
             for (int a = 0; a < 3; ++a)
@@ -228,52 +246,52 @@ __global__ void __launch_bounds__(256) cartGradients(CartView v, const ReactiveT
 #pragma unroll
         for (int jj = 0; jj < 9; ++jj) grad[size_t(jj) * v.cells + c] = g[jj];
         if (v.wale) {
-            const double volume = 1 / iv;
-            double delta = 0, nu = 0;
-            bool ok = isfinite(volume) && volume > 0;
-            if (ok) { delta = cbrt(volume); ok = isfinite(delta) && delta > 0; }
-            ok = ok && waleEddyViscosity(g, delta, v.cw, nu);
-            if (!ok || !isfinite(nu) || nu < 0 || !isfinite(C.rho * nu)) atomicOr(error, 1u);
+            const R volume = R(1) / iv;
+            R delta = R(0), nu = R(0);
+            bool ok = isfinite(volume) && volume > R(0);
+            if (ok) { delta = cbrt(volume); ok = isfinite(delta) && delta > R(0); }
+            ok = ok && waleEddyViscosityT<R>(g, delta, R(v.cw), nu);
+            if (!ok || !isfinite(nu) || nu < R(0) || !isfinite(R(C.rho) * nu)) atomicOr(error, 1u);
             else nut[c] = nu;
         }
     }
 }
 
 // The flux of side s of cell c and this cell's incidence sign for it.
-template <int NS>
+template <int NS, class R>
 __device__ __forceinline__ void sideFlux(const CartView& v, const double* __restrict__ q,
                                          const ReactiveTransportState* __restrict__ st,
-                                         const double* __restrict__ grad, const double* __restrict__ nut, size_t c,
+                                         const R* __restrict__ grad, const R* __restrict__ nut, size_t c,
                                          int s, bool interior, int i, int j, int k, const CellData& C,
-                                         const double* gC, double nutC, double* F, double& sign, bool& bad) {
+                                         const R* gC, R nutC, R* F, double& sign, bool& bad) {
     const int axis = s >> 1;
     const bool viscous = v.viscosity > 0 || v.wale;
     if (interior) {
         const size_t nb = neighbourOf(v, s, c);
         CellData N;
         loadCell<NS>(v, q, st, nb, N, true);
-        double gN[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        R gN[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
             for (int jj = 0; jj < 9; ++jj) gN[jj] = grad[size_t(jj) * v.cells + nb];
         }
-        const double nutN = v.wale ? nut[nb] : 0;
+        const R nutN = v.wale ? nut[nb] : R(0);
         if (s & 1) {  // this cell owns the face
-            faceFluxCart<NS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, C, N, gC, gN, nutC, nutN, F,
-                             bad);
+            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, C, N, gC, gN, nutC, nutN, F,
+                                bad);
             sign = -1;
         } else {
-            faceFluxCart<NS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, N, C, gN, gC, nutN, nutC, F,
-                             bad);
+            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, N, C, gN, gC, nutN, nutC, F,
+                                bad);
             sign = 1;
         }
     } else {
         const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
-        CellData R;
-        boundaryRight<NS>(v, q, st, f, axis, C, R, true);
+        CellData Rt;
+        boundaryRight<NS>(v, q, st, f, axis, C, Rt, true);
         // a boundary face's right-side WALE viscosity is the owner's
-        faceFluxCart<NS>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false, C, R, gC,
-                         gC, nutC, nutC, F, bad);
+        faceFluxCart<NS, R>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false, C, Rt,
+                            gC, gC, nutC, nutC, F, bad);
         sign = -1;
     }
 }
@@ -281,46 +299,57 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
 // Sum of the six face fluxes of every cell and the SSPRK2 update:
 // mode 0 rate -> out (stride outStride), 1 out = q + dt rate,
 // 2 out = .5 out + .5 (q + dt rate) (out holds q^n).
-template <int NS>
+// R = double: the face graph's FP64 sums. R = float (mixed): FP32 face fluxes,
+// summed per cell with Neumaier compensation (the sum and its error term are
+// added in FP64), divided by the volume in FP64, and the update applied to the
+// FP64 conserved state in FP64. Each internal face's FP32 flux is computed from
+// the same inputs by both of its cells, so it cancels exactly between them.
+template <int NS, class R>
 __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __restrict__ q,
                                                  const ReactiveTransportState* __restrict__ st,
-                                                 const double* __restrict__ grad, const double* __restrict__ nut,
+                                                 const R* __restrict__ grad, const R* __restrict__ nut,
                                                  double* out, size_t outStride, int mode, double dt,
                                                  unsigned* error) {
+    constexpr bool fp64 = sizeof(R) == sizeof(double);
     const bool viscous = v.viscosity > 0 || v.wale;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
         loadCell<NS>(v, q, st, c, C, true);
-        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        R gC[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
             for (int jj = 0; jj < 9; ++jj) gC[jj] = grad[size_t(jj) * v.cells + c];
         }
-        const double nutC = v.wale ? nut[c] : 0;
+        const R nutC = v.wale ? nut[c] : R(0);
         const double iv = v.invV[c];
-        double rate[NS + 4];
+        R rate[NS + 4], comp[NS + 4];
 #pragma unroll
-        for (int kk = 0; kk < NS + 4; ++kk) rate[kk] = 0;
+        for (int kk = 0; kk < NS + 4; ++kk) rate[kk] = comp[kk] = R(0);
         bool bad = false;
 #pragma unroll
         for (int n = 0; n < 12; ++n) {
             const int s = sideOf(n);
             const bool interior = hasNeighbour(v, s, i, j, k);
             if (interior != (n < 6)) continue;
-            double F[NS + 4], sign;
-            sideFlux<NS>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad);
+            R F[NS + 4];
+            double sign;
+            sideFlux<NS, R>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad);
 #pragma unroll
-            for (int kk = 0; kk < NS + 4; ++kk) rate[kk] += sign * F[kk] * iv;
+            for (int kk = 0; kk < NS + 4; ++kk) {
+                if constexpr (fp64) rate[kk] += sign * F[kk] * iv;
+                else twoSum(rate[kk], comp[kk], sign > 0 ? F[kk] : -F[kk]);
+            }
         }
         if (bad) atomicOr(error, 1u);
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) {
+            const double r = fp64 ? double(rate[kk]) : (double(rate[kk]) + double(comp[kk])) * iv;
             const size_t o = size_t(kk) * outStride + c;
-            if (mode == 0) out[o] = rate[kk];
-            else if (mode == 1) out[o] = C.q[kk] + dt * rate[kk];
-            else out[o] = .5 * out[o] + .5 * (C.q[kk] + dt * rate[kk]);
+            if (mode == 0) out[o] = r;
+            else if (mode == 1) out[o] = C.q[kk] + dt * r;
+            else out[o] = .5 * out[o] + .5 * (C.q[kk] + dt * r);
         }
     }
 }
@@ -343,9 +372,9 @@ __device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, dou
 
 // CFL step of every cell from its six face speeds (cellSteps), folded to one
 // partial minimum per block with invalid steps absorbing as -1 (minimumReduce).
-template <int NS>
+template <int NS, class R>
 __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTransportState* __restrict__ st,
-                                                 const double* __restrict__ nut, double cfl, double maximumStep,
+                                                 const R* __restrict__ nut, double cfl, double maximumStep,
                                                  double* partial) {
     __shared__ double warpValues[32];
     double m = HUGE_VAL;
@@ -354,7 +383,7 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
         cellCoords(v, c, i, j, k);
         CellData C;
         loadCell<NS>(v, nullptr, st, c, C, false);
-        const double nutC = v.wale ? nut[c] : 0;
+        const double nutC = v.wale ? double(nut[c]) : 0;
         double denominator = 0;
         bool bad = false;
 #pragma unroll
@@ -368,15 +397,15 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
                 const size_t nb = neighbourOf(v, s, c);
                 CellData N;
                 loadCell<NS>(v, nullptr, st, nb, N, false);
-                const double nutN = v.wale ? nut[nb] : 0;
+                const double nutN = v.wale ? double(nut[nb]) : 0;
                 speed = (s & 1) ? faceSpeedCart(v, axis, 1.0, v.dist[axis], .5, C, N, nutC, nutN)
                                 : faceSpeedCart(v, axis, 1.0, v.dist[axis], .5, N, C, nutN, nutC);
                 area = v.area[axis];
             } else {
                 const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
-                CellData R;
-                boundaryRight<NS>(v, nullptr, st, f, axis, C, R, false);
-                speed = faceSpeedCart(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight, C, R, nutC, nutC);
+                CellData Rt;
+                boundaryRight<NS>(v, nullptr, st, f, axis, C, Rt, false);
+                speed = faceSpeedCart(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight, C, Rt, nutC, nutC);
                 area = f.area;
             }
             if (!isfinite(speed) || speed < 0) { bad = true; break; }
@@ -399,10 +428,10 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
 // Boundary ledger: the sum over boundary faces of each variable's face flux.
 // Pass 1 (this kernel) writes one partial per (block, variable) in a fixed
 // partition, pass 2 (foldPartials) adds them in block order: deterministic.
-template <int NS>
+template <int NS, class R>
 __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __restrict__ q,
                                                   const ReactiveTransportState* __restrict__ st,
-                                                  const double* __restrict__ grad, const double* __restrict__ nut,
+                                                  const R* __restrict__ grad, const R* __restrict__ nut,
                                                   double* partial) {
     __shared__ double warpValues[kCartMaxNs + 4][32];
     double sum[NS + 4];
@@ -416,20 +445,20 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
         const size_t c = size_t(f.owner);
         const int axis = f.normal[0] != 0 ? 0 : (f.normal[1] != 0 ? 1 : 2);
         const double sgn = f.normal[axis] > 0 ? 1.0 : -1.0;
-        CellData C, R;
+        CellData C, Rt;
         loadCell<NS>(v, q, st, c, C, true);
-        boundaryRight<NS>(v, q, st, f, axis, C, R, true);
-        double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        boundaryRight<NS>(v, q, st, f, axis, C, Rt, true);
+        R g[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
             for (int jj = 0; jj < 9; ++jj) g[jj] = grad[size_t(jj) * v.cells + c];
         }
-        const double nutC = v.wale ? nut[c] : 0;
-        double F[NS + 4];
-        faceFluxCart<NS>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, C, R, g, g, nutC, nutC, F,
+        const R nutC = v.wale ? nut[c] : R(0);
+        R F[NS + 4];
+        faceFluxCart<NS, R>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, C, Rt, g, g, nutC, nutC, F,
                          bad);
 #pragma unroll
-        for (int kk = 0; kk < NS + 4; ++kk) sum[kk] += F[kk];
+        for (int kk = 0; kk < NS + 4; ++kk) sum[kk] += double(F[kk]);
     }
 #pragma unroll
     for (int kk = 0; kk < NS + 4; ++kk) {

@@ -64,6 +64,9 @@ struct Transport {
     // structured Cartesian fast path (device-resident entries only)
     bool boxDetected = false, structured = false;
     CartView box{};
+    bool mixed = false;
+    float* gradF = nullptr;  // 9 x cells, mixed path
+    float* nutF = nullptr;   // cells, mixed path
     double* ledgerPartial = nullptr;
     unsigned ledgerBlocks = 0;
     ReactiveTransportStats stats{};
@@ -460,60 +463,88 @@ struct Transport {
         launched();
     }
     template <int NS> struct GradientsK {
-        static void run(const CartView& b, const ReactiveTransportState* st, double* grad, double* nut,
-                        unsigned* error, cudaStream_t s) {
-            cartGradients<NS><<<gridFor(b.cells, 256), 256, 0, s>>>(b, st, grad, nut, error);
+        template <class R>
+        static void run(const CartView& b, const ReactiveTransportState* st, R* grad, R* nut, unsigned* error,
+                        cudaStream_t s) {
+            cartGradients<NS, R><<<gridFor(b.cells, 256), 256, 0, s>>>(b, st, grad, nut, error);
         }
     };
     template <int NS> struct RatesK {
-        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
-                        const double* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
+        template <class R>
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
+                        const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
                         cudaStream_t s) {
-            cartRates<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error);
+            cartRates<NS, R><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error);
         }
     };
     template <int NS> struct StepsK {
-        static void run(const CartView& b, const ReactiveTransportState* st, const double* nut, double cfl,
+        template <class R>
+        static void run(const CartView& b, const ReactiveTransportState* st, const R* nut, double cfl,
                         double maximumStep, double* partial, unsigned blocks, cudaStream_t s) {
-            cartSteps<NS><<<blocks, 256, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
+            cartSteps<NS, R><<<blocks, 256, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
         }
     };
     template <int NS> struct LedgerK {
-        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
-                        const double* nut, double* partial, unsigned blocks, cudaStream_t s) {
-            cartLedger<NS><<<blocks, 256, 0, s>>>(b, q, st, grad, nut, partial);
+        template <class R>
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
+                        const R* nut, double* partial, unsigned blocks, cudaStream_t s) {
+            cartLedger<NS, R><<<blocks, 256, 0, s>>>(b, q, st, grad, nut, partial);
         }
     };
     // Gradient (+ WALE viscosity) of the structured box, when the operator needs it.
-    void launchBoxGradients(const ReactiveTransportState* state, cudaStream_t s) {
+    template <class R> void launchBoxGradientsT(const ReactiveTransportState* state, R* grad, R* nut, cudaStream_t s) {
         if (!(v.wale || cfg.viscosity > 0)) return;
-        bySpecies<GradientsK>(boxView(), state, v.grad, v.nut, flags, s);
+        bySpecies<GradientsK>(boxView(), state, grad, nut, flags, s);
         if (v.wale) {
             ++waleProfile.gradientBuilds;
             ++waleProfile.viscosityBuilds;
             waleProfile.cellsEvaluated += v.cells;
         }
     }
-    void launchBoxStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt, int stage,
-                        double* rate, cudaStream_t s) {
-        launchBoxGradients(state, s);
+    template <class R>
+    void launchBoxStageT(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt, int stage,
+                         double* rate, R* grad, R* nut, cudaStream_t s) {
+        launchBoxGradientsT(state, grad, nut, s);
         if (rate) {
-            bySpecies<LedgerK>(boxView(), qIn, state, v.grad, v.nut, ledgerPartial, ledgerBlocks, s);
+            bySpecies<LedgerK>(boxView(), qIn, state, static_cast<const R*>(grad), static_cast<const R*>(nut),
+                               ledgerPartial, ledgerBlocks, s);
             foldPartials<<<1, 32 * unsigned(cfg.variables), 0, s>>>(ledgerPartial, int(ledgerBlocks),
                                                                     int(cfg.variables), rate);
             launched();
         }
-        bySpecies<RatesK>(boxView(), qIn, state, v.grad, v.nut, qOut, v.all, stage == 0 ? 1 : 2, dt, flags, s);
+        bySpecies<RatesK>(boxView(), qIn, state, static_cast<const R*>(grad), static_cast<const R*>(nut), qOut, v.all,
+                          stage == 0 ? 1 : 2, dt, flags, s);
         ++deviceProfile.transportFaceLaunches;
     }
-    void launchBoxStep(const ReactiveTransportState* state, double cfl, double maximumStep, double* result,
-                       cudaStream_t s) {
-        if (v.wale) launchBoxGradients(state, s);
+    template <class R>
+    void launchBoxStepT(const ReactiveTransportState* state, double cfl, double maximumStep, double* result, R* grad,
+                        R* nut, cudaStream_t s) {
+        if (v.wale) launchBoxGradientsT(state, grad, nut, s);
         const unsigned blocks = unsigned(reduceBlocks);
-        bySpecies<StepsK>(boxView(), state, v.nut, cfl, maximumStep, reduceScratch, blocks, s);
+        bySpecies<StepsK>(boxView(), state, static_cast<const R*>(nut), cfl, maximumStep, reduceScratch, blocks, s);
         ++deviceProfile.cflFaceLaunches;
         minimumReduce<<<1, 1024, 0, s>>>(reduceScratch, blocks, result);
         launched();
+    }
+    void launchBoxStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt, int stage,
+                        double* rate, cudaStream_t s) {
+        if (mixed) launchBoxStageT(qIn, qOut, state, dt, stage, rate, gradF, nutF, s);
+        else launchBoxStageT(qIn, qOut, state, dt, stage, rate, v.grad, v.nut, s);
+    }
+    void launchBoxStep(const ReactiveTransportState* state, double cfl, double maximumStep, double* result,
+                       cudaStream_t s) {
+        if (mixed) launchBoxStepT(state, cfl, maximumStep, result, gradF, nutF, s);
+        else launchBoxStepT(state, cfl, maximumStep, result, v.grad, v.nut, s);
+    }
+    // Mixed precision of the structured path: FP32 gradients, WALE and face
+    // fluxes, compensated per-cell sums, FP64 conserved state and update.
+    void setMixed(bool on) {
+        if (on) {
+            require(structured, "Mixed precision needs the structured Cartesian path (reactive_transport_structured_v3)");
+            if (!gradF) gradF = arena.get<float>(product(cfg.cells, 9));
+            if (!nutF) nutF = arena.get<float>(cfg.cells);
+        }
+        mixed = on;
     }
 
     // ------------------------------------------------------- reference contract

@@ -30,6 +30,25 @@ class FlowError(RuntimeError):
     pass
 
 
+def field_errors(q, s, ref_q, ref_s):
+    """Per-field error of a run (cell-major q, thermo states s) against a
+    reference run: relative per cell for the positive fields (each species mass,
+    rho, rhoE, p, T), scaled by the field's largest magnitude for the momentum
+    components (which pass through zero)."""
+    ns = q.shape[1] - 4
+    rel = lambda a, b: float(np.max(np.abs(a - b) / np.abs(b)))
+    out = {"rho": rel(q[:, :ns].sum(axis=1), ref_q[:, :ns].sum(axis=1))}
+    if ns > 1:
+        out.update({f"q{k}": rel(q[:, k], ref_q[:, k]) for k in range(ns)})
+    for d, name in enumerate(("rhoU", "rhoV", "rhoW")):
+        m = ref_q[:, ns + d]
+        out[name] = float(np.max(np.abs(q[:, ns + d] - m)) / max(np.abs(m).max(), 1e-300))
+    out["rhoE"] = rel(q[:, ns + 3], ref_q[:, ns + 3])
+    out["p"] = rel(s["p"], ref_s["p"])
+    out["T"] = rel(s["T"], ref_s["T"])
+    return out
+
+
 def _check(lib, handle, rc):
     if rc:
         raise FlowError(lib.reactive_transport_error(handle).decode())
@@ -37,9 +56,13 @@ def _check(lib, handle, rc):
 
 class Flow:
     def __init__(self, faces, volume, q0, guess0, fixed_q, fixed_guess, viscosity=0.0, conductivity=0.0,
-                 wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda"):
+                 wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda", precision="fp64"):
         """faces: FACE_DTYPE array; q0: cell-major (cells, 5) conserved state;
-        guess0/fixed_guess: THERMO_DTYPE seeds used for the initial recovery."""
+        guess0/fixed_guess: THERMO_DTYPE seeds used for the initial recovery.
+        precision: "fp64", or "mixed" (FP32 gradients, WALE and face fluxes with
+        compensated per-cell sums into the FP64 state; needs a structured box)."""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"unknown precision {precision!r}")
         self.lib = _lib.load()
         self.device = torch.device(device)
         self.cells = len(volume)
@@ -76,6 +99,9 @@ class Flow:
         if wale_cw is not None:
             opts = A.WaleOptions(1, C.sizeof(A.WaleOptions), wale_cw)
             _check(self.lib, self.transport, self.lib.reactive_transport_set_wale_v1(self.transport, C.byref(opts)))
+        self.precision = precision
+        if precision == "mixed":
+            _check(self.lib, self.transport, self.lib.reactive_transport_precision_v3(self.transport, 1, None))
         all_ = self.cells + self.fixed
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)
@@ -122,6 +148,13 @@ class Flow:
         self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s,
                             per_cell)
 
+    def ledger(self, dt):
+        """Boundary ledger of the last step, .5 dt (B0 + B1) per variable (host;
+        synchronises the flow's stream)."""
+        self.stream.synchronize()
+        b = self.boundary.cpu().numpy()
+        return .5 * dt * (b[0] + b[1])
+
     def capture(self, dt):
         """Capture one step as a CUDA graph (replayed by step(dt) for this dt)."""
         self.graph = torch.cuda.CUDAGraph()
@@ -162,9 +195,12 @@ class Flow:
     # --------------------------------------------------------------- views
     def conserved(self):
         """Cell-major host copy of the conserved state (cells, nv)."""
+        self.stream.synchronize()
         return self.qn[:, :self.cells].T.contiguous().cpu().numpy()
 
     def states(self):
+        """Host copy of the thermodynamic states (THERMO_DTYPE)."""
+        self.stream.synchronize()
         return self.sn.cpu().numpy().view(A.THERMO_DTYPE)
 
     def close(self):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from spuma_multiphysics_b200 import cases, thermo_data as td
-from spuma_multiphysics_b200.flow import Flow
+from spuma_multiphysics_b200.flow import Flow, field_errors
 import rk_oracle
 
 pytestmark = pytest.mark.gpu
@@ -52,3 +52,36 @@ def test_flow_matches_reference_rk_driver(graph):
     assert abs((mass[4] - mass0[4]) + ledger[4]) <= 1e-10 * abs(mass0[4])
     ref.close()
     flow.close()
+
+
+def test_mixed_precision_flow_against_fp64():
+    """FP32 gradients/WALE/fluxes with compensated sums against the FP64 path
+    (itself matched to the reference RK driver above): per-field error after 10
+    steps, and the mixed run conserves against its own ledger."""
+    n, steps, dt = 16, 10, 1e-8
+    faces, volume, init = small_case(n)
+    kw = dict(viscosity=1.821e-5, conductivity=0.02587, wale_cw=0.325)
+    fp64 = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], **kw)
+    mixed = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], precision="mixed",
+                 **kw)
+    mass0 = (init["q"] * volume[:, None]).sum(axis=0)
+    ledger = np.zeros(5)
+    for _ in range(steps):
+        fp64.step(dt)
+        mixed.step(dt)
+        ledger += mixed.ledger(dt)
+    fp64.check(dt)
+    mixed.check(dt)
+    q, s = mixed.conserved(), mixed.states()
+    errors = field_errors(q, s, fp64.conserved(), fp64.states())
+    # the north-star bar: p and T within 1e-6 (and the other positive fields)
+    assert max(errors[k] for k in ("rho", "rhoE", "p", "T")) < 1e-6, errors
+    # momentum scaled by its own (small, the flow starts at rest) maximum: the
+    # FP32 pressure-flux differences of the 40 bar background set its error
+    assert max(errors[k] for k in ("rhoU", "rhoV", "rhoW")) < 1e-5, errors
+    assert errors["rho"] > 0  # the mixed form does differ from FP64
+    mass = (q * volume[:, None]).sum(axis=0)
+    assert abs((mass[0] - mass0[0]) + ledger[0]) <= 1e-10 * mass0[0]
+    assert abs((mass[4] - mass0[4]) + ledger[4]) <= 1e-10 * abs(mass0[4])
+    fp64.close()
+    mixed.close()

@@ -160,3 +160,35 @@ def test_non_canonical_face_order_uses_the_face_graph():
         assert b"not a structured Cartesian box" in lib.reactive_transport_error(h)
     finally:
         lib.reactive_transport_destroy(h)
+
+
+@pytest.mark.parametrize("spec", BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_mixed_precision_stage_against_oracle(spec):
+    """The mixed form's stage-0 rate ((q1 - q0) / dt) against the FP64 oracle:
+    FP32 flux arithmetic, so a scaled error of order 1e-7 instead of 1e-12."""
+    import torch
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    cw = spec.get("wale")
+    h = T.create(lib, 1, case, wale_cw=cw)
+    try:
+        active = C.c_int(-1)
+        assert L.reactive_transport_precision_v3(h, 1, C.byref(active)) == 0 and active.value == 1
+        stream = torch.cuda.current_stream().cuda_stream
+        got = _stage_pair(L, h, case, stream, torch)
+        assert got["status"] == 0 and got["tail"]
+        wale_cw = -1.0 if cw is None else cw
+        rhs, exp_br, _, _, status = oracle.transport_rhs(case, case["q"], case["states"].ctypes.data_as(C.c_void_p),
+                                                         wale_cw=wale_cw)
+        assert status == 0
+        rate = (got["q1"] - case["q"]) / got["step"]
+        assert T.scaled_error(rate, rhs) <= 2e-5
+        assert T.scaled_error(got["br0"][None], exp_br[None]) <= 2e-5
+        # selecting the face graph returns to FP64
+        assert L.reactive_transport_structured_v3(h, 0, None) == 0
+        assert L.reactive_transport_precision_v3(h, -1, C.byref(active)) == 0 and active.value == 0
+        assert L.reactive_transport_precision_v3(h, 1, None) == 1
+    finally:
+        lib.reactive_transport_destroy(h)
