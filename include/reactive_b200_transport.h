@@ -141,6 +141,17 @@ int reactive_transport_structured_v3(void* transport, int request, int* active);
  * structured path; selecting the face graph returns to FP64. *active (may be
  * NULL) receives 1 for mixed. */
 int reactive_transport_precision_v3(void* transport, int request, int* active);
+/* Vector-Jacobian product of the rate operator of the device stage entries (no
+ * reference counterpart; the reference has no adjoint). With rate(q, state) the
+ * per-cell right-hand side L that stage_device_v3 applies (q SoA with the fixed
+ * tail, stride cells+fixed) and w its adjoint (SoA, stride cells), writes
+ * qBar = (dL/dq)^T w (SoA, stride cells) and stateBar = (dL/dstate)^T w per cell
+ * (the p and sound fields; the inviscid flux reads no other state field).
+ * Structured path, inviscid operator (viscosity 0, conductivity 0, no WALE);
+ * the derivative of the FP64 operator, with the HLL wave-speed switches taken
+ * piecewise. Asynchronous on `stream`. */
+int reactive_transport_rate_vjp_v3(void* transport, const double* q, const ReactiveTransportState* state,
+    const double* w, double* qBar, ReactiveTransportState* stateBar, void* stream);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);

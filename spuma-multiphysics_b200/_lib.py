@@ -45,6 +45,7 @@ TRANSPORT = {
     "status_v3": ([_v, C.POINTER(C.c_uint), C.c_int, _v], C.c_int),
     "structured_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "precision_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "rate_vjp_v3": ([_v, _v, _v, _v, _v, _v, _v], C.c_int),
 }
 
 HEM = {
@@ -63,6 +64,16 @@ HEM = {
 _lib = None
 
 
+IDEAL = {
+    "create_v3": ([_v, C.c_size_t, C.c_double, C.c_double, C.c_double, C.c_char_p, C.c_size_t], _v),
+    "destroy_v3": ([_v], None),
+    "run_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, _v, _v, C.c_char_p, C.c_size_t],
+                      C.c_int),
+    "vjp_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, C.c_size_t, _v, C.c_char_p,
+                       C.c_size_t], C.c_int),
+}
+
+
 def load():
     """The loaded library with typed entry points (raises if it is absent)."""
     global _lib
@@ -70,7 +81,8 @@ def load():
         if not LIB_PATH.exists():
             raise RuntimeError(f"{LIB_PATH} is missing: run __graft_entry__.build() (the CUDA library is required)")
         lib = C.CDLL(str(LIB_PATH))
-        for table, prefix in ((TRANSPORT, "reactive_transport_"), (HEM, "reactive_gpu_hem_")):
+        for table, prefix in ((TRANSPORT, "reactive_transport_"), (HEM, "reactive_gpu_hem_"),
+                              (IDEAL, "reactive_ideal_gas_")):
             for name, (args, ret) in table.items():
                 fn = getattr(lib, prefix + name, None)
                 if fn is None:

@@ -177,3 +177,49 @@ def impingement(n, fluid=None, seed=1234, ambient_p=40e5, ambient_T=293.15, inle
     fixed_guess["liquidMass"][:, 0] = liq["rho"][0]
     fixed_guess["activeLiquids"] = 1
     return dict(q=q, guess=guess, fixed_q=fixed_q, fixed_guess=fixed_guess)
+
+
+def blast_box(n=64, edge=0.064, p_drive=10e5, p_ambient=1e5, T0=300.0, radius=0.016, noise=0.005, seed=4242,
+              species=None):
+    """The two-species ideal-gas blast box: an n^3 cube (dx = edge/n) with a
+    sphere of radius `radius` at the centre holding N2O at p_drive, N2 at
+    p_ambient elsewhere, both at T0 and at rest, and a seeded uniform +-noise
+    perturbation of the density. Boundaries: extrapolate (transmissive).
+
+    Returns faces, volumes and the nominal density field rho0 (the sphere's
+    pressure fixes the density through rho = p / (r T0) before the noise)."""
+    from .thermo_data import GAS_CONSTANT, N2, N2O
+    species = species or (N2O, N2)
+    faces, volume = box_faces((n, n, n), edge / n, (2, 2, 2, 2, 2, 2))
+    h = edge / n
+    k, j, i = np.indices((n, n, n))
+    centre = edge / 2
+    r2 = ((i.ravel() + .5) * h - centre) ** 2 + ((j.ravel() + .5) * h - centre) ** 2 + \
+        ((k.ravel() + .5) * h - centre) ** 2
+    inside = r2 < radius ** 2
+    rng = np.random.default_rng(seed)
+    r_in, r_out = GAS_CONSTANT / species[0]["W"], GAS_CONSTANT / species[1]["W"]
+    rho0 = np.where(inside, p_drive / (r_in * T0), p_ambient / (r_out * T0)) * (1 + noise * rng.uniform(-1, 1, n ** 3))
+    return dict(faces=faces, volume=volume, inside=inside, rho0=rho0, p_drive=p_drive, p_ambient=p_ambient,
+                T0=T0, species=species, n=n, h=h)
+
+
+def blast_initial(box, rho0, p_drive, xp=np):
+    """Conserved SoA state (nv, cells) of the blast box from the density field
+    rho0 and the driver pressure (numpy, or torch tensors with xp=torch so the
+    map is differentiable): inside the sphere N2O at T = p_drive / (rho0 r),
+    outside N2 at T = p_ambient / (rho0 r), at rest, E = rho0 e(T)."""
+    from .thermo_data import GAS_CONSTANT, ideal_energy
+    sp_in, sp_out = box["species"]
+    inside = box["inside"]
+    if xp is not np:
+        import torch
+        inside = torch.as_tensor(inside, device=rho0.device)
+    r_in, r_out = GAS_CONSTANT / sp_in["W"], GAS_CONSTANT / sp_out["W"]
+    T_in = p_drive / (rho0 * r_in)
+    T_out = box["p_ambient"] / (rho0 * r_out)
+    E = xp.where(inside, rho0 * ideal_energy(sp_in, T_in, xp), rho0 * ideal_energy(sp_out, T_out, xp))
+    zero = rho0 * 0
+    q_in = xp.where(inside, rho0, zero)
+    q_out = xp.where(inside, zero, rho0)
+    return xp.stack([q_in, q_out, zero, zero, zero, E])

@@ -21,6 +21,7 @@
 // bitwise identical stage results.
 #pragma once
 #include "transport_kernels.cuh"
+#include "dual.cuh"
 
 namespace rb200 {
 
@@ -45,6 +46,23 @@ struct CellData {
     double u[3];
     double p, T, rho, cv, c;
 };
+
+// A cell's flux inputs in arithmetic type R (double, float, or a dual number
+// for the adjoint), each rounded from the FP64 data once.
+template <class R> struct CellT {
+    R q[kCartMaxNs + 4];
+    R u[3];
+    R p, T, rho, cv, c;
+};
+template <int NS, class R> __device__ __forceinline__ CellT<R> asCell(const CellData& d) {
+    CellT<R> r;
+#pragma unroll
+    for (int k = 0; k < NS + 4; ++k) r.q[k] = R(d.q[k]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.u[a] = R(d.u[a]);
+    r.p = R(d.p); r.T = R(d.T); r.rho = R(d.rho); r.cv = R(d.cv); r.c = R(d.c);
+    return r;
+}
 
 template <int NS>
 __device__ __forceinline__ void loadCell(const CartView& v, const double* __restrict__ q,
@@ -101,21 +119,21 @@ __device__ __forceinline__ void twoSum(float& s, float& c, float x) {
 // on the mixed path (inputs rounded to FP32 once, every operation in FP32).
 template <int NS, class R>
 __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double sgnD, double areaD, double distD,
-                                             double wD, int kind, bool internal, const CellData& L, const CellData& Rt,
-                                             const R* gL, const R* gR, R nutL, R nutR, R* F, bool& bad) {
+                                             double wD, int kind, bool internal, const CellT<R>& L,
+                                             const CellT<R>& Rt, const R* gL, const R* gR, R nutL, R nutR, R* F,
+                                             bool& bad) {
     const R sgn = R(sgnD), w = R(wD), dist = R(distD), area = R(areaD);
-    const R unL = R(L.u[axis]) * sgn, unR = R(Rt.u[axis]) * sgn;
-    const R aL = R(v.waveFactor) * R(L.c), aR = R(v.waveFactor) * R(Rt.c);
+    const R unL = L.u[axis] * sgn, unR = Rt.u[axis] * sgn;
+    const R aL = R(v.waveFactor) * L.c, aR = R(v.waveFactor) * Rt.c;
     const R left = rmin(R(0), rmin(unL - aL, unR - aR)), right = rmax(R(0), rmax(unL + aL, unR + aR));
     const R inv = R(1) / (right - left);
     const R advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
-    const R pL = R(L.p), pR = R(Rt.p);
+    const R pL = L.p, pR = Rt.p;
     const R pM = (right * pL - left * pR) * inv, pE = (right * pL * unL - left * pR * unR) * inv;
     R traction[3] = {R(0), R(0), R(0)}, energy = R(0);
     if (v.viscosity > 0 || v.wale) {
-        R uL[3], uR[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) { uL[d] = R(L.u[d]); uR[d] = R(Rt.u[d]); }
+        const R* uL = L.u;
+        const R* uR = Rt.u;
         R g[9];
 #pragma unroll
         for (int j = 0; j < 9; ++j) g[j] = internal ? w * gL[j] + (R(1) - w) * gR[j] : gL[j];
@@ -129,7 +147,7 @@ __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double
             for (int d = 0; d < 3; ++d) g[i * 3 + d] += nrm(d, axis, sgn) * (target - normal);
         }
         const R div = g[0] + g[4] + g[8];
-        const R mu = R(v.viscosity) + (v.wale ? w * R(L.rho) * nutL + (R(1) - w) * R(Rt.rho) * nutR : R(0));
+        const R mu = R(v.viscosity) + (v.wale ? w * L.rho * nutL + (R(1) - w) * Rt.rho * nutR : R(0));
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -146,7 +164,7 @@ __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double
 #pragma unroll
         for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * uL[d] + (R(1) - w) * uR[d]);
     }
-    if (v.conductivity > 0 && kind != 1) energy -= R(v.conductivity) * (R(Rt.T) - R(L.T)) / dist;
+    if (v.conductivity > 0 && kind != 1) energy -= R(v.conductivity) * (Rt.T - L.T) / dist;
     if (v.wale) {
         bad |= !isfinite(energy);
 #pragma unroll
@@ -154,7 +172,7 @@ __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double
     }
 #pragma unroll
     for (int k = 0; k < NS + 4; ++k) {
-        R flux = advL * R(L.q[k]) + advR * R(Rt.q[k]);
+        R flux = advL * L.q[k] + advR * Rt.q[k];
         if (k >= NS && k < NS + 3) flux += pM * nrm(k - NS, axis, sgn);
         if (k == NS + 3) flux += pE;
         if (k >= NS && k < NS + 3) flux -= traction[k - NS];
@@ -276,12 +294,13 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
             for (int jj = 0; jj < 9; ++jj) gN[jj] = grad[size_t(jj) * v.cells + nb];
         }
         const R nutN = v.wale ? nut[nb] : R(0);
+        const CellT<R> cc = asCell<NS, R>(C), cn = asCell<NS, R>(N);
         if (s & 1) {  // this cell owns the face
-            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, C, N, gC, gN, nutC, nutN, F,
+            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc, cn, gC, gN, nutC, nutN, F,
                                 bad);
             sign = -1;
         } else {
-            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, N, C, gN, gC, nutN, nutC, F,
+            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cn, cc, gN, gC, nutN, nutC, F,
                                 bad);
             sign = 1;
         }
@@ -290,8 +309,8 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
         CellData Rt;
         boundaryRight<NS>(v, q, st, f, axis, C, Rt, true);
         // a boundary face's right-side WALE viscosity is the owner's
-        faceFluxCart<NS, R>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false, C, Rt,
-                            gC, gC, nutC, nutC, F, bad);
+        faceFluxCart<NS, R>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
+                            asCell<NS, R>(C), asCell<NS, R>(Rt), gC, gC, nutC, nutC, F, bad);
         sign = -1;
     }
 }
@@ -455,7 +474,7 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
         }
         const R nutC = v.wale ? nut[c] : R(0);
         R F[NS + 4];
-        faceFluxCart<NS, R>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, C, Rt, g, g, nutC, nutC, F,
+        faceFluxCart<NS, R>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, asCell<NS, R>(C), asCell<NS, R>(Rt), g, g, nutC, nutC, F,
                          bad);
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) sum[kk] += double(F[kk]);
@@ -473,6 +492,99 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
             s = warpSum(s);
             if (threadIdx.x == 0) partial[size_t(blockIdx.x) * (NS + 4) + kk] = s;
         }
+    }
+}
+
+// Vector-Jacobian product of the inviscid rate operator L(q, state) of the
+// structured box: given adjoint weights w (SoA nv x cells, the adjoint of each
+// cell's rate), qBar = (dL/dq)^T w and stateBar = (dL/d state)^T w (pressure
+// and sound speed: the state fields the inviscid flux reads). Gather form, no
+// atomics: cell c visits its six faces, evaluates each face flux with forward
+// dual numbers seeded on c's own inputs (conserved variables, through the
+// primitives u = m / rho, plus p and c; a boundary face's ghost follows its
+// owner's duals, a fixed state is constant) and contracts the flux
+// derivatives with the face's adjoint weight sum_side sign w / V.
+template <int NS>
+__global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __restrict__ q,
+                                                   const ReactiveTransportState* __restrict__ st,
+                                                   const double* __restrict__ w, double* __restrict__ qBar,
+                                                   ReactiveTransportState* __restrict__ stateBar) {
+    constexpr int N = NS + 6;
+    using D = Dual<N>;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        CellData C;
+        loadCell<NS>(v, q, st, c, C, true);
+        CellT<D> Cd = asCell<NS, D>(C);
+        D rho(0.0);
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) Cd.q[kk] = D::seed(C.q[kk], kk);
+#pragma unroll
+        for (int kk = 0; kk < NS; ++kk) rho += Cd.q[kk];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Cd.u[a] = Cd.q[NS + a] / rho;
+        Cd.p = D::seed(C.p, NS + 4);
+        Cd.c = D::seed(C.c, NS + 5);
+        const double ivc = v.invV[c];
+        double acc[N];
+#pragma unroll
+        for (int t = 0; t < N; ++t) acc[t] = 0;
+        bool bad = false;
+#pragma unroll 1
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            const int axis = s >> 1;
+            D F[NS + 4];
+            double W[NS + 4];
+            if (interior) {
+                const size_t nb = neighbourOf(v, s, c);
+                CellData Nc;
+                loadCell<NS>(v, q, st, nb, Nc, true);
+                const CellT<D> Nd = asCell<NS, D>(Nc);
+                const double ivn = v.invV[nb];
+                if (s & 1) {  // c owns the face
+                    faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Cd, Nd, nullptr,
+                                        nullptr, D(0.0), D(0.0), F, bad);
+#pragma unroll
+                    for (int kk = 0; kk < NS + 4; ++kk)
+                        W[kk] = w[size_t(kk) * v.cells + nb] * ivn - w[size_t(kk) * v.cells + c] * ivc;
+                } else {
+                    faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Nd, Cd, nullptr,
+                                        nullptr, D(0.0), D(0.0), F, bad);
+#pragma unroll
+                    for (int kk = 0; kk < NS + 4; ++kk)
+                        W[kk] = w[size_t(kk) * v.cells + c] * ivc - w[size_t(kk) * v.cells + nb] * ivn;
+                }
+            } else {
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                CellT<D> Rt;
+                if (f.kind == 3) {
+                    CellData Fx;
+                    loadCell<NS>(v, q, st, v.cells + size_t(f.fixed), Fx, true);
+                    Rt = asCell<NS, D>(Fx);
+                } else {
+                    Rt = Cd;
+                    if (f.kind == 1) {
+                        Rt.u[axis] = Cd.u[axis] - D(2.0) * Cd.u[axis];
+                        Rt.q[NS + axis] = Cd.q[NS + axis] - D(2.0) * Cd.q[NS + axis];
+                    }
+                }
+                faceFluxCart<NS, D>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
+                                    Cd, Rt, nullptr, nullptr, D(0.0), D(0.0), F, bad);
+#pragma unroll
+                for (int kk = 0; kk < NS + 4; ++kk) W[kk] = -w[size_t(kk) * v.cells + c] * ivc;
+            }
+#pragma unroll
+            for (int kk = 0; kk < NS + 4; ++kk)
+#pragma unroll
+                for (int t = 0; t < N; ++t) acc[t] += W[kk] * F[kk].d[t];
+        }
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) qBar[size_t(kk) * v.cells + c] = acc[kk];
+        stateBar[c] = ReactiveTransportState{acc[NS + 4], 0.0, 0.0, 0.0, acc[NS + 5], 0.0, 0.0};
     }
 }
 

@@ -25,7 +25,7 @@
 
 // Linkage of the flash-level routines (see RB200_EOS_FN).
 #ifndef RB200_FLASH_FN
-#define RB200_FLASH_FN __noinline__
+#define RB200_FLASH_FN static __noinline__
 #endif
 
 namespace rb200 {

@@ -20,7 +20,7 @@
 // different solver states side by side, and with every call site expanded the
 // code no longer fits the instruction cache.
 #ifndef RB200_EOS_FN
-#define RB200_EOS_FN __noinline__
+#define RB200_EOS_FN static __noinline__
 #endif
 
 namespace rb200 {

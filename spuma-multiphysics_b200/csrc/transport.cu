@@ -536,6 +536,20 @@ struct Transport {
         if (mixed) launchBoxStepT(state, cfl, maximumStep, result, gradF, nutF, s);
         else launchBoxStepT(state, cfl, maximumStep, result, v.grad, v.nut, s);
     }
+    template <int NS> struct RateVjpK {
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* w,
+                        double* qBar, ReactiveTransportState* stateBar, cudaStream_t s) {
+            cartRateVjp<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, w, qBar, stateBar);
+        }
+    };
+    void launchRateVjp(const double* q, const ReactiveTransportState* state, const double* w, double* qBar,
+                       ReactiveTransportState* stateBar, cudaStream_t s) {
+        require(structured, "The rate VJP needs the structured Cartesian path (reactive_transport_structured_v3)");
+        require(cfg.viscosity == 0 && cfg.conductivity == 0 && !v.wale,
+                "The rate VJP covers the inviscid operator (viscosity 0, conductivity 0, no WALE)");
+        launchPrimitives(q, s);
+        bySpecies<RateVjpK>(boxView(), q, state, w, qBar, stateBar, s);
+    }
     // Mixed precision of the structured path: FP32 gradients, WALE and face
     // fluxes, compensated per-cell sums, FP64 conserved state and update.
     void setMixed(bool on) {

@@ -18,6 +18,8 @@ the geometric a_ij mixing rule).
 import ctypes as C
 import math
 
+import numpy as np
+
 from ._abi import HemModel
 
 GAS_CONSTANT = 8314.46261815324  # J/(kmol K), CODATA 2018
@@ -125,3 +127,45 @@ def pure_model(sp=N2O, controls=N2O_FLASH, analytic_jacobian=1, scalar_recovery=
 
 def model_bytes(model):
     return bytes(C.string_at(C.addressof(model), C.sizeof(model)))
+
+
+def gas_table(species=(N2O, N2)):
+    """ReactiveB200Table image (the HEM model image's gas-table layout) of an
+    ideal-gas mixture; the ideal-gas closure reads the NASA regions and W."""
+    from ._abi import Table
+    t = Table()
+    _fill_table(t, list(species))
+    return bytes(C.string_at(C.addressof(t), C.sizeof(t)))
+
+
+def nasa_region(sp, T):
+    """Index of the NASA region of species sp that holds temperature T (the
+    device rule: a NASA9 region starts at its lower bound inclusive)."""
+    r = 0
+    for j in range(1, len(sp["nasa9"])):
+        if T >= sp["ranges"][j]:
+            r = j
+    return r
+
+
+def ideal_energy(sp, T, xp=np):
+    """Ideal-gas e = h - R T per mass [J/kg] of species sp at temperature T
+    (array of one NASA region, or a torch tensor with xp=torch)."""
+    r = GAS_CONSTANT / sp["W"]
+    region = nasa_region(sp, float(xp.max(T)) if xp is np else float(T.detach().max()))
+    a = sp["nasa9"][region]
+    iT = 1 / T
+    lT = xp.log(T)
+    hRT = (-a[0] * iT * iT + lT * a[1] * iT + a[2] + .5 * a[3] * T + a[4] * T * T / 3.0
+           + .25 * a[5] * T ** 3 + .2 * a[6] * T ** 4 + a[7] * iT)
+    return r * T * (hRT - 1)
+
+
+def ideal_cv(sp, T, xp=np):
+    """Ideal-gas cv = cp - R per mass [J/(kg K)] of species sp (one NASA region)."""
+    r = GAS_CONSTANT / sp["W"]
+    region = nasa_region(sp, float(xp.max(T)) if xp is np else float(T.detach().max()))
+    a = sp["nasa9"][region]
+    iT = 1 / T
+    cpR = a[0] * iT * iT + a[1] * iT + a[2] + a[3] * T + a[4] * T * T + a[5] * T ** 3 + a[6] * T ** 4
+    return r * (cpR - 1)
