@@ -435,6 +435,9 @@ def run_ours(args, rank, world):
                      "achieved": value * 1e6 * bytes_per_cell_step / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": value * 1e6 * bytes_per_cell_step / 1e9 / hbm,
                      "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback"}
+    adjoint = None if args.skip_adjoint else {
+        "hem": hem_adjoint_run(flow, n, steps=10, every=10),
+        "ideal_gas_blast_64": adjoint_run(64, steps=50, every=10, probes=0)}
     cpu = None
     if rank == 0 and not args.skip_cpu:
         cpu = cpu_reference(args, seconds_hint=20)
@@ -450,6 +453,7 @@ def run_ours(args, rank, world):
             "plain_fp64": {"ms_per_step": plain_ms, "value": world * cells / (plain_ms * 1e-3) / 1e6 if plain_ms
                            else None, "form": "FP64, kernels launched one by one, flash one thread per cell "
                                                "running the whole candidate search (no work queue, no pruning)"},
+            "adjoint": adjoint,
             "e2e": e2e, "roofline": roofline, "roofline_step_hbm": step_roofline, "cpu_baseline": cpu,
             "clocks": clock, "gpu_launches": launches_per_step * args.steps,
             "fp64_peak_tflops": fp64, "setup_s": setup_s}
@@ -555,6 +559,129 @@ def run_flash_batch(args):
             "clocks": clocks.summary(), "generation_s": gen_s}
 
 
+def hem_adjoint_run(flow, n, steps=10, every=10):
+    """The adjoint of the last `steps` steps of the 160^3 HEM case (config 5):
+    from the flow's current state, `steps` FP64 SSPRK2 + HEM steps recorded
+    with checkpoints every `every` steps, loss = N2O mass in the off-centre
+    sub-box [n/2, 3n/4) x [n/4, n/2) x [n/4, n/2), gradient with respect to the
+    state `steps` steps earlier by the hand-written adjoint (transport VJP with
+    viscous/WALE terms, flash by the implicit function theorem). Forward alone
+    and forward + adjoint timed with CUDA events."""
+    import torch
+    from spuma_multiphysics_b200.adjoint import HemStep, hem_rollout
+    stepper = HemStep(flow)
+    q0, s0 = flow.qn.clone(), flow.sn.clone()
+    k, j, i = np.indices((n, n, n))
+    sub = ((i >= n // 2) & (i < 3 * n // 4) & (j >= n // 4) & (j < n // 2) & (k >= n // 4) & (k < n // 2)).ravel()
+    weight = torch.zeros_like(q0)
+    weight[0, :flow.cells] = torch.from_numpy(sub.astype(np.float64) * (0.08 / n) ** 3).cuda()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    with torch.no_grad():
+        ev[0].record()
+        hem_rollout(stepper, q0, s0, steps, DT, every)
+        ev[1].record()
+    qg = q0.clone().requires_grad_(True)
+    ev[2].record()
+    out, _ = hem_rollout(stepper, qg, s0, steps, DT, every)
+    (grad,) = torch.autograd.grad((out * weight).sum(), qg)
+    ev[3].record()
+    torch.cuda.synchronize()
+    stepper.check()
+    fwd, both = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    return {"workload": f"adjoint of the last {steps} steps of the {n}^3 HEM case (viscous + WALE, flash by IFT), "
+                        f"checkpoints every {every}",
+            "forward_ms_per_step": fwd / steps, "forward_plus_adjoint_ms_per_step": both / steps,
+            "adjoint_ms_per_step": (both - fwd) / steps, "adjoint_over_forward": (both - fwd) / fwd,
+            "gradient_norm": float(grad.norm().item())}
+
+
+def adjoint_run(n=64, steps=50, every=10, probes=0, seed=11):
+    """The two-species ideal-gas blast box (N2O sphere at 10 bar in N2 at 1 bar,
+    300 K, +-0.5% density noise, dx = 1 mm, transmissive sides), `steps` fixed
+    SSPRK2 steps (dt = 0.3 x the initial CFL step), loss = N2O mass in the
+    off-centre 16^3 sub-box [40,56) x [24,40) x [24,40) (scaled to n). The
+    gradient of the loss with respect to the initial density field and the
+    driver pressure by the hand-written adjoint with checkpoints every `every`
+    steps; timings of the forward alone and of forward + adjoint; with probes >
+    0, central differences (h = 1e-6 relative) on that many random cells within
+    the sub-box's domain of dependence and on the driver pressure."""
+    import torch
+    load_package()
+    from spuma_multiphysics_b200 import cases
+    from spuma_multiphysics_b200.adjoint import IdealGasBox, rollout
+    spec = cases.blast_box(n, edge=n * 1e-3, radius=n * 0.25e-3)
+    box = IdealGasBox(spec["faces"], spec["volume"], spec["species"])
+    rho0 = torch.from_numpy(spec["rho0"]).cuda()
+    p_drive = torch.tensor(spec["p_drive"], dtype=torch.float64, device="cuda")
+    dt = .3 * box.stable_dt(cases.blast_initial(spec, rho0, p_drive, xp=torch))
+    lo, hi = int(n * 40 / 64), int(n * 56 / 64)
+    lo2, hi2 = int(n * 24 / 64), int(n * 40 / 64)
+    k, j, i = np.indices((n, n, n))
+    sub = ((i >= lo) & (i < hi) & (j >= lo2) & (j < hi2) & (k >= lo2) & (k < hi2)).ravel()
+    mask = torch.from_numpy(sub.astype(np.float64)).cuda() * box.volume
+
+    def loss(r, p):
+        return (rollout(box, cases.blast_initial(spec, r, p, xp=torch), steps, dt, every)[0] * mask).sum()
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    with torch.no_grad():
+        loss(rho0, p_drive)  # warm-up
+        ev[0].record()
+        J = loss(rho0, p_drive)
+        ev[1].record()
+    r = rho0.clone().requires_grad_(True)
+    p = p_drive.clone().requires_grad_(True)
+    ev[2].record()
+    Jg = loss(r, p)
+    ev[3].record()
+    g_rho, g_p = torch.autograd.grad(Jg, (r, p))
+    ev[4].record()
+    torch.cuda.synchronize()
+    box.check()
+    fwd = ev[0].elapsed_time(ev[1])
+    rec, bwd = ev[2].elapsed_time(ev[3]), ev[3].elapsed_time(ev[4])
+    out = {"workload": f"ideal-gas N2O/N2 blast box {n}^3, {steps} SSPRK2 steps, checkpoints every {every}",
+           "dt": dt, "loss": J.item(), "forward_ms_per_step": fwd / steps,
+           "recorded_forward_ms_per_step": rec / steps, "adjoint_ms_per_step": bwd / steps,
+           "adjoint_over_forward": bwd / fwd, "forward_plus_adjoint_over_forward": (rec + bwd) / fwd,
+           "dJ_dp_drive": g_p.item()}
+    if probes:
+        rng = np.random.default_rng(seed)
+        reach = int(np.ceil(steps * .3 * 1.2)) + 1  # CFL 0.3: at most ~0.4 cells per step either way
+        near = np.flatnonzero((i >= lo - reach) & (i < hi + reach) & (j >= lo2 - reach) & (j < hi2 + reach)
+                              & (k >= lo2 - reach) & (k < hi2 + reach))
+        cells = rng.choice(near, probes, replace=False)
+        fd = []
+        with torch.no_grad():
+            for c in cells:
+                h = 1e-6 * float(rho0[c])
+                rp, rm = rho0.clone(), rho0.clone()
+                rp[c] += h
+                rm[c] -= h
+                fd.append((loss(rp, p_drive) - loss(rm, p_drive)).item() / (2 * h))
+            hp = 1e-6 * spec["p_drive"]
+            fd_p = (loss(rho0, p_drive + hp) - loss(rho0, p_drive - hp)).item() / (2 * hp)
+        box.check()
+        g = g_rho[torch.as_tensor(cells)].cpu().numpy()
+        fd = np.array(fd)
+        big = np.abs(fd) > 1e-3 * np.abs(fd).max()
+        out["finite_differences"] = {
+            "probes": int(probes), "h": "1e-6 relative", "max_abs_gradient": float(np.abs(fd).max()),
+            "scaled_error": float(np.max(np.abs(g - fd)) / np.abs(fd).max()),
+            "relative_error_median": float(np.median(np.abs(g - fd)[big] / np.abs(fd[big]))),
+            "relative_error_max": float(np.max(np.abs(g - fd)[big] / np.abs(fd[big]))),
+            "p_drive_relative_error": abs(g_p.item() - fd_p) / abs(fd_p)}
+    box.close()
+    return out
+
+
+def run_adjoint_check(args):
+    line = {"metric": "adjoint gradient check and adjoint/forward time", "unit": "relative",
+            "data": "synthetic (seeded ideal-gas blast box)",
+            **adjoint_run(args.adjoint_check, steps=args.adjoint_steps, every=10, probes=32)}
+    return line
+
+
 def run_precision_study(args):
     """The 80^3 impingement case (viscosity, conduction, WALE) run in FP64 and in
     the mixed form side by side for --study-steps steps from the same state; the
@@ -612,6 +739,10 @@ def main():
     p.add_argument("--precision-study", type=int, default=0,
                    help="run FP64 and mixed side by side on this cube size and report per-field errors")
     p.add_argument("--study-steps", type=int, default=20)
+    p.add_argument("--adjoint-check", type=int, default=0,
+                   help="run the ideal-gas blast box adjoint check on this cube size")
+    p.add_argument("--adjoint-steps", type=int, default=50)
+    p.add_argument("--skip-adjoint", action="store_true")
     args = p.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -626,6 +757,8 @@ def main():
             line = run_flash_batch(args)
         elif args.precision_study:
             line = run_precision_study(args)
+        elif args.adjoint_check:
+            line = run_adjoint_check(args)
         else:
             line = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
     finally:

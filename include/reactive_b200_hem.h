@@ -63,6 +63,20 @@ int reactive_gpu_hem_run_device_v3(void* hem, const double* conserved, size_t st
 int reactive_gpu_hem_run_counters_v3(void* hem, ReactiveGpuHemProfileV1* profile, void* stream, char* error,
     size_t errorSize);
 
+/* Vector-Jacobian product of the flash (no reference counterpart; the
+ * reference's tangent precedent is its host IFT TangentContext,
+ * src/reactiveThermo/reactiveDirectional.inc:81-106). At the converged states
+ * `state` of cells with conserved SoA rows `conserved` (pure fluid, variables
+ * 5), adds to conservedBar (SoA, stride barStride) the adjoint of the
+ * transport-state outputs {p, T, rho, cv, frozen sound, gas mass} given in
+ * transportBar, by the implicit function theorem on the converged candidate's
+ * residual (two-phase (ln p, ln T, beta) or a single-phase (ln p, ln T)
+ * partition). Cells whose derivative could not be formed add nothing and
+ * increment *failed (device counter, may be NULL). Asynchronous on `stream`. */
+int reactive_gpu_hem_vjp_device_v3(void* hem, const double* conserved, size_t stride, size_t count,
+    size_t variables, const ReactiveThermoState* state, const ReactiveTransportState* transportBar,
+    double* conservedBar, size_t barStride, unsigned* failed, void* stream, char* error, size_t errorSize);
+
 /* Flash without any allocation. No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc when they need a flash, for example a solver
  * whose own memory pool owns the whole device and forbids other allocations. It

@@ -146,10 +146,13 @@ int reactive_transport_precision_v3(void* transport, int request, int* active);
  * per-cell right-hand side L that stage_device_v3 applies (q SoA with the fixed
  * tail, stride cells+fixed) and w its adjoint (SoA, stride cells), writes
  * qBar = (dL/dq)^T w (SoA, stride cells) and stateBar = (dL/dstate)^T w per cell
- * (the p and sound fields; the inviscid flux reads no other state field).
- * Structured path, inviscid operator (viscosity 0, conductivity 0, no WALE);
- * the derivative of the FP64 operator, with the HLL wave-speed switches taken
- * piecewise. Asynchronous on `stream`. */
+ * (the p, T, rho and sound fields the flux reads; the others are zero).
+ * Structured path, the whole operator: HLL (wave-speed switches taken
+ * piecewise), viscous/WALE traction through the cells' velocity gradients and
+ * eddy viscosities (with their own adjoints carried back through the WALE
+ * relation and the Green-Gauss gradient to the neighbours' velocities), and
+ * conduction. The derivative of the FP64 operator. The first call on a viscous
+ * handle allocates its scratch. Asynchronous on `stream`. */
 int reactive_transport_rate_vjp_v3(void* transport, const double* q, const ReactiveTransportState* state,
     const double* w, double* qBar, ReactiveTransportState* stateBar, void* stream);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading

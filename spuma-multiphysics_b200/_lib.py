@@ -59,6 +59,8 @@ HEM = {
     "run_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, _v, _v, C.c_int, _v, C.c_char_p,
                        C.c_size_t], C.c_int),
     "run_counters_v3": ([_v, C.POINTER(A.HemProfile), _v, C.c_char_p, C.c_size_t], C.c_int),
+    "vjp_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, C.c_size_t, _v, _v, C.c_char_p,
+                       C.c_size_t], C.c_int),
 }
 
 _lib = None

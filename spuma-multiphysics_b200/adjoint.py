@@ -209,3 +209,163 @@ def rollout(box, q0, steps, dt, checkpoint_every=10):
             q = _segment(q, box, dt, n)
         done += n
     return q
+
+
+# --------------------------------------------------------------------------
+# The HEM step (pure-fluid PR flash, structured viscous/WALE transport)
+
+
+def _compact(states_u8, cells):
+    """Transport states (cells, 7) of thermo states (uint8 view of cells x 176 B):
+    p, T, rho, cv, frozen sound, gas mass, 0 (the reference's compact,
+    ReactiveFoam.C:419-420)."""
+    s = states_u8.view(torch.float64).view(cells, 22)
+    tr = torch.zeros((cells, 7), dtype=torch.float64, device=states_u8.device)
+    tr[:, 0:3] = s[:, 0:3]
+    tr[:, 3] = s[:, 20]
+    tr[:, 4] = s[:, 5]
+    tr[:, 5] = s[:, 18]
+    return tr
+
+
+class HemStep:
+    """Functional SSPRK2 + HEM steps over a `flow.Flow`'s transport and HEM
+    handles (FP64, structured path), and their adjoint:
+
+        s_n = flash(q_n) (the previous step's recovery), tr = compact(s)
+        q_1 = q_n + dt L(q_n, tr_n);  s_1 = flash(q_1; seed s_n)
+        q_n+1 = q_n/2 + (q_1 + dt L(q_1, tr_1))/2;  s_n+1 = flash(q_n+1; seed s_n)
+
+    Conserved tensors are SoA (nv, cells + fixed) with the flow's fixed tail."""
+
+    def __init__(self, flow):
+        self.flow = flow
+        self.lib = flow.lib
+        self.cells, self.fixed, self.nv = flow.cells, flow.fixed, flow.nv
+        self.fixed_tr = flow.tr[self.cells:].clone()
+        self.failed = torch.zeros(1, dtype=torch.int32, device=flow.device)
+        self.err = C.create_string_buffer(1024)
+        if flow.precision != "fp64":
+            raise AdjointError("the adjoint differentiates the FP64 operator: use a precision='fp64' flow")
+
+    def _check(self, rc):
+        if rc:
+            raise AdjointError(self.lib.reactive_transport_error(self.flow.transport).decode())
+
+    def _tr_all(self, tr_cells):
+        return torch.cat([tr_cells, self.fixed_tr], 0).contiguous()
+
+    def _flash(self, q, seed):
+        f = self.flow
+        s = torch.cuda.current_stream().cuda_stream
+        out = torch.empty_like(seed)
+        tr = torch.empty((self.cells + self.fixed, 7), dtype=torch.float64, device=f.device)
+        tr[self.cells:] = self.fixed_tr
+        f.hem.run_device(q, q.shape[1], self.cells, self.nv, seed, out, tr, f.success, s)
+        self.failed += (f.success == 0).sum().to(torch.int32)
+        return out, tr
+
+    def _stage(self, q_in, q_out, tr, dt, stage):
+        f = self.flow
+        self._check(self.lib.reactive_transport_stage_device_v3(f.transport, q_in.data_ptr(), q_out.data_ptr(),
+                                                               tr.data_ptr(), dt, stage, None,
+                                                               torch.cuda.current_stream().cuda_stream))
+
+    def recover(self, q, seed):
+        """The recovered states of q (the flash seeded by `seed`): the s_n a
+        rollout from q must start with."""
+        states, _ = self._flash(q.contiguous(), seed)
+        return states
+
+    def forward_step(self, q_n, s_n, dt):
+        q_n = q_n.contiguous()
+        tr_n = self._tr_all(_compact(s_n, self.cells))
+        q_1 = q_n.clone()
+        self._stage(q_n, q_1, tr_n, dt, 0)
+        s_1, tr_1 = self._flash(q_1, s_n)
+        q_next = q_n.clone()
+        self._stage(q_1, q_next, tr_1, dt, 1)
+        s_next, _ = self._flash(q_next, s_n)
+        return q_next, s_next, (q_n, s_n, tr_n, q_1, s_1, tr_1)
+
+    def rate_vjp(self, q, tr, w):
+        f = self.flow
+        q_bar = torch.empty((self.nv, self.cells), dtype=torch.float64, device=f.device)
+        tr_bar = torch.empty((self.cells, 7), dtype=torch.float64, device=f.device)
+        self._check(self.lib.reactive_transport_rate_vjp_v3(f.transport, q.data_ptr(), tr.data_ptr(),
+                                                            w.contiguous().data_ptr(), q_bar.data_ptr(),
+                                                            tr_bar.data_ptr(), torch.cuda.current_stream().cuda_stream))
+        return q_bar, tr_bar
+
+    def hem_vjp(self, q, states, tr_bar, q_bar):
+        f = self.flow
+        rc = self.lib.reactive_gpu_hem_vjp_device_v3(f.hem.handle, q.data_ptr(), q.shape[1], self.cells, self.nv,
+                                                     states.data_ptr(), tr_bar.data_ptr(), q_bar.data_ptr(),
+                                                     q_bar.shape[1], self.failed.data_ptr(),
+                                                     torch.cuda.current_stream().cuda_stream, self.err, len(self.err))
+        if rc:
+            raise AdjointError(self.err.value.decode())
+        return q_bar
+
+    def step_vjp(self, lam, saved, dt):
+        q_n, s_n, tr_n, q_1, s_1, tr_1 = saved
+        lam = lam.contiguous()
+        q_bar1, tr_bar1 = self.rate_vjp(q_1, tr_1, (.5 * dt) * lam)
+        q_bar1 += .5 * lam
+        self.hem_vjp(q_1, s_1, tr_bar1, q_bar1)
+        q_barn, tr_barn = self.rate_vjp(q_n, tr_n, dt * q_bar1)
+        q_barn += .5 * lam + q_bar1
+        self.hem_vjp(q_n, s_n, tr_barn, q_barn)
+        return q_barn
+
+    def check(self):
+        """Every flash and every flash derivative since the last check succeeded (synchronises)."""
+        n = int(self.failed.item())
+        self.failed.zero_()
+        if n:
+            raise AdjointError(f"{n} cell flashes or flash derivatives failed")
+
+
+class HemSSPRK2Step(torch.autograd.Function):
+    """(q_n+1, s_n+1) = step(q_n, s_n) with the hand-written adjoint for q. The
+    states s are the step-start recoveries (a function of q through the flash);
+    they carry no gradient of their own."""
+
+    @staticmethod
+    def forward(ctx, q, s, stepper, dt):
+        q_next, s_next, saved = stepper.forward_step(q.detach(), s, dt)
+        ctx.stepper, ctx.dt = stepper, dt
+        ctx.save_for_backward(*saved)
+        ctx.mark_non_differentiable(s_next)
+        return q_next, s_next
+
+    @staticmethod
+    def backward(ctx, lam, _s_bar):
+        cells = ctx.stepper.cells
+        q_bar = ctx.stepper.step_vjp(lam[:, :cells], ctx.saved_tensors, ctx.dt)
+        # the fixed tail is constant: its adjoint is dropped
+        full = torch.zeros_like(lam)
+        full[:, :cells] = q_bar
+        return full, None, None, None
+
+
+def _hem_segment(q, s, stepper, dt, steps):
+    for _ in range(steps):
+        q, s = HemSSPRK2Step.apply(q, s, stepper, dt)
+    return q, s
+
+
+def hem_rollout(stepper, q0, s0, steps, dt, checkpoint_every=10):
+    """`steps` HEM steps from (q0, s0), s0 the recovery of q0
+    (`HemStep.recover`); with autograd recording, segments of `checkpoint_every`
+    run under torch.utils.checkpoint (recomputed in the reverse pass)."""
+    q, s = q0, s0
+    done = 0
+    while done < steps:
+        n = min(checkpoint_every, steps - done)
+        if torch.is_grad_enabled() and q.requires_grad:
+            q, s = torch.utils.checkpoint.checkpoint(_hem_segment, q, s, stepper, dt, n, use_reentrant=False)
+        else:
+            q, s = _hem_segment(q, s, stepper, dt, n)
+        done += n
+    return q, s

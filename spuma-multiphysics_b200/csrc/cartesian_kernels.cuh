@@ -495,37 +495,57 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
     }
 }
 
-// Vector-Jacobian product of the inviscid rate operator L(q, state) of the
-// structured box: given adjoint weights w (SoA nv x cells, the adjoint of each
-// cell's rate), qBar = (dL/dq)^T w and stateBar = (dL/d state)^T w (pressure
-// and sound speed: the state fields the inviscid flux reads). Gather form, no
-// atomics: cell c visits its six faces, evaluates each face flux with forward
-// dual numbers seeded on c's own inputs (conserved variables, through the
-// primitives u = m / rho, plus p and c; a boundary face's ghost follows its
-// owner's duals, a fixed state is constant) and contracts the flux
-// derivatives with the face's adjoint weight sum_side sign w / V.
-template <int NS>
+// Vector-Jacobian product of the rate operator L of the structured box. Given
+// adjoint weights w (SoA nv x cells, the adjoint of each cell's rate), a cell c
+// visits its six faces and evaluates each face flux in forward dual numbers
+// seeded on c's own inputs, then contracts the flux derivatives with the face's
+// adjoint weight sum_side sign w / V. Gather form, no atomics; the HLL
+// wave-speed switches are differentiated piecewise.
+//   MODE 0: seeds on c's conserved variables (and through u = m / rho on its
+//           velocity), p, sound, T and the state density; writes qBar (the
+//           direct part) and stateBar {p, T, rho, 0, sound, 0, 0}.
+//   MODE 1: seeds on c's velocity gradient (9) and WALE eddy viscosity; writes
+//           gBar (SoA 9 x cells) and nutBar. Only for the viscous operator.
+// A boundary face's ghost follows its owner's duals (slip: mirrored), a fixed
+// state is constant; a boundary face uses the owner's gradient and eddy
+// viscosity on both sides, as the forward does.
+template <int NS, int MODE>
 __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __restrict__ q,
                                                    const ReactiveTransportState* __restrict__ st,
+                                                   const double* __restrict__ grad, const double* __restrict__ nut,
                                                    const double* __restrict__ w, double* __restrict__ qBar,
-                                                   ReactiveTransportState* __restrict__ stateBar) {
-    constexpr int N = NS + 6;
+                                                   ReactiveTransportState* __restrict__ stateBar,
+                                                   double* __restrict__ gBar, double* __restrict__ nutBar) {
+    constexpr int N = MODE == 0 ? NS + 8 : 10;
     using D = Dual<N>;
+    const bool viscous = v.viscosity > 0 || v.wale;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
         loadCell<NS>(v, q, st, c, C, true);
         CellT<D> Cd = asCell<NS, D>(C);
-        D rho(0.0);
+        D gC[9], nutC(0.0);
 #pragma unroll
-        for (int kk = 0; kk < NS + 4; ++kk) Cd.q[kk] = D::seed(C.q[kk], kk);
+        for (int t = 0; t < 9; ++t) gC[t] = D(viscous ? grad[size_t(t) * v.cells + c] : 0.0);
+        if (v.wale) nutC = D(nut[c]);
+        if (MODE == 0) {
+            D rho(0.0);
 #pragma unroll
-        for (int kk = 0; kk < NS; ++kk) rho += Cd.q[kk];
+            for (int kk = 0; kk < NS + 4; ++kk) Cd.q[kk] = D::seed(C.q[kk], kk);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) Cd.u[a] = Cd.q[NS + a] / rho;
-        Cd.p = D::seed(C.p, NS + 4);
-        Cd.c = D::seed(C.c, NS + 5);
+            for (int kk = 0; kk < NS; ++kk) rho += Cd.q[kk];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Cd.u[a] = Cd.q[NS + a] / rho;
+            Cd.p = D::seed(C.p, NS + 4);
+            Cd.c = D::seed(C.c, NS + 5);
+            Cd.T = D::seed(C.T, NS + 6);
+            Cd.rho = D::seed(C.rho, NS + 7);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 9; ++t) gC[t] = D::seed(grad[size_t(t) * v.cells + c], t);
+            if (v.wale) nutC = D::seed(nut[c], 9);
+        }
         const double ivc = v.invV[c];
         double acc[N];
 #pragma unroll
@@ -544,16 +564,20 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
                 CellData Nc;
                 loadCell<NS>(v, q, st, nb, Nc, true);
                 const CellT<D> Nd = asCell<NS, D>(Nc);
+                D gN[9], nutN(0.0);
+#pragma unroll
+                for (int t = 0; t < 9; ++t) gN[t] = D(viscous ? grad[size_t(t) * v.cells + nb] : 0.0);
+                if (v.wale) nutN = D(nut[nb]);
                 const double ivn = v.invV[nb];
                 if (s & 1) {  // c owns the face
-                    faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Cd, Nd, nullptr,
-                                        nullptr, D(0.0), D(0.0), F, bad);
+                    faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Cd, Nd, gC, gN, nutC,
+                                        nutN, F, bad);
 #pragma unroll
                     for (int kk = 0; kk < NS + 4; ++kk)
                         W[kk] = w[size_t(kk) * v.cells + nb] * ivn - w[size_t(kk) * v.cells + c] * ivc;
                 } else {
-                    faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Nd, Cd, nullptr,
-                                        nullptr, D(0.0), D(0.0), F, bad);
+                    faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Nd, Cd, gN, gC, nutN,
+                                        nutC, F, bad);
 #pragma unroll
                     for (int kk = 0; kk < NS + 4; ++kk)
                         W[kk] = w[size_t(kk) * v.cells + c] * ivc - w[size_t(kk) * v.cells + nb] * ivn;
@@ -573,7 +597,7 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
                     }
                 }
                 faceFluxCart<NS, D>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
-                                    Cd, Rt, nullptr, nullptr, D(0.0), D(0.0), F, bad);
+                                    Cd, Rt, gC, gC, nutC, nutC, F, bad);
 #pragma unroll
                 for (int kk = 0; kk < NS + 4; ++kk) W[kk] = -w[size_t(kk) * v.cells + c] * ivc;
             }
@@ -582,9 +606,118 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
 #pragma unroll
                 for (int t = 0; t < N; ++t) acc[t] += W[kk] * F[kk].d[t];
         }
+        if (MODE == 0) {
 #pragma unroll
-        for (int kk = 0; kk < NS + 4; ++kk) qBar[size_t(kk) * v.cells + c] = acc[kk];
-        stateBar[c] = ReactiveTransportState{acc[NS + 4], 0.0, 0.0, 0.0, acc[NS + 5], 0.0, 0.0};
+            for (int kk = 0; kk < NS + 4; ++kk) qBar[size_t(kk) * v.cells + c] = acc[kk];
+            stateBar[c] = ReactiveTransportState{acc[NS + 4], acc[NS + 6], acc[NS + 7], 0.0, acc[NS + 5], 0.0, 0.0};
+        } else {
+#pragma unroll
+            for (int t = 0; t < 9; ++t) gBar[size_t(t) * v.cells + c] = acc[t];
+            if (nutBar) nutBar[c] = acc[9];
+        }
+    }
+}
+
+// gBar += nutBar * d nu_t / d g per cell (the WALE eddy viscosity of the cell's
+// gradient, the Nicoud-Ducros relation of wale.cuh written for duals:
+// nu_t = (Cw Delta)^2 |g|_max (Sd:Sd)^(3/2) / ((S:S)^(5/2) + (Sd:Sd)^(5/4))
+// with the invariants of g / |g|_max; zero where the forward gives zero).
+__global__ void cartWaleVjp(CartView v, const double* __restrict__ grad, const double* __restrict__ nutBar,
+                            double* __restrict__ gBar) {
+    using D = Dual<9>;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        const double nb = nutBar[c];
+        if (nb == 0) continue;
+        D g[9];
+        int largest = 0;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            g[t] = D::seed(grad[size_t(t) * v.cells + c], t);
+            if (::fabs(g[t].v) > ::fabs(g[largest].v)) largest = t;
+        }
+        const double delta = cbrt(1 / v.invV[c]);
+        if (g[largest].v == 0 || v.cw == 0 || delta == 0) continue;
+        D scale = fabs(g[largest]);
+        D h[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) h[t] = g[t] / scale;
+        D sq[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) sq[3 * a + b] = h[3 * a] * h[b] + h[3 * a + 1] * h[3 + b] + h[3 * a + 2] * h[6 + b];
+        const D trace = sq[0] + sq[4] + sq[8];
+        D ss(0.0), dd(0.0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const D sab = D(.5) * (h[3 * a + b] + h[3 * b + a]);
+                D dab = D(.5) * (sq[3 * a + b] + sq[3 * b + a]);
+                if (a == b) dab = dab - trace / D(3.0);
+                ss += sab * sab;
+                dd += dab * dab;
+            }
+        if (!(dd.v > 0)) continue;
+        const D rootD = sqrt(dd);
+        const D ratio = dd * rootD / (ss * ss * sqrt(ss) + dd * sqrt(rootD));
+        const D nutD = D(v.cw * delta * v.cw * delta) * scale * ratio;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) gBar[size_t(t) * v.cells + c] += nb * nutD.d[t];
+    }
+}
+
+// Transpose of the Green-Gauss gradient: uBar_c from the gradient adjoints of c
+// and of its neighbours (the face velocity of an internal face is the mean of
+// its two cells', a boundary face's is w u_c + (1 - w) u_ghost(u_c)), then
+// through u = m / rho into qBar (accumulated).
+template <int NS>
+__global__ void cartGradientVjp(CartView v, const double* __restrict__ q, const double* __restrict__ gBar,
+                                double* __restrict__ qBar) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        const double ivc = v.invV[c];
+        double uBar[3] = {0, 0, 0};
+#pragma unroll
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            const int axis = s >> 1;
+            if (interior) {
+                const size_t nb = neighbourOf(v, s, c);
+                // normal +e_axis; sign +1 for the face's owner (the lower cell)
+                const double sc = (s & 1) ? 1.0 : -1.0, sn = -sc;
+                const double area = v.area[axis];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    uBar[a] += .5 * (gBar[size_t(3 * a + axis) * v.cells + c] * sc * area * ivc
+                                     + gBar[size_t(3 * a + axis) * v.cells + nb] * sn * area * v.invV[nb]);
+            } else {
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                const double sgn = (s & 1) ? 1.0 : -1.0, wgt = f.ownerWeight;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    double du = wgt;  // d u_face[a] / d u_c[a]
+                    if (f.kind == 2) du = wgt + (1 - wgt);
+                    else if (f.kind == 1) du = wgt + (1 - wgt) * (a == axis ? -1.0 : 1.0);
+                    uBar[a] += gBar[size_t(3 * a + axis) * v.cells + c] * du * sgn * f.area * ivc;
+                }
+            }
+        }
+        double rho = 0;
+#pragma unroll
+        for (int kk = 0; kk < NS; ++kk) rho += q[size_t(kk) * v.all + c];
+        double rhoBar = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double m = q[size_t(NS + a) * v.all + c];
+            qBar[size_t(NS + a) * v.cells + c] += uBar[a] / rho;
+            rhoBar -= uBar[a] * m / (rho * rho);
+        }
+#pragma unroll
+        for (int kk = 0; kk < NS; ++kk) qBar[size_t(kk) * v.cells + c] += rhoBar;
     }
 }
 

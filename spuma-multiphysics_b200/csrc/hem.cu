@@ -252,6 +252,110 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passRestar
     flushCounts(n, totals);
 }
 
+// Vector-Jacobian product of the flash's transport-state outputs with respect
+// to the cell's conserved variables, by the implicit function theorem at the
+// converged candidate (no Newton unrolling). The candidate is read from the
+// state: two-phase (gas and liquid mass) with unknowns x = (ln p, ln T, beta)
+// and residual F = (V - 1, E - e, mu_l/RT - mu_g/RT); an all-gas or all-liquid
+// partition with x = (ln p, ln T) and F = (V - 1, E - e), where V and E are
+// the evaluation's volume and energy densities at the cell's density q and e is
+// the internal energy density of the conserved state. With y(x, q) = (p, T, cv,
+// frozen sound, gas mass) and ybar the adjoint of the outputs:
+//   F_x^T lambda = y_x^T ybar,  qbar_rho = ybar . y_q - lambda . F_q + rhobar,
+//   ebar = lambda_1 (dF_1/de = -1),
+// then e = E - |m|^2 / (2 rho) carries ebar to rho, m and E. The partials of
+// the closed-form evaluation are central differences (step 1e-6 in ln p, ln T
+// and beta, 1e-6 q in q).
+struct VjpPoint {
+    double F[3], y[5];
+};
+__device__ inline bool vjpPoint(const HemConst& C, int kind, double q, double e, const double x[3], VjpPoint& o,
+                                Counts& n) {
+    Eval v;
+    const double mass = kind == 2 ? x[2] * q : (kind == 1 ? q : 0.0);
+    if (!evaluate(C, q, mass, exp(x[0]), exp(x[1]), kind == 2, v, n)) return false;
+    o.F[0] = v.volume - 1;
+    o.F[1] = v.energy - e;
+    o.F[2] = kind == 2 ? v.muL - v.muG : 0.0;
+    o.y[0] = v.p; o.y[1] = v.T; o.y[2] = v.cv; o.y[3] = v.soundFrozen; o.y[4] = v.gasMass;
+    return fin(o.F[2]);
+}
+
+__global__ void hemStateVjp(const HemConst* __restrict__ Cp, const double* __restrict__ cons, size_t stride,
+                            size_t count, const ReactiveThermoState* __restrict__ state,
+                            const ReactiveTransportState* __restrict__ bar, double* qBar, size_t barStride,
+                            unsigned* failed) {
+    const HemConst& C = *Cp;
+    Counts n;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
+        const double q = cons[c], mx = cons[stride + c], my = cons[2 * stride + c], mz = cons[3 * stride + c],
+                     E = cons[4 * stride + c];
+        const double m2 = mx * mx + my * my + mz * mz;
+        const double e = E - .5 * m2 / q;
+        const ReactiveThermoState s = state[c];
+        const ReactiveTransportState b = bar[c];
+        const bool gas = s.gasMass > 0, liquid = s.liquidMass[0] > 0;
+        const int kind = gas && liquid ? 2 : (liquid ? 1 : 0);
+        const int nx = kind == 2 ? 3 : 2;
+        const double x[3] = {log(s.p), log(s.T), kind == 2 ? s.liquidMass[0] / q : 0.0};
+        const double ybar[5] = {b.p, b.T, b.cv, b.sound, b.gasMass};
+        double Fx[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, yx[5][3], Fq[3], yq[5];
+        bool ok = true;
+#pragma unroll 1
+        for (int i = 0; i < 4 && ok; ++i) {
+            if (i < 3 && i >= nx) continue;
+            const bool onQ = i == 3;
+            const double h = onQ ? 1e-6 * q : 1e-6;
+            double xp[3] = {x[0], x[1], x[2]}, xm[3] = {x[0], x[1], x[2]};
+            double qp = q, qm = q;
+            if (onQ) { qp += h; qm -= h; } else { xp[i] += h; xm[i] -= h; }
+            VjpPoint a, bm;
+            ok = vjpPoint(C, kind, qp, e, xp, a, n) && vjpPoint(C, kind, qm, e, xm, bm, n);
+            if (!ok) break;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const double d = (a.F[r] - bm.F[r]) / (2 * h);
+                if (onQ) Fq[r] = d; else Fx[r][i] = d;
+            }
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+                const double d = (a.y[r] - bm.y[r]) / (2 * h);
+                if (onQ) yq[r] = d; else yx[r][i] = d;
+            }
+        }
+        double lambda[3] = {0, 0, 0};
+        if (ok) {
+            // F_x^T lambda = y_x^T ybar
+            double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, rhs[3] = {0, 0, 0};
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) A[i][j] = i < nx && j < nx ? Fx[j][i] : 0.0;
+                double acc = 0;
+#pragma unroll
+                for (int r = 0; r < 5; ++r) acc += i < nx ? yx[r][i] * ybar[r] : 0.0;
+                rhs[i] = acc;
+            }
+            ok = solveSmall(A, rhs, nx, lambda);
+        }
+        if (!ok) {
+            if (failed) atomicAdd(failed, 1u);
+            continue;
+        }
+        double rhoBar = b.rho;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) rhoBar += ybar[r] * yq[r];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) rhoBar -= r < nx ? lambda[r] * Fq[r] : 0.0;
+        const double eBar = lambda[1];  // dF_1/de = -1 and F_x^T lambda carries y's e-dependence
+        qBar[c] += rhoBar + eBar * .5 * m2 / (q * q);
+        qBar[barStride + c] += -eBar * mx / q;
+        qBar[2 * barStride + c] += -eBar * my / q;
+        qBar[3 * barStride + c] += -eBar * mz / q;
+        qBar[4 * barStride + c] += eBar;
+    }
+}
+
 // Failed cells get their seed state back, so one contiguous copy of the
 // results leaves them unchanged in the caller's array.
 __global__ void keepFailed(const ReactiveThermoState* __restrict__ seed, const int* __restrict__ success,
@@ -709,6 +813,27 @@ int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t st
         rb200::check(cudaGetLastError(), "inputs");
         if (flags & 2) d.launchPerCell(count, seed, state, transport, success, s);
         else d.launchSearch(count, seed, state, transport, success, s);
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
+
+int reactive_gpu_hem_vjp_device_v3(void* raw, const double* conserved, size_t stride, size_t count, size_t variables,
+                                   const ReactiveThermoState* state, const ReactiveTransportState* transportBar,
+                                   double* conservedBar, size_t barStride, unsigned* failed, void* stream, char* error,
+                                   size_t size) {
+    try {
+        rb200::require(raw && conserved && state && transportBar && conservedBar && count && stride >= count
+                           && barStride >= count && variables == 5,
+                       "Invalid HEM VJP arguments (pure fluid: variables = 5)");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        auto s = static_cast<cudaStream_t>(stream);
+        rb200::hemStateVjp<<<rb200::gridFor(count, 128), 128, 0, s>>>(d.cst, conserved, stride, count, state,
+                                                                      transportBar, conservedBar, barStride, failed);
+        rb200::check(cudaGetLastError(), "hemStateVjp");
         return 0;
     } catch (const std::exception& e) {
         if (error && size) std::snprintf(error, size, "%s", e.what());

@@ -537,18 +537,34 @@ struct Transport {
         else launchBoxStepT(state, cfl, maximumStep, result, v.grad, v.nut, s);
     }
     template <int NS> struct RateVjpK {
-        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* w,
-                        double* qBar, ReactiveTransportState* stateBar, cudaStream_t s) {
-            cartRateVjp<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, w, qBar, stateBar);
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
+                        const double* nut, const double* w, double* qBar, ReactiveTransportState* stateBar,
+                        double* gBar, double* nutBar, bool viscous, cudaStream_t s) {
+            cartRateVjp<NS, 0><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, qBar, stateBar, nullptr,
+                                                                    nullptr);
+            if (!viscous) return;
+            cartRateVjp<NS, 1><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, nullptr, nullptr, gBar,
+                                                                    nutBar);
+            if (b.wale) cartWaleVjp<<<gridFor(b.cells, 128), 128, 0, s>>>(b, grad, nutBar, gBar);
+            cartGradientVjp<NS><<<gridFor(b.cells, 256), 256, 0, s>>>(b, q, gBar, qBar);
         }
     };
+    double* gradBar = nullptr;  // 9 x cells, rate VJP scratch
+    double* nutBarBuf = nullptr;
+    // (dL/dq)^T w and (dL/dstate)^T w of the FP64 structured operator at q: the
+    // forward gradient and eddy viscosity are rebuilt from q first.
     void launchRateVjp(const double* q, const ReactiveTransportState* state, const double* w, double* qBar,
                        ReactiveTransportState* stateBar, cudaStream_t s) {
         require(structured, "The rate VJP needs the structured Cartesian path (reactive_transport_structured_v3)");
-        require(cfg.viscosity == 0 && cfg.conductivity == 0 && !v.wale,
-                "The rate VJP covers the inviscid operator (viscosity 0, conductivity 0, no WALE)");
+        const bool viscous = cfg.viscosity > 0 || v.wale;
+        if (viscous && !gradBar) {
+            gradBar = arena.get<double>(product(cfg.cells, 9));
+            nutBarBuf = arena.get<double>(cfg.cells);
+        }
         launchPrimitives(q, s);
-        bySpecies<RateVjpK>(boxView(), q, state, w, qBar, stateBar, s);
+        if (viscous) launchBoxGradientsT(state, v.grad, v.nut, s);
+        bySpecies<RateVjpK>(boxView(), q, state, static_cast<const double*>(v.grad), static_cast<const double*>(v.nut),
+                            w, qBar, stateBar, gradBar, nutBarBuf, viscous, s);
     }
     // Mixed precision of the structured path: FP32 gradients, WALE and face
     // fluxes, compensated per-cell sums, FP64 conserved state and update.

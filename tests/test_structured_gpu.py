@@ -36,7 +36,9 @@ def box_case(dims, ns, side_kinds, viscous=False, conduction=False, seed=0):
     q[:, ns:ns + 3] = rho[:, None] * vel
     q[:, ns + 3] = rng.uniform(7.5e4, 1.25e5, nc) / .4 + .5 * rho * np.sum(vel ** 2, axis=1)
     n_fixed = int(np.any(faces_np["kind"] == 3))
+    # a fixed (inlet) state with its own velocity: no face's wave speeds tie
     fixed_q = np.ascontiguousarray(q[:1] * 1.013)
+    fixed_q[0, ns:ns + 3] += 7.0 * fixed_q[0, :ns].sum()
     fixed_states, fixed_y, fixed_h = T.ideal_states(fixed_q, ns)
     states, y, h = T.ideal_states(q, ns)
     arr = (A.Face * len(faces_np)).from_buffer_copy(faces_np.tobytes())
