@@ -354,6 +354,7 @@ def run_ours(args, rank, world):
     stats1 = pkg._abi.Stats()
     lib.reactive_transport_stats(mixed.transport, C.byref(stats1))
     launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
+    tuned = {"mixed": mixed.autotune(), "fp64": flow.autotune()}
     graph_ms, clocks = timed_graph_steps(mixed, True)
     fp64_ms, _ = timed_graph_steps(flow, False)
     # both runs took the same W + K steps from the same state
@@ -445,7 +446,8 @@ def run_ours(args, rank, world):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 state, f32 flux", "data": "synthetic (seeded N2O impingement initial state)",
-            "config": {**workload(n), "parallelism": f"{world} independent replicas (one per GPU)"},
+            "config": {**workload(n), "parallelism": f"{world} independent replicas (one per GPU)",
+                       "autotuned_launch_shapes": tuned},
             "form": "mixed precision (FP32 gradients/WALE/face fluxes, compensated sums into the FP64 state), "
                     "structured transport, work-queue FP64 flash, one CUDA graph per step",
             "mixed_field_error_vs_fp64": {"steps": args.warmup + args.steps, **mixed_errors},

@@ -63,6 +63,17 @@ int reactive_gpu_hem_run_device_v3(void* hem, const double* conserved, size_t st
 int reactive_gpu_hem_run_counters_v3(void* hem, ReactiveGpuHemProfileV1* profile, void* stream, char* error,
     size_t errorSize);
 
+/* Launch-shape autotuner of the work-queue flash (no reference counterpart).
+ * Runs the flash of `count` cells (conserved SoA rows with `stride`, seeds as
+ * run_device_v3 takes them) with 1, 2, ... up to the occupancy limit of
+ * resident queue blocks per SM, times each on `stream` and keeps the fastest
+ * for later launches (the results do not depend on it). Synchronous; allocates
+ * the host-path scratch on the first call; call it before capturing a graph.
+ * *blocksPerSm (may be NULL) receives the choice. */
+int reactive_gpu_hem_autotune_v3(void* hem, const double* conserved, size_t stride, size_t count,
+    size_t variables, const ReactiveThermoState* seed, void* stream, int* blocksPerSm, char* error,
+    size_t errorSize);
+
 /* Vector-Jacobian product of the flash (no reference counterpart; the
  * reference's tangent precedent is its host IFT TangentContext,
  * src/reactiveThermo/reactiveDirectional.inc:81-106). At the converged states

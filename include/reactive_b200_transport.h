@@ -155,6 +155,15 @@ int reactive_transport_precision_v3(void* transport, int request, int* active);
  * handle allocates its scratch. Asynchronous on `stream`. */
 int reactive_transport_rate_vjp_v3(void* transport, const double* q, const ReactiveTransportState* state,
     const double* w, double* qBar, ReactiveTransportState* stateBar, void* stream);
+/* Launch-shape autotuner of the structured path (no reference counterpart).
+ * Times the candidate block sizes of the stage (64, 96, 128 threads), gradient
+ * (64, 128, 256) and CFL (64, 128, 256) kernels on this handle's problem (q and
+ * state as stage_device_v3 takes them; neither is modified) and keeps the
+ * fastest for later launches; results do not depend on the choice. Synchronous;
+ * allocates one scratch copy of q on the first call; call it before capturing
+ * a graph. chosen (may be NULL) receives {stage, gradient, CFL} block sizes. */
+int reactive_transport_autotune_v3(void* transport, const double* q, const ReactiveTransportState* state,
+    void* stream, unsigned* chosen);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);

@@ -45,6 +45,7 @@ TRANSPORT = {
     "status_v3": ([_v, C.POINTER(C.c_uint), C.c_int, _v], C.c_int),
     "structured_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "precision_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "autotune_v3": ([_v, _v, _v, _v, C.POINTER(C.c_uint)], C.c_int),
     "rate_vjp_v3": ([_v, _v, _v, _v, _v, _v, _v], C.c_int),
 }
 
@@ -61,6 +62,8 @@ HEM = {
     "run_counters_v3": ([_v, C.POINTER(A.HemProfile), _v, C.c_char_p, C.c_size_t], C.c_int),
     "vjp_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, C.c_size_t, _v, _v, C.c_char_p,
                        C.c_size_t], C.c_int),
+    "autotune_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, C.POINTER(C.c_int), C.c_char_p,
+                     C.c_size_t], C.c_int),
 }
 
 _lib = None

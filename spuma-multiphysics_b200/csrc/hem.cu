@@ -841,6 +841,52 @@ int reactive_gpu_hem_vjp_device_v3(void* raw, const double* conserved, size_t st
     }
 }
 
+int reactive_gpu_hem_autotune_v3(void* raw, const double* conserved, size_t stride, size_t count, size_t variables,
+                                 const ReactiveThermoState* seed, void* stream, int* blocksPerSm, char* error,
+                                 size_t size) {
+    try {
+        rb200::require(raw && conserved && seed && count && stride >= count && variables >= 5,
+                       "Invalid HEM autotune arguments");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        rb200::require(count <= d.capacity, "CUDA HEM batch exceeds capacity");
+        rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+        auto s = static_cast<cudaStream_t>(stream);
+        int perSm = 0, sms = 0;
+        rb200::check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, rb200::passQueue, rb200::kPassThreads, 0),
+                     "occupancy");
+        rb200::check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device), "attribute");
+        d.ensureHostPath();  // scratch outputs of the timed runs
+        cudaEvent_t a, b;
+        rb200::check(cudaEventCreate(&a), "event");
+        rb200::check(cudaEventCreate(&b), "event");
+        float best = 1e30f;
+        int keep = std::max(1, perSm);
+        for (int k = 1; k <= std::max(1, perSm); ++k) {
+            d.passBlocks = k * sms;
+            for (int r = 0; r < 2; ++r) {  // the first run warms up
+                rb200::check(cudaEventRecord(a, s), "event");
+                rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1,
+                                                                                      seed, d.in);
+                d.launchSearch(count, seed, d.dout, nullptr, d.dsuccess, s);
+                rb200::check(cudaEventRecord(b, s), "event");
+                rb200::check(cudaEventSynchronize(b), "event");
+            }
+            float ms = 0;
+            rb200::check(cudaEventElapsedTime(&ms, a, b), "event");
+            if (ms < best) { best = ms; keep = k; }
+        }
+        d.passBlocks = keep * sms;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (blocksPerSm) *blocksPerSm = keep;
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
+
 int reactive_gpu_hem_run_counters_v3(void* raw, ReactiveGpuHemProfileV1* profile, void* stream, char* error,
                                      size_t size) {
     try {

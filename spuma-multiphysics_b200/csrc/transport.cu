@@ -462,26 +462,33 @@ struct Transport {
         }
         launched();
     }
+    // Block sizes of the structured kernels (reactive_transport_autotune_v3
+    // times the candidates on the handle's own problem and keeps the fastest;
+    // the results do not depend on them).
+    struct BoxLaunch {
+        unsigned rates = 128, gradients = 256, steps = 256;
+    } launch;
     template <int NS> struct GradientsK {
         template <class R>
         static void run(const CartView& b, const ReactiveTransportState* st, R* grad, R* nut, unsigned* error,
-                        cudaStream_t s) {
-            cartGradients<NS, R><<<gridFor(b.cells, 256), 256, 0, s>>>(b, st, grad, nut, error);
+                        unsigned block, cudaStream_t s) {
+            cartGradients<NS, R><<<gridFor(b.cells, block), block, 0, s>>>(b, st, grad, nut, error);
         }
     };
     template <int NS> struct RatesK {
         template <class R>
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                         const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
-                        cudaStream_t s) {
-            cartRates<NS, R><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error);
+                        unsigned block, cudaStream_t s) {
+            cartRates<NS, R><<<gridFor(b.cells, block), block, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt,
+                                                                     error);
         }
     };
     template <int NS> struct StepsK {
         template <class R>
         static void run(const CartView& b, const ReactiveTransportState* st, const R* nut, double cfl,
-                        double maximumStep, double* partial, unsigned blocks, cudaStream_t s) {
-            cartSteps<NS, R><<<blocks, 256, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
+                        double maximumStep, double* partial, unsigned blocks, unsigned block, cudaStream_t s) {
+            cartSteps<NS, R><<<blocks, block, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
         }
     };
     template <int NS> struct LedgerK {
@@ -494,7 +501,7 @@ struct Transport {
     // Gradient (+ WALE viscosity) of the structured box, when the operator needs it.
     template <class R> void launchBoxGradientsT(const ReactiveTransportState* state, R* grad, R* nut, cudaStream_t s) {
         if (!(v.wale || cfg.viscosity > 0)) return;
-        bySpecies<GradientsK>(boxView(), state, grad, nut, flags, s);
+        bySpecies<GradientsK>(boxView(), state, grad, nut, flags, launch.gradients, s);
         if (v.wale) {
             ++waleProfile.gradientBuilds;
             ++waleProfile.viscosityBuilds;
@@ -513,7 +520,7 @@ struct Transport {
             launched();
         }
         bySpecies<RatesK>(boxView(), qIn, state, static_cast<const R*>(grad), static_cast<const R*>(nut), qOut, v.all,
-                          stage == 0 ? 1 : 2, dt, flags, s);
+                          stage == 0 ? 1 : 2, dt, flags, launch.rates, s);
         ++deviceProfile.transportFaceLaunches;
     }
     template <class R>
@@ -521,7 +528,8 @@ struct Transport {
                         R* nut, cudaStream_t s) {
         if (v.wale) launchBoxGradientsT(state, grad, nut, s);
         const unsigned blocks = unsigned(reduceBlocks);
-        bySpecies<StepsK>(boxView(), state, static_cast<const R*>(nut), cfl, maximumStep, reduceScratch, blocks, s);
+        bySpecies<StepsK>(boxView(), state, static_cast<const R*>(nut), cfl, maximumStep, reduceScratch, blocks,
+                          launch.steps, s);
         ++deviceProfile.cflFaceLaunches;
         minimumReduce<<<1, 1024, 0, s>>>(reduceScratch, blocks, result);
         launched();
@@ -565,6 +573,53 @@ struct Transport {
         if (viscous) launchBoxGradientsT(state, v.grad, v.nut, s);
         bySpecies<RateVjpK>(boxView(), q, state, static_cast<const double*>(v.grad), static_cast<const double*>(v.nut),
                             w, qBar, stateBar, gradBar, nutBarBuf, viscous, s);
+    }
+    // Times each candidate block size on this handle's problem (q, state as
+    // the device stage entries take them) and keeps the fastest; synchronous.
+    void autotune(const double* q, const ReactiveTransportState* state, cudaStream_t s, unsigned* chosen) {
+        require(structured, "Autotuning covers the structured path (reactive_transport_structured_v3)");
+        double* out = arena.get<double>(product(v.all, cfg.variables));
+        check(cudaMemcpyAsync(out, q, product(v.all, cfg.variables) * sizeof(double), cudaMemcpyDeviceToDevice, s),
+              "copy");
+        cudaEvent_t a, b;
+        check(cudaEventCreate(&a), "event");
+        check(cudaEventCreate(&b), "event");
+        auto timeIt = [&](auto&& body) {
+            body();  // warm-up
+            float best = 1e30f;
+            for (int r = 0; r < 3; ++r) {
+                check(cudaEventRecord(a, s), "event");
+                body();
+                check(cudaEventRecord(b, s), "event");
+                check(cudaEventSynchronize(b), "event");
+                float ms = 0;
+                check(cudaEventElapsedTime(&ms, a, b), "event");
+                best = std::min(best, ms);
+            }
+            return best;
+        };
+        auto pick = [&](unsigned& slot, std::initializer_list<unsigned> candidates, auto&& body) {
+            float best = 1e30f;
+            unsigned keep = slot;
+            for (unsigned c : candidates) {
+                slot = c;
+                const float t = timeIt(body);
+                if (t < best) { best = t; keep = c; }
+            }
+            slot = keep;
+        };
+        launchPrimitives(q, s);
+        // candidates stay within each kernel's __launch_bounds__ (128 for the stage, 256 otherwise)
+        pick(launch.gradients, {64u, 128u, 256u}, [&] {
+            if (mixed) launchBoxGradientsT(state, gradF, nutF, s);
+            else launchBoxGradientsT(state, v.grad, v.nut, s);
+        });
+        pick(launch.rates, {64u, 96u, 128u}, [&] { launchBoxStage(q, out, state, 1e-30, 0, nullptr, s); });
+        pick(launch.steps, {64u, 128u, 256u}, [&] { launchBoxStep(state, .5, 1.0, reduceScratch + reduceBlocks, s); });
+        check(cudaEventDestroy(a), "event");
+        check(cudaEventDestroy(b), "event");
+        check(cudaStreamSynchronize(s), "sync");
+        if (chosen) { chosen[0] = launch.rates; chosen[1] = launch.gradients; chosen[2] = launch.steps; }
     }
     // Mixed precision of the structured path: FP32 gradients, WALE and face
     // fluxes, compensated per-cell sums, FP64 conserved state and update.

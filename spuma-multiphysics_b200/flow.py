@@ -148,6 +148,23 @@ class Flow:
         self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s,
                             per_cell)
 
+    def autotune(self):
+        """Choose the launch shapes of this flow's transport and flash kernels by
+        timing the candidates on its current state (synchronous; drops a
+        captured graph so the next step recaptures with the new shapes)."""
+        lib, t, s = self.lib, self.transport, self.stream.cuda_stream
+        chosen = (C.c_uint * 3)()
+        _check(lib, t, lib.reactive_transport_autotune_v3(t, self.qn.data_ptr(), self.tr.data_ptr(), s, chosen))
+        blocks = C.c_int()
+        err = C.create_string_buffer(1024)
+        if lib.reactive_gpu_hem_autotune_v3(self.hem.handle, self.qn.data_ptr(), self.qn.shape[1], self.cells, self.nv,
+                                            self.sn.data_ptr(), s, C.byref(blocks), err, len(err)):
+            raise FlowError(err.value.decode())
+        self.stream.synchronize()
+        self.graph = None
+        return {"stage_block": chosen[0], "gradient_block": chosen[1], "cfl_block": chosen[2],
+                "flash_blocks_per_sm": blocks.value}
+
     def ledger(self, dt):
         """Boundary ledger of the last step, .5 dt (B0 + B1) per variable (host;
         synchronises the flow's stream)."""

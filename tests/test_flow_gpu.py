@@ -85,3 +85,24 @@ def test_mixed_precision_flow_against_fp64():
     assert abs((mass[4] - mass0[4]) + ledger[4]) <= 1e-10 * abs(mass0[4])
     fp64.close()
     mixed.close()
+
+
+def test_autotune_keeps_results():
+    """The autotuner changes launch shapes only: a tuned flow reproduces the
+    untuned one's states bit for bit."""
+    n, steps, dt = 12, 2, 1e-8
+    faces, volume, init = small_case(n)
+    kw = dict(viscosity=1.821e-5, conductivity=0.02587, wale_cw=0.325)
+    runs = []
+    for tune in (False, True):
+        flow = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], **kw)
+        if tune:
+            chosen = flow.autotune()
+            assert chosen["stage_block"] in (64, 96, 128) and chosen["flash_blocks_per_sm"] >= 1
+        for _ in range(steps):
+            flow.step(dt)
+        flow.check(dt)
+        runs.append((flow.conserved(), flow.states()))
+        flow.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1].view(np.uint8), runs[1][1].view(np.uint8))
