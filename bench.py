@@ -265,8 +265,8 @@ class HostPath:
         self.h2d += self.q.nbytes
         br = np.zeros(5)
         stage_states = None
+        tr = tr0  # the step-start states' transport states, compacted once for the CFL query and stage 0
         for stage in (0, 1):
-            tr = self._compact(start if stage == 0 else stage_states)
             before = A.Token(self.attempt, stage, self.version)
             self.version += 1
             after = A.Token(self.attempt, stage + 1, self.version)
@@ -286,11 +286,11 @@ class HostPath:
             if stage == 0:
                 stage_states = out
                 prim = self._primitives(stage_states)
-                tr1 = self._compact(stage_states)
+                tr = self._compact(stage_states)  # reused by stage 1
                 self._check(lib.reactive_transport_stable_step_primitives(
-                    t, prim.ctypes.data_as(C.POINTER(A.Primitive)), tr1.ctypes.data_as(C.POINTER(A.State)), .5, dt,
+                    t, prim.ctypes.data_as(C.POINTER(A.Primitive)), tr.ctypes.data_as(C.POINTER(A.State)), .5, dt,
                     C.byref(dtc)))
-                self.h2d += tr1.nbytes + prim.nbytes
+                self.h2d += tr.nbytes + prim.nbytes
         self._check(lib.reactive_transport_end_attempt(t, self.attempt, 1))
 
     def close(self):
