@@ -626,8 +626,11 @@ def adjoint_run(n=64, steps=50, every=10, probes=0, seed=11):
         return (rollout(box, cases.blast_initial(spec, r, p, xp=torch), steps, dt, every)[0] * mask).sum()
 
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    # warm-up of both paths (the recorded one sets up autograd and checkpointing)
+    rw = rho0.clone().requires_grad_(True)
+    torch.autograd.grad(loss(rw, p_drive), rw)
     with torch.no_grad():
-        loss(rho0, p_drive)  # warm-up
+        loss(rho0, p_drive)
         ev[0].record()
         J = loss(rho0, p_drive)
         ev[1].record()

@@ -618,6 +618,139 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
     }
 }
 
+// Reverse-mode derivative of the inviscid HLL face flux, written out by hand.
+// With Wa the face's adjoint weights times the area and J = sum_k Wa_k F_k / A:
+// J = advL SL + advR SR + pM Wm + pE We (SL = Wa.qL, SR = Wa.qR, Wm the
+// axis-momentum weight times the normal sign, We the energy weight), whose
+// partials with respect to the normal velocities, sound speeds (through the
+// wave speeds, the active branch of each min/max as the forward selects it),
+// pressures and conserved variables of both sides are returned.
+struct HllBar {
+    double qL, qR;  // multipliers of Wa_k for d J / d qL_k, d qR_k (advL, advR)
+    double unL, unR, cL, cR, pL, pR;
+};
+__device__ __forceinline__ HllBar hllReverse(double wf, double unL, double unR, double cL, double cR, double pL,
+                                             double pR, double SL, double SR, double Wm, double We) {
+    const double aL = wf * cL, aR = wf * cR;
+    const double lo1 = unL - aL, lo2 = unR - aR, hi1 = unL + aL, hi2 = unR + aR;
+    const bool loFirst = lo1 < lo2, hiFirst = hi1 > hi2;
+    const double loIn = loFirst ? lo1 : lo2, hiIn = hiFirst ? hi1 : hi2;
+    const bool leftActive = !(0.0 < loIn), rightActive = !(0.0 > hiIn);
+    const double left = leftActive ? loIn : 0.0, right = rightActive ? hiIn : 0.0;
+    const double inv = 1 / (right - left);
+    const double advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
+    const double pM = (right * pL - left * pR) * inv, pE = (right * pL * unL - left * pR * unR) * inv;
+    const double J = advL * SL + advR * SR + pM * Wm + pE * We;
+    HllBar b;
+    b.qL = advL;
+    b.qR = advR;
+    b.unL = (right * SL + right * pL * We) * inv;
+    b.unR = (-left * SR - left * pR * We) * inv;
+    b.pL = (right * Wm + right * unL * We) * inv;
+    b.pR = (-left * Wm - left * unR * We) * inv;
+    const double dRight = ((unL - left) * SL + left * SR + pL * Wm + pL * unL * We - J) * inv;
+    const double dLeft = (-right * SL + (right - unR) * SR - pR * Wm - pR * unR * We + J) * inv;
+    double aLb = 0, aRb = 0;
+    if (leftActive) {
+        if (loFirst) { b.unL += dLeft; aLb -= dLeft; } else { b.unR += dLeft; aRb -= dLeft; }
+    }
+    if (rightActive) {
+        if (hiFirst) { b.unL += dRight; aLb += dRight; } else { b.unR += dRight; aRb += dRight; }
+    }
+    b.cL = wf * aLb;
+    b.cR = wf * aRb;
+    return b;
+}
+
+// (dL/dq)^T w and (dL/dstate)^T w of the inviscid operator of the structured
+// box with hllReverse, gather form: the same results as cartRateVjp<NS, 0> for
+// viscosity 0, conductivity 0 and no WALE, in registers.
+template <int NS>
+__global__ void __launch_bounds__(128) cartRateVjpInviscid(CartView v, const double* __restrict__ q,
+                                                           const ReactiveTransportState* __restrict__ st,
+                                                           const double* __restrict__ w, double* __restrict__ qBar,
+                                                           ReactiveTransportState* __restrict__ stateBar) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        CellData C;
+        loadCell<NS>(v, q, st, c, C, true);
+        const double ivc = v.invV[c];
+        double dq[NS + 4], du[3] = {0, 0, 0}, dp = 0, dc = 0;
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) dq[kk] = 0;
+#pragma unroll
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            const int axis = s >> 1;
+            CellData O;  // the other side
+            double Wa[NS + 4], sgn, area;
+            int kind = 0;
+            bool cIsLeft = true;
+            if (interior) {
+                const size_t nb = neighbourOf(v, s, c);
+                loadCell<NS>(v, q, st, nb, O, true);
+                const double ivn = v.invV[nb];
+                cIsLeft = s & 1;
+                sgn = 1;
+                area = v.area[axis];
+#pragma unroll
+                for (int kk = 0; kk < NS + 4; ++kk)
+                    Wa[kk] = area * (cIsLeft ? w[size_t(kk) * v.cells + nb] * ivn - w[size_t(kk) * v.cells + c] * ivc
+                                             : w[size_t(kk) * v.cells + c] * ivc - w[size_t(kk) * v.cells + nb] * ivn);
+            } else {
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                kind = f.kind;
+                boundaryRight<NS>(v, q, st, f, axis, C, O, true);
+                sgn = (s & 1) ? 1.0 : -1.0;
+                area = f.area;
+#pragma unroll
+                for (int kk = 0; kk < NS + 4; ++kk) Wa[kk] = -area * w[size_t(kk) * v.cells + c] * ivc;
+            }
+            const CellData& L = cIsLeft ? C : O;
+            const CellData& R = cIsLeft ? O : C;
+            double SL = 0, SR = 0;
+#pragma unroll
+            for (int kk = 0; kk < NS + 4; ++kk) { SL += Wa[kk] * L.q[kk]; SR += Wa[kk] * R.q[kk]; }
+            const HllBar b = hllReverse(v.waveFactor, L.u[axis] * sgn, R.u[axis] * sgn, L.c, R.c, L.p, R.p, SL, SR,
+                                        Wa[NS + axis] * sgn, Wa[NS + 3]);
+            // c's own side
+            const double qMul = cIsLeft ? b.qL : b.qR;
+#pragma unroll
+            for (int kk = 0; kk < NS + 4; ++kk) dq[kk] += Wa[kk] * qMul;
+            du[axis] += (cIsLeft ? b.unL : b.unR) * sgn;
+            dp += cIsLeft ? b.pL : b.pR;
+            dc += cIsLeft ? b.cL : b.cR;
+            // a boundary ghost made from c (extrapolate: itself; slip: axis momentum and velocity mirrored)
+            if (!interior && (kind == 1 || kind == 2)) {
+                const double mirror = kind == 1 ? -1.0 : 1.0;
+#pragma unroll
+                for (int kk = 0; kk < NS + 4; ++kk) dq[kk] += Wa[kk] * b.qR * (kk == NS + axis ? mirror : 1.0);
+                du[axis] += b.unR * sgn * mirror;
+                dp += b.pR;
+                dc += b.cR;
+            }
+        }
+        // u = m / rho with rho the sum of the species masses
+        double rho = 0;
+#pragma unroll
+        for (int kk = 0; kk < NS; ++kk) rho += C.q[kk];
+        double dRho = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            dq[NS + a] += du[a] / rho;
+            dRho -= du[a] * C.u[a] / rho;
+        }
+#pragma unroll
+        for (int kk = 0; kk < NS; ++kk) dq[kk] += dRho;
+#pragma unroll
+        for (int kk = 0; kk < NS + 4; ++kk) qBar[size_t(kk) * v.cells + c] = dq[kk];
+        stateBar[c] = ReactiveTransportState{dp, 0.0, 0.0, 0.0, dc, 0.0, 0.0};
+    }
+}
+
 // gBar += nutBar * d nu_t / d g per cell (the WALE eddy viscosity of the cell's
 // gradient, the Nicoud-Ducros relation of wale.cuh written for duals:
 // nu_t = (Cw Delta)^2 |g|_max (Sd:Sd)^(3/2) / ((S:S)^(5/2) + (Sd:Sd)^(5/4))

@@ -548,6 +548,10 @@ struct Transport {
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
                         const double* nut, const double* w, double* qBar, ReactiveTransportState* stateBar,
                         double* gBar, double* nutBar, bool viscous, cudaStream_t s) {
+            if (!viscous && b.conductivity == 0) {
+                cartRateVjpInviscid<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, w, qBar, stateBar);
+                return;
+            }
             cartRateVjp<NS, 0><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, qBar, stateBar, nullptr,
                                                                     nullptr);
             if (!viscous) return;

@@ -28,14 +28,17 @@ pytestmark = pytest.mark.gpu
 STATE_FIELDS = ("p", "T", "rho", "sound")
 
 
-@pytest.mark.parametrize("ns,wale,kinds", [(1, .325, "mixed"), (2, .5, (1, 2, 3, 2, 1, 2)), (1, None, (2,) * 6)])
-def test_rate_vjp_dot_product(ns, wale, kinds):
+@pytest.mark.parametrize("ns,wale,kinds,viscous", [(1, .325, "mixed", True), (2, .5, (1, 2, 3, 2, 1, 2), True),
+                                                   (1, None, (2,) * 6, True), (2, None, "mixed", False)])
+def test_rate_vjp_dot_product(ns, wale, kinds, viscous):
+    """viscous=False: the inviscid operator (the hand-derived reverse-mode HLL
+    kernel); True: viscosity and conduction (the dual-number kernels)."""
     import torch
     L = _lib.load()
     lib = T.bind(L)
     dims = (6, 5, 4)
     kinds = mixed_kinds(dims, 23) if kinds == "mixed" else kinds
-    case = box_case(dims, ns, kinds, viscous=True, conduction=True, seed=4)
+    case = box_case(dims, ns, kinds, viscous=viscous, conduction=viscous, seed=4)
     h = T.create(lib, 1, case, wale_cw=wale)
     nc, nv = case["nc"], case["nv"]
     rng = np.random.default_rng(31 + ns)
