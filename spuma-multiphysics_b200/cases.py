@@ -19,19 +19,32 @@ from .eos import PureFluid
 from .thermo_data import N2O
 
 
-def flash_batch(n, seed=20260303, two_phase_share=0.6, fluid=None, seed_policy="exact"):
-    """(q, e, guess states, generating labels) for n pure-fluid cells.
+def flash_batch(n, seed=20260303, two_phase_share=0.6, fluid=None, seed_policy="exact", saturation_levels=0):
+    """(rho, e, guess states) for n pure-fluid cells.
 
     seed_policy "exact": the generating (p, T, liquid mass) is the flash seed;
-    "fixed": every seed is 40 bar / 293.15 K gas.
+    "fixed": every seed is 40 bar / 293.15 K gas. saturation_levels > 0 draws the
+    two-phase temperatures uniformly from that many equally spaced levels in
+    [220, 305] K and solves the saturation pair once per level (for batches of
+    millions of cells); 0 draws them continuously.
     """
     fluid = fluid or PureFluid(N2O)
     rng = np.random.default_rng(seed)
     n2 = int(round(two_phase_share * n))
     n1 = n - n2
-    T2 = rng.uniform(220.0, 305.0, n2)
-    x = rng.uniform(0.0, 1.0, n2)
-    psat, gas, liq = fluid.saturation(T2)
+    if saturation_levels:
+        levels = np.linspace(220.0, 305.0, saturation_levels)
+        pick = rng.integers(0, saturation_levels, n2)
+        T2 = levels[pick]
+        x = rng.uniform(0.0, 1.0, n2)
+        ps, gs, ls = fluid.saturation(levels)
+        psat = ps[pick]
+        gas = {k: v[pick] for k, v in gs.items()}
+        liq = {k: v[pick] for k, v in ls.items()}
+    else:
+        T2 = rng.uniform(220.0, 305.0, n2)
+        x = rng.uniform(0.0, 1.0, n2)
+        psat, gas, liq = fluid.saturation(T2)
     v2 = x / gas["rho"] + (1 - x) / liq["rho"]
     rho2 = 1 / v2
     e2 = rho2 * (x * gas["e"] + (1 - x) * liq["e"])

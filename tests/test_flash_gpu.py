@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from spuma_multiphysics_b200 import _abi as A, cases
+from spuma_multiphysics_b200 import _abi as A, cases, thermo_data as td
 from spuma_multiphysics_b200.hem import GpuHem, HemError
 import flash_cases as F
 
@@ -132,3 +132,39 @@ def test_cuda_flash_device_resident_matches_host_path():
     assert np.array_equal(tr[both, 0], host["p"][both]) and np.array_equal(tr[both, 4], host["soundFrozen"][both])
     prof = hem.counters(stream)
     assert prof.flashCandidates > 0
+
+
+def test_cuda_flash_labels_match_reference_on_large_batch_sample():
+    """Config-3 style batch (60% saturated two-phase states on 65,536
+    temperature levels, 40% single phase), 40,000 cells: success flags and
+    phase labels bit-exact against the reference flash on the host (all host
+    cores), p and T within the flash tolerance."""
+    n = 40000
+    q, e, guess = cases.flash_batch(n, seed=20260303, saturation_levels=65536)
+    model = td.model_bytes(td.pure_model())
+    hem = GpuHem(capacity=n)
+    got = guess.copy()
+    ok, _ = hem.run(q, e, got)
+    hem.close()
+    ref, ref_ok, _ = oracle.ref_flash_recover(model, q, e, guess, threads=oracle.cpu_threads())
+    s = F.compare(got, ok, ref, ref_ok)
+    assert s["success_equal"] and s["label_mismatch"] == 0, s
+    assert s["p_rel"] <= F.P_T_TOL and s["T_rel"] <= F.P_T_TOL, s
+
+
+def test_cuda_flash_fails_where_the_reference_fails():
+    """A near-critical state (313 K, 78 bar) from the 4,096,000-cell batch that
+    the reference flash cannot recover: the CUDA flash reports the same failure
+    and leaves the state unchanged."""
+    q = np.array([432.822060758171])
+    e = np.array([729723467.9575783])
+    guess = np.zeros(1, dtype=A.THERMO_DTYPE)
+    guess["p"], guess["T"], guess["rho"] = 7822403.962295835, 312.965328917707, 432.822060758171
+    model = td.model_bytes(td.pure_model())
+    _, ref_ok, _ = oracle.ref_flash_recover(model, q, e, guess.copy())
+    hem = GpuHem(capacity=1)
+    got = guess.copy()
+    ok, _ = hem.run(q, e, got)
+    hem.close()
+    assert ref_ok[0] == 0 and ok[0] == 0
+    assert got.tobytes() == guess.tobytes()
