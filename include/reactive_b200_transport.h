@@ -132,6 +132,16 @@ int reactive_transport_stable_step_device_v3(void* transport, const double* q,
  * queries, 0 selects the face graph, 1 the structured path (an error when the
  * face list is not such a box); *active (may be NULL) receives the selection. */
 int reactive_transport_structured_v3(void* transport, int request, int* active);
+/* Face flux of the structured path (no C-ABI counterpart: the reference applies
+ * its HLLC core only inside the capillary option, reactive_transport_set_capillary_v1,
+ * with the interface geometry). request -1 only queries, 0 selects HLL, 1 HLLC:
+ * the reference's contact-preserving core with no capillary terms
+ * (src/reactiveInterface/reactiveBalancedCapillary.h:55-142), falling back to
+ * the HLL coefficients when the star speed leaves the wave fan. A face whose
+ * HLLC state cannot be formed sets bit 1 of the status word. Selecting the face
+ * graph returns to HLL; the rate VJP covers HLL only. *active (may be NULL)
+ * receives the scheme. */
+int reactive_transport_flux_v3(void* transport, int request, int* active);
 /* Arithmetic of the structured path (no reference counterpart; the reference
  * transport is FP64 only). request -1 only queries, 0 selects FP64, 1 the mixed
  * form: velocity gradients, WALE eddy viscosity and face fluxes (HLL, traction,
@@ -164,7 +174,8 @@ int reactive_transport_rate_vjp_v3(void* transport, const double* q, const React
  * a graph. chosen (may be NULL) receives {stage, gradient, CFL} block sizes. */
 int reactive_transport_autotune_v3(void* transport, const double* q, const ReactiveTransportState* state,
     void* stream, unsigned* chosen);
-/* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite. Reading
+/* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite,
+ * bit 1 = an HLLC face could not be formed. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);
 

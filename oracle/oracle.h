@@ -14,6 +14,9 @@
  * ledger (variables), optional per-cell WALE nu_t (waleCw < 0 disables WALE) and
  * optional per-cell CFL denominator sum_f area*speed. Returns 0, or a nonzero
  * code when a WALE value or a face speed is invalid. */
+void oracle_set_flux_scheme(int scheme);
+int oracle_hllc_face(double rhoL, const double uL[3], double pL, double aL, double EL, double rhoR,
+                     const double uR[3], double pR, double aR, double ER, const double normal[3], double out[5]);
 int oracle_transport_rhs(const ReactiveTransportConfig* cfg, const double* volume,
     const ReactiveTransportFace* faces, const double* fixedQ, const ReactiveTransportState* fixedStates,
     const double* fixedY, const double* fixedH, double waleCw,

@@ -33,6 +33,7 @@ def _load(path):
 _oracle = None
 _ref_transport = None
 _ref_flash = None
+_ref_hllc = None
 
 
 def oracle_lib():
@@ -47,6 +48,11 @@ def oracle_lib():
         _oracle.oracle_transport_stable_dt.restype = C.c_double
         _oracle.oracle_wale_nut.argtypes = [_d, C.c_double, C.c_double, _d]
         _oracle.oracle_wale_nut.restype = C.c_int
+        _oracle.oracle_set_flux_scheme.argtypes = [C.c_int]
+        _oracle.oracle_set_flux_scheme.restype = None
+        _oracle.oracle_hllc_face.argtypes = [C.c_double, _d, C.c_double, C.c_double, C.c_double, C.c_double, _d,
+                                             C.c_double, C.c_double, C.c_double, _d, _d]
+        _oracle.oracle_hllc_face.restype = C.c_int
         if hasattr(_oracle, "oracle_flash_recover"):
             _oracle.oracle_flash_recover.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _v, C.POINTER(C.c_int),
                                                      C.POINTER(C.c_uint64), C.c_int]
@@ -62,6 +68,34 @@ def ref_transport_lib():
             build()
         _ref_transport = C.CDLL(str(REF_TRANSPORT))
     return _ref_transport
+
+
+def ref_hllc_lib():
+    """The reference's HLLC face core compiled for the host."""
+    global _ref_hllc
+    if _ref_hllc is None:
+        path = HERE / "_ref" / "libref_hllc.so"
+        if not path.exists():
+            build()
+        _ref_hllc = C.CDLL(str(path))
+        _ref_hllc.ref_hllc_face.argtypes = [C.c_double, _d, C.c_double, C.c_double, C.c_double, C.c_double, _d,
+                                            C.c_double, C.c_double, C.c_double, _d, _d]
+        _ref_hllc.ref_hllc_face.restype = C.c_int
+    return _ref_hllc
+
+
+def hllc_face(lib_fn, L, R, normal):
+    """(ok, [contact, advectLeft, advectRight, pressureMomentum, pressureEnergy]) of one face;
+    L, R = (rho, u[3], p, a, E)."""
+    out = np.zeros(5)
+    a = lambda x: np.ascontiguousarray(x, dtype=np.float64).ctypes.data_as(_d)
+    ok = lib_fn(L[0], a(L[1]), L[2], L[3], L[4], R[0], a(R[1]), R[2], R[3], R[4], a(normal), out.ctypes.data_as(_d))
+    return ok, out
+
+
+def set_flux_scheme(scheme):
+    """Flux scheme of transport_rhs / transport_stable_dt: 0 HLL, 1 HLLC."""
+    oracle_lib().oracle_set_flux_scheme(int(scheme))
 
 
 def ref_flash_lib():

@@ -195,6 +195,65 @@ static void gas_side(const Ctx* c, const ReactiveTransportFace* f, int right, co
     }
 }
 
+/* Flux scheme of oracle_transport_rhs: 0 HLL, 1 HLLC. */
+static int g_scheme = 0;
+void oracle_set_flux_scheme(int scheme) { g_scheme = scheme; }
+
+/* HLLC face coefficients: the reference's contact-preserving core
+ * (src/reactiveInterface/reactiveBalancedCapillary.h:55-142) with no capillary
+ * terms (sigma = 0, so pi = p), as the transport's Faces functor applies it
+ * (src/reactiveTransport/reactiveTransportKernels.h:357-417): wave speeds from
+ * waveFactor * sound, star speed from the two one-sided momentum balances,
+ * the HLL coefficients when the star speed leaves (S_L, S_R), else the upwind
+ * star (or supersonic) state of the side the contact moves away from.
+ * out = {contact speed, advectLeft, advectRight, pressureMomentum, pressureEnergy}.
+ * Returns 0 when the face cannot be formed (the reference's capillary failure). */
+int oracle_hllc_face(double rhoL, const double uL[3], double pL, double aL, double EL, double rhoR,
+                     const double uR[3], double pR, double aR, double ER, const double normal[3], double out[5]) {
+    double unL = 0, unR = 0, sl, sr, den, star;
+    if (!(isfinite(rhoL) && rhoL > 0 && isfinite(rhoR) && rhoR > 0 && isfinite(pL) && pL > 0 && isfinite(pR)
+          && pR > 0 && isfinite(aL) && aL > 0 && isfinite(aR) && aR > 0 && isfinite(EL) && isfinite(ER)))
+        return 0;
+    for (int d = 0; d < 3; ++d) { unL += uL[d] * normal[d]; unR += uR[d] * normal[d]; }
+    sl = minimum(0, minimum(unL - aL, unR - aR));
+    sr = maximum(0, maximum(unL + aL, unR + aR));
+    den = rhoL * (sl - unL) - rhoR * (sr - unR);
+    if (!isfinite(den) || den == 0 || !isfinite(sl) || !isfinite(sr) || sr <= sl) return 0;
+    star = (pR - pL + rhoL * unL * (sl - unL) - rhoR * unR * (sr - unR)) / den;
+    if (!isfinite(star) || star <= sl || star >= sr) {
+        const double inv = 1 / (sr - sl);
+        out[0] = (sr * unL - sl * unR) * inv;
+        out[1] = sr * (unL - sl) * inv;
+        out[2] = sl * (sr - unR) * inv;
+        out[3] = (sr * pL - sl * pR) * inv;
+        out[4] = (sr * pL * unL - sl * pR * unR) * inv;
+    } else {
+        const int left = star >= 0;
+        const double rho = left ? rhoL : rhoR, un = left ? unL : unR, wave = left ? sl : sr;
+        const double p = left ? pL : pR, E = left ? EL : ER;
+        const int supersonic = (left && sl >= 0) || (!left && sr <= 0);
+        double mass;
+        out[0] = supersonic ? un : star;
+        if (supersonic) {
+            mass = rho * un;
+            out[3] = p;
+            out[4] = p * un;
+        } else {
+            const double rhoStar = rho * (wave - un) / (wave - star);
+            const double pStar = p + rho * (wave - un) * (star - un);
+            const double eStar = ((wave - un) * E - p * un + pStar * star) / (wave - star);
+            mass = rhoStar * star;
+            out[3] = pStar + mass * (star - un);
+            out[4] = star * (eStar + pStar) - mass * E / rho;
+        }
+        out[1] = left ? mass / rhoL : 0;
+        out[2] = left ? 0 : mass / rhoR;
+    }
+    for (int k = 0; k < 5; ++k)
+        if (!isfinite(out[k])) return 0;
+    return 1;
+}
+
 int oracle_transport_rhs(const ReactiveTransportConfig* cfg, const double* volume,
     const ReactiveTransportFace* faces, const double* fixedQ, const ReactiveTransportState* fixedStates,
     const double* fixedY, const double* fixedH, double waleCw,
@@ -230,6 +289,12 @@ int oracle_transport_rhs(const ReactiveTransportConfig* cfg, const double* volum
         advR = left * (right - unR) * inv;
         pM = (right * sl->p - left * sr->p) * inv;
         pE = (right * sl->p * unL - left * sr->p * unR) * inv;
+        if (g_scheme == 1) {
+            double h[5];
+            const double EL = ql[ns + 3], ER = qr[ns + 3];
+            if (!oracle_hllc_face(sl->rho, ul, sl->p, aL, EL, sr->rho, ur, sr->p, aR, ER, f->normal, h)) status = 3;
+            fv = h[0]; advL = h[1]; advR = h[2]; pM = h[3]; pE = h[4];
+        }
         if (denominator) {
             const double speed = face_speed(&c, f);
             if (speed < 0) status = 2;

@@ -45,6 +45,7 @@ TRANSPORT = {
     "status_v3": ([_v, C.POINTER(C.c_uint), C.c_int, _v], C.c_int),
     "structured_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "precision_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "flux_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "autotune_v3": ([_v, _v, _v, _v, C.POINTER(C.c_uint)], C.c_int),
     "rate_vjp_v3": ([_v, _v, _v, _v, _v, _v, _v], C.c_int),
 }

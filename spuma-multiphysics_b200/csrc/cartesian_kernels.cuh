@@ -39,6 +39,7 @@ struct CartView {
     double viscosity, conductivity, waveFactor;
     bool wale;
     double cw;
+    int scheme;  // 0 HLL, 1 HLLC
 };
 
 struct CellData {
@@ -121,15 +122,50 @@ template <int NS, class R>
 __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double sgnD, double areaD, double distD,
                                              double wD, int kind, bool internal, const CellT<R>& L,
                                              const CellT<R>& Rt, const R* gL, const R* gR, R nutL, R nutR, R* F,
-                                             bool& bad) {
+                                             bool& bad, bool& faceBad) {
     const R sgn = R(sgnD), w = R(wD), dist = R(distD), area = R(areaD);
     const R unL = L.u[axis] * sgn, unR = Rt.u[axis] * sgn;
     const R aL = R(v.waveFactor) * L.c, aR = R(v.waveFactor) * Rt.c;
     const R left = rmin(R(0), rmin(unL - aL, unR - aR)), right = rmax(R(0), rmax(unL + aL, unR + aR));
     const R inv = R(1) / (right - left);
-    const R advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
+    R advL = right * (unL - left) * inv, advR = left * (right - unR) * inv;
     const R pL = L.p, pR = Rt.p;
-    const R pM = (right * pL - left * pR) * inv, pE = (right * pL * unL - left * pR * unR) * inv;
+    R pM = (right * pL - left * pR) * inv, pE = (right * pL * unL - left * pR * unR) * inv;
+    if (v.scheme == 1) {
+        // HLLC: the reference's contact-preserving core with no capillary terms
+        // (src/reactiveInterface/reactiveBalancedCapillary.h:55-142, applied by
+        // src/reactiveTransport/reactiveTransportKernels.h:357-417). The HLL
+        // coefficients above stand when the star speed leaves the wave fan.
+        const R rhoL = L.rho, rhoR = Rt.rho;
+        const R den = rhoL * (left - unL) - rhoR * (right - unR);
+        if (!(rhoL > R(0) && rhoR > R(0) && pL > R(0) && pR > R(0) && isfinite(den) && den != R(0)
+              && right > left)) {
+            faceBad = true;
+        } else {
+            const R star = (pR - pL + rhoL * unL * (left - unL) - rhoR * unR * (right - unR)) / den;
+            if (isfinite(star) && star > left && star < right) {
+                const bool useLeft = star >= R(0);
+                const R rho = useLeft ? rhoL : rhoR, un = useLeft ? unL : unR, wave = useLeft ? left : right;
+                const R p = useLeft ? pL : pR, E = useLeft ? L.q[NS + 3] : Rt.q[NS + 3];
+                const bool supersonic = (useLeft && left >= R(0)) || (!useLeft && right <= R(0));
+                R mass;
+                if (supersonic) {
+                    mass = rho * un;
+                    pM = p;
+                    pE = p * un;
+                } else {
+                    const R rhoStar = rho * (wave - un) / (wave - star);
+                    const R pStar = p + rho * (wave - un) * (star - un);
+                    const R eStar = ((wave - un) * E - p * un + pStar * star) / (wave - star);
+                    mass = rhoStar * star;
+                    pM = pStar + mass * (star - un);
+                    pE = star * (eStar + pStar) - mass * E / rho;
+                }
+                advL = useLeft ? mass / rhoL : R(0);
+                advR = useLeft ? R(0) : mass / rhoR;
+            }
+        }
+    }
     R traction[3] = {R(0), R(0), R(0)}, energy = R(0);
     if (v.viscosity > 0 || v.wale) {
         const R* uL = L.u;
@@ -281,7 +317,7 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
                                          const ReactiveTransportState* __restrict__ st,
                                          const R* __restrict__ grad, const R* __restrict__ nut, size_t c,
                                          int s, bool interior, int i, int j, int k, const CellData& C,
-                                         const R* gC, R nutC, R* F, double& sign, bool& bad) {
+                                         const R* gC, R nutC, R* F, double& sign, bool& bad, bool& faceBad) {
     const int axis = s >> 1;
     const bool viscous = v.viscosity > 0 || v.wale;
     if (interior) {
@@ -297,11 +333,11 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
         const CellT<R> cc = asCell<NS, R>(C), cn = asCell<NS, R>(N);
         if (s & 1) {  // this cell owns the face
             faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc, cn, gC, gN, nutC, nutN, F,
-                                bad);
+                                bad, faceBad);
             sign = -1;
         } else {
             faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cn, cc, gN, gC, nutN, nutC, F,
-                                bad);
+                                bad, faceBad);
             sign = 1;
         }
     } else {
@@ -310,7 +346,7 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
         boundaryRight<NS>(v, q, st, f, axis, C, Rt, true);
         // a boundary face's right-side WALE viscosity is the owner's
         faceFluxCart<NS, R>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
-                            asCell<NS, R>(C), asCell<NS, R>(Rt), gC, gC, nutC, nutC, F, bad);
+                            asCell<NS, R>(C), asCell<NS, R>(Rt), gC, gC, nutC, nutC, F, bad, faceBad);
         sign = -1;
     }
 }
@@ -346,7 +382,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
         R rate[NS + 4], comp[NS + 4];
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) rate[kk] = comp[kk] = R(0);
-        bool bad = false;
+        bool bad = false, faceBad = false;
 #pragma unroll
         for (int n = 0; n < 12; ++n) {
             const int s = sideOf(n);
@@ -354,7 +390,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
             if (interior != (n < 6)) continue;
             R F[NS + 4];
             double sign;
-            sideFlux<NS, R>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad);
+            sideFlux<NS, R>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad, faceBad);
 #pragma unroll
             for (int kk = 0; kk < NS + 4; ++kk) {
                 if constexpr (fp64) rate[kk] += sign * F[kk] * iv;
@@ -362,6 +398,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
             }
         }
         if (bad) atomicOr(error, 1u);
+        if (faceBad) atomicOr(error, 2u);
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) {
             const double r = fp64 ? double(rate[kk]) : (double(rate[kk]) + double(comp[kk])) * iv;
@@ -404,7 +441,7 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
         loadCell<NS>(v, nullptr, st, c, C, false);
         const double nutC = v.wale ? double(nut[c]) : 0;
         double denominator = 0;
-        bool bad = false;
+        bool bad = false, faceBad = false;
 #pragma unroll
         for (int n = 0; n < 12; ++n) {
             const int s = sideOf(n);
@@ -457,7 +494,7 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
 #pragma unroll
     for (int kk = 0; kk < NS + 4; ++kk) sum[kk] = 0;
     const bool viscous = v.viscosity > 0 || v.wale;
-    bool bad = false;
+    bool bad = false, faceBad = false;
     for (size_t b = blockIdx.x * size_t(blockDim.x) + threadIdx.x; b < v.nBoundary;
          b += size_t(blockDim.x) * gridDim.x) {
         const ReactiveTransportFace f = v.face[v.boundaryBase + b];
@@ -475,7 +512,7 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
         const R nutC = v.wale ? nut[c] : R(0);
         R F[NS + 4];
         faceFluxCart<NS, R>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, asCell<NS, R>(C), asCell<NS, R>(Rt), g, g, nutC, nutC, F,
-                         bad);
+                         bad, faceBad);
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) sum[kk] += double(F[kk]);
     }
@@ -550,7 +587,7 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
         double acc[N];
 #pragma unroll
         for (int t = 0; t < N; ++t) acc[t] = 0;
-        bool bad = false;
+        bool bad = false, faceBad = false;
 #pragma unroll 1
         for (int n = 0; n < 12; ++n) {
             const int s = sideOf(n);
@@ -571,13 +608,13 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
                 const double ivn = v.invV[nb];
                 if (s & 1) {  // c owns the face
                     faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Cd, Nd, gC, gN, nutC,
-                                        nutN, F, bad);
+                                        nutN, F, bad, faceBad);
 #pragma unroll
                     for (int kk = 0; kk < NS + 4; ++kk)
                         W[kk] = w[size_t(kk) * v.cells + nb] * ivn - w[size_t(kk) * v.cells + c] * ivc;
                 } else {
                     faceFluxCart<NS, D>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, Nd, Cd, gN, gC, nutN,
-                                        nutC, F, bad);
+                                        nutC, F, bad, faceBad);
 #pragma unroll
                     for (int kk = 0; kk < NS + 4; ++kk)
                         W[kk] = w[size_t(kk) * v.cells + c] * ivc - w[size_t(kk) * v.cells + nb] * ivn;
@@ -597,7 +634,7 @@ __global__ void __launch_bounds__(128) cartRateVjp(CartView v, const double* __r
                     }
                 }
                 faceFluxCart<NS, D>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
-                                    Cd, Rt, gC, gC, nutC, nutC, F, bad);
+                                    Cd, Rt, gC, gC, nutC, nutC, F, bad, faceBad);
 #pragma unroll
                 for (int kk = 0; kk < NS + 4; ++kk) W[kk] = -w[size_t(kk) * v.cells + c] * ivc;
             }

@@ -72,6 +72,7 @@ template <int N> __device__ __forceinline__ bool operator>(const Dual<N>& a, con
 template <int N> __device__ __forceinline__ bool operator<=(const Dual<N>& a, const Dual<N>& b) { return a.v <= b.v; }
 template <int N> __device__ __forceinline__ bool operator>=(const Dual<N>& a, const Dual<N>& b) { return a.v >= b.v; }
 template <int N> __device__ __forceinline__ bool operator==(const Dual<N>& a, const Dual<N>& b) { return a.v == b.v; }
+template <int N> __device__ __forceinline__ bool operator!=(const Dual<N>& a, const Dual<N>& b) { return a.v != b.v; }
 template <int N> __device__ __forceinline__ bool isfinite(const Dual<N>& a) { return ::isfinite(a.v); }
 template <int N> __device__ __forceinline__ Dual<N> sqrt(const Dual<N>& a) {
     Dual<N> r;

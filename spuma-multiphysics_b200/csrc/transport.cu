@@ -447,10 +447,12 @@ struct Transport {
         box.viscosity = cfg.viscosity; box.conductivity = cfg.conductivity; box.waveFactor = cfg.waveFactor;
         return true;
     }
+    int fluxScheme = 0;  // structured path: 0 HLL, 1 HLLC
     CartView boxView() const {
         CartView b = box;
         b.wale = v.wale;
         b.cw = v.cw;
+        b.scheme = fluxScheme;
         return b;
     }
     template <template <int> class K, class... Args> void bySpecies(Args&&... args) {
@@ -568,6 +570,7 @@ struct Transport {
     void launchRateVjp(const double* q, const ReactiveTransportState* state, const double* w, double* qBar,
                        ReactiveTransportState* stateBar, cudaStream_t s) {
         require(structured, "The rate VJP needs the structured Cartesian path (reactive_transport_structured_v3)");
+        require(fluxScheme == 0, "The rate VJP covers the HLL flux");
         const bool viscous = cfg.viscosity > 0 || v.wale;
         if (viscous && !gradBar) {
             gradBar = arena.get<double>(product(cfg.cells, 9));

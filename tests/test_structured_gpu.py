@@ -194,3 +194,53 @@ def test_mixed_precision_stage_against_oracle(spec):
         assert L.reactive_transport_precision_v3(h, 1, None) == 1
     finally:
         lib.reactive_transport_destroy(h)
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("spec", BOXES[1:4], ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_hllc_stage_against_oracle(spec, mixed):
+    """HLLC on the structured path against the oracle's HLLC (itself equal to the
+    reference's core bit for bit): both stages, FP64 at the reference tolerance,
+    the mixed form at its FP32 tolerance."""
+    import torch
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    cw = spec.get("wale")
+    h = T.create(lib, 1, case, wale_cw=cw)
+    oracle.set_flux_scheme(1)
+    try:
+        active = C.c_int(-1)
+        assert L.reactive_transport_flux_v3(h, 1, C.byref(active)) == 0 and active.value == 1
+        if mixed:
+            assert L.reactive_transport_precision_v3(h, 1, None) == 0
+        stream = torch.cuda.current_stream().cuda_stream
+        got = _stage_pair(L, h, case, stream, torch)
+        assert got["status"] == 0 and got["tail"]
+        wale_cw = -1.0 if cw is None else cw
+        states_p = case["states"].ctypes.data_as(C.c_void_p)
+        rhs, exp_br, _, _, status = oracle.transport_rhs(case, case["q"], states_p, wale_cw=wale_cw)
+        assert status == 0
+        tol = 2e-5 if mixed else T.RHS_TOL
+        step = got["step"]
+        if mixed:
+            assert T.scaled_error((got["q1"] - case["q"]) / step, rhs) <= tol
+        else:
+            assert T.scaled_error(got["q1"], case["q"] + step * rhs) <= tol
+        assert T.scaled_error(got["br0"][None], exp_br[None]) <= tol
+        rhs1, exp_br1, _, _, _ = oracle.transport_rhs(case, got["q1"], got["st1"].ctypes.data_as(C.c_void_p),
+                                                      wale_cw=wale_cw)
+        if not mixed:
+            assert T.scaled_error(got["qn"], .5 * case["q"] + .5 * (got["q1"] + step * rhs1)) <= tol
+            assert T.scaled_error(got["br1"][None], exp_br1[None]) <= tol
+        # HLLC differs from HLL on these states
+        oracle.set_flux_scheme(0)
+        hll, _, _, _, _ = oracle.transport_rhs(case, case["q"], states_p, wale_cw=wale_cw)
+        assert T.scaled_error(rhs, hll) > 1e-6
+        # the face graph is HLL only
+        assert L.reactive_transport_structured_v3(h, 0, None) == 0
+        assert L.reactive_transport_flux_v3(h, -1, C.byref(active)) == 0 and active.value == 0
+    finally:
+        oracle.set_flux_scheme(0)
+        lib.reactive_transport_destroy(h)
