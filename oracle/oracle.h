@@ -15,6 +15,8 @@
  * optional per-cell CFL denominator sum_f area*speed. Returns 0, or a nonzero
  * code when a WALE value or a face speed is invalid. */
 void oracle_set_flux_scheme(int scheme);
+void oracle_set_wale_scalars(double pr, double sc, const double* cellCp, const double* fixedCp,
+                             const double* cellH, const double* fixedH);
 int oracle_hllc_face(double rhoL, const double uL[3], double pL, double aL, double EL, double rhoR,
                      const double uR[3], double pR, double aR, double ER, const double normal[3], double out[5]);
 int oracle_transport_rhs(const ReactiveTransportConfig* cfg, const double* volume,

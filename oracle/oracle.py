@@ -48,6 +48,8 @@ def oracle_lib():
         _oracle.oracle_transport_stable_dt.restype = C.c_double
         _oracle.oracle_wale_nut.argtypes = [_d, C.c_double, C.c_double, _d]
         _oracle.oracle_wale_nut.restype = C.c_int
+        _oracle.oracle_set_wale_scalars.argtypes = [C.c_double, C.c_double, _d, _d, _d, _d]
+        _oracle.oracle_set_wale_scalars.restype = None
         _oracle.oracle_set_flux_scheme.argtypes = [C.c_int]
         _oracle.oracle_set_flux_scheme.restype = None
         _oracle.oracle_hllc_face.argtypes = [C.c_double, _d, C.c_double, C.c_double, C.c_double, C.c_double, _d,
@@ -91,6 +93,19 @@ def hllc_face(lib_fn, L, R, normal):
     a = lambda x: np.ascontiguousarray(x, dtype=np.float64).ctypes.data_as(_d)
     ok = lib_fn(L[0], a(L[1]), L[2], L[3], L[4], R[0], a(R[1]), R[2], R[3], R[4], a(normal), out.ctypes.data_as(_d))
     return ok, out
+
+
+_scalar_fields = None
+
+
+def set_wale_scalars(pr=0.0, sc=0.0, cell_cp=None, fixed_cp=None, cell_h=None, fixed_h=None):
+    """WALE scalar closure of transport_rhs / transport_stable_dt (0 disables a
+    flux; the arrays are held here while the closure is set)."""
+    global _scalar_fields
+    arrays = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+              for a in (cell_cp, fixed_cp, cell_h, fixed_h)]
+    _scalar_fields = arrays
+    oracle_lib().oracle_set_wale_scalars(float(pr), float(sc), *[_p(a) for a in arrays])
 
 
 def set_flux_scheme(scheme):

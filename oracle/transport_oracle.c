@@ -161,6 +161,30 @@ static double face_nut(const Ctx* c, const ReactiveTransportFace* f, int right) 
     return c->nut[right && f->neighbour >= 0 ? f->neighbour : f->owner];
 }
 
+/* WALE scalar closure (src/reactiveTransport/reactiveTransport.cpp:653-702,
+ * reactiveTransportKernels.h:150-168, :323-336, :440-444, :462-477): turbulent
+ * Prandtl / Schmidt numbers (0 disables that flux) and the caller's fields:
+ * mixture cp per cell and per fixed state, effective species enthalpies
+ * (cell-major). Active only together with WALE. */
+static double g_pr = 0, g_sc = 0;
+static const double *g_cellCp, *g_fixedCp, *g_cellH, *g_fixedH;
+void oracle_set_wale_scalars(double pr, double sc, const double* cellCp, const double* fixedCp,
+                             const double* cellH, const double* fixedH) {
+    g_pr = pr; g_sc = sc; g_cellCp = cellCp; g_fixedCp = fixedCp; g_cellH = cellH; g_fixedH = fixedH;
+}
+
+/* cp and species enthalpies of the face's right cell (the owner's for slip and extrapolate). */
+static double right_cp(const ReactiveTransportFace* f) {
+    if (f->neighbour >= 0) return g_cellCp[f->neighbour];
+    if (f->kind == 3) return g_fixedCp[f->fixed];
+    return g_cellCp[f->owner];
+}
+static const double* right_h(const ReactiveTransportFace* f, size_t ns) {
+    if (f->neighbour >= 0) return g_cellH + (size_t)f->neighbour * ns;
+    if (f->kind == 3) return g_fixedH + (size_t)f->fixed * ns;
+    return g_cellH + (size_t)f->owner * ns;
+}
+
 /* CFL face speed (-1 when invalid). */
 static double face_speed(const Ctx* c, const ReactiveTransportFace* f) {
     const ReactiveTransportConfig* cfg = c->cfg;
@@ -177,7 +201,18 @@ static double face_speed(const Ctx* c, const ReactiveTransportFace* f) {
     mu = cfg->viscosity + rhoNut;
     D = cfg->diffusivity + maximum(maximum(4 * mu / (3 * sl->rho), 4 * mu / (3 * sr->rho)),
                                    maximum(cfg->conductivity / (sl->rho * sl->cv), cfg->conductivity / (sr->rho * sr->cv)));
-    speed = maximum(fabs(unL) + aL, fabs(unR) + aR) + 2 * D / f->distance;
+    {
+        double scalar = 0;
+        if (c->wale && (g_pr > 0 || g_sc > 0) && f->kind != 1) {
+            if (g_pr > 0) {
+                const double k = rhoNut * (f->ownerWeight * g_cellCp[f->owner] + (1 - f->ownerWeight) * right_cp(f))
+                    / g_pr;
+                scalar = maximum(scalar, maximum(k / (sl->rho * sl->cv), k / (sr->rho * sr->cv)));
+            }
+            if (g_sc > 0) scalar = maximum(scalar, maximum(rhoNut / sl->rho, rhoNut / sr->rho) / g_sc);
+        }
+        speed = maximum(fabs(unL) + aL, fabs(unR) + aR) + 2 * (D + scalar) / f->distance;
+    }
     if (!isfinite(unL) || !isfinite(unR) || !isfinite(speed) || !isfinite(1 / (right - left)) || right <= left) speed = -1;
     if (big != buf) free(big);
     return speed;
@@ -326,6 +361,11 @@ int oracle_transport_rhs(const ReactiveTransportConfig* cfg, const double* volum
             for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * ul[d] + (1 - w) * ur[d]);
         }
         if (cfg->conductivity > 0 && f->kind != 1) energy -= cfg->conductivity * (sr->T - sl->T) / f->distance;
+        if (c.wale && g_pr > 0 && f->kind != 1) {
+            const double rhoNut = w * sl->rho * face_nut(&c, f, 0) + (1 - w) * sr->rho * face_nut(&c, f, 1);
+            const double cp = w * g_cellCp[f->owner] + (1 - w) * right_cp(f);
+            energy -= rhoNut * cp / g_pr * (sr->T - sl->T) / f->distance;
+        }
         for (size_t k = 0; k < nv; ++k) flux[k] = advL * ql[k] + advR * qr[k];
         for (int d = 0; d < 3; ++d) flux[ns + d] += pM * f->normal[d] - traction[d];
         flux[ns + 3] += pE + energy;
@@ -348,6 +388,30 @@ int oracle_transport_rhs(const ReactiveTransportConfig* cfg, const double* volum
                 double J;
                 if (k == carrier) continue;
                 J = diffusion * (yr[k] - yl[k]) - (w * yl[k] + (1 - w) * yr[k]) * sumJ;
+                carrierFlux -= J;
+                flux[k] += J;
+                flux[ns + 3] += J * ((w * hl[k] + (1 - w) * hr[k]) - hc);
+            }
+            flux[carrier] += carrierFlux;
+        }
+        if (c.wale && g_sc > 0 && f->kind != 1) {
+            const double rhoNut = w * sl->rho * face_nut(&c, f, 0) + (1 - w) * sr->rho * face_nut(&c, f, 1);
+            const double sgs = -rhoNut / g_sc / f->distance;
+            const double *hl = g_cellH + (size_t)f->owner * ns, *hr = right_h(f, ns);
+            double sumJ = 0, largest = -1, carrierFlux = 0, hc;
+            size_t carrier = 0;
+            for (size_t k = 0; k < ns; ++k) {
+                const double yl = ql[k] / sl->rho, yr = qr[k] / sr->rho;
+                const double y = w * yl + (1 - w) * yr;
+                sumJ += sgs * (yr - yl);
+                if (y > largest) { largest = y; carrier = k; }
+            }
+            hc = w * hl[carrier] + (1 - w) * hr[carrier];
+            for (size_t k = 0; k < ns; ++k) {
+                double J;
+                const double yl = ql[k] / sl->rho, yr = qr[k] / sr->rho;
+                if (k == carrier) continue;
+                J = sgs * (yr - yl) - (w * yl + (1 - w) * yr) * sumJ;
                 carrierFlux -= J;
                 flux[k] += J;
                 flux[ns + 3] += J * ((w * hl[k] + (1 - w) * hr[k]) - hc);

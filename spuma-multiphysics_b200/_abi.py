@@ -73,6 +73,16 @@ class WaleProfile(C.Structure):
         (n, C.c_uint64) for n in ("gradientBuilds", "viscosityBuilds", "cellsEvaluated", "workspaceBytes")]
 
 
+class WaleScalarOptions(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32), ("turbulentPrandtl", C.c_double),
+                ("turbulentSchmidt", C.c_double)]
+
+
+class WaleScalarProfile(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32)] + [
+        (n, C.c_uint64) for n in ("fieldUploads", "fieldUploadBytes", "workspaceBytes")]
+
+
 class ThermoState(C.Structure):
     _fields_ = [(k, C.c_double) for k in (
         "p", "T", "rho", "e", "entropy", "soundFrozen", "soundEquilibrium",

@@ -131,7 +131,7 @@ def scaled_error(a, b):
     return float(np.max(np.abs(a - b) / scale))
 
 
-def create(lib, backend, case, wale_cw=None):
+def create(lib, backend, case, wale_cw=None, wale_scalars=None):
     error = C.create_string_buffer(4096)
     cfg = case["config"]
     handle = lib.reactive_transport_create(
@@ -143,7 +143,26 @@ def create(lib, backend, case, wale_cw=None):
         opts = A.WaleOptions(1, C.sizeof(A.WaleOptions), wale_cw)
         if lib.reactive_transport_set_wale_v1(C.c_void_p(handle), C.byref(opts)):
             raise RuntimeError(lib.reactive_transport_error(C.c_void_p(handle)).decode())
+    if wale_scalars is not None:
+        opts = A.WaleScalarOptions(1, C.sizeof(A.WaleScalarOptions), *wale_scalars)
+        if lib.reactive_transport_set_wale_scalars_v1(C.c_void_p(handle), C.byref(opts)):
+            raise RuntimeError(lib.reactive_transport_error(C.c_void_p(handle)).decode())
     return C.c_void_p(handle)
+
+
+def scalar_fields(case, seed=0):
+    """Mixture cp (J/kg/K) and effective species enthalpies (J/kg, cell-major)
+    for the cells and the fixed states of a case."""
+    rng = np.random.default_rng(700 + seed)
+    nc, ns, nf = case["nc"], case["ns"], max(1, case["config"].fixed)
+    return dict(cell_cp=rng.uniform(900, 1600, nc), fixed_cp=rng.uniform(900, 1600, nf),
+                cell_h=rng.uniform(-2e6, 3e6, (nc, ns)), fixed_h=rng.uniform(-2e6, 3e6, (nf, ns)))
+
+
+def upload_scalar_fields(lib, handle, fields, with_h=True):
+    return lib.reactive_transport_wale_scalar_fields_v1(
+        handle, dp(fields["cell_cp"]), dp(fields["cell_h"]) if with_h else None, dp(fields["fixed_cp"]),
+        dp(fields["fixed_h"]) if with_h else None)
 
 
 def bind(lib):
@@ -159,6 +178,9 @@ def bind(lib):
         "stable_step": ([v, d, s, C.c_double, C.c_double, d], C.c_int),
         "set_wale_v1": ([v, C.POINTER(A.WaleOptions)], C.c_int),
         "wale_primitives_v1": ([v, C.POINTER(A.Primitive), s, d], C.c_int),
+        "set_wale_scalars_v1": ([v, C.POINTER(A.WaleScalarOptions)], C.c_int),
+        "wale_scalar_profile_v1": ([v, C.POINTER(A.WaleScalarProfile)], C.c_int),
+        "wale_scalar_fields_v1": ([v, d, d, d, d], C.c_int),
     }
     for name, (args, ret) in sig.items():
         fn = getattr(lib, "reactive_transport_" + name)
