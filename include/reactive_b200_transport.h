@@ -78,13 +78,28 @@ int reactive_transport_replace_stage_state_v1(void* transport, ReactiveTransport
 /* src/reactiveTransport/reactiveTurbulence.h:20-25 (impl. reactiveTransport.cpp:1668-1709) */
 int reactive_transport_set_wale_v1(void* transport, const ReactiveWaleOptionsV1* options);
 int reactive_transport_wale_profile_v1(void* transport, ReactiveWaleProfileV1* profile);
+/* WALE scalar closure (src/reactiveTransport/reactiveTurbulence.h:26-45,
+ * src/reactiveTransport/reactiveTransport.cpp:653-702, 1671-1681): the
+ * turbulent heat flux rho nu_t cp / Pr_t grad T and the turbulent mixing of the
+ * total species mass fractions rho nu_t / Sc_t grad Y (with its enthalpy flux)
+ * on every non-slip face, and their diffusivities in the CFL step. Zero disables
+ * a term. Installed once, after set_wale_v1 and before any stage; species
+ * mixing needs variables == species + 4. The fields are the current mixture cp
+ * (J/kg/K) and the effective species enthalpies (J/kg), cell-major, for the
+ * cells and the fixed states (fixed pointers may be NULL without fixed
+ * states). NULL enthalpies refresh cp only (enough for the CFL step) and
+ * invalidate the previous enthalpies: a stage needs both. */
+int reactive_transport_set_wale_scalars_v1(void* transport, const ReactiveWaleScalarOptionsV1* options);
+int reactive_transport_wale_scalar_profile_v1(void* transport, ReactiveWaleScalarProfileV1* profile);
+int reactive_transport_wale_scalar_fields_v1(void* transport, const double* cellCp,
+    const double* cellSpeciesH, const double* fixedCp, const double* fixedSpeciesH);
 int reactive_transport_wale_primitives_v1(void* transport, const ReactiveTransportPrimitive* primitive,
     const ReactiveTransportState* state, double* nut);
 /* Out-of-scope reference entry points kept as stubs that return 1 with a
  * message, as the reference's own CPU build does for its CUDA-only paths
  * (src/reactiveTransport/reactiveTransport.cpp:1613-1630):
  * src/reactiveTransport/reactiveTransport.h:93-102 (NASA-generated gas properties),
- * :48-54 (capillary), src/reactiveTransport/reactiveTurbulence.h:47-85 (WALE scalars/PR). */
+ * :48-54 (capillary), src/reactiveTransport/reactiveTurbulence.h:47-85 (WALE PR properties). */
 int reactive_transport_set_gas_thermo(void* transport, const ReactiveGasThermoSpecies* species,
     size_t count, const ReactiveGasThermoRegion* regions, size_t regionCount,
     const int64_t* liquidSpecies, size_t liquids);
@@ -99,10 +114,6 @@ int reactive_transport_set_capillary_v1(void* transport, const void* options);
 int reactive_transport_capillary_geometry_v1(void* transport, const double* cellColor,
     const double* fixedColor, double* surfaceEnergy, double* curvature, double* normalXYZ);
 int reactive_transport_capillary_profile_v1(void* transport, void* profile);
-int reactive_transport_set_wale_scalars_v1(void* transport, const void* options);
-int reactive_transport_wale_scalar_profile_v1(void* transport, void* profile);
-int reactive_transport_wale_scalar_fields_v1(void* transport, const double* cellCp,
-    const double* cellSpeciesH, const double* fixedCp, const double* fixedSpeciesH);
 
 /* ---- additive device-resident entry points (no reference counterpart; the
  * reference's resident path is advance_resident_v2 + download_conserved,
@@ -161,8 +172,9 @@ int reactive_transport_precision_v3(void* transport, int request, int* active);
  * piecewise), viscous/WALE traction through the cells' velocity gradients and
  * eddy viscosities (with their own adjoints carried back through the WALE
  * relation and the Green-Gauss gradient to the neighbours' velocities), and
- * conduction. The derivative of the FP64 operator. The first call on a viscous
- * handle allocates its scratch. Asynchronous on `stream`. */
+ * conduction. The derivative of the FP64 operator; a handle with the WALE
+ * scalar closure is refused. The first call on a viscous handle allocates its
+ * scratch. Asynchronous on `stream`. */
 int reactive_transport_rate_vjp_v3(void* transport, const double* q, const ReactiveTransportState* state,
     const double* w, double* qBar, ReactiveTransportState* stateBar, void* stream);
 /* Launch-shape autotuner of the structured path (no reference counterpart).
@@ -174,8 +186,21 @@ int reactive_transport_rate_vjp_v3(void* transport, const double* q, const React
  * a graph. chosen (may be NULL) receives {stage, gradient, CFL} block sizes. */
 int reactive_transport_autotune_v3(void* transport, const double* q, const ReactiveTransportState* state,
     void* stream, unsigned* chosen);
+/* Device-resident refresh of the WALE scalar fields for the device stage
+ * entries (no reference counterpart: the reference fills them from the host or
+ * from its own PR property pass). Stream-ordered and allocation-free, so it can
+ * sit inside a captured graph. Reads cp[c * cpStride] and h[c * hStride + k]
+ * (k < species) for the cells c < cells and, when the fixed pointers are not
+ * NULL, the same strides for the fixed states; NULL fixed pointers keep the
+ * fixed values last set. cellCp is required when Pr_t > 0; NULL cellH
+ * invalidates the enthalpies, except with one species, whose mixing carries no
+ * flux. A cp that is not finite and positive or an enthalpy that is not finite
+ * sets bit 2 of the status word. */
+int reactive_transport_wale_scalar_fields_device_v3(void* transport, const double* cellCp, const double* cellH,
+    const double* fixedCp, const double* fixedH, size_t cpStride, size_t hStride, void* stream);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite,
- * bit 1 = an HLLC face could not be formed. Reading
+ * bit 1 = an HLLC face could not be formed, bit 2 = an invalid WALE scalar
+ * field from wale_scalar_fields_device_v3. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);
 

@@ -12,6 +12,7 @@
  *   ReactiveTransportToken                  src/reactiveTransport/reactiveTransport.h:34
  *   ReactiveTransportOptionsV21/ProfileV21  src/reactiveTransport/reactiveTransportV21.h:4-16
  *   ReactiveWaleOptionsV1 / ProfileV1       src/reactiveTransport/reactiveTurbulence.h:12-19
+ *   ReactiveWaleScalarOptionsV1 / ProfileV1 src/reactiveTransport/reactiveTurbulence.h:28-35
  *   ReactiveGasThermoSpecies/Region/Partition src/reactiveThermo/reactiveGasThermo.h:12-21
  *   ReactiveThermoState                     src/reactiveThermo/reactiveThermo.h:11-19
  *   ReactiveGpuHemProfileV1                 src/reactiveThermo/reactiveGpuHem.h:14-21
@@ -99,6 +100,16 @@ typedef struct ReactiveWaleProfileV1 {
     uint64_t gradientBuilds, viscosityBuilds, cellsEvaluated, workspaceBytes;
 } ReactiveWaleProfileV1;
 
+typedef struct ReactiveWaleScalarOptionsV1 {
+    uint32_t abiVersion, structBytes;
+    double turbulentPrandtl, turbulentSchmidt;
+} ReactiveWaleScalarOptionsV1;
+
+typedef struct ReactiveWaleScalarProfileV1 {
+    uint32_t abiVersion, structBytes;
+    uint64_t fieldUploads, fieldUploadBytes, workspaceBytes;
+} ReactiveWaleScalarProfileV1;
+
 typedef struct ReactiveGasThermoSpecies {
     uint64_t regionOffset, regionCount;
     double gasConstant;
@@ -183,6 +194,8 @@ typedef struct ReactiveB200HemModel {
 static_assert(sizeof(ReactiveTransportFace) == 80, "face layout");
 static_assert(sizeof(ReactiveTransportState) == 56, "state layout");
 static_assert(sizeof(ReactiveThermoState) == 176, "thermo state layout");
+static_assert(sizeof(ReactiveWaleScalarOptionsV1) == 24, "WALE scalar options layout");
+static_assert(sizeof(ReactiveWaleScalarProfileV1) == 32, "WALE scalar profile layout");
 static_assert(sizeof(ReactiveGpuHemOutputV1) == 184, "HEM output layout");
 static_assert(sizeof(ReactiveB200HemModel) == 47448, "HEM model image layout");
 static_assert(offsetof(ReactiveB200HemModel, stableGasPrune) == 45004, "HEM model image layout");

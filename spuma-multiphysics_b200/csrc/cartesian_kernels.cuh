@@ -40,12 +40,19 @@ struct CartView {
     bool wale;
     double cw;
     int scheme;  // 0 HLL, 1 HLLC
+    // WALE scalar closure: turbulent Prandtl / Schmidt numbers (0 disables a
+    // term), mixture cp (all) and effective species enthalpies (SoA ns x all)
+    bool sgs;
+    double pr, sc;
+    const double* mixCp;
+    const double* spH;
 };
 
 struct CellData {
     double q[kCartMaxNs + 4];
     double u[3];
     double p, T, rho, cv, c;
+    double cp, h[kCartMaxNs];  // WALE scalar closure only
 };
 
 // A cell's flux inputs in arithmetic type R (double, float, or a dual number
@@ -54,24 +61,37 @@ template <class R> struct CellT {
     R q[kCartMaxNs + 4];
     R u[3];
     R p, T, rho, cv, c;
+    R cp, h[kCartMaxNs];  // WALE scalar closure only
 };
-template <int NS, class R> __device__ __forceinline__ CellT<R> asCell(const CellData& d) {
+template <int NS, class R, bool SGS = false> __device__ __forceinline__ CellT<R> asCell(const CellData& d) {
     CellT<R> r;
 #pragma unroll
     for (int k = 0; k < NS + 4; ++k) r.q[k] = R(d.q[k]);
 #pragma unroll
     for (int a = 0; a < 3; ++a) r.u[a] = R(d.u[a]);
     r.p = R(d.p); r.T = R(d.T); r.rho = R(d.rho); r.cv = R(d.cv); r.c = R(d.c);
+    if constexpr (SGS) {
+        r.cp = R(d.cp);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) r.h[k] = R(d.h[k]);
+    }
     return r;
 }
 
-template <int NS>
+// SGS: also the cell's mixture cp (when Pr_t > 0) and, with its conserved
+// variables, its species enthalpies (when Sc_t > 0).
+template <int NS, bool SGS = false>
 __device__ __forceinline__ void loadCell(const CartView& v, const double* __restrict__ q,
                                          const ReactiveTransportState* __restrict__ st, size_t c, CellData& d,
                                          bool needQ) {
     if (needQ) {
 #pragma unroll
         for (int k = 0; k < NS + 4; ++k) d.q[k] = q[size_t(k) * v.all + c];
+    }
+    if constexpr (SGS) {
+        d.cp = v.pr > 0 ? v.mixCp[c] : 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) d.h[k] = needQ && v.sc > 0 ? v.spH[size_t(k) * v.all + c] : 0.0;
     }
     const ReactiveTransportPrimitive pr = v.primitive[c];
 #pragma unroll
@@ -82,13 +102,13 @@ __device__ __forceinline__ void loadCell(const CartView& v, const double* __rest
 
 // Right state of a boundary face of kind 1 (slip: velocity and momentum
 // mirrored), 2 (extrapolate: owner), 3 (fixed state).
-template <int NS>
+template <int NS, bool SGS = false>
 __device__ __forceinline__ void boundaryRight(const CartView& v, const double* __restrict__ q,
                                               const ReactiveTransportState* __restrict__ st,
                                               const ReactiveTransportFace& f, int axis, const CellData& L,
                                               CellData& R, bool needQ) {
     if (f.kind == 3) {
-        loadCell<NS>(v, q, st, v.cells + size_t(f.fixed), R, needQ);
+        loadCell<NS, SGS>(v, q, st, v.cells + size_t(f.fixed), R, needQ);
         return;
     }
     R = L;
@@ -118,7 +138,11 @@ __device__ __forceinline__ void twoSum(float& s, float& c, float x) {
 // the WALE viscosities of the owner and right sides. R is the arithmetic type:
 // double on the FP64 path (the face graph's exact operation sequence), float
 // on the mixed path (inputs rounded to FP32 once, every operation in FP32).
-template <int NS, class R>
+// SGS adds the WALE scalar closure: the turbulent heat flux rho nu_t cp / Pr_t
+// (T_R - T_L) / d and the turbulent species mixing of total mass fractions with
+// its enthalpy flux, in the face graph's operation order
+// (src/reactiveTransport/reactiveTransportKernels.h:150-168, :440-477).
+template <int NS, class R, bool SGS = false>
 __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double sgnD, double areaD, double distD,
                                              double wD, int kind, bool internal, const CellT<R>& L,
                                              const CellT<R>& Rt, const R* gL, const R* gR, R nutL, R nutR, R* F,
@@ -201,8 +225,47 @@ __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double
         for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * uL[d] + (R(1) - w) * uR[d]);
     }
     if (v.conductivity > 0 && kind != 1) energy -= R(v.conductivity) * (Rt.T - L.T) / dist;
+    R sgsJ[NS], sgsD = R(0), sgsSum = R(0), sgsCarrierFlux = R(0);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) sgsJ[k] = R(0);
+    if constexpr (SGS) {
+        if (v.pr > 0 && kind != 1) {
+            const R rhoNut = w * L.rho * nutL + (R(1) - w) * Rt.rho * nutR;
+            const R cp = w * L.cp + (R(1) - w) * Rt.cp;
+            energy -= rhoNut * cp / R(v.pr) * (Rt.T - L.T) / dist;
+        }
+        if (v.sc > 0 && kind != 1) {
+            const R rhoNut = w * L.rho * nutL + (R(1) - w) * Rt.rho * nutR;
+            sgsD = -rhoNut / R(v.sc) / dist;
+            R largest = R(-1), yL[NS], yR[NS];
+            int carrier = 0;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                yL[k] = L.q[k] / L.rho;
+                yR[k] = Rt.q[k] / Rt.rho;
+                sgsSum += sgsD * (yR[k] - yL[k]);
+                const R y = w * yL[k] + (R(1) - w) * yR[k];
+                if (y > largest) { largest = y; carrier = k; }
+            }
+            R hc = R(0);
+#pragma unroll
+            for (int k = 0; k < NS; ++k)
+                if (k == carrier) hc = w * L.h[k] + (R(1) - w) * Rt.h[k];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                if (k == carrier) continue;
+                const R J = sgsD * (yR[k] - yL[k]) - (w * yL[k] + (R(1) - w) * yR[k]) * sgsSum;
+                sgsCarrierFlux -= J;
+                energy += J * ((w * L.h[k] + (R(1) - w) * Rt.h[k]) - hc);
+                sgsJ[k] = J;
+            }
+#pragma unroll
+            for (int k = 0; k < NS; ++k)
+                if (k == carrier) sgsJ[k] = sgsCarrierFlux;
+        }
+    }
     if (v.wale) {
-        bad |= !isfinite(energy);
+        bad |= !isfinite(energy) || !isfinite(sgsD) || !isfinite(sgsSum) || !isfinite(sgsCarrierFlux);
 #pragma unroll
         for (int d = 0; d < 3; ++d) bad |= !isfinite(traction[d]);
     }
@@ -211,7 +274,12 @@ __device__ __forceinline__ void faceFluxCart(const CartView& v, int axis, double
         R flux = advL * L.q[k] + advR * Rt.q[k];
         if (k >= NS && k < NS + 3) flux += pM * nrm(k - NS, axis, sgn);
         if (k == NS + 3) flux += pE;
-        if (k >= NS && k < NS + 3) flux -= traction[k - NS];
+        if (k < NS) {
+            // species diffusion: no molecular term on this path, the mixing flux when on
+            R diffusion = R(0);
+            if (sgsD != R(0)) diffusion += sgsJ[k];
+            flux += diffusion;
+        } else if (k < NS + 3) flux -= traction[k - NS];
         else if (k == NS + 3) flux += energy;
         F[k] = flux * area;
     }
@@ -312,7 +380,7 @@ __global__ void __launch_bounds__(256) cartGradients(CartView v, const ReactiveT
 }
 
 // The flux of side s of cell c and this cell's incidence sign for it.
-template <int NS, class R>
+template <int NS, class R, bool SGS = false>
 __device__ __forceinline__ void sideFlux(const CartView& v, const double* __restrict__ q,
                                          const ReactiveTransportState* __restrict__ st,
                                          const R* __restrict__ grad, const R* __restrict__ nut, size_t c,
@@ -323,30 +391,30 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
     if (interior) {
         const size_t nb = neighbourOf(v, s, c);
         CellData N;
-        loadCell<NS>(v, q, st, nb, N, true);
+        loadCell<NS, SGS>(v, q, st, nb, N, true);
         R gN[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
             for (int jj = 0; jj < 9; ++jj) gN[jj] = grad[size_t(jj) * v.cells + nb];
         }
         const R nutN = v.wale ? nut[nb] : R(0);
-        const CellT<R> cc = asCell<NS, R>(C), cn = asCell<NS, R>(N);
+        const CellT<R> cc = asCell<NS, R, SGS>(C), cn = asCell<NS, R, SGS>(N);
         if (s & 1) {  // this cell owns the face
-            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc, cn, gC, gN, nutC, nutN, F,
-                                bad, faceBad);
+            faceFluxCart<NS, R, SGS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc, cn, gC, gN, nutC,
+                                     nutN, F, bad, faceBad);
             sign = -1;
         } else {
-            faceFluxCart<NS, R>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cn, cc, gN, gC, nutN, nutC, F,
-                                bad, faceBad);
+            faceFluxCart<NS, R, SGS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cn, cc, gN, gC, nutN,
+                                     nutC, F, bad, faceBad);
             sign = 1;
         }
     } else {
         const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
         CellData Rt;
-        boundaryRight<NS>(v, q, st, f, axis, C, Rt, true);
+        boundaryRight<NS, SGS>(v, q, st, f, axis, C, Rt, true);
         // a boundary face's right-side WALE viscosity is the owner's
-        faceFluxCart<NS, R>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
-                            asCell<NS, R>(C), asCell<NS, R>(Rt), gC, gC, nutC, nutC, F, bad, faceBad);
+        faceFluxCart<NS, R, SGS>(v, axis, (s & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind, false,
+                                 asCell<NS, R, SGS>(C), asCell<NS, R, SGS>(Rt), gC, gC, nutC, nutC, F, bad, faceBad);
         sign = -1;
     }
 }
@@ -359,7 +427,7 @@ __device__ __forceinline__ void sideFlux(const CartView& v, const double* __rest
 // added in FP64), divided by the volume in FP64, and the update applied to the
 // FP64 conserved state in FP64. Each internal face's FP32 flux is computed from
 // the same inputs by both of its cells, so it cancels exactly between them.
-template <int NS, class R>
+template <int NS, class R, bool SGS = false>
 __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __restrict__ q,
                                                  const ReactiveTransportState* __restrict__ st,
                                                  const R* __restrict__ grad, const R* __restrict__ nut,
@@ -371,7 +439,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
-        loadCell<NS>(v, q, st, c, C, true);
+        loadCell<NS, SGS>(v, q, st, c, C, true);
         R gC[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
@@ -390,7 +458,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
             if (interior != (n < 6)) continue;
             R F[NS + 4];
             double sign;
-            sideFlux<NS, R>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad, faceBad);
+            sideFlux<NS, R, SGS>(v, q, st, grad, nut, c, s, interior, i, j, k, C, gC, nutC, F, sign, bad, faceBad);
 #pragma unroll
             for (int kk = 0; kk < NS + 4; ++kk) {
                 if constexpr (fp64) rate[kk] += sign * F[kk] * iv;
@@ -411,8 +479,10 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
 }
 
 // Wave/diffusion speed of one face (faceSpeeds of the face graph); -1 when invalid.
+template <bool SGS = false>
 __device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, double sgn, double dist, double w,
-                                                const CellData& L, const CellData& R, double nutL, double nutR) {
+                                                int kind, const CellData& L, const CellData& R, double nutL,
+                                                double nutR) {
     const double unL = L.u[axis] * sgn, unR = R.u[axis] * sgn;
     const double aL = v.waveFactor * L.c, aR = v.waveFactor * R.c;
     const double left = dmin(0, dmin(unL - aL, unR - aR)), right = dmax(0, dmax(unL + aL, unR + aR));
@@ -421,14 +491,24 @@ __device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, dou
     const double mu = v.viscosity + rhoNut;
     const double D = 0.0 + dmax(dmax(4 * mu / (3 * L.rho), 4 * mu / (3 * R.rho)),
                                 dmax(v.conductivity / (L.rho * L.cv), v.conductivity / (R.rho * R.cv)));
-    double speed = dmax(fabs(unL) + aL, fabs(unR) + aR) + 2 * D / dist;
+    double scalar = 0;
+    if constexpr (SGS) {
+        if (kind != 1) {
+            if (v.pr > 0) {
+                const double k = rhoNut * (w * L.cp + (1 - w) * R.cp) / v.pr;
+                scalar = dmax(scalar, dmax(k / (L.rho * L.cv), k / (R.rho * R.cv)));
+            }
+            if (v.sc > 0) scalar = dmax(scalar, dmax(rhoNut / L.rho, rhoNut / R.rho) / v.sc);
+        }
+    }
+    double speed = dmax(fabs(unL) + aL, fabs(unR) + aR) + 2 * (D + scalar) / dist;
     if (!isfinite(unL) || !isfinite(unR) || !isfinite(speed) || !isfinite(invWave) || right <= left) speed = -1;
     return speed;
 }
 
 // CFL step of every cell from its six face speeds (cellSteps), folded to one
 // partial minimum per block with invalid steps absorbing as -1 (minimumReduce).
-template <int NS, class R>
+template <int NS, class R, bool SGS = false>
 __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTransportState* __restrict__ st,
                                                  const R* __restrict__ nut, double cfl, double maximumStep,
                                                  double* partial) {
@@ -438,7 +518,7 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
-        loadCell<NS>(v, nullptr, st, c, C, false);
+        loadCell<NS, SGS>(v, nullptr, st, c, C, false);
         const double nutC = v.wale ? double(nut[c]) : 0;
         double denominator = 0;
         bool bad = false, faceBad = false;
@@ -452,16 +532,17 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
             if (interior) {
                 const size_t nb = neighbourOf(v, s, c);
                 CellData N;
-                loadCell<NS>(v, nullptr, st, nb, N, false);
+                loadCell<NS, SGS>(v, nullptr, st, nb, N, false);
                 const double nutN = v.wale ? double(nut[nb]) : 0;
-                speed = (s & 1) ? faceSpeedCart(v, axis, 1.0, v.dist[axis], .5, C, N, nutC, nutN)
-                                : faceSpeedCart(v, axis, 1.0, v.dist[axis], .5, N, C, nutN, nutC);
+                speed = (s & 1) ? faceSpeedCart<SGS>(v, axis, 1.0, v.dist[axis], .5, 0, C, N, nutC, nutN)
+                                : faceSpeedCart<SGS>(v, axis, 1.0, v.dist[axis], .5, 0, N, C, nutN, nutC);
                 area = v.area[axis];
             } else {
                 const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
                 CellData Rt;
-                boundaryRight<NS>(v, nullptr, st, f, axis, C, Rt, false);
-                speed = faceSpeedCart(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight, C, Rt, nutC, nutC);
+                boundaryRight<NS, SGS>(v, nullptr, st, f, axis, C, Rt, false);
+                speed = faceSpeedCart<SGS>(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight, f.kind, C, Rt,
+                                           nutC, nutC);
                 area = f.area;
             }
             if (!isfinite(speed) || speed < 0) { bad = true; break; }
@@ -484,7 +565,7 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
 // Boundary ledger: the sum over boundary faces of each variable's face flux.
 // Pass 1 (this kernel) writes one partial per (block, variable) in a fixed
 // partition, pass 2 (foldPartials) adds them in block order: deterministic.
-template <int NS, class R>
+template <int NS, class R, bool SGS = false>
 __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __restrict__ q,
                                                   const ReactiveTransportState* __restrict__ st,
                                                   const R* __restrict__ grad, const R* __restrict__ nut,
@@ -502,8 +583,8 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
         const int axis = f.normal[0] != 0 ? 0 : (f.normal[1] != 0 ? 1 : 2);
         const double sgn = f.normal[axis] > 0 ? 1.0 : -1.0;
         CellData C, Rt;
-        loadCell<NS>(v, q, st, c, C, true);
-        boundaryRight<NS>(v, q, st, f, axis, C, Rt, true);
+        loadCell<NS, SGS>(v, q, st, c, C, true);
+        boundaryRight<NS, SGS>(v, q, st, f, axis, C, Rt, true);
         R g[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
@@ -511,8 +592,8 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
         }
         const R nutC = v.wale ? nut[c] : R(0);
         R F[NS + 4];
-        faceFluxCart<NS, R>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false, asCell<NS, R>(C), asCell<NS, R>(Rt), g, g, nutC, nutC, F,
-                         bad, faceBad);
+        faceFluxCart<NS, R, SGS>(v, axis, sgn, f.area, f.distance, f.ownerWeight, f.kind, false,
+                                 asCell<NS, R, SGS>(C), asCell<NS, R, SGS>(Rt), g, g, nutC, nutC, F, bad, faceBad);
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) sum[kk] += double(F[kk]);
     }

@@ -74,6 +74,8 @@ struct Transport {
     ReactiveTransportDeviceProfile deviceProfile{};
     ReactiveTransportProfileV21 cost{};
     ReactiveWaleProfileV1 waleProfile{1, sizeof(ReactiveWaleProfileV1), 0, 0, 0, 0};
+    ReactiveWaleScalarProfileV1 waleScalarProfile{1, sizeof(ReactiveWaleScalarProfileV1), 0, 0, 0};
+    bool scalarCp = false, scalarH = false;  // WALE scalar fields present for the next stage
     std::string physicalHash;
     uint64_t attemptId = 0, lastAttempt = 0, tokenStage = 0;
     bool attemptOpen = false;
@@ -453,6 +455,11 @@ struct Transport {
         b.wale = v.wale;
         b.cw = v.cw;
         b.scheme = fluxScheme;
+        b.sgs = v.sgs;
+        b.pr = v.pr;
+        b.sc = v.sc;
+        b.mixCp = v.mixCp;
+        b.spH = v.spH;
         return b;
     }
     template <template <int> class K, class... Args> void bySpecies(Args&&... args) {
@@ -482,22 +489,28 @@ struct Transport {
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                         const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
                         unsigned block, cudaStream_t s) {
-            cartRates<NS, R><<<gridFor(b.cells, block), block, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt,
-                                                                     error);
+            if (b.sgs)
+                cartRates<NS, R, true><<<gridFor(b.cells, block), block, 0, s>>>(b, q, st, grad, nut, out, stride,
+                                                                               mode, dt, error);
+            else
+                cartRates<NS, R><<<gridFor(b.cells, block), block, 0, s>>>(b, q, st, grad, nut, out, stride, mode,
+                                                                         dt, error);
         }
     };
     template <int NS> struct StepsK {
         template <class R>
         static void run(const CartView& b, const ReactiveTransportState* st, const R* nut, double cfl,
                         double maximumStep, double* partial, unsigned blocks, unsigned block, cudaStream_t s) {
-            cartSteps<NS, R><<<blocks, block, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
+            if (b.sgs) cartSteps<NS, R, true><<<blocks, block, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
+            else cartSteps<NS, R><<<blocks, block, 0, s>>>(b, st, nut, cfl, maximumStep, partial);
         }
     };
     template <int NS> struct LedgerK {
         template <class R>
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                         const R* nut, double* partial, unsigned blocks, cudaStream_t s) {
-            cartLedger<NS, R><<<blocks, 256, 0, s>>>(b, q, st, grad, nut, partial);
+            if (b.sgs) cartLedger<NS, R, true><<<blocks, 256, 0, s>>>(b, q, st, grad, nut, partial);
+            else cartLedger<NS, R><<<blocks, 256, 0, s>>>(b, q, st, grad, nut, partial);
         }
     };
     // Gradient (+ WALE viscosity) of the structured box, when the operator needs it.
@@ -571,6 +584,7 @@ struct Transport {
                        ReactiveTransportState* stateBar, cudaStream_t s) {
         require(structured, "The rate VJP needs the structured Cartesian path (reactive_transport_structured_v3)");
         require(fluxScheme == 0, "The rate VJP covers the HLL flux");
+        require(!v.sgs, "The rate VJP does not cover the WALE scalar closure");
         const bool viscous = cfg.viscosity > 0 || v.wale;
         if (viscous && !gradBar) {
             gradBar = arena.get<double>(product(cfg.cells, 9));
@@ -641,6 +655,8 @@ struct Transport {
 
     // ------------------------------------------------------- reference contract
     void prepareResident(const ReactiveTransportState* states, const double* gasY, const double* gasH, bool transport) {
+        requireScalarFields(transport);
+        ensureGraphScalarWork();
         uploadState(states);
         if (transport && cfg.diffusivity > 0) {
             packInto(const_cast<double*>(v.gasY), gasY, cfg.cells, cfg.species, v.all, 0);
@@ -712,6 +728,114 @@ struct Transport {
         v.cw = options.Cw;
         v.wale = true;
         waleProfile.workspaceBytes = arena.bytes - before + sizeof(uint32_t);
+    }
+    // WALE scalar closure (src/reactiveTransport/reactiveTransport.cpp:653-702).
+    void installWaleScalars(const ReactiveWaleScalarOptionsV1& options) {
+        require(options.abiVersion == 1 && options.structBytes == sizeof(options), "Invalid WALE scalar options ABI");
+        require(v.wale && !v.sgs && !highestVersion && !stats.stages && !stats.stepQueries
+                    && profile.conservedUploads == 0 && profile.stateUploadBytes == 0,
+                "WALE scalar closure is immutable and must be installed before stepping");
+        require(!cfg.mechanical, "WALE scalar mechanical-environment closure is not implemented");
+        require(std::isfinite(options.turbulentPrandtl) && std::isfinite(options.turbulentSchmidt)
+                    && options.turbulentPrandtl >= 0 && options.turbulentSchmidt >= 0,
+                "Invalid turbulent Prandtl/Schmidt number");
+        require(options.turbulentSchmidt == 0 || cfg.variables == cfg.species + 4,
+                "WALE total-species mixing requires equilibrium phase partition; frozen inventories are unsupported");
+        const size_t before = arena.bytes;
+        if (options.turbulentPrandtl > 0) v.mixCp = arena.get<double>(v.all);
+        if (options.turbulentSchmidt > 0) {
+            double* h = arena.get<double>(product(v.all, cfg.species));
+            check(cudaMemsetAsync(h, 0, product(v.all, cfg.species) * sizeof(double), stream), "memset");
+            v.spH = h;
+        }
+        v.pr = options.turbulentPrandtl;
+        v.sc = options.turbulentSchmidt;
+        v.sgs = true;
+        if (!structured) ensureGraphScalarWork();
+        finish();
+        waleScalarProfile.workspaceBytes = arena.bytes - before;
+    }
+    // The face graph's per-face mixing record (allocated on first use of the
+    // face graph: at install, on leaving the structured path, or by a host entry).
+    void ensureGraphScalarWork() {
+        if (!v.sgs || v.sc == 0 || v.sgsWork) return;
+        const size_t before = arena.bytes;
+        v.sgsWork = arena.get<double>(product(cfg.faces, 3));
+        v.sgsCarrier = arena.get<int>(cfg.faces);
+        waleScalarProfile.workspaceBytes += arena.bytes - before;
+    }
+    void uploadWaleScalarFields(const double* cellCp, const double* cellH, const double* fixedCp,
+                                const double* fixedH) {
+        require(v.sgs, "WALE scalar closure is not selected");
+        const bool uploadH = cellH || fixedH;
+        if (v.pr > 0) {
+            require(cellCp && (!cfg.fixed || fixedCp), "Missing WALE mixture heat capacities");
+            require(firstFailure(cfg.cells, [&](size_t c) { return std::isfinite(cellCp[c]) && cellCp[c] > 0; })
+                        == cfg.cells,
+                    "Invalid WALE mixture heat capacity");
+            require(firstFailure(cfg.fixed, [&](size_t c) { return std::isfinite(fixedCp[c]) && fixedCp[c] > 0; })
+                        == cfg.fixed,
+                    "Invalid fixed WALE mixture heat capacity");
+        }
+        if (v.sc > 0) {
+            require(!uploadH || (cellH && (!cfg.fixed || fixedH)), "Incomplete WALE effective species enthalpies");
+            if (uploadH) {
+                const size_t n = cfg.cells * cfg.species, m = cfg.fixed * cfg.species;
+                require(firstFailure(n, [&](size_t j) { return std::isfinite(cellH[j]); }) == n,
+                        "Invalid WALE effective species enthalpy");
+                require(firstFailure(m, [&](size_t j) { return std::isfinite(fixedH[j]); }) == m,
+                        "Invalid fixed WALE effective species enthalpy");
+            }
+        }
+        if (v.pr > 0) {
+            upload(const_cast<double*>(v.mixCp), cellCp, cfg.cells);
+            upload(const_cast<double*>(v.mixCp) + cfg.cells, fixedCp, cfg.fixed);
+        }
+        if (v.sc > 0 && uploadH) {
+            packInto(const_cast<double*>(v.spH), cellH, cfg.cells, cfg.species, v.all, 0);
+            packInto(const_cast<double*>(v.spH), fixedH, cfg.fixed, cfg.species, v.all, cfg.cells);
+        }
+        finish();
+        scalarCp = v.pr == 0 || cellCp;
+        scalarH = v.sc == 0 || uploadH;
+        ++waleScalarProfile.fieldUploads;
+        waleScalarProfile.fieldUploadBytes += (v.pr > 0 ? v.all * sizeof(double) : 0)
+            + (v.sc > 0 && uploadH ? v.all * cfg.species * sizeof(double) : 0);
+    }
+    void uploadWaleScalarFieldsDevice(const double* cellCp, const double* cellH, const double* fixedCp,
+                                      const double* fixedH, size_t cpStride, size_t hStride, cudaStream_t s) {
+        require(v.sgs, "WALE scalar closure is not selected");
+        require(v.pr == 0 || cellCp, "Missing WALE mixture heat capacities");
+        require((!cellCp || cpStride >= 1) && (!cellH || hStride >= cfg.species), "Invalid WALE scalar field strides");
+        const double* cp = v.pr > 0 ? cellCp : nullptr;
+        const double* h = v.sc > 0 ? cellH : nullptr;
+        if (cp || h) {
+            gatherScalarFields<<<gridFor(cfg.cells, 256), 256, 0, s>>>(cp, h, cpStride, hStride, cfg.cells, 0,
+                                                                       cfg.species, v.all, const_cast<double*>(v.mixCp),
+                                                                       const_cast<double*>(v.spH), flags);
+            launched();
+        }
+        const double* fcp = v.pr > 0 ? fixedCp : nullptr;
+        const double* fh = v.sc > 0 ? fixedH : nullptr;
+        if (cfg.fixed && (fcp || fh)) {
+            gatherScalarFields<<<gridFor(cfg.fixed, 256), 256, 0, s>>>(fcp, fh, cpStride, hStride, cfg.fixed,
+                                                                       cfg.cells, cfg.species, v.all,
+                                                                       const_cast<double*>(v.mixCp),
+                                                                       const_cast<double*>(v.spH), flags);
+            launched();
+        }
+        scalarCp = true;
+        scalarH = v.sc == 0 || cellH || cfg.species == 1;
+        ++waleScalarProfile.fieldUploads;
+    }
+    // Stage / CFL preconditions (src/reactiveTransport/reactiveTransport.cpp:1395-1397, 1415-1416).
+    void requireScalarFields(bool transport) const {
+        if (!v.sgs) return;
+        if (transport)
+            require((v.pr == 0 || scalarCp) && (v.sc == 0 || scalarH),
+                    "WALE scalar heat capacities/enthalpies were not uploaded for this thermodynamic stage");
+        else
+            require(v.pr == 0 || scalarCp, "WALE scalar heat capacities were not uploaded for this thermodynamic stage");
     }
     void uploadPrimitives(const ReactiveTransportPrimitive* primitive, const ReactiveTransportState* state) {
         require(primitive, "Null transport primitives");

@@ -7,7 +7,8 @@
 //   cellWale         <- WaleViscosities  :303-313
 //   faceSpeeds       <- FaceSpeeds       :315-341
 //   faceWork         <- Faces            :343-500 (HLL core, viscous/WALE traction,
-//                                                  conduction, Fick diffusion)
+//                                                  conduction, Fick diffusion, WALE
+//                                                  scalar heat flux and species mixing)
 //   cellRates        <- Rhs / Advance    :502-528, :551-560
 //   cellSteps        <- Step             :529-549
 // The data layout is this project's: conserved and gas fields are SoA with
@@ -50,6 +51,20 @@ struct GraphView {
     double* faceSpeed = nullptr;                     // faces
     double* step = nullptr;                          // cells
     unsigned* waleError = nullptr;
+    // WALE scalar closure (turbulent Prandtl heat flux rho nu_t cp / Pr_t grad T,
+    // turbulent Schmidt species mixing rho nu_t / Sc_t grad Y); 0 disables a term
+    bool sgs = false;
+    double pr = 0, sc = 0;
+    const double* mixCp = nullptr;                   // all, mixture cp
+    const double* spH = nullptr;                     // SoA ns x all, effective species enthalpies
+    double* sgsWork = nullptr;                       // SoA 3 x faces: diffusion, sumJ, carrier flux
+    int* sgsCarrier = nullptr;                       // faces
+};
+
+// The species-mixing record of one face (zero diffusion: no mixing flux).
+struct SgsFace {
+    double diffusion = 0, sumJ = 0, carrierFlux = 0, rhoL = 1, rhoR = 1;
+    int carrier = 0;
 };
 
 __device__ __forceinline__ size_t rightCell(const GraphView& v, const ReactiveTransportFace& f) {
@@ -71,6 +86,19 @@ __device__ __forceinline__ void sideVelocities(const GraphView& v, const Reactiv
 __device__ __forceinline__ double faceNut(const GraphView& v, const ReactiveTransportFace& f, bool right) {
     if (!v.wale) return 0;
     return v.nut[right && f.neighbour >= 0 ? size_t(f.neighbour) : size_t(f.owner)];
+}
+
+__device__ __forceinline__ SgsFace loadSgs(const GraphView& v, const ReactiveTransportFace& f, size_t fi, size_t r) {
+    SgsFace g;
+    if (v.sgs && v.sc > 0) {
+        g.diffusion = v.sgsWork[fi];
+        g.sumJ = v.sgsWork[v.faces + fi];
+        g.carrierFlux = v.sgsWork[2 * v.faces + fi];
+        g.carrier = v.sgsCarrier[fi];
+        g.rhoL = v.state[f.owner].rho;
+        g.rhoR = v.state[r].rho;
+    }
+    return g;
 }
 
 __global__ void cellPrimitives(GraphView v, size_t begin, size_t end) {
@@ -139,7 +167,16 @@ __global__ void faceSpeeds(GraphView v) {
         const double D = v.diffusivity
             + dmax(dmax(4 * mu / (3 * sl.rho), 4 * mu / (3 * sr.rho)),
                    dmax(v.conductivity / (sl.rho * sl.cv), v.conductivity / (sr.rho * sr.cv)));
-        double speed = dmax(fabs(unL) + aL, fabs(unR) + aR) + 2 * D / f.distance;
+        double scalar = 0;
+        if (v.sgs && f.kind != 1) {
+            const size_t r = rightCell(v, f);
+            if (v.pr > 0) {
+                const double k = rhoNut * (f.ownerWeight * v.mixCp[f.owner] + (1 - f.ownerWeight) * v.mixCp[r]) / v.pr;
+                scalar = dmax(scalar, dmax(k / (sl.rho * sl.cv), k / (sr.rho * sr.cv)));
+            }
+            if (v.sc > 0) scalar = dmax(scalar, dmax(rhoNut / sl.rho, rhoNut / sr.rho) / v.sc);
+        }
+        double speed = dmax(fabs(unL) + aL, fabs(unR) + aR) + 2 * (D + scalar) / f.distance;
         if (!isfinite(unL) || !isfinite(unR) || !isfinite(speed) || !isfinite(invWave) || right <= left)
             speed = -1;
         v.faceSpeed[fi] = speed;
@@ -192,6 +229,11 @@ __global__ void faceWork(GraphView v) {
             for (int d = 0; d < 3; ++d) energy -= traction[d] * (w * ul[d] + (1 - w) * ur[d]);
         }
         if (v.conductivity > 0 && f.kind != 1) energy -= v.conductivity * (sr.T - sl.T) / f.distance;
+        if (v.sgs && v.pr > 0 && f.kind != 1) {
+            const double rhoNut = w * sl.rho * faceNut(v, f, false) + (1 - w) * sr.rho * faceNut(v, f, true);
+            const double cp = w * v.mixCp[l] + (1 - w) * v.mixCp[r];
+            energy -= rhoNut * cp / v.pr * (sr.T - sl.T) / f.distance;
+        }
         int carrier = 0;
         if (v.diffusivity > 0 && sl.gasMass > 0 && sr.gasMass > 0 && f.kind != 1) {
             const double mass = f.neighbour >= 0
@@ -218,8 +260,36 @@ __global__ void faceWork(GraphView v) {
             out[FW_SUM_J] = sumJ;
             out[FW_CARRIER_FLUX] = carrierFlux;
         }
+        SgsFace sg;
+        if (v.sgs && v.sc > 0 && f.kind != 1) {
+            const double rhoNut = w * sl.rho * faceNut(v, f, false) + (1 - w) * sr.rho * faceNut(v, f, true);
+            sg.diffusion = -rhoNut / v.sc / f.distance;
+            double largest = -1;
+            for (size_t k = 0; k < v.ns; ++k) {
+                const double yl = v.q[k * v.all + l] / sl.rho, yr = v.q[k * v.all + r] / sr.rho;
+                sg.sumJ += sg.diffusion * (yr - yl);
+                const double y = w * yl + (1 - w) * yr;
+                if (y > largest) { largest = y; sg.carrier = int(k); }
+            }
+            const size_t kc = size_t(sg.carrier);
+            const double hc = w * v.spH[kc * v.all + l] + (1 - w) * v.spH[kc * v.all + r];
+            for (size_t k = 0; k < v.ns; ++k) {
+                if (k == kc) continue;
+                const double yl = v.q[k * v.all + l] / sl.rho, yr = v.q[k * v.all + r] / sr.rho;
+                const double J = sg.diffusion * (yr - yl) - (w * yl + (1 - w) * yr) * sg.sumJ;
+                sg.carrierFlux -= J;
+                const double hk = w * v.spH[k * v.all + l] + (1 - w) * v.spH[k * v.all + r];
+                energy += J * (hk - hc);
+            }
+        }
+        if (v.sgs && v.sc > 0) {
+            v.sgsWork[fi] = sg.diffusion;
+            v.sgsWork[v.faces + fi] = sg.sumJ;
+            v.sgsWork[2 * v.faces + fi] = sg.carrierFlux;
+            v.sgsCarrier[fi] = sg.carrier;
+        }
         if (v.wale) {
-            bool bad = !isfinite(energy);
+            bool bad = !isfinite(energy) || !isfinite(sg.diffusion) || !isfinite(sg.sumJ) || !isfinite(sg.carrierFlux);
             for (int d = 0; d < 3; ++d) bad |= !isfinite(traction[d]);
             if (bad) atomicOr(v.waleError, 1u);
         }
@@ -233,9 +303,10 @@ __global__ void faceWork(GraphView v) {
 }
 
 // Flux of variable k through face fi, times the face area (the reference's
-// View::faceFlux, src/reactiveTransport/reactiveTransportKernels.h:180-191).
+// View::faceFlux with speciesDiffusion and sgsSpeciesFlux,
+// src/reactiveTransport/reactiveTransportKernels.h:150-191).
 __device__ __forceinline__ double faceFluxK(const GraphView& v, const ReactiveTransportFace& f, size_t fi,
-                                            size_t r, size_t k, const double* wk, int carrier) {
+                                            size_t r, size_t k, const double* wk, int carrier, const SgsFace& sg) {
     const size_t l = size_t(f.owner);
     const double ql = v.q[k * v.all + l];
     double qr = v.q[k * v.all + r];
@@ -249,13 +320,23 @@ __device__ __forceinline__ double faceFluxK(const GraphView& v, const ReactiveTr
     if (k >= ns && k < ns + 3) flux += wk[FW_P_MOM] * f.normal[k - ns];
     if (k == ns + 3) flux += wk[FW_P_ENERGY];
     if (k < ns) {
+        double diffusion = 0;
         if (wk[FW_DIFFUSION] != 0) {
-            if (int(k) == carrier) flux += wk[FW_CARRIER_FLUX];
+            if (int(k) == carrier) diffusion += wk[FW_CARRIER_FLUX];
             else {
                 const double yl = v.gasY[k * v.all + l], yr = v.gasY[k * v.all + r];
-                flux += wk[FW_DIFFUSION] * (yr - yl) - (f.ownerWeight * yl + (1 - f.ownerWeight) * yr) * wk[FW_SUM_J];
+                diffusion += wk[FW_DIFFUSION] * (yr - yl)
+                    - (f.ownerWeight * yl + (1 - f.ownerWeight) * yr) * wk[FW_SUM_J];
             }
         }
+        if (sg.diffusion != 0) {
+            if (int(k) == sg.carrier) diffusion += sg.carrierFlux;
+            else {
+                const double yl = v.q[k * v.all + l] / sg.rhoL, yr = v.q[k * v.all + r] / sg.rhoR;
+                diffusion += sg.diffusion * (yr - yl) - (f.ownerWeight * yl + (1 - f.ownerWeight) * yr) * sg.sumJ;
+            }
+        }
+        flux += diffusion;
     } else if (k < ns + 3) flux -= wk[FW_TRACTION_X + (k - ns)];
     else if (k == ns + 3) flux += wk[FW_ENERGY];
     return flux * f.area;
@@ -294,10 +375,11 @@ __global__ void cellRates(GraphView v, double* out, size_t outStride, int mode, 
 #pragma unroll
                 for (int t = 0; t < FW_FIELDS; ++t) wk[t] = v.work[size_t(t) * v.faces + fi];
                 const int carrier = v.carrier[fi];
+                const SgsFace sg = loadSgs(v, f, fi, r);
 #pragma unroll
                 for (int kk = 0; kk < CHUNK; ++kk) {
                     const size_t k = k0 + kk;
-                    if (k < v.nv) acc[kk] += sign * faceFluxK(v, f, fi, r, k, wk, carrier) * iv;
+                    if (k < v.nv) acc[kk] += sign * faceFluxK(v, f, fi, r, k, wk, carrier, sg) * iv;
                 }
             }
 #pragma unroll
@@ -365,7 +447,8 @@ __global__ void boundaryLedger(GraphView v, double* rate) {
         const ReactiveTransportFace f = v.face[fi];
         double wk[FW_FIELDS];
         for (int t = 0; t < FW_FIELDS; ++t) wk[t] = v.work[size_t(t) * v.faces + fi];
-        s += faceFluxK(v, f, fi, rightCell(v, f), k, wk, v.carrier[fi]);
+        const size_t r = rightCell(v, f);
+        s += faceFluxK(v, f, fi, r, k, wk, v.carrier[fi], loadSgs(v, f, fi, r));
     }
     s = warpSum(s);
     if ((threadIdx.x & 31) == 0) warpValues[threadIdx.x >> 5] = s;
@@ -374,6 +457,30 @@ __global__ void boundaryLedger(GraphView v, double* rate) {
         s = threadIdx.x < (blockDim.x >> 5) ? warpValues[threadIdx.x] : 0.0;
         s = warpSum(s);
         if (threadIdx.x == 0) rate[k] = s;
+    }
+}
+
+// Strided gather of the WALE scalar fields into the handle's arrays: cp of entry
+// c to mixCp[offset + c], enthalpy k to spH[k * all + offset + c]. A cp that is
+// not finite and positive or a non-finite enthalpy sets bit 2 of the status.
+__global__ void gatherScalarFields(const double* __restrict__ cp, const double* __restrict__ h, size_t cpStride,
+                                   size_t hStride, size_t count, size_t offset, size_t ns, size_t all,
+                                   double* __restrict__ mixCp, double* __restrict__ spH, unsigned* status) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
+        bool bad = false;
+        if (cp) {
+            const double x = cp[c * cpStride];
+            bad |= !(isfinite(x) && x > 0);
+            mixCp[offset + c] = x;
+        }
+        if (h) {
+            for (size_t k = 0; k < ns; ++k) {
+                const double y = h[c * hStride + k];
+                bad |= !isfinite(y);
+                spH[k * all + offset + c] = y;
+            }
+        }
+        if (bad) atomicOr(status, 4u);
     }
 }
 

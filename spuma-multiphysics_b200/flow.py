@@ -56,11 +56,15 @@ def _check(lib, handle, rc):
 
 class Flow:
     def __init__(self, faces, volume, q0, guess0, fixed_q, fixed_guess, viscosity=0.0, conductivity=0.0,
-                 wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda", precision="fp64"):
+                 wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda", precision="fp64",
+                 turbulent_prandtl=None, turbulent_schmidt=None):
         """faces: FACE_DTYPE array; q0: cell-major (cells, 5) conserved state;
         guess0/fixed_guess: THERMO_DTYPE seeds used for the initial recovery.
         precision: "fp64", or "mixed" (FP32 gradients, WALE and face fluxes with
-        compensated per-cell sums into the FP64 state; needs a structured box)."""
+        compensated per-cell sums into the FP64 state; needs a structured box).
+        turbulent_prandtl / turbulent_schmidt: the WALE scalar closure (needs
+        wale_cw; 0 disables a term), fed each stage with the mixture cp of that
+        stage's equilibrium states."""
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"unknown precision {precision!r}")
         self.lib = _lib.load()
@@ -99,6 +103,12 @@ class Flow:
         if wale_cw is not None:
             opts = A.WaleOptions(1, C.sizeof(A.WaleOptions), wale_cw)
             _check(self.lib, self.transport, self.lib.reactive_transport_set_wale_v1(self.transport, C.byref(opts)))
+        self.scalars = turbulent_prandtl is not None or turbulent_schmidt is not None
+        if self.scalars:
+            opts = A.WaleScalarOptions(1, C.sizeof(A.WaleScalarOptions), turbulent_prandtl or 0.0,
+                                       turbulent_schmidt or 0.0)
+            _check(self.lib, self.transport,
+                   self.lib.reactive_transport_set_wale_scalars_v1(self.transport, C.byref(opts)))
         self.precision = precision
         if precision == "mixed":
             _check(self.lib, self.transport, self.lib.reactive_transport_precision_v3(self.transport, 1, None))
@@ -121,7 +131,11 @@ class Flow:
                             ("gasMass", "gasMass")):
             tr0[k_out] = state0[k_in]
         self.tr[:self.cells] = torch.from_numpy(tr0.view(np.float64).reshape(self.cells, 7)).to(dev)
+        # fixed-state thermo (constant): the WALE scalar closure's fixed cp
+        self.fixed_thermo = torch.from_numpy(fixed_state.view(np.uint8).copy()).to(dev)
         torch.cuda.synchronize(dev)
+        if self.scalars:
+            self._scalar_fields(self.sn, fixed=True)
         _check(self.lib, self.transport,
                self.lib.reactive_transport_fill_fixed_v3(self.transport, self.qn.data_ptr(), self.tr.data_ptr(), s))
         _check(self.lib, self.transport,
@@ -132,14 +146,29 @@ class Flow:
         self.steps = 0
 
     # ------------------------------------------------------------------ step
+    _CP_OFFSET = A.THERMO_DTYPE.fields["cp"][1]
+    _THERMO_DOUBLES = A.THERMO_DTYPE.itemsize // 8
+
+    def _scalar_fields(self, thermo, fixed=False):
+        """Point the WALE scalar closure at the mixture cp of `thermo` (one
+        species: no enthalpies are needed)."""
+        lib, t, s = self.lib, self.transport, self.stream.cuda_stream
+        fixed_cp = self.fixed_thermo.data_ptr() + self._CP_OFFSET if fixed and self.fixed else None
+        _check(lib, t, lib.reactive_transport_wale_scalar_fields_device_v3(
+            t, thermo.data_ptr() + self._CP_OFFSET, None, fixed_cp, None, self._THERMO_DOUBLES, 1, s))
+
     def _launch_step(self, dt, per_cell=False):
         lib, t, s = self.lib, self.transport, self.stream.cuda_stream
+        if self.scalars:
+            self._scalar_fields(self.sn)
         _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.qn.data_ptr(), self.tr.data_ptr(),
                                                                     self.cfl, dt, self.dt_cfl.data_ptr(), s))
         _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.qn.data_ptr(), self.q1.data_ptr(),
                                                               self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(), s))
         self.hem.run_device(self.q1, self.qn.shape[1], self.cells, self.nv, self.sn, self.s1, self.tr, self.success, s,
                             per_cell)
+        if self.scalars:
+            self._scalar_fields(self.s1)
         _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.q1.data_ptr(), self.tr.data_ptr(),
                                                                     self.cfl, dt, self.dt_cfl[1:].data_ptr(), s))
         _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.q1.data_ptr(), self.qn.data_ptr(),
@@ -201,8 +230,12 @@ class Flow:
                self.lib.reactive_transport_status_v3(self.transport, C.byref(status), 1, self.stream.cuda_stream))
         failed = int((self.success == 0).sum().item())
         cfl = self.dt_cfl.min().item()
-        if status.value:
+        if status.value & 1:
             raise FlowError("WALE gradient/viscosity/traction became non-finite")
+        if status.value & 2:
+            raise FlowError("an HLLC face flux could not be formed")
+        if status.value & 4:
+            raise FlowError("a WALE scalar field (mixture cp) was not finite and positive")
         if failed:
             raise FlowError(f"HEM recovery failed in {failed} cells")
         if not (cfl > 0 and dt <= cfl * (1 + 1e-10)):

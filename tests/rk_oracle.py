@@ -25,7 +25,7 @@ def internal_energy(q):
 
 class ReferenceFlow:
     def __init__(self, faces, volume, q0, guess0, fixed_q, fixed_guess, viscosity, conductivity, wale_cw, image,
-                 wave_factor=1.1, threads=1):
+                 wave_factor=1.1, threads=1, turbulent_prandtl=None, turbulent_schmidt=None):
         self.lib = oracle.ref_transport_lib()
         self.image = image
         self.threads = threads
@@ -54,9 +54,28 @@ class ReferenceFlow:
         if wale_cw is not None:
             opts = A.WaleOptions(1, C.sizeof(A.WaleOptions), wale_cw)
             assert self.lib.reactive_transport_set_wale_v1(self.h, C.byref(opts)) == 0
+        self.scalars = turbulent_prandtl is not None or turbulent_schmidt is not None
+        if self.scalars:
+            # the WALE scalar closure, fed each stage with that stage's mixture
+            # cp through the host field upload (one species: the enthalpies
+            # carry no flux, zeros stand in for them)
+            opts = A.WaleScalarOptions(1, C.sizeof(A.WaleScalarOptions), turbulent_prandtl or 0.0,
+                                       turbulent_schmidt or 0.0)
+            assert self.lib.reactive_transport_set_wale_scalars_v1(self.h, C.byref(opts)) == 0, \
+                self.lib.reactive_transport_error(self.h)
+            self.lib.reactive_transport_wale_scalar_fields_v1.argtypes = [C.c_void_p, d, d, d, d]
+            self.zero_h = np.zeros(len(volume) + len(fixed_q))
         self.boundary = np.zeros(5)
 
     def _stage(self, states, dt, stage):
+        if self.scalars:
+            d = C.POINTER(C.c_double)
+            cp = np.ascontiguousarray(states["cp"])
+            fixed_cp = np.ascontiguousarray(self.fixed_state["cp"])
+            rc = self.lib.reactive_transport_wale_scalar_fields_v1(
+                self.h, cp.ctypes.data_as(d), self.zero_h.ctypes.data_as(d), fixed_cp.ctypes.data_as(d),
+                self.zero_h.ctypes.data_as(d))
+            assert rc == 0, self.lib.reactive_transport_error(self.h)
         tr = compact(states)
         br = np.zeros(5)
         rc = self.lib.reactive_transport_stage(self.h, self.q.ctypes.data_as(C.POINTER(C.c_double)),

@@ -67,52 +67,4 @@ def test_wale_scalars_oracle_matches_reference_cpu(ref, spec, pr, sc):
 def test_wale_scalar_contract_on_reference_cpu(ref):
     """Install preconditions, field validation and the stage/CFL preconditions
     (reactiveTransport.cpp:653-702, :1395-1397, :1415-1416)."""
-    ns, nc, kind, spatial, viscous, cw = T.WALE_CASES[1]
-    case = T.make_case(ns, nc, kind, spatial=spatial, viscous_only=viscous, seed=5)
-    fields = T.scalar_fields(case)
-    q, st = case["q"], case["states"]
-    rhs, br, dt = np.empty_like(q), np.empty(case["nv"]), C.c_double()
-    opts = lambda pr, sc: C.byref(A.WaleScalarOptions(1, C.sizeof(A.WaleScalarOptions), pr, sc))
-    h = T.create(ref, 0, case)
-    try:  # without WALE
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) != 0
-    finally:
-        ref.reactive_transport_destroy(h)
-    h = T.create(ref, 0, case, wale_cw=cw)
-    try:
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(-1, .7)) != 0
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(.9, float("nan"))) != 0
-        bad = A.WaleScalarOptions(2, C.sizeof(A.WaleScalarOptions), .9, .7)
-        assert ref.reactive_transport_set_wale_scalars_v1(h, C.byref(bad)) != 0
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) == 0
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) != 0  # immutable
-        # not uploaded: stage and CFL refuse
-        assert ref.reactive_transport_rhs(h, T.dp(q), T.states_ptr(st), None, None, T.dp(rhs), T.dp(br)) != 0
-        assert ref.reactive_transport_stable_step(h, T.dp(q), T.states_ptr(st), .23, .1, C.byref(dt)) != 0
-        badcp = dict(fields, cell_cp=fields["cell_cp"].copy())
-        badcp["cell_cp"][3] = 0.0
-        assert T.upload_scalar_fields(ref, h, badcp) != 0
-        badh = dict(fields, fixed_h=fields["fixed_h"].copy())
-        badh["fixed_h"][0, 1] = float("inf")
-        assert T.upload_scalar_fields(ref, h, badh) != 0
-        # cp only: the CFL runs, the RHS needs the enthalpies too
-        assert T.upload_scalar_fields(ref, h, fields, with_h=False) == 0
-        assert ref.reactive_transport_stable_step(h, T.dp(q), T.states_ptr(st), .23, .1, C.byref(dt)) == 0
-        assert ref.reactive_transport_rhs(h, T.dp(q), T.states_ptr(st), None, None, T.dp(rhs), T.dp(br)) != 0
-        assert T.upload_scalar_fields(ref, h, fields) == 0
-        assert ref.reactive_transport_rhs(h, T.dp(q), T.states_ptr(st), None, None, T.dp(rhs), T.dp(br)) == 0
-        prof = A.WaleScalarProfile(1, C.sizeof(A.WaleScalarProfile))
-        assert ref.reactive_transport_wale_scalar_profile_v1(h, C.byref(prof)) == 0
-        all_ = nc + case["config"].fixed
-        assert prof.fieldUploads == 2
-        assert prof.fieldUploadBytes == 2 * all_ * 8 + all_ * ns * 8
-    finally:
-        ref.reactive_transport_destroy(h)
-    # species mixing needs variables == species + 4
-    frozen = T.make_case(2, 7, 2, transport=True, frozen=1)
-    h = T.create(ref, 0, frozen, wale_cw=.325)
-    try:
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) != 0
-        assert ref.reactive_transport_set_wale_scalars_v1(h, opts(.9, 0)) == 0
-    finally:
-        ref.reactive_transport_destroy(h)
+    T.wale_scalar_contract(ref, 0)

@@ -331,3 +331,58 @@ def large_cfl_walk(lib, backend, nc):
         assert prof.conservedUploadBytes == 0
     finally:
         lib.reactive_transport_destroy(handle)
+
+
+def wale_scalar_contract(lib, backend):
+    """The WALE scalar closure's install preconditions, field validation and
+    stage/CFL preconditions (src/reactiveTransport/reactiveTransport.cpp:653-702,
+    :1395-1397, :1415-1416) on one implementation."""
+    ns, nc, kind, spatial, viscous, cw = WALE_CASES[1]
+    case = make_case(ns, nc, kind, spatial=spatial, viscous_only=viscous, seed=5)
+    fields = scalar_fields(case)
+    q, st = case["q"], case["states"]
+    rhs, br, dt = np.empty_like(q), np.empty(case["nv"]), C.c_double()
+    opts = lambda pr, sc: C.byref(A.WaleScalarOptions(1, C.sizeof(A.WaleScalarOptions), pr, sc))
+    h = create(lib, backend, case)
+    try:  # without WALE
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) != 0
+    finally:
+        lib.reactive_transport_destroy(h)
+    h = create(lib, backend, case, wale_cw=cw)
+    try:
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(-1, .7)) != 0
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(.9, float("nan"))) != 0
+        bad = A.WaleScalarOptions(2, C.sizeof(A.WaleScalarOptions), .9, .7)
+        assert lib.reactive_transport_set_wale_scalars_v1(h, C.byref(bad)) != 0
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) == 0
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) != 0  # immutable
+        # not uploaded: stage and CFL refuse
+        assert lib.reactive_transport_rhs(h, dp(q), states_ptr(st), None, None, dp(rhs), dp(br)) != 0
+        assert lib.reactive_transport_stable_step(h, dp(q), states_ptr(st), .23, .1, C.byref(dt)) != 0
+        badcp = dict(fields, cell_cp=fields["cell_cp"].copy())
+        badcp["cell_cp"][3] = 0.0
+        assert upload_scalar_fields(lib, h, badcp) != 0
+        badh = dict(fields, fixed_h=fields["fixed_h"].copy())
+        badh["fixed_h"][0, 1] = float("inf")
+        assert upload_scalar_fields(lib, h, badh) != 0
+        # cp only: the CFL runs, the RHS needs the enthalpies too
+        assert upload_scalar_fields(lib, h, fields, with_h=False) == 0
+        assert lib.reactive_transport_stable_step(h, dp(q), states_ptr(st), .23, .1, C.byref(dt)) == 0
+        assert lib.reactive_transport_rhs(h, dp(q), states_ptr(st), None, None, dp(rhs), dp(br)) != 0
+        assert upload_scalar_fields(lib, h, fields) == 0
+        assert lib.reactive_transport_rhs(h, dp(q), states_ptr(st), None, None, dp(rhs), dp(br)) == 0
+        prof = A.WaleScalarProfile(1, C.sizeof(A.WaleScalarProfile))
+        assert lib.reactive_transport_wale_scalar_profile_v1(h, C.byref(prof)) == 0
+        all_ = nc + case["config"].fixed
+        assert prof.fieldUploads == 2
+        assert prof.fieldUploadBytes == 2 * all_ * 8 + all_ * ns * 8
+    finally:
+        lib.reactive_transport_destroy(h)
+    # species mixing needs variables == species + 4
+    frozen = make_case(2, 7, 2, transport=True, frozen=1)
+    h = create(lib, backend, frozen, wale_cw=.325)
+    try:
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(.9, .7)) != 0
+        assert lib.reactive_transport_set_wale_scalars_v1(h, opts(.9, 0)) == 0
+    finally:
+        lib.reactive_transport_destroy(h)
