@@ -534,9 +534,19 @@ def run_flash_batch(args):
     pkg = load_package()
     from spuma_multiphysics_b200 import _abi as A, cases, thermo_data as td
     from spuma_multiphysics_b200.hem import GpuHem
-    n = args.flash_batch
     t0 = time.time()
-    q, e, guess = cases.flash_batch(n, seed=20260303, saturation_levels=65536 if n > 1000000 else 0)
+    if args.flash_checkpoint:
+        # the cells of a committed checkpoint, seeded by their committed states
+        from spuma_multiphysics_b200 import checkpoint
+        q, e, guess, _ = checkpoint.flash_batch(args.flash_checkpoint)
+        n = len(q)
+        workload = f"batched HEM UV flash of the {n:,} cells of checkpoint {Path(args.flash_checkpoint).name}"
+        data = "checkpoint cells"
+    else:
+        n = args.flash_batch
+        q, e, guess = cases.flash_batch(n, seed=20260303, saturation_levels=65536 if n > 1000000 else 0)
+        workload = f"batched HEM UV flash, {n:,} pure-N2O cells, 60% two-phase"
+        data = "synthetic (seeded pure-N2O states generated forward)"
     gen_s = time.time() - t0
     hem = GpuHem(model=td.pure_model(stable_gas_prune=args.flash_prune), capacity=n)
     dev = torch.device("cuda")
@@ -566,14 +576,13 @@ def run_flash_batch(args):
     generated_two = guess["liquidMass"][:, 0] > 0  # generated on the saturation curve with quality in [0, 1)
     return {"metric": "HEM UV flash calls/s (standalone batch)", "value": n / (ms * 1e-3), "unit": "flash/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "dtype": "f64", "data": "synthetic (seeded pure-N2O states generated forward)",
-            "config": {"workload": f"batched HEM UV flash, {n:,} pure-N2O cells, 60% two-phase",
-                       "stableGasPrune": args.flash_prune},
+            "dtype": "f64", "data": data,
+            "config": {"workload": workload, "stableGasPrune": args.flash_prune},
             "succeeded": int(ok.sum().item()), "labels": np.bincount(labels, minlength=3).tolist(),
             "iterations": {"p50": float(np.percentile(iters, 50)), "p90": float(np.percentile(iters, 90)),
                            "p99": float(np.percentile(iters, 99)), "max": int(iters.max()),
                            "histogram": np.bincount(iters.clip(0, 31), minlength=32).tolist()},
-            "generated_phase_agreement": {
+            "generated_phase_agreement": None if args.flash_checkpoint else {
                 "two_phase_recovered_two_phase": float(np.mean(labels[generated_two] == 2)),
                 "single_phase_recovered_single_phase": float(np.mean(labels[~generated_two] != 2))},
             "cpu_label_agreement": "bit-exact labels against the reference flash on seeded samples "
@@ -763,6 +772,8 @@ def main():
                    help="DRAM bytes per PR phase evaluation of the flash kernels (from an ncu capture)")
     p.add_argument("--flash-batch", type=int, default=0, help="run the standalone batched flash on this many cells")
     p.add_argument("--flash-prune", type=int, default=0, help="the model's stableGasPrune flag for --flash-batch")
+    p.add_argument("--flash-checkpoint", default=None,
+                   help="flash the cells of this committed checkpoint time directory (the --flash-batch mode)")
     p.add_argument("--precision-study", type=int, default=0,
                    help="run FP64 and mixed side by side on this cube size and report per-field errors")
     p.add_argument("--study-steps", type=int, default=20)
@@ -780,7 +791,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.flash_batch:
+        if args.flash_batch or args.flash_checkpoint:
             line = run_flash_batch(args)
         elif args.precision_study:
             line = run_precision_study(args)

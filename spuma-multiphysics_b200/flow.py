@@ -70,6 +70,7 @@ class Flow:
         self.lib = _lib.load()
         self.device = torch.device(device)
         self.cells = len(volume)
+        self.volume = np.ascontiguousarray(volume, dtype=np.float64)
         self.fixed = len(fixed_q)
         self.nv = q0.shape[1]
         self.cfl = cfl
@@ -241,6 +242,58 @@ class Flow:
         if not (cfl > 0 and dt <= cfl * (1 + 1e-10)):
             raise FlowError(f"dt={dt} exceeds the wave/diffusion CFL step {cfl}")
         return dict(cfl_dt=cfl)
+
+    # ----------------------------------------------------------- checkpoints
+    def history(self, time, initial=None, boundary=None):
+        """A checkpoint history for the current state: the conservation scales
+        the solver derives at start (src/reactiveFoam/ReactiveFoam.C:1402-1407),
+        the current totals as the baseline unless given, zero boundary
+        integral unless given."""
+        from .checkpoint import History
+        q, s = self.conserved(), self.states()
+        totals = (q * self.volume[:, None]).sum(axis=0)
+        speed = np.sqrt((q[:, 1:4] ** 2).sum(axis=1)) / q[:, 0] + s["soundFrozen"]
+        mass0 = float(totals[0] if initial is None else initial[0])
+        energy_scale = max(float((np.abs(q[:, 4]) * self.volume).sum()), mass0 * 1e5)
+        return History(initial=totals if initial is None else np.asarray(initial, float),
+                       boundary=np.zeros(self.nv) if boundary is None else np.asarray(boundary, float),
+                       steps=self.steps, time=float(time), velocity_scale=max(1.0, float(speed.max())),
+                       energy_scale=energy_scale)
+
+    def save_checkpoint(self, root, time, history=None, identity=None, last_dt=0.0, run_id="b200"):
+        """Commit a schema-3 checkpoint of the current state under root/<time>
+        (synchronises). identity: the identity dictionary's fields; by default
+        this library's own digests of the model image (a reference solver
+        restart needs the reference's own hashes)."""
+        import hashlib
+        from . import checkpoint
+        hist = history if history is not None else self.history(time)
+        hist.last_dt = last_dt
+        if identity is None:
+            image = self.hem.image
+            digest = hashlib.sha256(image).hexdigest()
+            identity = dict(fingerprint=digest, physical_model_hash=digest,
+                            numerical_policy_hash=hashlib.sha256(image[-2448:]).hexdigest(), species_count=1,
+                            closure="HEM")
+        return checkpoint.save(root, self.conserved(), self.states(), hist, identity, run_id=run_id)
+
+    def load_checkpoint(self, directory):
+        """Restart from a committed checkpoint: its conserved state and its
+        thermodynamic states (the next step's seeds) replace this flow's
+        (synchronises). Returns the checkpoint's History."""
+        from . import checkpoint
+        q, states, hist, _ = checkpoint.load(directory, self.cells, self.nv)
+        self.stream.synchronize()
+        self.qn[:, :self.cells] = torch.from_numpy(np.ascontiguousarray(q.T)).to(self.device)
+        self.sn.copy_(torch.from_numpy(states.view(np.uint8).copy()))
+        tr = np.zeros(self.cells, dtype=A.STATE_DTYPE)
+        for k_out, k_in in (("p", "p"), ("T", "T"), ("rho", "rho"), ("cv", "cv"), ("sound", "soundFrozen"),
+                            ("gasMass", "gasMass")):
+            tr[k_out] = states[k_in]
+        self.tr[:self.cells] = torch.from_numpy(tr.view(np.float64).reshape(self.cells, 7)).to(self.device)
+        torch.cuda.synchronize(self.device)
+        self.steps = int(hist.steps)
+        return hist
 
     # --------------------------------------------------------------- views
     def conserved(self):
