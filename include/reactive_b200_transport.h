@@ -168,8 +168,8 @@ int reactive_transport_precision_v3(void* transport, int request, int* active);
  * tail, stride cells+fixed) and w its adjoint (SoA, stride cells), writes
  * qBar = (dL/dq)^T w (SoA, stride cells) and stateBar = (dL/dstate)^T w per cell
  * (the p, T, rho and sound fields the flux reads; the others are zero).
- * Structured path, the whole operator: HLL (wave-speed switches taken
- * piecewise), viscous/WALE traction through the cells' velocity gradients and
+ * Structured path, the whole operator: HLL or HLLC (wave-speed and star-state
+ * switches taken piecewise, on the branch the forward selects), viscous/WALE traction through the cells' velocity gradients and
  * eddy viscosities (with their own adjoints carried back through the WALE
  * relation and the Green-Gauss gradient to the neighbours' velocities), and
  * conduction. The derivative of the FP64 operator; a handle with the WALE

@@ -319,11 +319,17 @@ class HemStep:
         return q_barn
 
     def check(self):
-        """Every flash and every flash derivative since the last check succeeded (synchronises)."""
+        """Every flash and every flash derivative since the last check succeeded,
+        and the transport status word is clear (synchronises)."""
         n = int(self.failed.item())
         self.failed.zero_()
+        status = C.c_uint()
+        self._check(self.lib.reactive_transport_status_v3(self.flow.transport, C.byref(status), 1,
+                                                          torch.cuda.current_stream().cuda_stream))
         if n:
             raise AdjointError(f"{n} cell flashes or flash derivatives failed")
+        if status.value:
+            raise AdjointError(f"transport status {status.value:#x} (1 WALE, 2 HLLC, 4 WALE scalar field)")
 
 
 class HemSSPRK2Step(torch.autograd.Function):

@@ -618,7 +618,8 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
 // visits its six faces and evaluates each face flux in forward dual numbers
 // seeded on c's own inputs, then contracts the flux derivatives with the face's
 // adjoint weight sum_side sign w / V. Gather form, no atomics; the HLL
-// wave-speed switches are differentiated piecewise.
+// wave-speed switches and the HLLC star-side and supersonic switches are
+// differentiated piecewise, on the branch the forward takes.
 //   MODE 0: seeds on c's conserved variables (and through u = m / rho on its
 //           velocity), p, sound, T and the state density; writes qBar (the
 //           direct part) and stateBar {p, T, rho, 0, sound, 0, 0}.

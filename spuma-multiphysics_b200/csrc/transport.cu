@@ -563,7 +563,7 @@ struct Transport {
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
                         const double* nut, const double* w, double* qBar, ReactiveTransportState* stateBar,
                         double* gBar, double* nutBar, bool viscous, cudaStream_t s) {
-            if (!viscous && b.conductivity == 0) {
+            if (!viscous && b.conductivity == 0 && b.scheme == 0) {
                 cartRateVjpInviscid<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, w, qBar, stateBar);
                 return;
             }
@@ -583,7 +583,6 @@ struct Transport {
     void launchRateVjp(const double* q, const ReactiveTransportState* state, const double* w, double* qBar,
                        ReactiveTransportState* stateBar, cudaStream_t s) {
         require(structured, "The rate VJP needs the structured Cartesian path (reactive_transport_structured_v3)");
-        require(fluxScheme == 0, "The rate VJP covers the HLL flux");
         require(!v.sgs, "The rate VJP does not cover the WALE scalar closure");
         const bool viscous = cfg.viscosity > 0 || v.wale;
         if (viscous && !gradBar) {

@@ -57,16 +57,19 @@ def _check(lib, handle, rc):
 class Flow:
     def __init__(self, faces, volume, q0, guess0, fixed_q, fixed_guess, viscosity=0.0, conductivity=0.0,
                  wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda", precision="fp64",
-                 turbulent_prandtl=None, turbulent_schmidt=None):
+                 turbulent_prandtl=None, turbulent_schmidt=None, flux="hll"):
         """faces: FACE_DTYPE array; q0: cell-major (cells, 5) conserved state;
         guess0/fixed_guess: THERMO_DTYPE seeds used for the initial recovery.
         precision: "fp64", or "mixed" (FP32 gradients, WALE and face fluxes with
         compensated per-cell sums into the FP64 state; needs a structured box).
         turbulent_prandtl / turbulent_schmidt: the WALE scalar closure (needs
         wale_cw; 0 disables a term), fed each stage with the mixture cp of that
-        stage's equilibrium states."""
+        stage's equilibrium states. flux: "hll", or "hllc" (the contact-preserving
+        flux; needs a structured box)."""
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"unknown precision {precision!r}")
+        if flux not in ("hll", "hllc"):
+            raise ValueError(f"unknown flux {flux!r}")
         self.lib = _lib.load()
         self.device = torch.device(device)
         self.cells = len(volume)
@@ -113,6 +116,9 @@ class Flow:
         self.precision = precision
         if precision == "mixed":
             _check(self.lib, self.transport, self.lib.reactive_transport_precision_v3(self.transport, 1, None))
+        self.flux = flux
+        if flux == "hllc":
+            _check(self.lib, self.transport, self.lib.reactive_transport_flux_v3(self.transport, 1, None))
         all_ = self.cells + self.fixed
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)

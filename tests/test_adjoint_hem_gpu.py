@@ -104,7 +104,9 @@ def test_hem_vjp_against_cellwise_differences():
         return cons, state, tr.cpu().numpy(), ok.cpu().numpy()
 
     cons, state, tr0, ok0 = flash(q)
-    ybar = rng.normal(size=(n, 7)) * np.abs(tr0).max(axis=0) ** -1
+    scale = np.abs(tr0).max(axis=0)
+    scale[scale == 0] = 1.0
+    ybar = rng.normal(size=(n, 7)) / scale
     ybar[:, 6] = 0
     q_bar = torch.zeros((5, n), dtype=torch.float64, device="cuda")
     failed = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -161,6 +163,118 @@ def test_hem_step_gradient_against_finite_differences():
         (g,) = torch.autograd.grad(loss(qg), qg)
         stepper.check()
         rng = np.random.default_rng(3)
+        probes = rng.choice(np.flatnonzero(sub), 6, replace=False)
+        with torch.no_grad():
+            for c in probes:
+                for var in (0, 4):
+                    h = 1e-6 * abs(float(q0[var, c]))
+                    qp, qm = q0.clone(), q0.clone()
+                    qp[var, c] += h
+                    qm[var, c] -= h
+                    fd = (loss(qp) - loss(qm)).item() / (2 * h)
+                    got = g[var, c].item()
+                    assert abs(got - fd) <= 2e-4 * abs(fd) + 1e-12 * abs(g[var]).max().item(), (c, var, got, fd)
+        stepper.check()
+    finally:
+        flow.close()
+
+
+@pytest.mark.parametrize("ns,wale,kinds,viscous", [(1, .325, "mixed", True), (2, None, (1, 2, 3, 2, 1, 2), False),
+                                                   (3, .5, (3, 1, 1, 2, 2, 3), True)])
+def test_hllc_rate_vjp_dot_product(ns, wale, kinds, viscous):
+    """The HLLC operator's VJP (dual numbers through the templated face flux,
+    star-side switches taken on the forward's branch) by the dot-product test
+    against central differences of the oracle's HLLC right-hand side (the
+    oracle's HLLC core equals the reference's bit for bit)."""
+    from oracle import oracle
+    L = _lib.load()
+    lib = T.bind(L)
+    dims = (6, 5, 4)
+    kinds = mixed_kinds(dims, 23) if kinds == "mixed" else kinds
+    case = box_case(dims, ns, kinds, viscous=viscous, conduction=viscous, seed=4)
+    h = T.create(lib, 1, case, wale_cw=wale)
+    nc, nv = case["nc"], case["nv"]
+    rng = np.random.default_rng(37 + ns)
+    cw = -1.0 if wale is None else wale
+    oracle.set_flux_scheme(1)
+    try:
+        assert L.reactive_transport_flux_v3(h, 1, None) == 0
+        q, st = case["q"], case["states"]
+
+        def rhs(qq, ss):
+            out, _, _, _, status = oracle.transport_rhs(case, np.ascontiguousarray(qq), ss.ctypes.data_as(C.c_void_p),
+                                                        wale_cw=cw)
+            assert status == 0
+            return out
+
+        vq = rng.normal(size=q.shape) * np.abs(q).max(axis=0)
+        vs = {f: rng.normal(size=nc) * np.abs(st[f]).max() * .1 for f in STATE_FIELDS}
+        w = rng.normal(size=q.shape)
+        eps = 1e-6
+        sp, sm = st.copy(), st.copy()
+        for f in STATE_FIELDS:
+            sp[f] += eps * vs[f]
+            sm[f] -= eps * vs[f]
+        fd = float(np.sum(w * (rhs(q + eps * vq, sp) - rhs(q - eps * vq, sm)) / (2 * eps)))
+        cells, fixed, nvar, nsp = (C.c_size_t() for _ in range(4))
+        assert L.reactive_transport_layout_v3(h, C.byref(cells), C.byref(fixed), C.byref(nvar), C.byref(nsp)) == 0
+        all_ = nc + fixed.value
+        stream = torch.cuda.current_stream().cuda_stream
+        qd = torch.zeros((nv, all_), dtype=torch.float64, device="cuda")
+        qd[:, :nc] = torch.from_numpy(q.T.copy()).cuda()
+        sd = torch.zeros((all_, 7), dtype=torch.float64, device="cuda")
+        sd[:nc] = torch.from_numpy(st.view(np.float64).reshape(nc, 7)).cuda()
+        assert L.reactive_transport_fill_fixed_v3(h, qd.data_ptr(), sd.data_ptr(), stream) == 0
+        wd = torch.from_numpy(w.T.copy()).cuda()
+        q_bar = torch.empty((nv, nc), dtype=torch.float64, device="cuda")
+        s_bar = torch.empty((nc, 7), dtype=torch.float64, device="cuda")
+        assert L.reactive_transport_rate_vjp_v3(h, qd.data_ptr(), sd.data_ptr(), wd.data_ptr(), q_bar.data_ptr(),
+                                                s_bar.data_ptr(), stream) == 0, lib.reactive_transport_error(h)
+        torch.cuda.synchronize()
+        qb = q_bar.cpu().numpy().T
+        sb = s_bar.cpu().numpy().view(A.STATE_DTYPE).reshape(nc)
+        adj = float(np.sum(qb * vq)) + sum(float(np.sum(sb[f] * vs[f])) for f in STATE_FIELDS)
+        assert abs(adj - fd) <= 1e-6 * max(abs(fd), 1e-300), (adj, fd)
+        # the HLLC operator's derivative is not the HLL one's
+        assert L.reactive_transport_flux_v3(h, 0, None) == 0
+        assert L.reactive_transport_rate_vjp_v3(h, qd.data_ptr(), sd.data_ptr(), wd.data_ptr(), q_bar.data_ptr(),
+                                                s_bar.data_ptr(), stream) == 0
+        torch.cuda.synchronize()
+        hll = float(np.sum(q_bar.cpu().numpy().T * vq))
+        assert abs(hll - float(np.sum(qb * vq))) > 1e-6 * abs(hll)
+    finally:
+        oracle.set_flux_scheme(0)
+        lib.reactive_transport_destroy(h)
+
+
+def test_hllc_hem_step_gradient_against_finite_differences():
+    """The SSPRK2 + HEM step adjoint with the HLLC flux (config-5 physics)."""
+    n, steps, dt = 12, 2, 1e-8
+    faces, volume = cases.cartesian_faces(n, edge=n * 1e-3, port_diameter=0.005, port_z=n * 0.5e-3,
+                                          port_offset=0.004)
+    init = cases.impingement(n, seed=11)
+    flow = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], viscosity=1.821e-5,
+                conductivity=0.02587, wale_cw=0.325, flux="hllc")
+    stepper = HemStep(flow)
+    cells = flow.cells
+    try:
+        q0 = flow.qn.clone()
+        s0 = flow.sn.clone()
+        k, j, i = np.indices((n, n, n))
+        sub = ((i >= 2) & (i < 6) & (j >= 2) & (j < 6) & (k >= 4) & (k < 8)).ravel()
+        weight = torch.zeros_like(q0)
+        weight[0, :cells] = torch.from_numpy(sub * volume).cuda()
+        weight[4, :cells] = torch.from_numpy(sub * volume).cuda() * 1e-6
+
+        def loss(q):
+            s = stepper.recover(q.detach(), s0)
+            out, _ = hem_rollout(stepper, q, s, steps, dt, checkpoint_every=1)
+            return (out * weight).sum()
+
+        qg = q0.clone().requires_grad_(True)
+        (g,) = torch.autograd.grad(loss(qg), qg)
+        stepper.check()
+        rng = np.random.default_rng(5)
         probes = rng.choice(np.flatnonzero(sub), 6, replace=False)
         with torch.no_grad():
             for c in probes:
