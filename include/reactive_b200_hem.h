@@ -29,8 +29,13 @@ void reactive_gpu_hem_destroy_v1(void* hem);
  * cell, energy the internal energy density, state the seed in / the result out. */
 int reactive_gpu_hem_run_v1(void* hem, const double* q, const double* energy, size_t count,
     ReactiveThermoState* state, int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);
-/* src/reactiveThermo/reactiveGpuHem.h:63-72, :81-84: capillary and primitive-initialisation
- * paths; outside this build's scope, they return 1 with a message. */
+/* src/reactiveThermo/reactiveGpuHem.h:63-65, :72-84: the capillary batches. This build runs them
+ * for UV phase equilibrium without a pressure jump (capillary NULL for the resident form, or every
+ * entry with pressureJump = 0 and equilibrium = 1), which is the plain flash of run_v1; a pressure
+ * jump or the frozen partition returns 1 with a message. run_resident_v1: device pointers indexed
+ * by global cell, order[0..count) names the cells, each result (state, success) goes to
+ * output[cell], a failed cell returns its seed; synchronous, batch totals in *profile.
+ * src/reactiveThermo/reactiveGpuHem.h:66-71 (primitive initialisation) returns 1 with a message. */
 int reactive_gpu_hem_run_v2(void* hem, const double* q, const double* energy,
     const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* state, int* success,
     ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);

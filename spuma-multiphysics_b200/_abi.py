@@ -100,6 +100,11 @@ THERMO_DTYPE = np.dtype([
     ("alphaLiquid", "<f8", (2,)), ("rhoGas", "<f8"), ("rhoLiquid", "<f8", (2,)),
     ("liquidMass", "<f8", (2,)), ("gasMass", "<f8"), ("cp", "<f8"), ("cv", "<f8"),
     ("activeLiquids", "<i4"), ("iterations", "<i4")])
+
+# ReactiveGpuHemOutputV1 (184 B) and ReactiveGpuHemCapillaryInputV2 (24 B)
+HEM_OUTPUT_DTYPE = np.dtype([("state", THERMO_DTYPE), ("success", "<i4"), ("reserved", "<i4")])
+CAPILLARY_DTYPE = np.dtype([("color", "<f8"), ("pressureJump", "<f8"), ("equilibrium", "<i4"), ("pad", "<i4")])
+assert HEM_OUTPUT_DTYPE.itemsize == 184 and CAPILLARY_DTYPE.itemsize == 24
 assert THERMO_DTYPE.itemsize == 176
 
 STATE_DTYPE = np.dtype([(k, "<f8") for k in ("p", "T", "rho", "cv", "sound", "gasMass", "dilatation")])

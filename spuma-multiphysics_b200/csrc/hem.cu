@@ -62,6 +62,36 @@ __global__ void inputsFromHost(const double* q, const double* energy, const Reac
     }
 }
 
+// Inputs of a device-resident batch named by `order` (global cell indices):
+// q holds ns masses per cell, energy the bulk internal energy density; the
+// seeds are gathered too (a failed cell returns its seed). A capillary entry
+// that asks for a pressure jump or the frozen partition sets *unsupported.
+__global__ void inputsFromResident(const double* q, const double* energy, const ReactiveThermoState* seed,
+                                   const ReactiveGpuHemCapillaryInputV2* capillary, const uint32_t* order,
+                                   size_t count, int ns, CellInput* in, ReactiveThermoState* guess,
+                                   unsigned* unsupported) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = order[i];
+        if (capillary && !(capillary[c].pressureJump == 0.0 && capillary[c].equilibrium == 1)) atomicOr(unsupported, 1u);
+        double rho = 0;
+        for (int k = 0; k < ns; ++k) rho += q[c * size_t(ns) + k];
+        const ReactiveThermoState g = seed[c];
+        guess[i] = g;
+        in[i] = CellInput{rho, energy[c], g.p, g.T, g.liquidMass[0]};
+    }
+}
+
+// Results of a resident batch to output[order[i]].
+__global__ void scatterResident(const ReactiveThermoState* state, const int* success, const uint32_t* order,
+                                size_t count, ReactiveGpuHemOutputV1* output) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(blockDim.x) * gridDim.x) {
+        ReactiveGpuHemOutputV1& o = output[order[i]];
+        o.state = state[i];
+        o.success = success[i];
+        o.reserved = 0;
+    }
+}
+
 // Internal energy density E - |m|^2/(2 rho) from the SoA conserved rows.
 __global__ void inputsFromConserved(const double* cons, size_t stride, size_t count, int ns,
                                     const ReactiveThermoState* seed, CellInput* in) {
@@ -810,22 +840,89 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
     }
 }
 
-int reactive_gpu_hem_run_v2(void*, const double*, const double*, const ReactiveGpuHemCapillaryInputV2*, size_t,
-                            ReactiveThermoState*, int*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
-    if (error && size) std::snprintf(error, size, "Capillary HEM is not part of this B200 build");
-    return 1;
+int reactive_gpu_hem_run_v2(void* raw, const double* q, const double* energy,
+                            const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* states,
+                            int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t size) {
+    // without a pressure jump and in equilibrium the capillary batch is the plain UV flash
+    if (!capillary && count) {
+        if (error && size) std::snprintf(error, size, "Null capillary input");
+        return 1;
+    }
+    for (size_t c = 0; c < count; ++c)
+        if (!(capillary[c].pressureJump == 0.0 && capillary[c].equilibrium == 1)) {
+            if (error && size)
+                std::snprintf(error, size, "Capillary pressure jumps and the frozen partition are not part of this "
+                                           "B200 build");
+            return 1;
+        }
+    return reactive_gpu_hem_run_v1(raw, q, energy, count, states, success, profile, error, size);
 }
 int reactive_gpu_hem_initialize_tp_v1(void*, double*, double*, const ReactiveGpuHemCapillaryInputV2*, size_t,
                                       ReactiveThermoState*, int*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
     if (error && size) std::snprintf(error, size, "Capillary primitive initialisation is not part of this B200 build");
     return 1;
 }
-int reactive_gpu_hem_run_resident_v1(void*, const double*, const double*, const ReactiveThermoState*,
-                                     const ReactiveGpuHemCapillaryInputV2*, const uint32_t*, size_t,
-                                     ReactiveGpuHemOutputV1*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
-    if (error && size)
-        std::snprintf(error, size, "The capillary resident HEM is not part of this B200 build; use run_device_v3");
-    return 1;
+// The reference's device-resident batch (src/reactiveThermo/reactiveGpuHem.h:72-84)
+// for UV phase equilibrium without a pressure jump (capillary may be NULL, or
+// hold pressureJump = 0 and equilibrium = 1 for every named cell): gather the
+// named cells, the work-queue search, failed cells keep their seed, scatter to
+// output[cell]. Synchronous on the handle's stream; only batch totals reach
+// the host.
+int reactive_gpu_hem_run_resident_v1(void* raw, const double* q, const double* energy, const ReactiveThermoState* seed,
+                                     const ReactiveGpuHemCapillaryInputV2* capillary, const uint32_t* order,
+                                     size_t count, ReactiveGpuHemOutputV1* output, ReactiveGpuHemProfileV1* profile,
+                                     char* error, size_t size) {
+    try {
+        rb200::require(raw && q && energy && seed && order && output && profile && profile->abiVersion == 1
+                           && profile->structBytes == sizeof(*profile),
+                       "Invalid resident CUDA HEM batch arguments");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        rb200::require(count && count <= d.capacity, "Resident CUDA HEM batch exceeds capacity");
+        rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+        d.ensureHostPath();  // gathered seeds, results and flags
+        const auto begin = std::chrono::steady_clock::now();
+        cudaStream_t s = d.stream;
+        unsigned* unsupported = d.counters + rb200::FAILED;  // reset by the search before its own use
+        rb200::check(cudaMemsetAsync(unsupported, 0, sizeof(unsigned), s), "memset");
+        rb200::inputsFromResident<<<rb200::gridFor(count, 256), 256, 0, s>>>(q, energy, seed, capillary, order, count,
+                                                                            1, d.in, d.dguess, unsupported);
+        rb200::check(cudaGetLastError(), "inputs");
+        unsigned flag = 0;
+        rb200::check(cudaMemcpyAsync(&flag, unsupported, sizeof(flag), cudaMemcpyDeviceToHost, s), "D2H flag");
+        rb200::check(cudaStreamSynchronize(s), "sync");
+        rb200::require(!flag, "Capillary pressure jumps and the frozen partition are not part of this B200 build");
+        cudaEvent_t first, last;
+        rb200::check(cudaEventCreate(&first), "event");
+        rb200::check(cudaEventCreate(&last), "event");
+        rb200::check(cudaEventRecord(first, s), "event");
+        rb200::check(cudaMemsetAsync(d.dsuccess, 0, count * sizeof(int), s), "memset");
+        d.launchSearch(count, d.dguess, d.dout, nullptr, d.dsuccess, s);
+        rb200::keepFailed<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.dguess, d.dsuccess, count, d.dout);
+        rb200::check(cudaGetLastError(), "keepFailed");
+        rb200::scatterResident<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.dout, d.dsuccess, order, count, output);
+        rb200::check(cudaGetLastError(), "scatter");
+        rb200::check(cudaEventRecord(last, s), "event");
+        ReactiveGpuHemProfileV1 p{};
+        p.abiVersion = 1;
+        p.structBytes = sizeof(p);
+        rb200::readTotals(d, p, s);  // synchronises
+        float kernel = 0;
+        cudaEventElapsedTime(&kernel, first, last);
+        cudaEventDestroy(first);
+        cudaEventDestroy(last);
+        p.batches = 1;
+        p.submitted = count;
+        p.succeeded = count - p.deviceFailures;
+        p.deviceBytes = d.bytes;
+        p.kernelSeconds = kernel / 1000.;
+        p.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+        *profile = p;
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
 }
 
 int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t stride, size_t count, size_t variables,
