@@ -186,6 +186,10 @@ class HostPath:
         self.prim = self._pinned((n, 4), np.float64)
         self.rho = self._pinned((n,), np.float64)
         self.e = self._pinned((n,), np.float64)
+        self.ok = self._pinned((n,), np.int32)
+        # the seed copy of a stage runs beside the transport stage it does not depend on
+        import concurrent.futures
+        self._pool = concurrent.futures.ThreadPoolExecutor(1)
         self.hem = flow.hem
         cfg = A.Config(n, 1, 5, len(faces), len(fixed_q), VISCOSITY, CONDUCTIVITY, 0.0, 1.1, 1.6e11, 0)
         fixed_tr = np.frombuffer(flow.tr[n:].cpu().numpy().tobytes(), dtype=A.STATE_DTYPE).copy()
@@ -229,8 +233,9 @@ class HostPath:
         dst[:, 6] = 0.0
         return self.tr
 
-    def _primitives(self, states):
-        src, q, prim = self._f64(states, 22), self.torch.from_numpy(self.q), self.torch.from_numpy(self.prim)
+    def _primitives(self, tr):
+        """Primitives (rho, u) from the compacted transport states."""
+        src, q, prim = self._f64(tr, 7), self.torch.from_numpy(self.q), self.torch.from_numpy(self.prim)
         prim[:, 0] = src[:, 2]
         self.torch.div(q[:, 1:4], src[:, 2:3], out=prim[:, 1:])
         return self.prim
@@ -253,7 +258,7 @@ class HostPath:
         self.states, self.start = self.start, start
         dtc = C.c_double()
         tr0 = self._compact(start)
-        prim = self._primitives(start)
+        prim = self._primitives(tr0)
         self._check(lib.reactive_transport_stable_step_primitives(t, prim.ctypes.data_as(C.POINTER(A.Primitive)),
                                                                   tr0.ctypes.data_as(C.POINTER(A.State)), .5, dt,
                                                                   C.byref(dtc)))
@@ -267,26 +272,29 @@ class HostPath:
         stage_states = None
         tr = tr0  # the step-start states' transport states, compacted once for the CFL query and stage 0
         for stage in (0, 1):
+            out = self.seeds if stage == 0 else self.states
+            copied = self._pool.submit(self._copy, out, start)
             before = A.Token(self.attempt, stage, self.version)
             self.version += 1
             after = A.Token(self.attempt, stage + 1, self.version)
-            self._check(lib.reactive_transport_advance_resident_v2(t, before, after, tr.ctypes.data_as(
-                C.POINTER(A.State)), None, None, None, dt, A.dptr(br)))
-            self._check(lib.reactive_transport_download_conserved(t, after, A.dptr(self.q)))
+            try:
+                self._check(lib.reactive_transport_advance_resident_v2(t, before, after, tr.ctypes.data_as(
+                    C.POINTER(A.State)), None, None, None, dt, A.dptr(br)))
+                self._check(lib.reactive_transport_download_conserved(t, after, A.dptr(self.q)))
+            finally:
+                copied.result()
             self.h2d += tr.nbytes
             self.d2h += self.q.nbytes
-            out = self.seeds if stage == 0 else self.states
-            self._copy(out, start)
             self._energy()
-            ok, _ = self.hem.run(self.rho, self.e, out)
+            ok, _ = self.hem.run(self.rho, self.e, out, success=self.ok)
             if not ok.all():
                 raise RuntimeError("HEM recovery failed")
             self.h2d += self.rho.nbytes + self.e.nbytes + out.nbytes
             self.d2h += out.nbytes + ok.nbytes
             if stage == 0:
                 stage_states = out
-                prim = self._primitives(stage_states)
                 tr = self._compact(stage_states)  # reused by stage 1
+                prim = self._primitives(tr)
                 self._check(lib.reactive_transport_stable_step_primitives(
                     t, prim.ctypes.data_as(C.POINTER(A.Primitive)), tr.ctypes.data_as(C.POINTER(A.State)), .5, dt,
                     C.byref(dtc)))
@@ -294,6 +302,7 @@ class HostPath:
         self._check(lib.reactive_transport_end_attempt(t, self.attempt, 1))
 
     def close(self):
+        self._pool.shutdown()
         self.lib.reactive_transport_destroy(self.t)
 
 

@@ -105,19 +105,6 @@ __global__ void inputsFromConserved(const double* cons, size_t stride, size_t co
     }
 }
 
-__device__ inline void finishCandidate(const HemConst& C, const CellInput& in, bool ok, const Eval& v,
-                                       const CandidateOut& o, CandRecord* rec, Counts& n) {
-    int status = 0;
-    if (ok) {
-        stateFromEval(v, in.q, o, rec->st);
-        rec->entropyD = v.entropyD;
-        const double mass = v.liqMass, p = v.p, T = v.T;
-        status = stableAt(C, in.q, mass, p, T, n) ? 2 : 1;
-    }
-    if (status == 2) ++n.stable; else ++n.failures;
-    rec->status = status;
-}
-
 struct MainRecords {
     CandRecord* rec;
     size_t count;

@@ -61,6 +61,7 @@ struct Transport {
     double* boundaryRate = nullptr;
     ReactiveTransportState* stateDevice = nullptr;
     unsigned* flags = nullptr;  // [0] WALE failure
+    unsigned long long* invalid = nullptr;  // first invalid uploaded state / primitive
     // structured Cartesian fast path (device-resident entries only)
     bool boxDetected = false, structured = false;
     CartView box{};
@@ -183,6 +184,7 @@ struct Transport {
         auto* step = arena.get<double>(cfg.cells);
         boundaryRate = arena.get<double>(cfg.variables);
         flags = arena.get<unsigned>(4);
+        invalid = arena.get<unsigned long long>(2);
         reduceBlocks = std::min<size_t>(1024, (cfg.cells + 255) / 256);
         reduceScratch = arena.get<double>(reduceBlocks + 1);
         double* gasY = nullptr;
@@ -290,11 +292,27 @@ struct Transport {
         ++profile.conservedUploads;
         profile.conservedUploadBytes += cfg.cells * cfg.variables * sizeof(double);
     }
-    void uploadState(const ReactiveTransportState* states) {
+    // States (and primitives) are validated on the device after the copy; the
+    // call fails with the host validation's message before anything is formed
+    // from them.
+    void uploadState(const ReactiveTransportState* states, const ReactiveTransportPrimitive* primitive = nullptr) {
         require(!cfg.cells || states, "Null transport state");
-        validateStates(states, cfg.cells);
         upload(stateDevice, states, cfg.cells);
         profile.stateUploadBytes += cfg.cells * sizeof(ReactiveTransportState);
+        if (primitive) {
+            upload(v.primitive, primitive, cfg.cells);
+            profile.primitiveUploadBytes += cfg.cells * sizeof(ReactiveTransportPrimitive);
+        }
+        check(cudaMemsetAsync(invalid, 0xff, 2 * sizeof(unsigned long long), stream), "memset");
+        validateUploads<<<gridFor(cfg.cells, 256), 256, 0, stream>>>(stateDevice, primitive ? v.primitive : nullptr,
+                                                                    cfg.cells, invalid);
+        launched();
+        unsigned long long first[2];
+        download(first, invalid, 2);
+        finish();
+        if (primitive && first[1] != ~0ull)
+            require(false, (first[1] & 1) ? "Invalid primitive velocity" : "Invalid primitive density");
+        require(first[0] == ~0ull, "Invalid recovered transport state");
     }
     void unpackQ(double* hostQ) {
         unpackFrom(hostQ, q, cfg.cells, cfg.variables, v.all, 0);
@@ -322,7 +340,8 @@ struct Transport {
     void buildWaleChecked() {
         if (!v.wale) return;
         check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
-        launchWale(stream, stateDevice);
+        if (structured) launchHostBoxGradients();
+        else launchWale(stream, stateDevice);
         unsigned status = 0;
         download(&status, flags, 1);
         finish();
@@ -655,7 +674,7 @@ struct Transport {
     // ------------------------------------------------------- reference contract
     void prepareResident(const ReactiveTransportState* states, const double* gasY, const double* gasH, bool transport) {
         requireScalarFields(transport);
-        ensureGraphScalarWork();
+        if (!structured) ensureGraphScalarWork();
         uploadState(states);
         if (transport && cfg.diffusivity > 0) {
             packInto(const_cast<double*>(v.gasY), gasY, cfg.cells, cfg.species, v.all, 0);
@@ -664,6 +683,12 @@ struct Transport {
         }
         launchPrimitives(q, stream);
         if (v.wale) buildWaleChecked();
+        if (structured) {
+            // the host-array entries on the structured box: FP64 HLL stencils, bitwise
+            // equal to the face graph; rates, ledger and CFL are formed by the caller steps
+            if (!v.wale && cfg.viscosity > 0) launchHostBoxGradients();
+            return;
+        }
         if (transport) {
             GraphView g = v;
             if (!v.wale && cfg.viscosity > 0) {
@@ -688,23 +713,81 @@ struct Transport {
         prepareResident(states, gasY, gasH, transport);
     }
     void gather(bool materialize) {
-        if (materialize) {
-            if (!rhs) rhs = arena.get<double>(product(cfg.cells, cfg.variables));
-            launchRates(q, stateDevice, rhs, cfg.cells, 0, 0, stream);
+        if (materialize && !rhs) rhs = arena.get<double>(product(cfg.cells, cfg.variables));
+        if (structured) {
+            const CartView b = hostBoxView();
+            if (materialize) {
+                if (v.wale) check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
+                bySpecies<RatesK>(b, static_cast<const double*>(q), static_cast<const ReactiveTransportState*>(
+                                      stateDevice), static_cast<const double*>(v.grad),
+                                  static_cast<const double*>(v.nut), rhs, size_t(cfg.cells), 0, 0.0, flags,
+                                  launch.rates, stream);
+                ++deviceProfile.transportFaceLaunches;
+                requireFiniteTraction();
+            }
+            bySpecies<LedgerK>(b, static_cast<const double*>(q), static_cast<const ReactiveTransportState*>(
+                                   stateDevice), static_cast<const double*>(v.grad), static_cast<const double*>(v.nut),
+                               ledgerPartial, ledgerBlocks, stream);
+            foldPartials<<<1, 32 * unsigned(cfg.variables), 0, stream>>>(ledgerPartial, int(ledgerBlocks),
+                                                                          int(cfg.variables), boundaryRate);
+            launched();
+            return;
         }
+        if (materialize) launchRates(q, stateDevice, rhs, cfg.cells, 0, 0, stream);
         launchLedger(q, stateDevice, boundaryRate, stream);
+    }
+    // The structured view the host-array entries use: FP64 HLL whatever the
+    // device entries' precision and flux scheme.
+    CartView hostBoxView() const {
+        CartView b = boxView();
+        b.scheme = 0;
+        return b;
+    }
+    void launchHostBoxGradients() {
+        bySpecies<GradientsK>(hostBoxView(), static_cast<const ReactiveTransportState*>(stateDevice), v.grad, v.nut,
+                              flags, launch.gradients, stream);
+        if (v.wale) {
+            ++waleProfile.gradientBuilds;
+            ++waleProfile.viscosityBuilds;
+            waleProfile.cellsEvaluated += v.cells;
+        }
+    }
+    // A non-finite WALE traction or energy flux fails the call before anything
+    // is committed (the face graph checks the same after its face pass).
+    void requireFiniteTraction() {
+        if (!v.wale) return;
+        unsigned status = 0;
+        download(&status, flags, 1);
+        finish();
+        require(!(status & 1u), "Nonfinite WALE traction/energy flux; stage remains uncommitted");
     }
     void stableStep(double cfl, double maximumStep, double* dt) {
         require(dt && std::isfinite(cfl) && cfl > 0 && cfl <= .5 && std::isfinite(maximumStep) && maximumStep > 0,
                 "Invalid transport CFL controls");
-        launchStep(cfl, maximumStep, reduceScratch + reduceBlocks, stream);
+        if (structured) {
+            const unsigned blocks = unsigned(reduceBlocks);
+            bySpecies<StepsK>(hostBoxView(), static_cast<const ReactiveTransportState*>(stateDevice),
+                              static_cast<const double*>(v.nut), cfl, maximumStep, reduceScratch, blocks, launch.steps,
+                              stream);
+            ++deviceProfile.cflFaceLaunches;
+            minimumReduce<<<1, 1024, 0, stream>>>(reduceScratch, blocks, reduceScratch + reduceBlocks);
+            launched();
+        } else launchStep(cfl, maximumStep, reduceScratch + reduceBlocks, stream);
         download(dt, reduceScratch + reduceBlocks, 1);
         finish();
         require(std::isfinite(*dt) && *dt > 0, "Invalid wave/diffusion timestep");
         ++stats.stepQueries;
     }
     void advance(double dt, int stage, double* hostQ, double* boundary) {
-        launchRates(q, stateDevice, initial, v.all, stage == 0 ? 1 : 2, dt, stream);
+        if (structured) {
+            if (v.wale) check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
+            bySpecies<RatesK>(hostBoxView(), static_cast<const double*>(q),
+                              static_cast<const ReactiveTransportState*>(stateDevice),
+                              static_cast<const double*>(v.grad), static_cast<const double*>(v.nut), initial, v.all,
+                              stage == 0 ? 1 : 2, dt, flags, launch.rates, stream);
+            ++deviceProfile.transportFaceLaunches;
+            requireFiniteTraction();
+        } else launchRates(q, stateDevice, initial, v.all, stage == 0 ? 1 : 2, dt, stream);
         std::swap(q, initial);
         v.q = q;
         if (hostQ) unpackQ(hostQ);
@@ -838,17 +921,7 @@ struct Transport {
     }
     void uploadPrimitives(const ReactiveTransportPrimitive* primitive, const ReactiveTransportState* state) {
         require(primitive, "Null transport primitives");
-        const size_t bad = firstFailure(cfg.cells, [&](size_t c) {
-            return std::isfinite(primitive[c].rho) && primitive[c].rho > 0 && std::isfinite(primitive[c].u[0])
-                && std::isfinite(primitive[c].u[1]) && std::isfinite(primitive[c].u[2]);
-        });
-        if (bad < cfg.cells) {
-            require(std::isfinite(primitive[bad].rho) && primitive[bad].rho > 0, "Invalid primitive density");
-            require(false, "Invalid primitive velocity");
-        }
-        uploadState(state);
-        upload(v.primitive, primitive, cfg.cells);
-        profile.primitiveUploadBytes += cfg.cells * sizeof(ReactiveTransportPrimitive);
+        uploadState(state, primitive);
     }
 };
 

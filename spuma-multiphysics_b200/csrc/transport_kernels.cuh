@@ -460,6 +460,32 @@ __global__ void boundaryLedger(GraphView v, double* rate) {
     }
 }
 
+// Input validation of the host-array entries on the device, after the upload:
+// the first cell whose recovered state is not admissible (p, T, rho, sound, cv
+// finite and positive, gas mass finite and non-negative, dilatation finite) to
+// first[0]; the first invalid primitive to first[1] as 2 c (density not finite
+// and positive) or 2 c + 1 (a velocity component not finite), so the density
+// of a cell is reported before its velocity.
+__global__ void validateUploads(const ReactiveTransportState* __restrict__ st,
+                                const ReactiveTransportPrimitive* __restrict__ prim, size_t count,
+                                unsigned long long* first) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
+        if (st) {
+            const ReactiveTransportState s = st[c];
+            const bool ok = isfinite(s.p) && s.p > 0 && isfinite(s.T) && s.T > 0 && isfinite(s.rho) && s.rho > 0
+                && isfinite(s.sound) && s.sound > 0 && isfinite(s.cv) && s.cv > 0 && isfinite(s.gasMass)
+                && s.gasMass >= 0 && isfinite(s.dilatation);
+            if (!ok) atomicMin(first, (unsigned long long)c);
+        }
+        if (prim) {
+            const ReactiveTransportPrimitive p = prim[c];
+            if (!(isfinite(p.rho) && p.rho > 0)) atomicMin(first + 1, 2ull * c);
+            else if (!(isfinite(p.u[0]) && isfinite(p.u[1]) && isfinite(p.u[2])))
+                atomicMin(first + 1, 2ull * c + 1);
+        }
+    }
+}
+
 // Strided gather of the WALE scalar fields into the handle's arrays: cp of entry
 // c to mixCp[offset + c], enthalpy k to spH[k * all + offset + c]. A cp that is
 // not finite and positive or a non-finite enthalpy sets bit 2 of the status.

@@ -39,14 +39,18 @@ class GpuHem:
     def device_bytes(self):
         return self.lib.reactive_gpu_hem_device_bytes_v1(self.handle)
 
-    def run(self, q, energy, states):
+    def run(self, q, energy, states, success=None):
         """Flash host arrays in place: states (THERMO_DTYPE) are seeds in, results
-        out for successful cells. Returns (success int32 array, profile)."""
+        out for successful cells. success: an int32 array of the batch size to
+        fill (pinned memory keeps its copy asynchronous), or None for a new one.
+        Returns (success int32 array, profile)."""
         q = np.ascontiguousarray(q, dtype=np.float64)
         energy = np.ascontiguousarray(energy, dtype=np.float64)
         assert states.dtype == A.THERMO_DTYPE and states.flags.c_contiguous
         n = len(energy)
-        success = np.zeros(n, dtype=np.int32)
+        if success is None:
+            success = np.zeros(n, dtype=np.int32)
+        assert success.dtype == np.int32 and success.shape == (n,) and success.flags.c_contiguous
         prof = A.HemProfile(1, C.sizeof(A.HemProfile))
         err = C.create_string_buffer(1024)
         rc = self.lib.reactive_gpu_hem_run_v1(self.handle, A.dptr(q), A.dptr(energy), n,

@@ -244,3 +244,59 @@ def test_hllc_stage_against_oracle(spec, mixed):
     finally:
         oracle.set_flux_scheme(0)
         lib.reactive_transport_destroy(h)
+
+
+def _host_walk(lib, h, case, y=None, hh=None):
+    """The host-array entries on one handle: RHS, CFL (both forms), a stage
+    pair, and a resident stage pair under an attempt."""
+    q, st = case["q"].copy(), case["states"]
+    nv, ns = case["nv"], case["ns"]
+    out = {}
+    rhs, br = np.empty_like(q), np.empty(nv)
+    assert lib.reactive_transport_rhs(h, T.dp(q), T.states_ptr(st), None, None, T.dp(rhs), T.dp(br)) == 0, \
+        lib.reactive_transport_error(h)
+    out["rhs"], out["br"] = rhs, br.copy()
+    dt = C.c_double()
+    assert lib.reactive_transport_stable_step(h, T.dp(q), T.states_ptr(st), .23, .1, C.byref(dt)) == 0
+    out["dt"] = dt.value
+    prim = T.primitives(q, st, ns)
+    assert lib.reactive_transport_stable_step_primitives(h, prim, T.states_ptr(st), .23, .1, C.byref(dt)) == 0
+    out["dt_prim"] = dt.value
+    step = .1 * out["dt"]
+    b0, b1 = np.empty(nv), np.empty(nv)
+    assert lib.reactive_transport_stage(h, T.dp(q), T.states_ptr(st), None, None, step, 0, T.dp(b0)) == 0
+    out["q1"] = q.copy()
+    st1, _, _ = T.ideal_states(q, ns)
+    assert lib.reactive_transport_stage(h, T.dp(q), T.states_ptr(st1), None, None, step, 1, T.dp(b1)) == 0
+    out["qn"], out["b0"], out["b1"] = q.copy(), b0, b1
+    return out
+
+
+@pytest.mark.parametrize("spec", BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_host_entries_on_the_structured_box_match_the_face_graph(spec):
+    """The host-array entries use the structured FP64 HLL stencils on a
+    canonical box (whatever precision and flux the device entries use): RHS,
+    CFL steps and stages bitwise equal to the face graph's, ledgers within the
+    operator tolerance."""
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    cw = spec.get("wale")
+    results = []
+    for structured in (1, 0):
+        h = T.create(lib, 1, case, wale_cw=cw)
+        try:
+            assert L.reactive_transport_structured_v3(h, structured, None) == 0
+            if structured:  # device-entry settings do not reach the host entries
+                assert L.reactive_transport_precision_v3(h, 1, None) == 0
+                assert L.reactive_transport_flux_v3(h, 1, None) == 0
+            results.append(_host_walk(lib, h, case))
+        finally:
+            lib.reactive_transport_destroy(h)
+    box, graph = results
+    for key in ("rhs", "q1", "qn"):
+        assert np.array_equal(box[key], graph[key]), key
+    assert box["dt"] == graph["dt"] and box["dt_prim"] == graph["dt_prim"]
+    for key in ("br", "b0", "b1"):
+        assert T.scaled_error(box[key][None], graph[key][None]) <= T.RHS_TOL
