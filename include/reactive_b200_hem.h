@@ -79,6 +79,22 @@ int reactive_gpu_hem_autotune_v3(void* hem, const double* conserved, size_t stri
     size_t variables, const ReactiveThermoState* seed, void* stream, int* blocksPerSm, char* error,
     size_t errorSize);
 
+/* Two-phase admissibility bound of the work-queue search (no reference
+ * counterpart). For a pure fluid a two-phase candidate can only converge to a
+ * mixture on a saturation tie line of the model's cubic (chemical potentials
+ * equal to mutol, volume and energy to vtol and etol). At create the handle
+ * tabulates the tie lines (4,096 temperatures over the liquid range) and bounds
+ * the specific internal energy of the mixtures at each specific volume; a cell
+ * outside that region, widened by 1e-3 of the latent energy and ten tolerances,
+ * has its two-phase seeds (and restart seeds) recorded as failed without the
+ * Newton solves, which could not converge. Results are the exhaustive search's
+ * bit for bit; the work counters count the skipped seeds as failed candidates
+ * without phase evaluations. On by default where the bound is built (a pure
+ * fluid, mutol <= 1e-5, a liquid range ending at or below the cubic's critical
+ * temperature); request 0 turns it off, 1 on, -1 queries; *active (may be NULL)
+ * receives the state. The plain per-cell form and the static entry run the
+ * exhaustive search. */
+int reactive_gpu_hem_two_phase_bound_v3(void* hem, int request, int* active, char* error, size_t errorSize);
 /* Vector-Jacobian product of the flash (no reference counterpart; the
  * reference's tangent precedent is its host IFT TangentContext,
  * src/reactiveThermo/reactiveDirectional.inc:81-106). At the converged states

@@ -69,6 +69,7 @@ HEM = {
     "run_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, _v, _v, C.c_int, _v, C.c_char_p,
                        C.c_size_t], C.c_int),
     "run_counters_v3": ([_v, C.POINTER(A.HemProfile), _v, C.c_char_p, C.c_size_t], C.c_int),
+    "two_phase_bound_v3": ([_v, C.c_int, C.POINTER(C.c_int), C.c_char_p, C.c_size_t], C.c_int),
     "vjp_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, C.c_size_t, _v, _v, C.c_char_p,
                        C.c_size_t], C.c_int),
     "autotune_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, C.POINTER(C.c_int), C.c_char_p,
@@ -83,6 +84,7 @@ IDEAL = {
     "destroy_v3": ([_v], None),
     "run_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, _v, _v, C.c_char_p, C.c_size_t],
                       C.c_int),
+    "two_phase_bound_v3": ([_v, C.c_int, C.POINTER(C.c_int), C.c_char_p, C.c_size_t], C.c_int),
     "vjp_device_v3": ([_v, _v, C.c_size_t, C.c_size_t, C.c_size_t, _v, _v, _v, C.c_size_t, _v, C.c_char_p,
                        C.c_size_t], C.c_int),
 }

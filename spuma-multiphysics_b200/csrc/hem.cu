@@ -52,13 +52,13 @@ __device__ __forceinline__ unsigned fetchItems(unsigned* counter) {
     return __shfl_sync(0xffffffffu, base, 0);
 }
 
-__global__ void inputsFromHost(const double* q, const double* energy, const ReactiveThermoState* guess, size_t count,
-                               int ns, CellInput* in) {
+__global__ void inputsFromHost(const HemConst* __restrict__ Cp, const double* q, const double* energy,
+                               const ReactiveThermoState* guess, size_t count, int ns, CellInput* in) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
         double rho = 0;
         for (int k = 0; k < ns; ++k) rho += q[c * ns + k];
         const ReactiveThermoState g = guess[c];
-        in[c] = CellInput{rho, energy[c], g.p, g.T, g.liquidMass[0]};
+        in[c] = CellInput{rho, energy[c], g.p, g.T, g.liquidMass[0], twoPhaseImpossible(*Cp, rho, energy[c])};
     }
 }
 
@@ -66,10 +66,10 @@ __global__ void inputsFromHost(const double* q, const double* energy, const Reac
 // q holds ns masses per cell, energy the bulk internal energy density; the
 // seeds are gathered too (a failed cell returns its seed). A capillary entry
 // that asks for a pressure jump or the frozen partition sets *unsupported.
-__global__ void inputsFromResident(const double* q, const double* energy, const ReactiveThermoState* seed,
-                                   const ReactiveGpuHemCapillaryInputV2* capillary, const uint32_t* order,
-                                   size_t count, int ns, CellInput* in, ReactiveThermoState* guess,
-                                   unsigned* unsupported) {
+__global__ void inputsFromResident(const HemConst* __restrict__ Cp, const double* q, const double* energy,
+                                   const ReactiveThermoState* seed, const ReactiveGpuHemCapillaryInputV2* capillary,
+                                   const uint32_t* order, size_t count, int ns, CellInput* in,
+                                   ReactiveThermoState* guess, unsigned* unsupported) {
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(blockDim.x) * gridDim.x) {
         const size_t c = order[i];
         if (capillary && !(capillary[c].pressureJump == 0.0 && capillary[c].equilibrium == 1)) atomicOr(unsupported, 1u);
@@ -77,7 +77,7 @@ __global__ void inputsFromResident(const double* q, const double* energy, const 
         for (int k = 0; k < ns; ++k) rho += q[c * size_t(ns) + k];
         const ReactiveThermoState g = seed[c];
         guess[i] = g;
-        in[i] = CellInput{rho, energy[c], g.p, g.T, g.liquidMass[0]};
+        in[i] = CellInput{rho, energy[c], g.p, g.T, g.liquidMass[0], twoPhaseImpossible(*Cp, rho, energy[c])};
     }
 }
 
@@ -93,15 +93,15 @@ __global__ void scatterResident(const ReactiveThermoState* state, const int* suc
 }
 
 // Internal energy density E - |m|^2/(2 rho) from the SoA conserved rows.
-__global__ void inputsFromConserved(const double* cons, size_t stride, size_t count, int ns,
-                                    const ReactiveThermoState* seed, CellInput* in) {
+__global__ void inputsFromConserved(const HemConst* __restrict__ Cp, const double* cons, size_t stride, size_t count,
+                                    int ns, const ReactiveThermoState* seed, CellInput* in) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
         double rho = 0;
         for (int k = 0; k < ns; ++k) rho += cons[size_t(k) * stride + c];
         const double mx = cons[size_t(ns) * stride + c], my = cons[size_t(ns + 1) * stride + c],
                      mz = cons[size_t(ns + 2) * stride + c], E = cons[size_t(ns + 3) * stride + c];
         const double e = E - .5 * (mx * mx + my * my + mz * mz) / rho;
-        in[c] = CellInput{rho, e, seed[c].p, seed[c].T, seed[c].liquidMass[0]};
+        in[c] = CellInput{rho, e, seed[c].p, seed[c].T, seed[c].liquidMass[0], twoPhaseImpossible(*Cp, rho, e)};
     }
 }
 
@@ -156,6 +156,13 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
                         L.mass = kind == 1 ? L.x.q : 0.0;
                         L.st = kind >= 2 ? Q_TP_START : Q_FZ_START;
                         L.req = REQ_NONE;
+                        if (kind >= 2 && L.x.noTwoPhase) {
+                            // outside every saturation tie line: the seed cannot converge
+                            ++n.candidates;
+                            ++n.failures;
+                            records.status(L, 0);
+                            L.st = Q_FREE;
+                        }
                     } else exhausted = true;
                 }
             }
@@ -243,7 +250,10 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passRestar
             const CellInput x = in[fallback[slot]];
             CandRecord* out = fb + size_t(t) * capacity + slot;
             out->status = 0;
-            if (upper > lower) {
+            if (x.noTwoPhase) {  // no restart seed can converge either
+                n.candidates += 5;
+                n.failures += 5;
+            } else if (upper > lower) {
                 const double restartT = lower + (upper - lower) * kRestart[t];
                 bool have = false;
                 double bestEntropy = 0;
@@ -412,6 +422,52 @@ __global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsi
 // ------------------------------------------------------------------ host
 std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C);
 
+// Saturation tie lines of a pure fluid on a temperature grid, one thread per
+// temperature: the pressure where the chemical potentials of the smallest and
+// largest cubic roots agree, by bisection in ln p (below it the liquid root has
+// the higher potential or only a vapour-like root exists; above it the reverse
+// or only a liquid-like root). out[5 i..5 i+4] = {valid, v_l, v_g, u_l, u_g}.
+__global__ void domeSaturation(const HemConst* __restrict__ Cp, int n, double T0, double dT, double* out) {
+    const HemConst& C = *Cp;
+    const PureSpecies& sp = C.gas;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x) {
+        double* o = out + 5 * size_t(i);
+        o[0] = 0;
+        const double T = T0 + dT * i;
+        TTerms t;
+        if (tTerms(sp, T, t) != EOS_OK) continue;
+        const double Tcm = sp.a * kOmegaB / (sp.b * kOmegaA * kGas), pc = kOmegaB * kGas * Tcm / sp.b;
+        double lo = log(1e-9 * pc), hi = log(2.0 * pc);
+        bool ok = true;
+        for (int it = 0; it < 160 && ok; ++it) {
+            const double lp = .5 * (lo + hi);
+            Roots r;
+            if (cubicRoots(sp, T, exp(lp), t.aa, r) != EOS_OK) { ok = false; break; }
+            if (r.count >= 2) {
+                PhaseProps L, G;
+                int ph;
+                if (prTrhoT(sp, t, sp.W / r.lo, true, L, ph) != EOS_OK || prTrhoT(sp, t, sp.W / r.hi, true, G, ph) != EOS_OK) {
+                    ok = false;
+                    break;
+                }
+                if (L.mu > G.mu) lo = lp; else hi = lp;
+            } else if (r.liquid && !r.gas) hi = lp;
+            else lo = lp;
+        }
+        if (!ok) continue;
+        const double p = exp(.5 * (lo + hi));
+        Roots r;
+        PhaseProps L, G;
+        int ph;
+        if (cubicRoots(sp, T, p, t.aa, r) != EOS_OK || r.count < 2 || prTrhoT(sp, t, sp.W / r.lo, true, L, ph) != EOS_OK
+            || prTrhoT(sp, t, sp.W / r.hi, true, G, ph) != EOS_OK)
+            continue;
+        if (!(fabs(L.mu - G.mu) <= 1e-9 * kGas * T) || !(G.rho < L.rho)) continue;
+        o[1] = 1 / L.rho; o[2] = 1 / G.rho; o[3] = L.e; o[4] = G.e;
+        o[0] = 1;
+    }
+}
+
 struct HemDevice {
     std::mutex entry;
     int device = 0;
@@ -434,6 +490,7 @@ struct HemDevice {
     ReactiveThermoState* dout = nullptr;
     int* dsuccess = nullptr;
     int passBlocks = 0;
+    int domeBuilt = 0;  // grid points of the two-phase bound (0: none for this model)
     size_t bytes = 0;
     std::vector<void*> blocks;
 
@@ -496,6 +553,98 @@ struct HemDevice {
     }
 };
 
+// The two-phase admissibility bound of a pure fluid (HemConst::dome*): the
+// saturation tie lines on 4,096 temperatures from the liquid range's lower end
+// to its critical end, then per point of a 8,192-point log grid in specific
+// volume the largest and smallest specific internal energy of the tie lines
+// through it (and of the tie-line ends between it and its neighbours). Tie
+// lines are straight in (v, u) with positive slope, so an interval's extremes
+// sit at its ends or at a tie line's end inside it. The tie lines above the
+// last resolved temperature lie in the box of the last one. Margins: 1e-3 of
+// the largest latent energy plus ten energy tolerances, 1e-4 plus ten volume
+// tolerances in v. Not built (no bound) for two tables, a loose chemical
+// tolerance, a liquid range past the cubic's critical temperature, or any
+// unresolved temperature below the last resolved one.
+void buildDome(HemDevice& d) {
+    HemConst& C = d.hostConst;
+    C.domeN = 0;
+    const PureSpecies& sp = C.gas;
+    const double Tcm = sp.a * kOmegaB / (sp.b * kOmegaA * kGas);
+    const double T0 = std::max(C.Tmin, C.liquidTmin), T1 = std::min(C.Tmax, C.liquidTc * (1 - 1e-10));
+    if (!C.samePure || !(C.mutol <= 1e-5) || !(C.liquidTc * (1 - 1e-10) <= Tcm) || !(T1 > T0)) return;
+    constexpr int nT = 4096, nV = 8192;
+    const double dT = (T1 - T0) / (nT - 1);
+    double* dev = nullptr;
+    check(cudaMalloc(&dev, sizeof(double) * 5 * nT), "cudaMalloc");
+    domeSaturation<<<nT / 128, 128, 0, d.stream>>>(d.cst, nT, T0, dT, dev);
+    std::vector<double> t(5 * nT);
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaMemcpyAsync(t.data(), dev, sizeof(double) * 5 * nT, cudaMemcpyDeviceToHost, d.stream);
+    cudaError_t e3 = cudaStreamSynchronize(d.stream);
+    cudaFree(dev);
+    check(e1, "domeSaturation");
+    check(e2, "D2H dome");
+    check(e3, "sync");
+    int last = -1;
+    for (int i = 0; i < nT; ++i)
+        if (t[5 * i] == 1) {
+            if (last != i - 1) return;  // a gap below a resolved temperature
+            last = i;
+        }
+    if (last < 1 || last < nT - 8) return;
+    double vlo = HUGE_VAL, vhi = 0, latent = 0;
+    for (int i = 0; i <= last; ++i) {
+        vlo = std::min(vlo, t[5 * i + 1]);
+        vhi = std::max(vhi, t[5 * i + 2]);
+        latent = std::max(latent, t[5 * i + 4] - t[5 * i + 3]);
+    }
+    if (!(vlo > 0 && vhi > vlo && latent > 0)) return;
+    const double lnV0 = std::log(vlo), step = std::log(vhi / vlo) / (nV - 1);
+    std::vector<double> up(nV, -HUGE_VAL), lo(nV, HUGE_VAL), vgrid(nV);
+    for (int j = 0; j < nV; ++j) vgrid[j] = std::exp(lnV0 + j * step);
+    auto index = [&](double v) { return int(std::floor((std::log(v) - lnV0) / step)); };
+    auto touch = [&](int j, double u) {
+        for (int k = j; k <= j + 1; ++k)
+            if (k >= 0 && k < nV) { up[k] = std::max(up[k], u); lo[k] = std::min(lo[k], u); }
+    };
+    for (int i = 0; i <= last; ++i) {
+        const double vl = t[5 * i + 1], vg = t[5 * i + 2], ul = t[5 * i + 3], ug = t[5 * i + 4];
+        for (int j = std::max(0, index(vl)); j <= std::min(nV - 1, index(vg) + 1); ++j) {
+            const double vj = vgrid[j];
+            if (vj < vl || vj > vg) continue;
+            const double u = ul + (ug - ul) * (vj - vl) / (vg - vl);
+            up[j] = std::max(up[j], u);
+            lo[j] = std::min(lo[j], u);
+        }
+        touch(index(vl), ul);
+        touch(index(vg), ug);
+    }
+    {  // the critical end above the last resolved temperature
+        const double vl = t[5 * last + 1], vg = t[5 * last + 2], ul = t[5 * last + 3], ug = t[5 * last + 4];
+        for (int j = std::max(0, index(vl)); j <= std::min(nV - 1, index(vg) + 1); ++j) {
+            up[j] = std::max(up[j], ug);
+            lo[j] = std::min(lo[j], ul);
+        }
+    }
+    std::vector<double> packed(2 * nV);
+    std::copy(up.begin(), up.end(), packed.begin());
+    std::copy(lo.begin(), lo.end(), packed.begin() + nV);
+    double* table = d.alloc<double>(2 * nV);
+    check(cudaMemcpyAsync(table, packed.data(), sizeof(double) * 2 * nV, cudaMemcpyHostToDevice, d.stream), "H2D dome");
+    C.domeUp = table;
+    C.domeLo = table + nV;
+    C.domeLnV0 = lnV0;
+    C.domeInvStep = 1 / step;
+    C.domeVlo = vlo;
+    C.domeVhi = vhi;
+    C.domeMarginU = 1e-3 * latent + 10 * C.etol * std::max(1e5, 2000 * C.Tmax);
+    C.domeMarginV = 1e-4 + 10 * C.vtol;
+    C.domeN = nV;
+    d.domeBuilt = nV;
+    check(cudaMemcpyAsync(d.cst, &C, sizeof(HemConst), cudaMemcpyHostToDevice, d.stream), "H2D constants");
+    check(cudaStreamSynchronize(d.stream), "sync");
+}
+
 void* create(const void* raw, size_t bytes, size_t capacity, bool hostPath, char* error, size_t size) {
     try {
         require(raw && bytes == sizeof(ReactiveB200HemModel) && capacity && capacity <= UINT32_MAX / 8,
@@ -526,6 +675,7 @@ void* create(const void* raw, size_t bytes, size_t capacity, bool hostPath, char
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "attribute");
         d->passBlocks = std::max(1, perSm) * std::max(1, sms);
         if (hostPath) d->ensureHostPath();
+        buildDome(*d);
         check(cudaStreamSynchronize(d->stream), "sync");
         return d.release();
     } catch (const std::exception& e) {
@@ -782,7 +932,8 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
             rb200::check(cudaStreamWaitEvent(s, uploaded[i], 0), "wait");
             if (i == 0) rb200::check(cudaEventRecord(first, s), "event");
             rb200::check(cudaMemsetAsync(d.dsuccess + off, 0, n * sizeof(int), s), "memset");
-            rb200::inputsFromHost<<<rb200::gridFor(n, 256), 256, 0, s>>>(d.dq + off, d.de + off, d.dguess + off, n, 1,
+            rb200::inputsFromHost<<<rb200::gridFor(n, 256), 256, 0, s>>>(d.cst, d.dq + off, d.de + off, d.dguess + off,
+                                                                         n, 1,
                                                                          d.in);
             rb200::check(cudaGetLastError(), "inputs");
             d.launchSearch(n, d.dguess + off, d.dout + off, nullptr, d.dsuccess + off, s);
@@ -872,7 +1023,8 @@ int reactive_gpu_hem_run_resident_v1(void* raw, const double* q, const double* e
         cudaStream_t s = d.stream;
         unsigned* unsupported = d.counters + rb200::FAILED;  // reset by the search before its own use
         rb200::check(cudaMemsetAsync(unsupported, 0, sizeof(unsigned), s), "memset");
-        rb200::inputsFromResident<<<rb200::gridFor(count, 256), 256, 0, s>>>(q, energy, seed, capillary, order, count,
+        rb200::inputsFromResident<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.cst, q, energy, seed, capillary, order,
+                                                                            count,
                                                                             1, d.in, d.dguess, unsupported);
         rb200::check(cudaGetLastError(), "inputs");
         unsigned flag = 0;
@@ -924,10 +1076,31 @@ int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t st
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count <= d.capacity, "Device HEM batch exceeds capacity");
         auto s = static_cast<cudaStream_t>(stream);
-        rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1, seed, d.in);
+        rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.cst, conserved, stride, count, 1, seed,
+                                                                             d.in);
         rb200::check(cudaGetLastError(), "inputs");
         if (flags & 2) d.launchPerCell(count, seed, state, transport, success, s);
         else d.launchSearch(count, seed, state, transport, success, s);
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
+}
+
+int reactive_gpu_hem_two_phase_bound_v3(void* raw, int request, int* active, char* error, size_t size) {
+    try {
+        rb200::require(raw && request >= -1 && request <= 1, "Invalid two-phase bound request");
+        auto& d = *static_cast<HemDevice*>(raw);
+        std::lock_guard<std::mutex> lock(d.entry);
+        rb200::require(request != 1 || d.domeBuilt, "This model has no two-phase bound (see the header)");
+        if (request >= 0) {
+            d.hostConst.domeN = request ? d.domeBuilt : 0;
+            rb200::check(cudaMemcpyAsync(d.cst, &d.hostConst, sizeof(d.hostConst), cudaMemcpyHostToDevice, d.stream),
+                         "H2D constants");
+            rb200::check(cudaStreamSynchronize(d.stream), "sync");
+        }
+        if (active) *active = d.hostConst.domeN ? 1 : 0;
         return 0;
     } catch (const std::exception& e) {
         if (error && size) std::snprintf(error, size, "%s", e.what());
@@ -981,8 +1154,8 @@ int reactive_gpu_hem_autotune_v3(void* raw, const double* conserved, size_t stri
             d.passBlocks = k * sms;
             for (int r = 0; r < 2; ++r) {  // the first run warms up
                 rb200::check(cudaEventRecord(a, s), "event");
-                rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1,
-                                                                                      seed, d.in);
+                rb200::inputsFromConserved<<<rb200::gridFor(count, 256), 256, 0, s>>>(d.cst, conserved, stride, count,
+                                                                                      1, seed, d.in);
                 d.launchSearch(count, seed, d.dout, nullptr, d.dsuccess, s);
                 rb200::check(cudaEventRecord(b, s), "event");
                 rb200::check(cudaEventSynchronize(b), "event");
@@ -1118,7 +1291,7 @@ extern "C" int reactive_gpu_hem_run_static_v3(const void* model, size_t modelByt
         check(cudaGetLastError(), "storeConstants");
         check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "clear counters");
         check(cudaMemsetAsync(totals, 0, NTOTALS * sizeof(unsigned long long), s), "clear totals");
-        inputsFromConserved<<<gridFor(count, 256), 256, 0, s>>>(conserved, stride, count, 1, seed, in);
+        inputsFromConserved<<<gridFor(count, 256), 256, 0, s>>>(cst, conserved, stride, count, 1, seed, in);
         check(cudaGetLastError(), "inputs");
         if (hostConst.stableGasPrune) {
             passQueue<<<blocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 2, rec, counters, Q_A, totals);

@@ -42,11 +42,41 @@ struct HemConst {
     // falls with T and the liquid range ends at or below its Tc; the all-liquid volume
     // residual q/rho_l - 1 then stays below q/rho_c - 1 < -vtol.
     double liquidFloor;
+    // Two-phase admissibility bound of a pure fluid (domeN = 0: none). A two-phase
+    // candidate can only converge to a mixture of the two roots of one cubic at a
+    // (p, T) where their chemical potentials agree to mutol, so the cell's specific
+    // volume and internal energy must lie (within the volume and energy
+    // tolerances) on a saturation tie line. domeUp[j] / domeLo[j] bound the
+    // specific internal energy of every tie-line point whose specific volume lies
+    // within one grid step of v_j = exp(domeLnV0 + j / domeInvStep).
+    const double* domeUp;
+    const double* domeLo;
+    int domeN;
+    double domeLnV0, domeInvStep, domeVlo, domeVhi, domeMarginU, domeMarginV;
 };
 
 struct CellInput {
     double q, e, gp, gT, gml;  // mass density, internal energy density, seed p, T, liquid mass
+    int noTwoPhase;            // no two-phase candidate can converge (the dome bound)
 };
+
+// True when the cell's (1/q, e/q) lies provably outside every saturation tie
+// line widened by the margins: the two-phase seeds would all fail.
+__device__ inline bool twoPhaseImpossible(const HemConst& C, double q, double e) {
+    if (C.domeN < 4 || !(q > 0) || !isfinite(q) || !isfinite(e)) return false;
+    const double v = 1 / q, u = e / q;
+    if (v < C.domeVlo * (1 - C.domeMarginV) || v > C.domeVhi * (1 + C.domeMarginV)) return true;
+    int j = int(floor((log(v) - C.domeLnV0) * C.domeInvStep));
+    j = j < 1 ? 1 : (j > C.domeN - 3 ? C.domeN - 3 : j);
+    double up = C.domeUp[j - 1], lo = C.domeLo[j - 1];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        up = fmax(up, C.domeUp[j + k]);
+        lo = fmin(lo, C.domeLo[j + k]);
+    }
+    const double margin = C.domeMarginU + 10 * C.etol * fabs(u);
+    return u > up + margin || u < lo - margin;
+}
 
 struct Counts {
     unsigned phases = 0, residuals = 0, candidates = 0, stable = 0, failures = 0, analytic = 0, fd = 0;
