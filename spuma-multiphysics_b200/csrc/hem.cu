@@ -188,6 +188,57 @@ __device__ __forceinline__ bool gasDecides(const HemConst& C, const CandRecord& 
     return C.stableGasPrune && gas.status == 2 && gas.st.gasMass > 0;
 }
 
+// Cells whose two-phase seeds provably fail (the two-phase bound) have only
+// their all-gas and all-liquid candidates to solve: one thread per cell runs them
+// through the same out-of-line solvers the work queue's state machines restate,
+// so the records are bit for bit the queue's, and the seed records are marked
+// failed. The other cells are listed for the work queue.
+__global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSinglePhase(const HemConst* __restrict__ Cp,
+                                                                const CellInput* __restrict__ in, size_t count,
+                                                                CandRecord* rec, unsigned* list, unsigned* counters,
+                                                                unsigned long long* totals) {
+    const HemConst& C = *Cp;
+    Counts n;
+    for (size_t base = blockIdx.x * size_t(blockDim.x); base < count; base += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = base + threadIdx.x;
+        bool queue = false;
+        if (c < count) {
+            const CellInput x = in[c];
+            if (!x.noTwoPhase) queue = true;
+            else {
+                for (int kind = 0; kind < 2; ++kind) {
+                    CandRecord& r = rec[size_t(kind) * count + c];
+                    const double mass = kind ? x.q : 0.0;
+                    Eval v;
+                    CandidateOut o{};
+                    const bool floor = kind == 1 && x.q * (1 + 1e-12) < C.liquidFloor;
+                    if (floor || !frozenSolve(C, x, mass, 0, v, o, n)) {
+                        r.status = 0;
+                        ++n.failures;
+                        continue;
+                    }
+                    stateFromEval(v, x.q, o, r.st);
+                    r.entropyD = v.entropyD;
+                    const bool stable = stableAt(C, x.q, v.liqMass, v.p, v.T, n);
+                    r.status = stable ? 2 : 1;
+                    if (stable) ++n.stable; else ++n.failures;
+                }
+                for (int kind = 2; kind < 7; ++kind) {
+                    rec[size_t(kind) * count + c].status = 0;
+                    ++n.candidates;
+                    ++n.failures;
+                }
+            }
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, queue);
+        unsigned slot = 0;
+        if ((threadIdx.x & 31) == 0 && mask) slot = atomicAdd(counters + LIST, unsigned(__popc(mask)));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (queue) list[slot + __popc(mask & ((1u << (threadIdx.x & 31)) - 1))] = unsigned(c);
+    }
+    flushCounts(n, totals);
+}
+
 __global__ void compactSeedCells(const HemConst* __restrict__ Cp, const CandRecord* rec, size_t count,
                                  unsigned* list, unsigned* counters) {
     const HemConst& C = *Cp;
@@ -537,6 +588,12 @@ struct HemDevice {
             compactSeedCells<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, list, counters);
             check(cudaGetLastError(), "compactSeedCells");
             passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, 2, 5, rec, counters, Q_B, totals);
+            check(cudaGetLastError(), "passQueue");
+        } else if (hostConst.domeN) {
+            // single-phase cells one thread each, the rest through the work queue
+            passSinglePhase<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, rec, list, counters, totals);
+            check(cudaGetLastError(), "passSinglePhase");
+            passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, 0, 7, rec, counters, Q_A, totals);
             check(cudaGetLastError(), "passQueue");
         } else {
             passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 7, rec, counters, Q_A, totals);

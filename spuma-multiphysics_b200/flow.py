@@ -184,6 +184,30 @@ class Flow:
         self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s,
                             per_cell)
 
+    def two_phase_bound(self, on=None):
+        """Query (on=None) or set the flash's two-phase admissibility bound
+        (reactive_gpu_hem_two_phase_bound_v3); drops a captured graph."""
+        active = C.c_int()
+        err = C.create_string_buffer(512)
+        request = -1 if on is None else int(bool(on))
+        if self.lib.reactive_gpu_hem_two_phase_bound_v3(self.hem.handle, request, C.byref(active), err, len(err)):
+            raise FlowError(err.value.decode())
+        if on is not None:
+            self.graph = None
+        return bool(active.value)
+
+    def stage0(self, dt):
+        """Stage 0 of a step on the resident state (CFL query and q1 = qn + dt L(qn)),
+        leaving q1 and the step-start states as the step's first recovery takes
+        them (asynchronous on the flow's stream)."""
+        lib, t, s = self.lib, self.transport, self.stream.cuda_stream
+        if self.scalars:
+            self._scalar_fields(self.sn)
+        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.qn.data_ptr(), self.tr.data_ptr(),
+                                                                    self.cfl, dt, self.dt_cfl.data_ptr(), s))
+        _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.qn.data_ptr(), self.q1.data_ptr(),
+                                                              self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(), s))
+
     def autotune(self):
         """Choose the launch shapes of this flow's transport and flash kernels by
         timing the candidates on its current state (synchronous; drops a
