@@ -189,52 +189,69 @@ __device__ __forceinline__ bool gasDecides(const HemConst& C, const CandRecord& 
 }
 
 // Cells whose two-phase seeds provably fail (the two-phase bound) have only
-// their all-gas and all-liquid candidates to solve: one thread per cell runs them
-// through the same out-of-line solvers the work queue's state machines restate,
-// so the records are bit for bit the queue's, and the seed records are marked
-// failed. The other cells are listed for the work queue.
+// their all-gas and all-liquid candidates: one thread per cell solves them
+// through the same out-of-line solvers the work queue's state machines restate
+// (bit for bit the queue's candidates), selects as selectCandidates does (the
+// stable candidate of larger entropy, the all-gas one on a tie) and writes the
+// outputs; a cell with neither goes to the restart list. The other cells are
+// listed for the work queue.
+__device__ __forceinline__ void appendTo(unsigned* list, unsigned* counter, bool take, unsigned value) {
+    const unsigned mask = __ballot_sync(0xffffffffu, take);
+    unsigned slot = 0;
+    if ((threadIdx.x & 31) == 0 && mask) slot = atomicAdd(counter, unsigned(__popc(mask)));
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if (take) list[slot + __popc(mask & ((1u << (threadIdx.x & 31)) - 1))] = value;
+}
+
 __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSinglePhase(const HemConst* __restrict__ Cp,
                                                                 const CellInput* __restrict__ in, size_t count,
-                                                                CandRecord* rec, unsigned* list, unsigned* counters,
+                                                                ReactiveThermoState* state,
+                                                                ReactiveTransportState* transport, int* success,
+                                                                unsigned* list, unsigned* fallback, unsigned* counters,
                                                                 unsigned long long* totals) {
     const HemConst& C = *Cp;
     Counts n;
     for (size_t base = blockIdx.x * size_t(blockDim.x); base < count; base += size_t(blockDim.x) * gridDim.x) {
         const size_t c = base + threadIdx.x;
-        bool queue = false;
+        bool queue = false, restart = false;
         if (c < count) {
             const CellInput x = in[c];
             if (!x.noTwoPhase) queue = true;
             else {
+                ReactiveThermoState best;
+                double bestEntropy = 0;
+                bool have = false;
                 for (int kind = 0; kind < 2; ++kind) {
-                    CandRecord& r = rec[size_t(kind) * count + c];
                     const double mass = kind ? x.q : 0.0;
                     Eval v;
                     CandidateOut o{};
                     const bool floor = kind == 1 && x.q * (1 + 1e-12) < C.liquidFloor;
                     if (floor || !frozenSolve(C, x, mass, 0, v, o, n)) {
-                        r.status = 0;
                         ++n.failures;
                         continue;
                     }
-                    stateFromEval(v, x.q, o, r.st);
-                    r.entropyD = v.entropyD;
                     const bool stable = stableAt(C, x.q, v.liqMass, v.p, v.T, n);
-                    r.status = stable ? 2 : 1;
-                    if (stable) ++n.stable; else ++n.failures;
+                    if (!stable) {
+                        ++n.failures;
+                        continue;
+                    }
+                    ++n.stable;
+                    if (!have || v.entropyD > bestEntropy) {
+                        have = true;
+                        bestEntropy = v.entropyD;
+                        stateFromEval(v, x.q, o, best);
+                    }
                 }
-                for (int kind = 2; kind < 7; ++kind) {
-                    rec[size_t(kind) * count + c].status = 0;
-                    ++n.candidates;
-                    ++n.failures;
-                }
+                n.candidates += 5;  // the two-phase seeds, failed without their solves
+                n.failures += 5;
+                if (have) {
+                    writeOutputs(best, c, state, transport);
+                    if (success) success[c] = 1;
+                } else restart = true;
             }
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, queue);
-        unsigned slot = 0;
-        if ((threadIdx.x & 31) == 0 && mask) slot = atomicAdd(counters + LIST, unsigned(__popc(mask)));
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        if (queue) list[slot + __popc(mask & ((1u << (threadIdx.x & 31)) - 1))] = unsigned(c);
+        appendTo(list, counters + LIST, queue, unsigned(c));
+        appendTo(fallback, counters + FALLBACK, restart, unsigned(c));
     }
     flushCounts(n, totals);
 }
@@ -253,12 +270,15 @@ __global__ void compactSeedCells(const HemConst* __restrict__ Cp, const CandReco
     }
 }
 
+// Selection over every cell, or (list) over the cells the work queue solved.
 __global__ void selectCandidates(const HemConst* __restrict__ Cp, const CandRecord* rec, size_t count,
-                                 ReactiveThermoState* state, ReactiveTransportState* transport, int* success,
-                                 unsigned* fallback, unsigned* counters) {
+                                 const unsigned* list, ReactiveThermoState* state, ReactiveTransportState* transport,
+                                 int* success, unsigned* fallback, unsigned* counters) {
     const HemConst& C = *Cp;
-    for (size_t base = blockIdx.x * size_t(blockDim.x); base < count; base += size_t(blockDim.x) * gridDim.x) {
-        const size_t c = base + threadIdx.x;
+    const size_t items = list ? counters[LIST] : count;
+    for (size_t base = blockIdx.x * size_t(blockDim.x); base < items; base += size_t(blockDim.x) * gridDim.x) {
+        const size_t i = base + threadIdx.x;
+        const size_t c = i < items ? (list ? list[i] : i) : count;  // lanes past the end select nothing
         int best = -1;
         double bestEntropy = 0;
         if (c < count) {
@@ -581,6 +601,7 @@ struct HemDevice {
     void launchSearch(size_t count, const ReactiveThermoState* seed, ReactiveThermoState* state,
                       ReactiveTransportState* transport, int* success, cudaStream_t s) {
         check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "memset counters");
+        const unsigned* selectList = !hostConst.stableGasPrune && hostConst.domeN ? list : nullptr;
         if (hostConst.stableGasPrune) {
             // all-gas and all-liquid first; the seeds only for cells the gas does not decide
             passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 2, rec, counters, Q_A, totals);
@@ -590,8 +611,10 @@ struct HemDevice {
             passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, 2, 5, rec, counters, Q_B, totals);
             check(cudaGetLastError(), "passQueue");
         } else if (hostConst.domeN) {
-            // single-phase cells one thread each, the rest through the work queue
-            passSinglePhase<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, rec, list, counters, totals);
+            // single-phase cells one thread each (selected and written there), the
+            // rest through the work queue and the selection below
+            passSinglePhase<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, state, transport, success, list,
+                                                                fallback, counters, totals);
             check(cudaGetLastError(), "passSinglePhase");
             passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, list, 0, 7, rec, counters, Q_A, totals);
             check(cudaGetLastError(), "passQueue");
@@ -599,8 +622,8 @@ struct HemDevice {
             passQueue<<<passBlocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 7, rec, counters, Q_A, totals);
             check(cudaGetLastError(), "passQueue");
         }
-        selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, state, transport, success, fallback,
-                                                             counters);
+        selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, selectList, state, transport, success,
+                                                             fallback, counters);
         check(cudaGetLastError(), "selectCandidates");
         passRestarts<<<passBlocks, kPassThreads, 0, s>>>(cst, in, fallback, fb, capacity, counters, totals);
         check(cudaGetLastError(), "passRestarts");
@@ -1358,8 +1381,8 @@ extern "C" int reactive_gpu_hem_run_static_v3(const void* model, size_t modelByt
             passQueue<<<blocks, kPassThreads, 0, s>>>(cst, in, count, nullptr, 0, 7, rec, counters, Q_A, totals);
         }
         check(cudaGetLastError(), "passQueue");
-        selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, state, transport, success, fallback,
-                                                             counters);
+        selectCandidates<<<gridFor(count, 256), 256, 0, s>>>(cst, rec, count, nullptr, state, transport, success,
+                                                             fallback, counters);
         passRestarts<<<blocks, kPassThreads, 0, s>>>(cst, in, fallback, fb, kStaticHemCells, counters, totals);
         selectRestarts<<<gridFor(count, 256), 256, 0, s>>>(fb, kStaticHemCells, fallback, seed, state, transport,
                                                            success, counters);
