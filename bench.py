@@ -38,14 +38,14 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Mcell-steps/s at 160³, plain FP64 vs mixed/batched; adjoint/forward time"
 UNIT = "Mcell-steps/s"
-# Per-unit figures of the dominant kernel (the work-queue flash, passQueue), from
-# an ncu capture of the 40^3 impingement flash (the command is in
-# profiles/passQueue_flops_impingement40.md): FP64 FLOPs = 2 DFMA + DADD + DMUL
-# thread instructions, and DRAM read+write bytes, each per PR phase evaluation
-# (the device counter the flash reports). Both scale with phase evaluations, not
-# cells: the DRAM traffic is the solver's local-memory (stack) traffic.
-FLOPS_PER_PHASE_EVAL = 418.85
-DRAM_BYTES_PER_PHASE_EVAL = 74.8
+# Per-unit figures of the dominant kernel (the flash: its one-thread-per-cell
+# single-phase pass, with the work queue for the cells the two-phase bound keeps),
+# from an ncu capture of one recovery of the 40^3 impingement step (the command is
+# in profiles/passSinglePhase_flops_impingement40.md): FP64 FLOPs = 2 DFMA + DADD +
+# DMUL thread instructions, and DRAM read+write bytes, each per PR phase
+# evaluation (the device counter the flash reports).
+FLOPS_PER_PHASE_EVAL = 1068.7
+DRAM_BYTES_PER_PHASE_EVAL = 9.7
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
 
 
@@ -454,7 +454,8 @@ def run_ours(args, rank, world):
     if flash_ms:
         flops_per_eval = args.flops_per_phase_eval
         achieved = flops_per_eval * flash_phase_evals / (flash_ms * 1e-3) / 1e12 if flops_per_eval else None
-        roofline = {"bound": "fp64", "kernel": "HEM flash (candidate passes, one recovery of all cells)",
+        roofline = {"bound": "fp64", "kernel": "HEM flash, one recovery of all cells (passSinglePhase + passQueue "
+                                                "+ selection + restarts) on a step's stage-0 state",
                     "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                     "frac": achieved / fp64 if achieved else None,
                     "peak_source": "measured in this run (FP64 FMA-chain probe)",

@@ -781,31 +781,46 @@ __device__ __forceinline__ HllBar hllReverse(double wf, double unL, double unR, 
     return b;
 }
 
-// (dL/dq)^T w and (dL/dstate)^T w of the inviscid operator of the structured
-// box with hllReverse, gather form: the same results as cartRateVjp<NS, 0> for
-// viscosity 0, conductivity 0 and no WALE, in registers.
+// (dL/dq)^T w and (dL/dstate)^T w of the HLL operator of the structured box at
+// fixed cell gradients and eddy viscosities (the part cartRateVjp<NS, 0> forms
+// in dual numbers), gather form, in registers: the HLL flux by hllReverse; the
+// viscous traction through the velocities (the face-gradient correction's
+// target (u_R - u_L) / d and the work's u_bar) and through rho in the WALE
+// viscosity; conduction through T. With dJ/dG' = mu (a n^T + n a^T - 2/3 (a.n) I)
+// (a = -(W_m + W_E u_bar) A, projected on n at a slip wall): dJ/dt = dJ/dG' n,
+// dJ/du_bar = -W_E A tau, dJ/dmu = a . tau / mu. The gradients' and eddy
+// viscosities' own adjoints are cartViscousGradVjp's.
 template <int NS>
 __global__ void __launch_bounds__(128) cartRateVjpInviscid(CartView v, const double* __restrict__ q,
                                                            const ReactiveTransportState* __restrict__ st,
+                                                           const double* __restrict__ grad,
+                                                           const double* __restrict__ nut,
                                                            const double* __restrict__ w, double* __restrict__ qBar,
                                                            ReactiveTransportState* __restrict__ stateBar) {
+    const bool viscous = v.viscosity > 0 || v.wale;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
         loadCell<NS>(v, q, st, c, C, true);
         const double ivc = v.invV[c];
-        double dq[NS + 4], du[3] = {0, 0, 0}, dp = 0, dc = 0;
+        double dq[NS + 4], du[3] = {0, 0, 0}, dp = 0, dc = 0, dT = 0, dRhoState = 0;
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) dq[kk] = 0;
+        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (viscous) {
 #pragma unroll
+            for (int t = 0; t < 9; ++t) gC[t] = grad[size_t(t) * v.cells + c];
+        }
+        const double nutC = v.wale ? nut[c] : 0.0;
+#pragma unroll 1
         for (int n = 0; n < 12; ++n) {
             const int s = sideOf(n);
             const bool interior = hasNeighbour(v, s, i, j, k);
             if (interior != (n < 6)) continue;
             const int axis = s >> 1;
             CellData O;  // the other side
-            double Wa[NS + 4], sgn, area;
+            double Wa[NS + 4], sgn, area, wf, dist, gO[9], nutO = nutC;
             int kind = 0;
             bool cIsLeft = true;
             if (interior) {
@@ -815,6 +830,13 @@ __global__ void __launch_bounds__(128) cartRateVjpInviscid(CartView v, const dou
                 cIsLeft = s & 1;
                 sgn = 1;
                 area = v.area[axis];
+                wf = .5;
+                dist = v.dist[axis];
+                if (viscous) {
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) gO[t] = grad[size_t(t) * v.cells + nb];
+                }
+                if (v.wale) nutO = nut[nb];
 #pragma unroll
                 for (int kk = 0; kk < NS + 4; ++kk)
                     Wa[kk] = area * (cIsLeft ? w[size_t(kk) * v.cells + nb] * ivn - w[size_t(kk) * v.cells + c] * ivc
@@ -825,6 +847,10 @@ __global__ void __launch_bounds__(128) cartRateVjpInviscid(CartView v, const dou
                 boundaryRight<NS>(v, q, st, f, axis, C, O, true);
                 sgn = (s & 1) ? 1.0 : -1.0;
                 area = f.area;
+                wf = f.ownerWeight;
+                dist = f.distance;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) gO[t] = gC[t];
 #pragma unroll
                 for (int kk = 0; kk < NS + 4; ++kk) Wa[kk] = -area * w[size_t(kk) * v.cells + c] * ivc;
             }
@@ -851,6 +877,95 @@ __global__ void __launch_bounds__(128) cartRateVjpInviscid(CartView v, const dou
                 dp += b.pR;
                 dc += b.cR;
             }
+            if (!viscous && !(v.conductivity > 0 && kind != 1)) continue;
+            // viscous traction and conduction at fixed gradients and eddy viscosities
+            double duL[3] = {0, 0, 0}, duR[3] = {0, 0, 0}, dTL = 0, dTR = 0, dRL = 0, dRR = 0;
+            double nv[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) nv[d] = d == axis ? sgn : 0.0;
+            if (viscous) {
+                const double* gL = cIsLeft ? gC : gO;
+                const double* gR = cIsLeft ? gO : gC;
+                const double nutL = cIsLeft ? nutC : nutO, nutR = cIsLeft ? nutO : nutC;
+                const double kd = (kind == 1 ? 2 : 1) * dist;
+                double g[9];
+#pragma unroll
+                for (int t = 0; t < 9; ++t) g[t] = interior ? wf * gL[t] + (1 - wf) * gR[t] : gL[t];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    double normal = 0;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) normal += g[a * 3 + d] * nv[d];
+                    const double target = (R.u[a] - L.u[a]) / kd;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) g[a * 3 + d] += nv[d] * (target - normal);
+                }
+                const double div = g[0] + g[4] + g[8];
+                const double mu = v.viscosity + (v.wale ? wf * L.rho * nutL + (1 - wf) * R.rho * nutR : 0.0);
+                double tau[3], tn = 0, av[3], an = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    double t = -2.0 / 3.0 * div * nv[a];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) t += (g[a * 3 + d] + g[d * 3 + a]) * nv[d];
+                    tau[a] = mu * t;
+                    tn += tau[a] * nv[a];
+                    av[a] = -(Wa[NS + a] + Wa[NS + 3] * (wf * L.u[a] + (1 - wf) * R.u[a]));
+                    an += av[a] * nv[a];
+                }
+                if (kind == 1) {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) { tau[a] = tn * nv[a]; av[a] = an * nv[a]; }
+                }
+                an = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) an += av[a] * nv[a];
+                double jmu = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    // dJ/dt_a = (dJ/dG' n)_a; dJ/du_bar_a = -W_E A tau_a
+                    double rn = 0;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        rn += mu * (av[a] * nv[d] + nv[a] * av[d] - (a == d ? 2.0 / 3.0 * an : 0.0)) * nv[d];
+                    const double dbar = -Wa[NS + 3] * tau[a];
+                    duL[a] = wf * dbar - rn / kd;
+                    duR[a] = (1 - wf) * dbar + rn / kd;
+                    double t = -2.0 / 3.0 * div * nv[a];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) t += (g[a * 3 + d] + g[d * 3 + a]) * nv[d];
+                    jmu += av[a] * t;
+                }
+                if (v.wale) {
+                    dRL = jmu * wf * nutL;
+                    dRR = jmu * (1 - wf) * nutR;
+                }
+            }
+            if (v.conductivity > 0 && kind != 1) {
+                dTL = Wa[NS + 3] * v.conductivity / dist;
+                dTR = -dTL;
+            }
+            if (interior) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) du[a] += cIsLeft ? duL[a] : duR[a];
+                dT += cIsLeft ? dTL : dTR;
+                dRhoState += cIsLeft ? dRL : dRR;
+            } else {
+                // the owner, and the ghost made from it (extrapolate: itself; slip: mirrored velocity)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) du[a] += duL[a];
+                dT += dTL;
+                dRhoState += dRL;
+                if (kind == 1 || kind == 2) {
+                    double rn = 0;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) rn += duR[a] * nv[a];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) du[a] += kind == 1 ? duR[a] - 2 * rn * nv[a] : duR[a];
+                    dT += dTR;
+                    dRhoState += dRR;
+                }
+            }
         }
         // u = m / rho with rho the sum of the species masses
         double rho = 0;
@@ -866,7 +981,145 @@ __global__ void __launch_bounds__(128) cartRateVjpInviscid(CartView v, const dou
         for (int kk = 0; kk < NS; ++kk) dq[kk] += dRho;
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) qBar[size_t(kk) * v.cells + c] = dq[kk];
-        stateBar[c] = ReactiveTransportState{dp, 0.0, 0.0, 0.0, dc, 0.0, 0.0};
+        stateBar[c] = ReactiveTransportState{dp, dT, dRhoState, 0.0, dc, 0.0, 0.0};
+    }
+}
+
+// Closed-form adjoint of the viscous/WALE traction with respect to the cells'
+// velocity gradients and eddy viscosities (the part cartRateVjp<NS, 1> forms in
+// dual numbers). The traction is bilinear in (mu, face gradient): with the
+// corrected face gradient G' = G (I - n n^T) + t n^T, tau = mu (G' n + G'^T n -
+// 2/3 tr(G') n) (projected on n at a slip wall), and J = a . tau for
+// a = -A (W_m + W_E u_bar) (a -> (a.n) n at a slip wall), so
+// dJ/dG' = mu (a n^T + n a^T - 2/3 (a.n) I), dJ/dG = dJ/dG' (I - n n^T) and
+// dJ/dmu = J / mu; G = w G_L + (1 - w) G_R (the owner's on a boundary face) and
+// mu = mu_0 + w rho_L nu_L + (1 - w) rho_R nu_R. Gather form per cell over its
+// faces in the forward's order.
+template <int NS>
+__global__ void __launch_bounds__(128) cartViscousGradVjp(CartView v, const double* __restrict__ q,
+                                                          const ReactiveTransportState* __restrict__ st,
+                                                          const double* __restrict__ grad,
+                                                          const double* __restrict__ nut,
+                                                          const double* __restrict__ w, double* __restrict__ gBar,
+                                                          double* __restrict__ nutBar) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        CellData C;
+        loadCell<NS>(v, q, st, c, C, false);
+        double gC[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) gC[t] = grad[size_t(t) * v.cells + c];
+        const double nutC = v.wale ? nut[c] : 0.0;
+        const double ivc = v.invV[c];
+        double gb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, nb = 0;
+#pragma unroll 1
+        for (int n = 0; n < 12; ++n) {
+            const int s = sideOf(n);
+            const bool interior = hasNeighbour(v, s, i, j, k);
+            if (interior != (n < 6)) continue;
+            const int axis = s >> 1;
+            CellData O;
+            double gO[9], nutO, W[4], sgn, wf, dist, area, weightC, dmu;
+            int kind = 0;
+            bool cLeft = true;
+            if (interior) {
+                const size_t nbr = neighbourOf(v, s, c);
+                loadCell<NS>(v, q, st, nbr, O, false);
+#pragma unroll
+                for (int t = 0; t < 9; ++t) gO[t] = grad[size_t(t) * v.cells + nbr];
+                nutO = v.wale ? nut[nbr] : 0.0;
+                cLeft = s & 1;
+                sgn = 1;
+                wf = .5;
+                dist = v.dist[axis];
+                area = v.area[axis];
+                const double ivn = v.invV[nbr];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const size_t kk = size_t(NS + t);
+                    W[t] = cLeft ? w[kk * v.cells + nbr] * ivn - w[kk * v.cells + c] * ivc
+                                 : w[kk * v.cells + c] * ivc - w[kk * v.cells + nbr] * ivn;
+                }
+                weightC = cLeft ? wf : 1 - wf;
+            } else {
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                boundaryRight<NS>(v, q, st, f, axis, C, O, false);
+#pragma unroll
+                for (int t = 0; t < 9; ++t) gO[t] = gC[t];
+                nutO = nutC;
+                kind = f.kind;
+                sgn = (s & 1) ? 1.0 : -1.0;
+                wf = f.ownerWeight;
+                dist = f.distance;
+                area = f.area;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) W[t] = -w[size_t(NS + t) * v.cells + c] * ivc;
+                weightC = 1;
+            }
+            const CellData& L = cLeft ? C : O;
+            const CellData& R = cLeft ? O : C;
+            const double* gL = cLeft ? gC : gO;
+            const double* gR = cLeft ? gO : gC;
+            const double nutL = cLeft ? nutC : nutO, nutR = cLeft ? nutO : nutC;
+            dmu = interior ? (cLeft ? wf * L.rho : (1 - wf) * R.rho) : wf * L.rho + (1 - wf) * R.rho;
+            double nv[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) nv[d] = d == axis ? sgn : 0.0;
+            // the forward's corrected face gradient and viscosity
+            double g[9];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) g[t] = interior ? wf * gL[t] + (1 - wf) * gR[t] : gL[t];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                double normal = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) normal += g[a * 3 + d] * nv[d];
+                const double target = (R.u[a] - L.u[a]) / ((kind == 1 ? 2 : 1) * dist);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) g[a * 3 + d] += nv[d] * (target - normal);
+            }
+            const double div = g[0] + g[4] + g[8];
+            const double mu = v.viscosity + (v.wale ? wf * L.rho * nutL + (1 - wf) * R.rho * nutR : 0.0);
+            double av[3], an = 0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                av[a] = -area * (W[a] + W[3] * (wf * L.u[a] + (1 - wf) * R.u[a]));
+                an += av[a] * nv[a];
+            }
+            if (kind == 1)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) av[a] = an * nv[a];
+            an = 0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) an += av[a] * nv[a];
+            // dJ/dG' then the correction's transpose
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                double row[3], rn = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    row[d] = mu * (av[a] * nv[d] + nv[a] * av[d] - (a == d ? 2.0 / 3.0 * an : 0.0));
+                    rn += row[d] * nv[d];
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) gb[a * 3 + d] += weightC * (row[d] - rn * nv[d]);
+            }
+            if (v.wale) {
+                double jmu = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    double t = -2.0 / 3.0 * div * nv[a];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) t += (g[a * 3 + d] + g[d * 3 + a]) * nv[d];
+                    jmu += av[a] * t;
+                }
+                nb += jmu * dmu;
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 9; ++t) gBar[size_t(t) * v.cells + c] = gb[t];
+        if (nutBar) nutBar[c] = nb;
     }
 }
 

@@ -582,15 +582,15 @@ struct Transport {
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
                         const double* nut, const double* w, double* qBar, ReactiveTransportState* stateBar,
                         double* gBar, double* nutBar, bool viscous, cudaStream_t s) {
-            if (!viscous && b.conductivity == 0 && b.scheme == 0) {
-                cartRateVjpInviscid<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, w, qBar, stateBar);
-                return;
-            }
-            cartRateVjp<NS, 0><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, qBar, stateBar, nullptr,
-                                                                    nullptr);
+            // the state-side derivatives: HLL by hand (with the viscous and conduction
+            // terms at fixed gradients), HLLC in dual numbers
+            if (b.scheme == 0)
+                cartRateVjpInviscid<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, qBar, stateBar);
+            else
+                cartRateVjp<NS, 0><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, qBar, stateBar,
+                                                                        nullptr, nullptr);
             if (!viscous) return;
-            cartRateVjp<NS, 1><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, nullptr, nullptr, gBar,
-                                                                    nutBar);
+            cartViscousGradVjp<NS><<<gridFor(b.cells, 128), 128, 0, s>>>(b, q, st, grad, nut, w, gBar, nutBar);
             if (b.wale) cartWaleVjp<<<gridFor(b.cells, 128), 128, 0, s>>>(b, grad, nutBar, gBar);
             cartGradientVjp<NS><<<gridFor(b.cells, 256), 256, 0, s>>>(b, q, gBar, qBar);
         }
