@@ -175,7 +175,10 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
         }
         if (pending) {
             if (L.req == REQ_POINT) L.ok = evaluate(C, L.x.q, L.rm, L.rp, L.rT, L.rv, v, n);
-            else if (L.req == REQ_PROBE) L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, n);
+            else if (L.req == REQ_PROBE) {
+                GasPoint g;
+                L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, g, n);
+            }
             else L.ok = tangentStable(C, L.rp, L.rT, n);
             L.req = REQ_NONE;
             pending = false;
@@ -225,12 +228,14 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSingle
                     const double mass = kind ? x.q : 0.0;
                     Eval v;
                     CandidateOut o{};
+                    GasPoint g;
+                    bool known = false;
                     const bool floor = kind == 1 && x.q * (1 + 1e-12) < C.liquidFloor;
-                    if (floor || !frozenSolve(C, x, mass, 0, v, o, n)) {
+                    if (floor || !frozenSolve(C, x, mass, 0, v, o, n, &g, &known)) {
                         ++n.failures;
                         continue;
                     }
-                    const bool stable = stableAt(C, x.q, v.liqMass, v.p, v.T, n);
+                    const bool stable = stableAt(C, x.q, v.liqMass, v.p, v.T, n, known ? &g : nullptr);
                     if (!stable) {
                         ++n.failures;
                         continue;

@@ -147,13 +147,25 @@ __device__ __forceinline__ int liquidFromShared(const HemConst& C, int shared, c
     return rootProps(C.liq, t, r, p, ROOT_LIQUID, chem, o);
 }
 
+// The gas table's T-terms, cubic roots and gas-root properties (without the
+// chemical potential) at one (p, T), each with status EOS_OK: what a gas probe
+// computed, handed to the evaluations that follow at the same point.
+struct GasPoint {
+    TTerms t;
+    Roots r;
+    PhaseProps gas;
+};
+
 // Phase sums at (p, T) for liquid mass `mass` out of total density q. With
 // `virt` the liquid is also evaluated when absent and both chemical potentials
 // are formed (two-phase residual and stability test). When both branches are
 // needed and the tables hold one species, the T-terms and the cubic are formed
 // once for both roots (the same arithmetic as two separate evaluations).
+// `known` (optional) holds the gas table's terms at exactly (p, T): they replace
+// the T-terms and the cubic of the shared path and, without `virt`, the gas
+// root's properties (the same values those calls return).
 __device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass, double p, double T, bool virt, Eval& v,
-                                Counts& n) {
+                                Counts& n, const GasPoint* known = nullptr) {
     v.p = p; v.T = T;
     v.volume = v.energy = v.entropyD = v.Vp = v.VT = v.Ep = v.ET = v.cpD = 0;
     v.muG = v.muL = 0;
@@ -173,13 +185,18 @@ __device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass
     TTerms t;
     Roots r;
     int sharedStatus = EOS_OK;
-    if (shared) {
+    if (shared && known) {
+        t = known->t;
+        r = known->r;
+    } else if (shared) {
         sharedStatus = tTerms(C.gas, T, t);
         if (sharedStatus == EOS_OK) sharedStatus = cubicRoots(C.gas, T, p, t.aa, r);
     }
     PhaseProps ph;
     if (gas > 0) {
-        const int st = shared ? gasFromShared(C, sharedStatus, t, r, p, virt, ph, n) : gasPhase(C, p, T, virt, ph, n);
+        int st = EOS_OK;
+        if (known && !virt) ph = known->gas;
+        else st = shared ? gasFromShared(C, sharedStatus, t, r, p, virt, ph, n) : gasPhase(C, p, T, virt, ph, n);
         if (st != EOS_OK) return false;
         addPhase(v, gas, ph, p);
         v.gRho = ph.rho; v.gE = ph.e; v.gV = ph.V; v.gH = ph.h;
@@ -275,16 +292,24 @@ __device__ RB200_FLASH_FN bool solveSmall(double a[3][3], double b[3], int n, do
     return true;
 }
 
-// Energy residual of the all-gas state at (T, rho) and the gas-root check.
+// Energy residual of the all-gas state at (T, rho) and the gas-root check: the
+// properties at (T, rho), then the gas root of the cubic at the resulting
+// pressure must be that density. One set of T-terms serves both (the same
+// values prTrho and gasPhase would each form); `g` receives them with the
+// roots and the gas root's properties at (p, T).
 __device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn, double T, double& F, double& cv, double& p,
-                                double& cp, Counts& n) {
-    PhaseProps prop, gas;
+                                double& cp, GasPoint& g, Counts& n) {
+    PhaseProps prop;
     int phase;
     ++n.phases;
-    if (prTrho(C.gas, T, q, false, prop, phase) != EOS_OK) return false;
-    p = prop.p;
+    if (!fin(T) || !fin(q) || T <= 0 || q <= 0) return false;
+    if (tTerms(C.gas, T, g.t) != EOS_OK || prTrhoT(C.gas, g.t, q, false, prop, phase) != EOS_OK) return false;
+    p = prop.p;  // finite and positive
     if (!inBounds(C, p, T)) return false;
-    if (gasPhase(C, prop.p, T, false, gas, n) != EOS_OK || fabs(gas.rho - q) > 1e-8 * q) return false;
+    ++n.phases;
+    if (C.enforceBounds && (T < C.gasTmin || T > C.gasTmax)) return false;
+    if (cubicRoots(C.gas, T, p, g.t.aa, g.r) != EOS_OK) return false;
+    if (rootProps(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas) != EOS_OK || fabs(g.gas.rho - q) > 1e-8 * q) return false;
     F = q * prop.e - eIn;
     cv = q * prop.cv;
     cp = prop.cp;
@@ -296,10 +321,14 @@ struct CandidateOut {
     int iterations;
 };
 
-__device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, Counts& n) {
+// Scalar T-Newton of the all-gas partition at fixed rho. `g` ends with the gas
+// table's terms at the converged (p, T), where the last probe left them.
+__device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, GasPoint& g,
+                                 Counts& n) {
     const double q = in.q;
     double T = clampd(in.gT, C.Tmin, C.Tmax), F, cv, p, cp;
-    if (!gasProbe(C, q, in.e, T, F, cv, p, cp, n)) return false;
+    GasPoint bracket;  // probes that only bracket the root
+    if (!gasProbe(C, q, in.e, T, F, cv, p, cp, g, n)) return false;
     const double scale = fmax(1e5 * q, q * cp * T);
     double lower = T, upper = T, fl = F, fh = F;
     if (fabs(F) > C.etol * scale) {
@@ -310,7 +339,7 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmax(C.Tmin, T - radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, n)) { fl = val; lower = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, bracket, n)) { fl = val; lower = cand; found = true; }
                     else cand = .5 * (lower + cand);
                 }
                 if (!found) return false;
@@ -319,13 +348,13 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmin(C.Tmax, T + radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, n)) { fh = val; upper = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, bracket, n)) { fh = val; upper = cand; found = true; }
                     else cand = .5 * (upper + cand);
                 }
                 if (!found) return false;
             }
-            if (fabs(fl) <= C.etol * scale) { T = lower; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, n)) return false; break; }
-            if (fabs(fh) <= C.etol * scale) { T = upper; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, n)) return false; break; }
+            if (fabs(fl) <= C.etol * scale) { T = lower; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false; break; }
+            if (fabs(fh) <= C.etol * scale) { T = upper; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false; break; }
             if (lower == C.Tmin && upper == C.Tmax) break;
         }
         if (!(fabs(F) <= C.etol * scale || (fl <= 0 && fh >= 0 && upper > lower))) return false;
@@ -336,10 +365,10 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
         const double next = T - F / cv;
         T = fin(next) && next > lower && next < upper ? next : .5 * (lower + upper);
         double d3;
-        if (!gasProbe(C, q, in.e, T, F, cv, p, d3, n)) return false;
+        if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false;
     }
     if (fabs(F) > C.etol * scale) return false;
-    if (!evaluate(C, q, 0.0, p, T, false, v, n)) return false;
+    if (!evaluate(C, q, 0.0, p, T, false, v, n, &g)) return false;
     o.vres = fabs(v.volume - 1);
     o.eres = fabs(v.energy - in.e) / energyScale(v, q);
     o.cres = 0;
@@ -348,11 +377,21 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
     return o.vres <= C.vtol && o.eres <= C.etol;
 }
 
-// Newton on (ln p, ln T) with the liquid partition held fixed.
+// Newton on (ln p, ln T) with the liquid partition held fixed. With `known`,
+// a converged scalar all-gas solve leaves the gas table's terms at its (p, T)
+// there and sets *haveKnown.
 __device__ RB200_FLASH_FN bool frozenSolve(const HemConst& C, const CellInput& in, double mass, int stallLimit, Eval& v,
-                                   CandidateOut& o, Counts& n) {
+                                   CandidateOut& o, Counts& n, GasPoint* known = nullptr, bool* haveKnown = nullptr) {
+    if (haveKnown) *haveKnown = false;
     if (!fin(in.e)) return false;
-    if (C.scalarRecovery && mass == 0 && scalarGas(C, in, v, o, n)) return true;
+    if (C.scalarRecovery && mass == 0) {
+        GasPoint local;
+        GasPoint& g = known ? *known : local;
+        if (scalarGas(C, in, v, o, g, n)) {
+            if (haveKnown) *haveKnown = true;
+            return true;
+        }
+    }
     double p = clampd(in.gp, C.pmin, C.pmax), T = clampd(in.gT, C.Tmin, C.Tmax);
     if (!evaluate(C, in.q, mass, p, T, false, v, n)) return false;
     int stalled = 0;
@@ -495,11 +534,13 @@ __device__ RB200_FLASH_FN bool twoPhaseSolve(const HemConst& C, const CellInput&
     return false;
 }
 
-// Stability of a converged candidate at (p, T) with liquid mass `mass`.
-__device__ RB200_FLASH_FN bool stableAt(const HemConst& C, double q, double mass, double p, double T, Counts& n) {
+// Stability of a converged candidate at (p, T) with liquid mass `mass`
+// (`known`: the gas table's terms at exactly (p, T), if the caller has them).
+__device__ RB200_FLASH_FN bool stableAt(const HemConst& C, double q, double mass, double p, double T, Counts& n,
+                                const GasPoint* known = nullptr) {
     if (q - mass > 0) {
         Eval cmp;
-        if (!evaluate(C, q, mass, p, T, true, cmp, n)) return false;
+        if (!evaluate(C, q, mass, p, T, true, cmp, n, known)) return false;
         const double affinity = cmp.muL - cmp.muG;
         if (mass > 0) return fin(affinity) && fabs(affinity) <= C.mutol * 2;
         return !(affinity < -C.mutol);
