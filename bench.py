@@ -312,6 +312,59 @@ class HostPath:
         self.lib.reactive_transport_destroy(self.t)
 
 
+def run_slab(args, rank, world):
+    """The 160^3 case decomposed into z-slabs over the ranks (strong scaling):
+    each rank steps its own layers plus two halo layers (mixed precision,
+    each half step a captured graph), with the halo exchange over NCCL after
+    each recovery; the CFL minimum over ranks is checked after the run. One
+    rank runs the undivided box through the same code."""
+    import torch
+    load_package()
+    from spuma_multiphysics_b200 import cases
+    from spuma_multiphysics_b200.slab import SlabFlow, global_cfl
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    n = args.size
+    init = cases.impingement(n, seed=2026)
+    slab = SlabFlow(n, rank, world, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
+                    precision="mixed", viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
+    f = slab.flow
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        slab.step(DT)
+    barrier()
+    sampler = ClockSampler(torch.cuda.current_device())
+    with sampler:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(f.stream)
+        for _ in range(args.steps):
+            slab.step(DT)
+        b.record(f.stream)
+        barrier()
+    ms = max_over_ranks(a.elapsed_time(b) / args.steps, world, "cuda")
+    cfl = global_cfl(slab, world)
+    failed = int((f.success[f.own[0]:f.own[1]] == 0).sum().item())
+    failed = int(max_over_ranks(float(failed), world, "cuda"))
+    if failed or not DT <= cfl * (1 + 1e-10):
+        raise RuntimeError(f"slab step failed: {failed} failed recoveries, CFL step {cfl}")
+    L = slab.layout
+    line = {"metric": METRIC, "value": n ** 3 / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64 state, f32 flux", "data": "synthetic",
+            "config": {**workload(n), "parallelism": f"z-slabs x{world} (own layers + 2 halo layers, "
+                                                     f"NCCL halo exchange after each recovery)",
+                       "own_layers_rank0": L.z1 - L.z0},
+            "e2e": None, "roofline": None, "cpu_baseline": None, "clocks": sampler.summary(),
+            "gpu_launches": None}
+    slab.close()
+    return line
+
+
 def run_ours(args, rank, world):
     import torch
     pkg = load_package()
@@ -824,6 +877,8 @@ def main():
                    help="run the ideal-gas blast box adjoint check on this cube size")
     p.add_argument("--adjoint-steps", type=int, default=50)
     p.add_argument("--skip-adjoint", action="store_true")
+    p.add_argument("--decompose", choices=("replicas", "slab"), default="replicas",
+                   help="N > 1: independent replicas (weak scaling) or the case split into z-slabs (strong scaling)")
     args = p.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -841,7 +896,12 @@ def main():
         elif args.adjoint_check:
             line = run_adjoint_check(args)
         else:
-            line = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+            if args.impl == "reference":
+                line = run_reference(args, rank, world)
+            elif args.decompose == "slab":
+                line = run_slab(args, rank, world)
+            else:
+                line = run_ours(args, rank, world)
     finally:
         if world > 1 and args.impl == "ours":
             import torch.distributed as dist

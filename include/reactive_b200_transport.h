@@ -162,6 +162,16 @@ int reactive_transport_flux_v3(void* transport, int request, int* active);
  * structured path; selecting the face graph returns to FP64. *active (may be
  * NULL) receives 1 for mixed. */
 int reactive_transport_precision_v3(void* transport, int request, int* active);
+/* Own cells of this handle (no reference counterpart; the reference runs one
+ * domain): a z-slab of a larger box holds its own cells [begin, end) and halo
+ * layers that a neighbour owns. The stage entries then update the own cells
+ * only (the halo cells' outputs are left as they were, for the halo exchange
+ * to overwrite), the CFL minimum covers the own cells only, and the boundary
+ * ledger sums the boundary faces of own cells only. Gradients, eddy
+ * viscosities and face fluxes still read every cell, so an own cell next to a
+ * halo sees the same neighbours as in the undivided box. Default: every cell.
+ * Requires begin < end <= cells. */
+int reactive_transport_owned_cells_v3(void* transport, uint64_t begin, uint64_t end);
 /* Vector-Jacobian product of the rate operator of the device stage entries (no
  * reference counterpart; the reference has no adjoint). With rate(q, state) the
  * per-cell right-hand side L that stage_device_v3 applies (q SoA with the fixed

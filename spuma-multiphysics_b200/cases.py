@@ -151,6 +151,13 @@ def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset
     belongs to a port when its centre lies inside the port circle
     (tools/impinging_cartesian_mesh.py:12-36,89-99).
     """
+    kinds = cartesian_side_kinds(n, edge, port_diameter, port_z, port_offset, boundary_kind)
+    return box_faces((n, n, n), edge / n, kinds)
+
+
+def cartesian_side_kinds(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset=0.006, boundary_kind=2):
+    """The six boundary sides' kinds of cartesian_faces, each an array in that
+    side's lateral order (fast, slow) = (y, z), (x, z), (x, y)."""
     h = edge / n
     r2 = (port_diameter / 2) ** 2
     kinds = []
@@ -163,7 +170,7 @@ def cartesian_faces(n, edge=0.08, port_diameter=0.005, port_z=0.040, port_offset
             zc = (slow.ravel() + .5) * h
             kind[(lateral_c - port_offset) ** 2 + (zc - port_z) ** 2 < r2] = 3
         kinds.append(kind)
-    return box_faces((n, n, n), h, kinds)
+    return kinds
 
 
 def impingement(n, fluid=None, seed=1234, ambient_p=40e5, ambient_T=293.15, inlet_p=56.01325e5, inlet_T=293.15,

@@ -46,6 +46,10 @@ struct CartView {
     double pr, sc;
     const double* mixCp;
     const double* spH;
+    // cells [ownBegin, ownEnd) are this handle's own: the stage update, the CFL
+    // minimum and the boundary ledger cover them only (a z-slab's halo layers
+    // are read as neighbours, and written by the halo exchange)
+    size_t ownBegin, ownEnd;
 };
 
 struct CellData {
@@ -436,6 +440,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
     constexpr bool fp64 = sizeof(R) == sizeof(double);
     const bool viscous = v.viscosity > 0 || v.wale;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        if (c < v.ownBegin || c >= v.ownEnd) continue;
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
@@ -513,8 +518,11 @@ __global__ void __launch_bounds__(256) cartSteps(CartView v, const ReactiveTrans
                                                  const R* __restrict__ nut, double cfl, double maximumStep,
                                                  double* partial) {
     __shared__ double warpValues[32];
-    double m = HUGE_VAL;
+    // every cell's step is at most maximumStep, so starting there changes no
+    // minimum and leaves a block without own cells a valid (positive) partial
+    double m = maximumStep;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        if (c < v.ownBegin || c >= v.ownEnd) continue;
         int i, j, k;
         cellCoords(v, c, i, j, k);
         CellData C;
@@ -580,6 +588,7 @@ __global__ void __launch_bounds__(256) cartLedger(CartView v, const double* __re
          b += size_t(blockDim.x) * gridDim.x) {
         const ReactiveTransportFace f = v.face[v.boundaryBase + b];
         const size_t c = size_t(f.owner);
+        if (c < v.ownBegin || c >= v.ownEnd) continue;
         const int axis = f.normal[0] != 0 ? 0 : (f.normal[1] != 0 ? 1 : 2);
         const double sgn = f.normal[axis] > 0 ? 1.0 : -1.0;
         CellData C, Rt;

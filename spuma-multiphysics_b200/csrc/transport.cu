@@ -468,9 +468,18 @@ struct Transport {
         box.viscosity = cfg.viscosity; box.conductivity = cfg.conductivity; box.waveFactor = cfg.waveFactor;
         return true;
     }
+    // Own cells [begin, end) (reactive_transport_owned_cells_v3): the stage
+    // update, the CFL minimum and the boundary ledger cover them only.
+    void setOwned(size_t begin, size_t end) {
+        require(begin < end && end <= cfg.cells, "Owned cell range must be non-empty and within the cells");
+        v.ownBegin = begin;
+        v.ownEnd = end;
+    }
     int fluxScheme = 0;  // structured path: 0 HLL, 1 HLLC
     CartView boxView() const {
         CartView b = box;
+        b.ownBegin = v.ownBegin;
+        b.ownEnd = v.ownEnd;
         b.wale = v.wale;
         b.cw = v.cw;
         b.scheme = fluxScheme;

@@ -30,6 +30,7 @@ enum FaceWorkField {
 
 struct GraphView {
     size_t cells = 0, fixed = 0, all = 0, ns = 0, nv = 0, faces = 0, nBoundary = 0;
+    size_t ownBegin = 0, ownEnd = SIZE_MAX;  // own cells: stage update, CFL minimum and ledger
     int mechanical = 0;
     double viscosity = 0, conductivity = 0, diffusivity = 0, waveFactor = 1;
     const ReactiveTransportFace* face = nullptr;
@@ -350,6 +351,7 @@ template <int CHUNK>
 __global__ void cellRates(GraphView v, double* out, size_t outStride, int mode, double dt) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells;
          c += size_t(blockDim.x) * gridDim.x) {
+        if (c < v.ownBegin || c >= v.ownEnd) continue;
         const double iv = v.invV[c];
         const int64_t begin = v.row[c], end = v.row[c + 1];
         double div = 0;
@@ -401,6 +403,7 @@ __global__ void cellRates(GraphView v, double* out, size_t outStride, int mode, 
 __global__ void cellSteps(GraphView v, double cfl, double maximumStep) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells;
          c += size_t(blockDim.x) * gridDim.x) {
+        if (c < v.ownBegin || c >= v.ownEnd) { v.step[c] = maximumStep; continue; }  // not this handle's cell
         double denominator = 0;
         bool bad = false;
         for (int64_t j = v.row[c]; j < v.row[c + 1]; ++j) {
@@ -445,6 +448,7 @@ __global__ void boundaryLedger(GraphView v, double* rate) {
     for (size_t j = threadIdx.x; j < v.nBoundary; j += blockDim.x) {
         const size_t fi = size_t(v.boundary[j]);
         const ReactiveTransportFace f = v.face[fi];
+        if (size_t(f.owner) < v.ownBegin || size_t(f.owner) >= v.ownEnd) continue;
         double wk[FW_FIELDS];
         for (int t = 0; t < FW_FIELDS; ++t) wk[t] = v.work[size_t(t) * v.faces + fi];
         const size_t r = rightCell(v, f);

@@ -57,7 +57,7 @@ def _check(lib, handle, rc):
 class Flow:
     def __init__(self, faces, volume, q0, guess0, fixed_q, fixed_guess, viscosity=0.0, conductivity=0.0,
                  wale_cw=None, wave_factor=1.1, model=None, cfl=0.5, device="cuda", precision="fp64",
-                 turbulent_prandtl=None, turbulent_schmidt=None, flux="hll"):
+                 turbulent_prandtl=None, turbulent_schmidt=None, flux="hll", owned=None):
         """faces: FACE_DTYPE array; q0: cell-major (cells, 5) conserved state;
         guess0/fixed_guess: THERMO_DTYPE seeds used for the initial recovery.
         precision: "fp64", or "mixed" (FP32 gradients, WALE and face fluxes with
@@ -65,7 +65,9 @@ class Flow:
         turbulent_prandtl / turbulent_schmidt: the WALE scalar closure (needs
         wale_cw; 0 disables a term), fed each stage with the mixture cp of that
         stage's equilibrium states. flux: "hll", or "hllc" (the contact-preserving
-        flux; needs a structured box)."""
+        flux; needs a structured box). owned: (begin, end), the cells this flow
+        updates, recovers and counts in its CFL minimum and ledger (a z-slab's
+        own cells; the others are halo cells that a halo exchange fills)."""
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"unknown precision {precision!r}")
         if flux not in ("hll", "hllc"):
@@ -119,6 +121,10 @@ class Flow:
         self.flux = flux
         if flux == "hllc":
             _check(self.lib, self.transport, self.lib.reactive_transport_flux_v3(self.transport, 1, None))
+        self.own = (0, self.cells) if owned is None else (int(owned[0]), int(owned[1]))
+        if owned is not None:
+            _check(self.lib, self.transport,
+                   self.lib.reactive_transport_owned_cells_v3(self.transport, self.own[0], self.own[1]))
         all_ = self.cells + self.fixed
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)
@@ -164,25 +170,32 @@ class Flow:
         _check(lib, t, lib.reactive_transport_wale_scalar_fields_device_v3(
             t, thermo.data_ptr() + self._CP_OFFSET, None, fixed_cp, None, self._THERMO_DOUBLES, 1, s))
 
-    def _launch_step(self, dt, per_cell=False):
+    def _flash(self, q, out, per_cell=False):
+        """Recovery of the own cells of q (SoA, stride cells+fixed) seeded by the
+        step-start states, into `out` and the transport states."""
+        b, e = self.own
+        size = A.THERMO_DTYPE.itemsize
+        self.hem.run_device(q.data_ptr() + 8 * b, self.qn.shape[1], e - b, self.nv, self.sn.data_ptr() + size * b,
+                            out.data_ptr() + size * b, self.tr.data_ptr() + 56 * b, self.success.data_ptr() + 4 * b,
+                            self.stream.cuda_stream, per_cell)
+
+    def _launch_half(self, dt, stage, per_cell=False):
+        """Stage 0 (CFL query, q1 = qn + dt L(qn), recovery of q1 into s1) or
+        stage 1 (CFL recheck at q1, q_{n+1} into qn, recovery in place)."""
         lib, t, s = self.lib, self.transport, self.stream.cuda_stream
+        q_in, q_out, seed_out = (self.qn, self.q1, self.s1) if stage == 0 else (self.q1, self.qn, self.sn)
         if self.scalars:
-            self._scalar_fields(self.sn)
-        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.qn.data_ptr(), self.tr.data_ptr(),
-                                                                    self.cfl, dt, self.dt_cfl.data_ptr(), s))
-        _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.qn.data_ptr(), self.q1.data_ptr(),
-                                                              self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(), s))
-        self.hem.run_device(self.q1, self.qn.shape[1], self.cells, self.nv, self.sn, self.s1, self.tr, self.success, s,
-                            per_cell)
-        if self.scalars:
-            self._scalar_fields(self.s1)
-        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.q1.data_ptr(), self.tr.data_ptr(),
-                                                                    self.cfl, dt, self.dt_cfl[1:].data_ptr(), s))
-        _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.q1.data_ptr(), self.qn.data_ptr(),
-                                                              self.tr.data_ptr(), dt, 1, self.boundary[1].data_ptr(), s))
-        # second recovery, seeded by the step-start states, results in place
-        self.hem.run_device(self.qn, self.qn.shape[1], self.cells, self.nv, self.sn, self.sn, self.tr, self.success, s,
-                            per_cell)
+            self._scalar_fields(self.sn if stage == 0 else self.s1)
+        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, q_in.data_ptr(), self.tr.data_ptr(), self.cfl,
+                                                                    dt, self.dt_cfl[stage:].data_ptr(), s))
+        _check(lib, t, lib.reactive_transport_stage_device_v3(t, q_in.data_ptr(), q_out.data_ptr(), self.tr.data_ptr(),
+                                                              dt, stage, self.boundary[stage].data_ptr(), s))
+        # both recoveries are seeded by the step-start states; the second one in place
+        self._flash(q_out, seed_out, per_cell)
+
+    def _launch_step(self, dt, per_cell=False):
+        self._launch_half(dt, 0, per_cell)
+        self._launch_half(dt, 1, per_cell)
 
     def two_phase_bound(self, on=None):
         """Query (on=None) or set the flash's two-phase admissibility bound
@@ -259,7 +272,7 @@ class Flow:
         status = C.c_uint()
         _check(self.lib, self.transport,
                self.lib.reactive_transport_status_v3(self.transport, C.byref(status), 1, self.stream.cuda_stream))
-        failed = int((self.success == 0).sum().item())
+        failed = int((self.success[self.own[0]:self.own[1]] == 0).sum().item())
         cfl = self.dt_cfl.min().item()
         if status.value & 1:
             raise FlowError("WALE gradient/viscosity/traction became non-finite")
