@@ -221,7 +221,6 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSingle
             const CellInput x = in[c];
             if (!x.noTwoPhase) queue = true;
             else {
-                ReactiveThermoState best;
                 double bestEntropy = 0;
                 bool have = false;
                 for (int kind = 0; kind < 2; ++kind) {
@@ -231,7 +230,7 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSingle
                     GasPoint g;
                     bool known = false;
                     const bool floor = kind == 1 && x.q * (1 + 1e-12) < C.liquidFloor;
-                    if (floor || !frozenSolve(C, x, mass, 0, v, o, n, &g, &known)) {
+                    if (floor || !frozenSolve(C, x, mass, 0, v, o, n, g, known)) {
                         ++n.failures;
                         continue;
                     }
@@ -242,15 +241,18 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSingle
                     }
                     ++n.stable;
                     if (!have || v.entropyD > bestEntropy) {
+                        // the best so far goes straight to the outputs (a later, better
+                        // candidate overwrites it); a cell with none keeps its state
                         have = true;
                         bestEntropy = v.entropyD;
-                        stateFromEval(v, x.q, o, best);
+                        ReactiveThermoState st;
+                        stateFromEval(v, x.q, o, st);
+                        writeOutputs(st, c, state, transport);
                     }
                 }
                 n.candidates += 5;  // the two-phase seeds, failed without their solves
                 n.failures += 5;
                 if (have) {
-                    writeOutputs(best, c, state, transport);
                     if (success) success[c] = 1;
                 } else restart = true;
             }

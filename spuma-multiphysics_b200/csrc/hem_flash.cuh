@@ -322,12 +322,13 @@ struct CandidateOut {
 };
 
 // Scalar T-Newton of the all-gas partition at fixed rho. `g` ends with the gas
-// table's terms at the converged (p, T), where the last probe left them.
+// table's terms at the converged (p, T): the probe that set them is the last
+// probe (a bracket search is always followed by a probe at the bracket end or
+// by at least one Newton probe, which rewrite `g`).
 __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, GasPoint& g,
                                  Counts& n) {
     const double q = in.q;
     double T = clampd(in.gT, C.Tmin, C.Tmax), F, cv, p, cp;
-    GasPoint bracket;  // probes that only bracket the root
     if (!gasProbe(C, q, in.e, T, F, cv, p, cp, g, n)) return false;
     const double scale = fmax(1e5 * q, q * cp * T);
     double lower = T, upper = T, fl = F, fh = F;
@@ -339,7 +340,7 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmax(C.Tmin, T - radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, bracket, n)) { fl = val; lower = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n)) { fl = val; lower = cand; found = true; }
                     else cand = .5 * (lower + cand);
                 }
                 if (!found) return false;
@@ -348,7 +349,7 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmin(C.Tmax, T + radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, bracket, n)) { fh = val; upper = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n)) { fh = val; upper = cand; found = true; }
                     else cand = .5 * (upper + cand);
                 }
                 if (!found) return false;
@@ -377,20 +378,16 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
     return o.vres <= C.vtol && o.eres <= C.etol;
 }
 
-// Newton on (ln p, ln T) with the liquid partition held fixed. With `known`,
-// a converged scalar all-gas solve leaves the gas table's terms at its (p, T)
-// there and sets *haveKnown.
+// Newton on (ln p, ln T) with the liquid partition held fixed. A converged
+// scalar all-gas solve leaves the gas table's terms at its (p, T) in `g` and
+// sets `known`.
 __device__ RB200_FLASH_FN bool frozenSolve(const HemConst& C, const CellInput& in, double mass, int stallLimit, Eval& v,
-                                   CandidateOut& o, Counts& n, GasPoint* known = nullptr, bool* haveKnown = nullptr) {
-    if (haveKnown) *haveKnown = false;
+                                   CandidateOut& o, Counts& n, GasPoint& g, bool& known) {
+    known = false;
     if (!fin(in.e)) return false;
-    if (C.scalarRecovery && mass == 0) {
-        GasPoint local;
-        GasPoint& g = known ? *known : local;
-        if (scalarGas(C, in, v, o, g, n)) {
-            if (haveKnown) *haveKnown = true;
-            return true;
-        }
+    if (C.scalarRecovery && mass == 0 && scalarGas(C, in, v, o, g, n)) {
+        known = true;
+        return true;
     }
     double p = clampd(in.gp, C.pmin, C.pmax), T = clampd(in.gT, C.Tmin, C.Tmax);
     if (!evaluate(C, in.q, mass, p, T, false, v, n)) return false;

@@ -29,8 +29,10 @@ __global__ void __launch_bounds__(kPassThreads, 1) flashPerCell(const HemConst* 
             Eval v;
             CandidateOut o{};
             bool ok;
-            if (k == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n);
-            else if (k == 1) ok = frozenSolve(C, x, x.q, 0, v, o, n);
+            GasPoint g;
+            bool known;
+            if (k == 0) ok = frozenSolve(C, x, 0.0, C.stableGasPrune ? 4 : 0, v, o, n, g, known);
+            else if (k == 1) ok = frozenSolve(C, x, x.q, 0, v, o, n, g, known);
             else ok = twoPhaseSolve(C, x, kSeeds[k - 2], -1.0, v, o, n);
             if (!ok) { ++n.failures; continue; }
             if (!stableAt(C, x.q, v.liqMass, v.p, v.T, n)) { ++n.failures; continue; }
