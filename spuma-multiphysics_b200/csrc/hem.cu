@@ -785,6 +785,9 @@ std::string species(const ReactiveB200Table& t, PureSpecies& sp) {
     if (t.aBinary[0][0] != s.a) return "Invalid HEM binary a";
     sp.a = s.a; sp.b = s.b; sp.kappa = s.kappa; sp.W = s.molecularWeight; sp.refP = t.refPressure;
     sp.Tc = s.a * kOmegaB / (s.b * kOmegaA * kGas);
+    sp.invW = 1.0 / sp.W;
+    sp.invL = 1.0 / (2.0 * kSqrt2 * sp.b);
+    sp.invL2 = 1.0 / (2.0 * kSqrt2 * sp.b * sp.b);
     sp.regionCount = s.regionCount;
     for (int r = 0; r < s.regionCount; ++r) {
         const auto& g = s.regions[r];

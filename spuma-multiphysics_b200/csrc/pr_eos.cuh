@@ -44,6 +44,7 @@ constexpr int kMaxRegions = 8;
 struct PureSpecies {
     double a, b, kappa, W, Tc, refP;
     double tcLine, rhoC, dRho, dT;  // reported-phase line
+    double invW, invL, invL2;       // 1/W, 1/(2 sqrt2 b), 1/(2 sqrt2 b^2)
     int regionCount;
     int polynomial[kMaxRegions];
     double regionMin[kMaxRegions];
@@ -248,36 +249,38 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
     if (!(V > b)) return EOS_NO_ROOT;
     const double den = V * V + 2.0 * V * b - b * b, vmb = V - b;
     if (!(den > 0) || !(vmb > 0)) return EOS_NO_ROOT;
-    const double p = kGas * T / vmb - aa / den;
+    // one reciprocal per repeated denominator (1/(V-b), 1/den, 1/W, 1/V, 1/dp/dV)
+    const double RT = kGas * T, iv = 1.0 / vmb, id = 1.0 / den, iW = sp.invW, iV = rho * iW;
+    const double p = RT * iv - aa * id;
     if (!fin(p) || p <= 0) return EOS_NO_ROOT;
-    const double dpdV = -kGas * T / (vmb * vmb) + 2.0 * aa * (V + b) / (den * den);
-    const double dpdT = kGas / vmb - da / den;
+    const double dpdV = -RT * (iv * iv) + 2.0 * aa * (V + b) * (id * id);
+    const double dpdT = kGas * iv - da * id;
     if (!fin(dpdV) || !fin(dpdT) || dpdV >= 0) return EOS_UNSTABLE;
+    const double idp = 1.0 / dpdV;
     const double logRatio = log((V + (1.0 + kSqrt2) * b) / (V + (1.0 - kSqrt2) * b));
-    const double L = logRatio / (2.0 * kSqrt2 * b);
-    const double z = p * V / (kGas * T);
-    const double hM = kGas * T * t.hRT + (kGas * T * (z - 1.0) + L * (T * da - aa));
-    const double sM = (kGas * t.sR - kGas * log(p / sp.refP)) + (kGas * log(z * (1.0 - b / V)) + L * da);
+    const double L = logRatio * sp.invL;
+    const double z = p * V / RT;
+    const double hM = RT * t.hRT + (RT * (z - 1.0) + L * (T * da - aa));
+    const double sM = (kGas * t.sR - kGas * log(p / sp.refP)) + (kGas * log(z * (1.0 - b * iV)) + L * da);
     const double dHdT = kGas * t.cpR + V * dpdT - kGas + L * T * d2a;
-    const double cpM = dHdT - (V + T * dpdT / dpdV) * dpdT;
-    const double cvM = cpM + T * dpdT * dpdT / dpdV;
+    const double cpM = dHdT - (V + T * dpdT * idp) * dpdT;
+    const double cvM = cpM + T * dpdT * dpdT * idp;
     s.p = p;
     s.rho = rho;
     s.V = V;
-    s.h = hM / W;
-    s.e = (hM - p * V) / W;
-    s.s = sM / W;
-    s.cp = cpM / W;
-    s.cv = cvM / W;
-    s.alpha = -dpdT / (V * dpdV);
-    s.kappaT = -1.0 / (V * dpdV);
-    const double sound2 = V * V * (-cpM / cvM * dpdV / W);
+    s.h = hM * iW;
+    s.e = (hM - p * V) * iW;
+    s.s = sM * iW;
+    s.cp = cpM * iW;
+    s.cv = cvM * iW;
+    s.alpha = -dpdT * idp * iV;
+    s.kappaT = -idp * iV;
+    const double sound2 = V * V * (-cpM / cvM * dpdV * iW);
     if (!(s.cp > 0) || !(s.cv > 0) || !(s.kappaT > 0) || !(sound2 > 0)) return EOS_UNSTABLE;
     if (chem) {
-        const double RT = kGas * T;
         const double pp = sp.a * (t.q * t.q), num = 2.0 * b * pp - aa * b;
-        s.mu = RT * (t.hRT - t.sR) + RT * log(p / sp.refP) - RT * log(p * V / RT) + RT * log(V / vmb)
-             + RT * b / vmb - num / (2.0 * kSqrt2 * b * b) * logRatio - aa * b * V / (b * den);
+        s.mu = RT * (t.hRT - t.sR) + RT * log(p / sp.refP) - RT * log(z) + RT * log(V * iv)
+             + RT * b * iv - num * sp.invL2 * logRatio - aa * V * id;
         if (!fin(s.mu)) return EOS_NONFINITE;
     }
     if (T >= sp.tcLine) phaseOut = -2;
