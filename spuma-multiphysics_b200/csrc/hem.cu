@@ -788,6 +788,11 @@ std::string species(const ReactiveB200Table& t, PureSpecies& sp) {
     sp.invW = 1.0 / sp.W;
     sp.invL = 1.0 / (2.0 * kSqrt2 * sp.b);
     sp.invL2 = 1.0 / (2.0 * kSqrt2 * sp.b * sp.b);
+    sp.invTc = 1.0 / sp.Tc;
+    {
+        const double pc = kOmegaB * kGas * sp.Tc / sp.b;
+        sp.vc = kOmegaVc * kGas * sp.Tc / pc;
+    }
     sp.regionCount = s.regionCount;
     for (int r = 0; r < s.regionCount; ++r) {
         const auto& g = s.regions[r];

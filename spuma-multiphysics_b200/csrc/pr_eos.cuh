@@ -45,6 +45,7 @@ struct PureSpecies {
     double a, b, kappa, W, Tc, refP;
     double tcLine, rhoC, dRho, dT;  // reported-phase line
     double invW, invL, invL2;       // 1/W, 1/(2 sqrt2 b), 1/(2 sqrt2 b^2)
+    double invTc, vc;               // 1/Tc; critical molar volume of the cubic (single-root side test)
     int regionCount;
     int polynomial[kMaxRegions];
     double regionMin[kMaxRegions];
@@ -69,6 +70,27 @@ __device__ __forceinline__ int nasaRegion(const PureSpecies& sp, double T) {
     return r;
 }
 
+constexpr double kThird = 1.0 / 3.0;
+
+// NASA7/9 cp/R, h/RT, s/R at T (iT = 1/T), thirds as products (the PR T-terms).
+__device__ __forceinline__ void nasaEvalT(const PureSpecies& sp, double T, double iT, double& cpR, double& hRT,
+                                          double& sR) {
+    const int r = nasaRegion(sp, T);
+    const double* a = sp.coeff[r];
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, lT = log(T);
+    if (sp.polynomial[r] == 7) {
+        cpR = a[0] + a[1] * T + a[2] * T2 + a[3] * T3 + a[4] * T4;
+        hRT = a[0] + .5 * a[1] * T + a[2] * T2 * kThird + .25 * a[3] * T3 + .2 * a[4] * T4 + a[5] * iT;
+        sR = a[0] * lT + a[1] * T + .5 * a[2] * T2 + a[3] * T3 * kThird + .25 * a[4] * T4 + a[6];
+    } else {
+        const double c0 = a[0] * iT * iT, c1 = a[1] * iT, c2 = a[2], c3 = a[3] * T, c4 = a[4] * T2,
+                     c5 = a[5] * T3, c6 = a[6] * T4;
+        cpR = c0 + c1 + c2 + c3 + c4 + c5 + c6;
+        hRT = -c0 + lT * c1 + c2 + .5 * c3 + c4 * kThird + .25 * c5 + .2 * c6 + a[7] * iT;
+        sR = -.5 * c0 - c1 + lT * c2 + c3 + .5 * c4 + c5 * kThird + .25 * c6 + a[8];
+    }
+}
+// NASA7/9 cp/R, h/RT, s/R at T (the ideal-gas closure's form).
 __device__ __forceinline__ void nasaEval(const PureSpecies& sp, double T, double& cpR, double& hRT, double& sR) {
     const int r = nasaRegion(sp, T);
     const double* a = sp.coeff[r];
@@ -152,10 +174,11 @@ __device__ __forceinline__ double polishRoot(double x, double bn, double cn, dou
 }
 
 __device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
-    const double b = sp.b, b2 = b * b, RTp = kGas * T / p, aap = aa / p, bn = b - RTp;
+    const double ip = 1.0 / p;
+    const double b = sp.b, b2 = b * b, RTp = kGas * T * ip, aap = aa * ip, bn = b - RTp;
     const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
-    const double center = -bn / 3.0, delta2 = (bn * bn - 3.0 * cn) / 9.0;
-    const double q = 2.0 * bn * bn * bn / 27.0 - bn * cn / 3.0 + dn;
+    const double center = -bn * kThird, delta2 = (bn * bn - 3.0 * cn) * (1.0 / 9.0);
+    const double q = 2.0 * bn * bn * bn * (1.0 / 27.0) - bn * cn * kThird + dn;
     const double delta = delta2 > 0 ? sqrt(delta2) : 0.0, h = 2.0 * delta * delta2;
     double disc = q * q - h * h;
     if (fabs(fabs(h) - fabs(q)) < 1e-10) {
@@ -176,10 +199,14 @@ __device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p
         rawCount = 1;
     } else if (disc < -1e-14) {
         const double arg = fmin(1.0, fmax(-1.0, -.5 * q / (delta * delta * delta)));
-        const double theta = acos(arg) / 3.0;
-        raw0 = center + 2.0 * delta * cos(theta);
-        raw1 = center + 2.0 * delta * cos(theta + 2.0 * kPi / 3.0);
-        raw2 = center + 2.0 * delta * cos(theta + 4.0 * kPi / 3.0);
+        // 2 delta cos(theta + 2 pi k / 3), k = 0, 1, 2, from one sine and cosine:
+        // cos(theta +- 2 pi / 3) = -cos(theta) / 2 -+ sqrt3 / 2 sin(theta)
+        double sn, cs;
+        sincos(acos(arg) * kThird, &sn, &cs);
+        const double dc = delta * cs, ds = 1.7320508075688772 * delta * sn;
+        raw0 = center + 2.0 * dc;
+        raw1 = center - dc - ds;
+        raw2 = center - dc + ds;
         rawCount = 3;
     } else return EOS_NO_ROOT;
     if (!side) {
@@ -207,11 +234,9 @@ __device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p
     } else if (n >= 2) {
         r.gas = r.liquid = true;
     } else {
-        const double Tcm = sp.a * kOmegaB / (b * kOmegaA * kGas);
-        const double pc = kOmegaB * kGas * Tcm / b, vc = kOmegaVc * kGas * Tcm / pc;
-        const bool liquidSign = T > Tcm ? r.lo < vc : r.lo < center;
+        const bool liquidSign = T > sp.Tc ? r.lo < sp.vc : r.lo < center;
         r.liquid = liquidSign;
-        r.gas = !liquidSign || T > Tcm;
+        r.gas = !liquidSign || T > sp.Tc;
     }
     return EOS_OK;
 }
@@ -224,18 +249,20 @@ struct TTerms {
 
 __device__ RB200_EOS_FN int tTerms(const PureSpecies& sp, double T, TTerms& t) {
     if (!fin(T) || T <= 0) return EOS_INVALID_INPUT;
-    const double sq = sqrt(T / sp.Tc), f = 1.0 + sp.kappa * (1.0 - sq);
+    const double iT = 1.0 / T;
+    const double sq = sqrt(T * sp.invTc), f = 1.0 + sp.kappa * (1.0 - sq);
     if (fabs(f) <= 1e-14) return EOS_NONFINITE;
     const double sign = f > 0 ? 1.0 : -1.0, q = fabs(f);
-    const double dq = -sign * sp.kappa / (2.0 * sp.Tc * sq);
-    const double d2q = sign * sp.kappa / (4.0 * sp.Tc * sp.Tc * sq * sq * sq);
+    // dq/dT = -kappa / (2 Tc sqrt(T/Tc)) and d2q/dT2 = -dq/dT / (2 T) (Tc sq^2 = T)
+    const double dq = -sign * sp.kappa * (.5 * sp.invTc) / sq;
+    const double d2q = -.5 * dq * iT;
     t.T = T;
     t.q = q;
     t.aa = sp.a * q * q;
     t.da = sp.a * (dq * q + q * dq);
     t.d2a = sp.a * (d2q * q + 2.0 * dq * dq + q * d2q);
     if (!(fin(t.aa) && fin(t.da) && fin(t.d2a) && t.aa > 0)) return EOS_NONFINITE;
-    nasaEval(sp, T, t.cpR, t.hRT, t.sR);
+    nasaEvalT(sp, T, iT, t.cpR, t.hRT, t.sR);
     return EOS_OK;
 }
 
