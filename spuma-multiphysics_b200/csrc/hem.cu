@@ -789,6 +789,7 @@ std::string species(const ReactiveB200Table& t, PureSpecies& sp) {
     sp.invL = 1.0 / (2.0 * kSqrt2 * sp.b);
     sp.invL2 = 1.0 / (2.0 * kSqrt2 * sp.b * sp.b);
     sp.invTc = 1.0 / sp.Tc;
+    sp.invRefP = 1.0 / sp.refP;
     {
         const double pc = kOmegaB * kGas * sp.Tc / sp.b;
         sp.vc = kOmegaVc * kGas * sp.Tc / pc;

@@ -46,6 +46,7 @@ struct PureSpecies {
     double tcLine, rhoC, dRho, dT;  // reported-phase line
     double invW, invL, invL2;       // 1/W, 1/(2 sqrt2 b), 1/(2 sqrt2 b^2)
     double invTc, vc;               // 1/Tc; critical molar volume of the cubic (single-root side test)
+    double invRefP;                 // 1/reference pressure
     int regionCount;
     int polynomial[kMaxRegions];
     double regionMin[kMaxRegions];
@@ -287,8 +288,11 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
     const double logRatio = log((V + (1.0 + kSqrt2) * b) / (V + (1.0 - kSqrt2) * b));
     const double L = logRatio * sp.invL;
     const double z = p * V / RT;
+    // ln(p/pref) - ln z(1 - b/V) = ln(RT / (pref (V - b))): the ideal-gas and residual
+    // logarithms of the entropy (and of the chemical potential) as one
+    const double lg = log(RT * iv * sp.invRefP);
     const double hM = RT * t.hRT + (RT * (z - 1.0) + L * (T * da - aa));
-    const double sM = (kGas * t.sR - kGas * log(p / sp.refP)) + (kGas * log(z * (1.0 - b * iV)) + L * da);
+    const double sM = kGas * (t.sR - lg) + L * da;
     const double dHdT = kGas * t.cpR + V * dpdT - kGas + L * T * d2a;
     const double cpM = dHdT - (V + T * dpdT * idp) * dpdT;
     const double cvM = cpM + T * dpdT * dpdT * idp;
@@ -306,8 +310,7 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
     if (!(s.cp > 0) || !(s.cv > 0) || !(s.kappaT > 0) || !(sound2 > 0)) return EOS_UNSTABLE;
     if (chem) {
         const double pp = sp.a * (t.q * t.q), num = 2.0 * b * pp - aa * b;
-        s.mu = RT * (t.hRT - t.sR) + RT * log(p / sp.refP) - RT * log(z) + RT * log(V * iv)
-             + RT * b * iv - num * sp.invL2 * logRatio - aa * V * id;
+        s.mu = RT * (t.hRT - t.sR) + RT * lg + RT * b * iv - num * sp.invL2 * logRatio - aa * V * id;
         if (!fin(s.mu)) return EOS_NONFINITE;
     }
     if (T >= sp.tcLine) phaseOut = -2;
@@ -316,8 +319,9 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
         if (!fin(rhoMid)) return EOS_NONFINITE;
         phaseOut = rho < rhoMid ? -1 : 0;
     }
+    // (sound2 > 0 here, so its square root is finite exactly when sound2 is)
     if (!fin(s.e) || !fin(s.h) || !fin(s.s) || !fin(s.cp) || !fin(s.cv) || !fin(s.alpha) || !fin(s.kappaT)
-        || !fin(sqrt(sound2)) || !fin(dpdT) || !fin(dpdV))
+        || !fin(sound2) || !fin(dpdT) || !fin(dpdV))
         return EOS_NONFINITE;
     return EOS_OK;
 }
