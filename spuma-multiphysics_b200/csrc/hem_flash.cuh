@@ -154,6 +154,7 @@ struct GasPoint {
     TTerms t;
     Roots r;
     PhaseProps gas;
+    ChemTerms chem;  // the gas root evaluation's chemical-potential intermediates
 };
 
 // Phase sums at (p, T) for liquid mass `mass` out of total density q. With
@@ -162,8 +163,9 @@ struct GasPoint {
 // needed and the tables hold one species, the T-terms and the cubic are formed
 // once for both roots (the same arithmetic as two separate evaluations).
 // `known` (optional) holds the gas table's terms at exactly (p, T): they replace
-// the T-terms and the cubic of the shared path and, without `virt`, the gas
-// root's properties (the same values those calls return).
+// the T-terms and the cubic of the shared path and the gas root's properties,
+// with `virt` its chemical potential from the kept intermediates (the same values
+// those calls return).
 __device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass, double p, double T, bool virt, Eval& v,
                                 Counts& n, const GasPoint* known = nullptr) {
     v.p = p; v.T = T;
@@ -195,8 +197,13 @@ __device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass
     PhaseProps ph;
     if (gas > 0) {
         int st = EOS_OK;
-        if (known && !virt) ph = known->gas;
-        else st = shared ? gasFromShared(C, sharedStatus, t, r, p, virt, ph, n) : gasPhase(C, p, T, virt, ph, n);
+        if (known) {
+            ph = known->gas;
+            if (virt) {
+                ph.mu = chemPotential(C.gas, known->t, ph.V, known->chem);
+                if (!fin(ph.mu)) st = EOS_NONFINITE;
+            }
+        } else st = shared ? gasFromShared(C, sharedStatus, t, r, p, virt, ph, n) : gasPhase(C, p, T, virt, ph, n);
         if (st != EOS_OK) return false;
         addPhase(v, gas, ph, p);
         v.gRho = ph.rho; v.gE = ph.e; v.gV = ph.V; v.gH = ph.h;
@@ -309,7 +316,8 @@ __device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn,
     ++n.phases;
     if (C.enforceBounds && (T < C.gasTmin || T > C.gasTmax)) return false;
     if (cubicRoots(C.gas, T, p, g.t.aa, g.r) != EOS_OK) return false;
-    if (rootProps(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas) != EOS_OK || fabs(g.gas.rho - q) > 1e-8 * q) return false;
+    if (rootProps(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas, &g.chem) != EOS_OK || fabs(g.gas.rho - q) > 1e-8 * q)
+        return false;
     F = q * prop.e - eIn;
     cv = q * prop.cv;
     cp = prop.cp;

@@ -267,10 +267,25 @@ __device__ RB200_EOS_FN int tTerms(const PureSpecies& sp, double T, TTerms& t) {
     return EOS_OK;
 }
 
+// The intermediates of a (T, rho) evaluation that its chemical potential reads:
+// 1/(V - b), 1/den, ln(RT / (pref (V - b))) and the attraction logarithm.
+struct ChemTerms {
+    double iv, id, lg, logRatio;
+};
+
+// Molar chemical potential at molar volume V from the T-terms and the
+// evaluation's intermediates (one routine, so every caller forms the same bits).
+__device__ __forceinline__ double chemPotential(const PureSpecies& sp, const TTerms& t, double V, const ChemTerms& c) {
+    const double RT = kGas * t.T, b = sp.b, aa = t.aa;
+    const double pp = sp.a * (t.q * t.q), num = 2.0 * b * pp - aa * b;
+    return RT * (t.hRT - t.sR) + RT * c.lg + RT * b * c.iv - num * sp.invL2 * c.logRatio - aa * V * c.id;
+}
+
 // Properties at (T, rho) from the T-only terms. chem: also the molar chemical
 // potential. phaseOut: -2 supercritical, -1 gas, 0 liquid by the reported-phase line.
+// keep (optional): the chemical potential's intermediates, on success.
 __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
-                              int& phaseOut) {
+                              int& phaseOut, ChemTerms* keep = nullptr) {
     const double T = t.T, aa = t.aa, da = t.da, d2a = t.d2a;
     if (!fin(rho) || rho <= 0) return EOS_INVALID_INPUT;
     const double b = sp.b, W = sp.W, V = W / rho;
@@ -308,9 +323,9 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
     s.kappaT = -idp * iV;
     const double sound2 = V * V * (-cpM / cvM * dpdV * iW);
     if (!(s.cp > 0) || !(s.cv > 0) || !(s.kappaT > 0) || !(sound2 > 0)) return EOS_UNSTABLE;
+    const ChemTerms ct{iv, id, lg, logRatio};
     if (chem) {
-        const double pp = sp.a * (t.q * t.q), num = 2.0 * b * pp - aa * b;
-        s.mu = RT * (t.hRT - t.sR) + RT * lg + RT * b * iv - num * sp.invL2 * logRatio - aa * V * id;
+        s.mu = chemPotential(sp, t, V, ct);
         if (!fin(s.mu)) return EOS_NONFINITE;
     }
     if (T >= sp.tcLine) phaseOut = -2;
@@ -323,6 +338,7 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
     if (!fin(s.e) || !fin(s.h) || !fin(s.s) || !fin(s.cp) || !fin(s.cv) || !fin(s.alpha) || !fin(s.kappaT)
         || !fin(sound2) || !fin(dpdT) || !fin(dpdV))
         return EOS_NONFINITE;
+    if (keep) *keep = ct;
     return EOS_OK;
 }
 
@@ -337,7 +353,7 @@ __device__ RB200_EOS_FN int prTrho(const PureSpecies& sp, double T, double rho, 
 // Root choice at (T, p) with the host postcondition |p(T, rho) - p| <= 1e-7 max(1, p)
 // and the reported-phase consistency of the chosen branch.
 __device__ RB200_EOS_FN int rootProps(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
-                                bool chem, PhaseProps& s) {
+                                bool chem, PhaseProps& s, ChemTerms* keep = nullptr) {
     int sel = r.count - 1;
     if (choice == ROOT_LIQUID) {
         if (!r.liquid) return EOS_UNAVAILABLE;
@@ -345,7 +361,7 @@ __device__ RB200_EOS_FN int rootProps(const PureSpecies& sp, const TTerms& t, co
     } else if (choice == ROOT_GAS && !r.gas) return EOS_UNAVAILABLE;
     const double V = sel == 0 ? r.lo : r.hi;
     int phase = 0;
-    const int st = prTrhoT(sp, t, sp.W / V, chem, s, phase);
+    const int st = prTrhoT(sp, t, sp.W / V, chem, s, phase, keep);
     if (st != EOS_OK) return st;
     if (fabs(s.p - p) > 1e-7 * fmax(1.0, p)) return EOS_NONFINITE;
     s.p = p;
