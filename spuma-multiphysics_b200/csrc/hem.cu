@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
     QueueLane L;
     L.st = Q_FREE;
     L.req = REQ_NONE;
+    L.known = false;
     Eval v;
     bool pending = false, exhausted = cells == 0;
     for (;;) {
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
                         L.mass = kind == 1 ? L.x.q : 0.0;
                         L.st = kind >= 2 ? Q_TP_START : Q_FZ_START;
                         L.req = REQ_NONE;
+                        L.known = false;
                         if (kind >= 2 && L.x.noTwoPhase) {
                             // outside every saturation tie line: the seed cannot converge
                             ++n.candidates;
@@ -174,11 +176,8 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
             continue;
         }
         if (pending) {
-            if (L.req == REQ_POINT) L.ok = evaluate(C, L.x.q, L.rm, L.rp, L.rT, L.rv, v, n);
-            else if (L.req == REQ_PROBE) {
-                GasPoint g;
-                L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, g, n);
-            }
+            if (L.req == REQ_POINT) L.ok = evaluate(C, L.x.q, L.rm, L.rp, L.rT, L.rv, v, n, L.known ? &L.g : nullptr);
+            else if (L.req == REQ_PROBE) L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, L.g, n);
             else L.ok = tangentStable(C, L.rp, L.rT, n);
             L.req = REQ_NONE;
             pending = false;

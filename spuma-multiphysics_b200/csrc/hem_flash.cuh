@@ -310,13 +310,14 @@ __device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn,
     int phase;
     ++n.phases;
     if (!fin(T) || !fin(q) || T <= 0 || q <= 0) return false;
-    if (tTerms(C.gas, T, g.t) != EOS_OK || prTrhoT(C.gas, g.t, q, false, prop, phase) != EOS_OK) return false;
+    if (tTermsBody(C.gas, T, g.t) != EOS_OK || prTrhoTBody(C.gas, g.t, q, false, prop, phase, nullptr) != EOS_OK)
+        return false;
     p = prop.p;  // finite and positive
     if (!inBounds(C, p, T)) return false;
     ++n.phases;
     if (C.enforceBounds && (T < C.gasTmin || T > C.gasTmax)) return false;
-    if (cubicRoots(C.gas, T, p, g.t.aa, g.r) != EOS_OK) return false;
-    if (rootProps(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas, &g.chem) != EOS_OK || fabs(g.gas.rho - q) > 1e-8 * q)
+    if (cubicRootsBody(C.gas, T, p, g.t.aa, g.r) != EOS_OK) return false;
+    if (rootPropsBody(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas, &g.chem) != EOS_OK || fabs(g.gas.rho - q) > 1e-8 * q)
         return false;
     F = q * prop.e - eIn;
     cv = q * prop.cv;

@@ -50,9 +50,12 @@ struct QueueLane {
     double mass, a0, a1, a2;  // frozen: p, T; two-phase: ln p, ln T, beta
     double f0, f1, f2, s0, s1, s2, prev, frac, scale;
     int it, k, stalled;
-    // scalar all-gas recovery
+    // scalar all-gas recovery; g: the last probe's gas-table terms, which the
+    // candidate's final point and stability test take once it converged (known)
     double T0, lower, upper, fl, fh, radius, cand, F, cv, P;
     int j, retry;
+    bool known;
+    GasPoint g;
     CandidateOut o;
 };
 
@@ -94,6 +97,7 @@ __device__ inline bool plan(const HemConst& C, QueueLane& L, Eval& v, Record rec
             L.st = Q_FZ_NEWTON_INIT;
             continue;
         case Q_FZ_NEWTON_INIT: {
+            L.known = false;
             L.a0 = clampd(L.x.gp, C.pmin, C.pmax);
             L.a1 = clampd(L.x.gT, C.Tmin, C.Tmax);
             L.req = REQ_POINT; L.rm = L.mass; L.rp = L.a0; L.rT = L.a1; L.rv = false;
@@ -207,7 +211,9 @@ __device__ inline bool plan(const HemConst& C, QueueLane& L, Eval& v, Record rec
         case Q_SG_NEWTON: {
             if (!(L.it < 70 && fabs(L.F) > C.etol * L.scale)) {
                 if (fabs(L.F) > C.etol * L.scale) { L.st = Q_FZ_NEWTON_INIT; continue; }
-                L.req = REQ_POINT; L.rm = 0; L.rp = L.P; L.rT = L.T0; L.rv = false; L.st = Q_SG_FINAL;
+                // (P, T0) are the last probe's point: its terms serve the final evaluation
+                L.req = REQ_POINT; L.rm = 0; L.rp = L.P; L.rT = L.T0; L.rv = false; L.known = true;
+                L.st = Q_SG_FINAL;
                 return true;
             }
             if (L.F > 0) L.upper = L.T0; else L.lower = L.T0;

@@ -174,7 +174,7 @@ __device__ __forceinline__ double polishRoot(double x, double bn, double cn, dou
     return x;
 }
 
-__device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
+__device__ __forceinline__ int cubicRootsBody(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
     const double ip = 1.0 / p;
     const double b = sp.b, b2 = b * b, RTp = kGas * T * ip, aap = aa * ip, bn = b - RTp;
     const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
@@ -241,6 +241,9 @@ __device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p
     }
     return EOS_OK;
 }
+__device__ RB200_EOS_FN int cubicRoots(const PureSpecies& sp, double T, double p, double aa, Roots& r) {
+    return cubicRootsBody(sp, T, p, aa, r);
+}
 
 // Temperature-only terms shared by every evaluation at one T: a*alpha and its
 // T-derivatives, |1 + kappa(1 - sqrt(T/Tc))|, and the NASA cp/R, h/RT, s/R.
@@ -248,7 +251,7 @@ struct TTerms {
     double T, aa, da, d2a, q, cpR, hRT, sR;
 };
 
-__device__ RB200_EOS_FN int tTerms(const PureSpecies& sp, double T, TTerms& t) {
+__device__ __forceinline__ int tTermsBody(const PureSpecies& sp, double T, TTerms& t) {
     if (!fin(T) || T <= 0) return EOS_INVALID_INPUT;
     const double iT = 1.0 / T;
     const double sq = sqrt(T * sp.invTc), f = 1.0 + sp.kappa * (1.0 - sq);
@@ -265,6 +268,9 @@ __device__ RB200_EOS_FN int tTerms(const PureSpecies& sp, double T, TTerms& t) {
     if (!(fin(t.aa) && fin(t.da) && fin(t.d2a) && t.aa > 0)) return EOS_NONFINITE;
     nasaEvalT(sp, T, iT, t.cpR, t.hRT, t.sR);
     return EOS_OK;
+}
+__device__ RB200_EOS_FN int tTerms(const PureSpecies& sp, double T, TTerms& t) {
+    return tTermsBody(sp, T, t);
 }
 
 // The intermediates of a (T, rho) evaluation that its chemical potential reads:
@@ -284,8 +290,8 @@ __device__ __forceinline__ double chemPotential(const PureSpecies& sp, const TTe
 // Properties at (T, rho) from the T-only terms. chem: also the molar chemical
 // potential. phaseOut: -2 supercritical, -1 gas, 0 liquid by the reported-phase line.
 // keep (optional): the chemical potential's intermediates, on success.
-__device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
-                              int& phaseOut, ChemTerms* keep = nullptr) {
+__device__ __forceinline__ int prTrhoTBody(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
+                              int& phaseOut, ChemTerms* keep) {
     const double T = t.T, aa = t.aa, da = t.da, d2a = t.d2a;
     if (!fin(rho) || rho <= 0) return EOS_INVALID_INPUT;
     const double b = sp.b, W = sp.W, V = W / rho;
@@ -341,6 +347,10 @@ __device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, doub
     if (keep) *keep = ct;
     return EOS_OK;
 }
+__device__ RB200_EOS_FN int prTrhoT(const PureSpecies& sp, const TTerms& t, double rho, bool chem, PhaseProps& s,
+                              int& phaseOut, ChemTerms* keep = nullptr) {
+    return prTrhoTBody(sp, t, rho, chem, s, phaseOut, keep);
+}
 
 __device__ RB200_EOS_FN int prTrho(const PureSpecies& sp, double T, double rho, bool chem, PhaseProps& s, int& phaseOut) {
     if (!fin(T) || !fin(rho) || T <= 0 || rho <= 0) return EOS_INVALID_INPUT;
@@ -352,8 +362,8 @@ __device__ RB200_EOS_FN int prTrho(const PureSpecies& sp, double T, double rho, 
 
 // Root choice at (T, p) with the host postcondition |p(T, rho) - p| <= 1e-7 max(1, p)
 // and the reported-phase consistency of the chosen branch.
-__device__ RB200_EOS_FN int rootProps(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
-                                bool chem, PhaseProps& s, ChemTerms* keep = nullptr) {
+__device__ __forceinline__ int rootPropsBody(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
+                                bool chem, PhaseProps& s, ChemTerms* keep) {
     int sel = r.count - 1;
     if (choice == ROOT_LIQUID) {
         if (!r.liquid) return EOS_UNAVAILABLE;
@@ -361,13 +371,17 @@ __device__ RB200_EOS_FN int rootProps(const PureSpecies& sp, const TTerms& t, co
     } else if (choice == ROOT_GAS && !r.gas) return EOS_UNAVAILABLE;
     const double V = sel == 0 ? r.lo : r.hi;
     int phase = 0;
-    const int st = prTrhoT(sp, t, sp.W / V, chem, s, phase, keep);
+    const int st = prTrhoTBody(sp, t, sp.W / V, chem, s, phase, keep);
     if (st != EOS_OK) return st;
     if (fabs(s.p - p) > 1e-7 * fmax(1.0, p)) return EOS_NONFINITE;
     s.p = p;
     if (choice == ROOT_GAS && phase >= 0) return EOS_UNAVAILABLE;
     if (choice == ROOT_LIQUID && phase < 0) return EOS_UNAVAILABLE;
     return EOS_OK;
+}
+__device__ RB200_EOS_FN int rootProps(const PureSpecies& sp, const TTerms& t, const Roots& r, double p, int choice,
+                                bool chem, PhaseProps& s, ChemTerms* keep = nullptr) {
+    return rootPropsBody(sp, t, r, p, choice, chem, s, keep);
 }
 
 __device__ RB200_EOS_FN int prTP(const PureSpecies& sp, double T, double p, int choice, bool chem, PhaseProps& s) {
