@@ -117,9 +117,26 @@ struct MainRecords {
     __device__ void status(const QueueLane& L, int code) const { at(L).status = code; }
 };
 
+// Lanes of a warp that help line searches once the queue is drained.
+constexpr int kLineHelpers = 8;
+
+__device__ __forceinline__ int nthSetBit(unsigned mask, int n) {
+    for (int i = 0; i < n; ++i) mask &= mask - 1;
+    return __ffs(mask) - 1;
+}
+
 // Persistent lane-level queue over items (kind, cell): kinds [kindBase,
 // kindBase+kinds), cells 0..count-1 or list[0..counters[LIST]) when list != null.
 // Items are kind-major, so consecutive items share a candidate kind.
+//
+// Once a warp's lanes find the queue empty, up to kLineHelpers of its idle lanes
+// evaluate the next trial fractions of the warp's line searches (frozen-partition
+// and two-phase Newton) beside the searching lanes' own trials (the r-th helper
+// takes searching lane r mod S, trial offset 1 + r / S). A searching lane whose
+// own trial is rejected walks its helpers' trials in order and takes the first
+// that passes the same acceptance test: the search ends on the same fraction with
+// the same evaluation (the same routine on the same inputs) as the serial search,
+// in fewer rounds of a lone lane's FP64 latency.
 __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(const HemConst* __restrict__ Cp,
                                                           const CellInput* __restrict__ in, size_t count,
                                                           const unsigned* __restrict__ list, int kindBase, int kinds,
@@ -132,6 +149,9 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
     const MainRecords records{rec, count};
     const int stallLimitGas = C.stableGasPrune ? 4 : 0;
     const unsigned lane = threadIdx.x & 31u;
+    __shared__ Eval helpEval[kPassThreads / 32][kLineHelpers];
+    __shared__ signed char helpResult[kPassThreads / 32][kLineHelpers];  // -1 no trial, 0 failed/skipped, 1 evaluated
+    const unsigned warp = threadIdx.x >> 5;
     QueueLane L;
     L.st = Q_FREE;
     L.req = REQ_NONE;
@@ -175,13 +195,103 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
             if (__all_sync(0xffffffffu, L.st == Q_FREE && exhausted)) break;
             continue;
         }
-        if (pending) {
-            if (L.req == REQ_POINT) L.ok = evaluate(C, L.x.q, L.rm, L.rp, L.rT, L.rv, v, n, L.known ? &L.g : nullptr);
-            else if (L.req == REQ_PROBE) L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, L.g, n);
+        // line-search helpers (a warp-uniform decision)
+        const bool tpSearch = pending && L.req == REQ_POINT && L.st == Q_TP_LS_AFTER;
+        const bool fzSearch = pending && L.req == REQ_POINT && L.st == Q_FZ_LS_AFTER;
+        const bool search = tpSearch || fzSearch;
+        const bool idle = !pending && L.st == Q_FREE && exhausted;
+        const unsigned searchMask = __ballot_sync(0xffffffffu, search);
+        const unsigned idleMask = __ballot_sync(0xffffffffu, idle);
+        const int nS = __popc(searchMask), nH = searchMask ? min(__popc(idleMask), kLineHelpers) : 0;
+        // one evaluation per lane at one call site: the lane's own request or a helper's trial
+        bool point = pending && L.req == REQ_POINT;
+        double eq = L.x.q, erm = L.rm, erp = L.rp, erT = L.rT;
+        bool erv = L.rv;
+        Eval* out = &v;
+        const GasPoint* kept = L.known ? &L.g : nullptr;
+        int helpSlot = -1;
+        if (nH > 0) {
+            const int r = idle ? __popc(idleMask & ((1u << lane) - 1)) : kLineHelpers;
+            const bool helper = idle && r < nH;
+            const int target = helper ? nthSetBit(searchMask, r % nS) : int(lane);
+            const double a0 = __shfl_sync(0xffffffffu, L.a0, target), a1 = __shfl_sync(0xffffffffu, L.a1, target);
+            const double a2 = __shfl_sync(0xffffffffu, L.a2, target), s0 = __shfl_sync(0xffffffffu, L.s0, target);
+            const double s1 = __shfl_sync(0xffffffffu, L.s1, target), s2 = __shfl_sync(0xffffffffu, L.s2, target);
+            const double f0 = __shfl_sync(0xffffffffu, L.frac, target), q = __shfl_sync(0xffffffffu, L.x.q, target);
+            const double mass = __shfl_sync(0xffffffffu, L.mass, target);
+            const int k0 = __shfl_sync(0xffffffffu, L.k, target);
+            const bool tp = __shfl_sync(0xffffffffu, tpSearch, target);
+            if (helper) {
+                helpSlot = r;
+                const int offset = 1 + r / nS;
+                signed char result = -1;  // beyond the search's 30 trials
+                if (k0 + offset < 30) {
+                    double frac = f0;
+                    for (int m = 0; m < offset; ++m) frac *= .5;
+                    if (tp && !(a2 + frac * s2 >= 0 && a2 + frac * s2 < 1)) result = 0;  // skipped, no evaluation
+                    else {
+                        point = true;
+                        eq = q;
+                        if (tp) {
+                            erm = (a2 + frac * s2) * q;
+                            erp = exp(a0 + frac * s0);
+                            erT = exp(a1 + frac * s1);
+                            erv = true;
+                        } else {
+                            erm = mass;
+                            erp = a0 * exp(frac * s0);
+                            erT = a1 * exp(frac * s1);
+                            erv = false;
+                        }
+                        out = &helpEval[warp][r];
+                        kept = nullptr;
+                    }
+                }
+                helpResult[warp][r] = result;
+            }
+        }
+        if (point) {
+            const bool ok = evaluate(C, eq, erm, erp, erT, erv, *out, n, kept);
+            if (helpSlot >= 0) helpResult[warp][helpSlot] = ok ? 1 : 0;
+            else L.ok = ok;
+        } else if (pending) {
+            if (L.req == REQ_PROBE) L.ok = gasProbe(C, L.x.q, L.x.e, L.rT, L.pF, L.pCv, L.pP, L.pCp, L.g, n);
             else L.ok = tangentStable(C, L.rp, L.rT, n);
+        }
+        if (pending) {
             L.req = REQ_NONE;
             pending = false;
         }
+        __syncwarp();
+        if (nH > 0 && search) {
+            double t0, t1, t2;
+            const bool own = tpSearch ? tpAccepts(v, L.ok, L.x.e, L.scale, L.prev, L.frac, t0, t1, t2)
+                                      : fzAccepts(C, v, L.ok, L.x.e, L.scale, L.prev, L.frac);
+            if (!own) {
+                // the serial search's next trials, in order, from the helpers
+                const int rank = __popc(searchMask & ((1u << lane) - 1));
+                bool found = false;
+                for (int r = rank; r < nH && !found; r += nS) {
+                    const signed char result = helpResult[warp][r];
+                    if (result < 0) break;
+                    if (tpSearch) ++n.residuals;
+                    ++L.k;
+                    L.frac *= .5;
+                    const Eval& h = helpEval[warp][r];
+                    if (result > 0 && (tpSearch ? tpAccepts(h, true, L.x.e, L.scale, L.prev, L.frac, t0, t1, t2)
+                                                : fzAccepts(C, h, true, L.x.e, L.scale, L.prev, L.frac))) {
+                        v = h;
+                        if (fzSearch) {  // the frozen step moves to the trial point itself
+                            L.rp = L.a0 * exp(L.frac * L.s0);
+                            L.rT = L.a1 * exp(L.frac * L.s1);
+                        }
+                        found = true;
+                    }
+                }
+                L.ok = found;  // none accepted: the search resumes after the last trial taken
+            }
+        }
+        __syncwarp();
     }
     flushCounts(n, totals);
 }

@@ -78,6 +78,22 @@ __device__ RB200_FLASH_FN bool tangentStable(const HemConst& C, double p, double
     return (gas.h - T * gas.s) * C.gas.W / (kGas * T) - muL >= -C.mutol;
 }
 
+// Acceptance tests of a line-search trial evaluated into v: the residual must
+// fall below the current one by the Armijo factor (the frozen partition's also
+// accepts a residual already within tolerance).
+__device__ __forceinline__ bool tpAccepts(const Eval& v, bool ok, double eIn, double scale, double prev, double frac,
+                                          double& t0, double& t1, double& t2) {
+    if (!(ok && v.gasMass > 0)) return false;
+    t0 = v.volume - 1; t1 = (v.energy - eIn) / scale; t2 = v.muL - v.muG;
+    return fin(t2) && fmax(fabs(t0), fmax(fabs(t1), fabs(t2))) < prev * (1 - 1e-4 * frac);
+}
+__device__ __forceinline__ bool fzAccepts(const HemConst& C, const Eval& v, bool ok, double eIn, double scale,
+                                          double prev, double frac) {
+    if (!ok) return false;
+    const double next = fmax(fabs(v.volume - 1), fabs(v.energy - eIn) / scale);
+    return next < prev * (1 - 1e-4 * frac) || next < fmin(C.vtol, C.etol);
+}
+
 // Advances one lane's solver until it issues a request (returns true) or the
 // candidate is finished (record written; returns false, lane becomes free).
 template <class Record>
@@ -131,9 +147,8 @@ __device__ inline bool plan(const HemConst& C, QueueLane& L, Eval& v, Record rec
             L.rv = false; L.st = Q_FZ_LS_AFTER;
             return true;
         case Q_FZ_LS_AFTER:
-            if (L.ok) {
-                const double next = fmax(fabs(v.volume - 1), fabs(v.energy - eIn) / L.scale);
-                if (next < L.prev * (1 - 1e-4 * L.frac) || next < fmin(C.vtol, C.etol)) {
+            {
+                if (fzAccepts(C, v, L.ok, eIn, L.scale, L.prev, L.frac)) {
                     L.a0 = L.rp; L.a1 = L.rT;
                     L.stalled = L.frac < 1. / 32 ? L.stalled + 1 : 0;
                     const int limit = L.kind == 0 ? stallLimitGas : 0;
@@ -300,14 +315,12 @@ __device__ inline bool plan(const HemConst& C, QueueLane& L, Eval& v, Record rec
             return true;
         }
         case Q_TP_LS_AFTER: {
-            if (L.ok && v.gasMass > 0) {
-                const double t0 = v.volume - 1, t1 = (v.energy - eIn) / L.scale, t2 = v.muL - v.muG;
-                if (fin(t2) && fmax(fabs(t0), fmax(fabs(t1), fabs(t2))) < L.prev * (1 - 1e-4 * L.frac)) {
-                    L.a0 = L.a0 + L.frac * L.s0; L.a1 = L.a1 + L.frac * L.s1; L.a2 = L.a2 + L.frac * L.s2;
-                    L.f0 = t0; L.f1 = t1; L.f2 = t2;
-                    ++L.it; L.st = Q_TP_ITER;
-                    continue;
-                }
+            double t0, t1, t2;
+            if (tpAccepts(v, L.ok, eIn, L.scale, L.prev, L.frac, t0, t1, t2)) {
+                L.a0 = L.a0 + L.frac * L.s0; L.a1 = L.a1 + L.frac * L.s1; L.a2 = L.a2 + L.frac * L.s2;
+                L.f0 = t0; L.f1 = t1; L.f2 = t2;
+                ++L.it; L.st = Q_TP_ITER;
+                continue;
             }
             ++L.k; L.frac *= .5; L.st = Q_TP_LS;
             continue;
