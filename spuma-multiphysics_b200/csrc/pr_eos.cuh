@@ -109,19 +109,6 @@ __device__ __forceinline__ void nasaEval(const PureSpecies& sp, double T, double
     }
 }
 
-// a*alpha(T) and its first two T-derivatives.
-__device__ __forceinline__ int alphaTerms(const PureSpecies& sp, double T, double& aa, double& da, double& d2a) {
-    const double sq = sqrt(T / sp.Tc), f = 1.0 + sp.kappa * (1.0 - sq);
-    if (fabs(f) <= 1e-14) return EOS_NONFINITE;
-    const double sign = f > 0 ? 1.0 : -1.0, q = fabs(f);
-    const double dq = -sign * sp.kappa / (2.0 * sp.Tc * sq);
-    const double d2q = sign * sp.kappa / (4.0 * sp.Tc * sp.Tc * sq * sq * sq);
-    aa = sp.a * q * q;
-    da = sp.a * (dq * q + q * dq);
-    d2a = sp.a * (d2q * q + 2.0 * dq * dq + q * d2q);
-    return fin(aa) && fin(da) && fin(d2a) && aa > 0 ? EOS_OK : EOS_NONFINITE;
-}
-
 __device__ __forceinline__ double cubicAt(double V, double bn, double cn, double dn) {
     return ((V + bn) * V + cn) * V + dn;
 }
