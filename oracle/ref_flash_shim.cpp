@@ -14,6 +14,7 @@
 //                                builds (reactiveGpuHem.cuh:31-36), threads optional
 //   ref_pr_evaluate_tp / _trho   ReactiveDevicePR::evaluateTPTrusted / evaluateTrhoTrusted
 //                                (reactiveDevicePR.h:575, :474) for EOS unit checks
+//   ref_pr_mix_tp / _trho        the same for a mixture table with mass fractions Y
 #include "reactiveDeviceFlash.h"
 #include <cstring>
 #include <thread>
@@ -110,6 +111,45 @@ int ref_pr_evaluate_trho(const void* image, int table, double T, double rho, int
     ReactiveDevicePR::State s{};
     const auto st = ReactiveDevicePR::evaluateTrhoTrusted(m->phase[table], T, rho, Y, s, chemical != 0);
     if (st == ReactiveDevicePR::Status::Success) packState(s, out, phase);
+    delete m;
+    return static_cast<int>(st);
+}
+
+// Mixture forms with mass fractions Y (table's ns entries); out receives the 15
+// properties of packState and then mu[0..ns).
+static void packMix(const ReactiveDevicePR::State& s, int ns, double* out, int* phaseOut) {
+    const double v[15] = {s.T, s.p, s.W, s.V, s.rho, s.e, s.h, s.s, s.cp, s.cv,
+                          s.alpha, s.kappaT, s.sound, s.dpdT, s.dpdV};
+    std::memcpy(out, v, sizeof(v));
+    for (int k = 0; k < ns; ++k) out[15 + k] = s.mu[k];
+    if (phaseOut) *phaseOut = s.phase;
+}
+
+int ref_pr_mix_trho(const void* image, int table, double T, double rho, const double* Yin, int chemical,
+                    double* out, int* phase) {
+    Model* m = new Model;
+    std::memcpy(m, image, sizeof(Model));
+    double Y[ReactiveDeviceFlash::maxSpecies]{};
+    const int ns = m->phase[table].ns;
+    for (int k = 0; k < ns; ++k) Y[k] = Yin[k];
+    ReactiveDevicePR::State s{};
+    const auto st = ReactiveDevicePR::evaluateTrhoTrusted(m->phase[table], T, rho, Y, s, chemical != 0);
+    if (st == ReactiveDevicePR::Status::Success) packMix(s, ns, out, phase);
+    delete m;
+    return static_cast<int>(st);
+}
+
+int ref_pr_mix_tp(const void* image, int table, double T, double p, const double* Yin, int choice, int chemical,
+                  double* out, int* phase) {
+    Model* m = new Model;
+    std::memcpy(m, image, sizeof(Model));
+    double Y[ReactiveDeviceFlash::maxSpecies]{};
+    const int ns = m->phase[table].ns;
+    for (int k = 0; k < ns; ++k) Y[k] = Yin[k];
+    ReactiveDevicePR::State s{};
+    const auto st = ReactiveDevicePR::evaluateTPTrusted(m->phase[table], T, p, Y,
+        static_cast<ReactiveDevicePR::RootChoice>(choice), s, chemical != 0);
+    if (st == ReactiveDevicePR::Status::Success) packMix(s, ns, out, phase);
     delete m;
     return static_cast<int>(st);
 }

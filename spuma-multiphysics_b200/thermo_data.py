@@ -3,7 +3,9 @@
 The numbers are physical input data of the reference's N2O case, restated here:
 * Peng-Robinson a [Pa m^6/kmol^2], b [m^3/kmol] and acentric factor, and the NASA9
   ideal-gas polynomials with their temperature ranges, from
-  examples/impinging-n2o-supercooled/cold-pr-148K.yaml:172-231 (N2O) and :52-111 (N2);
+  examples/impinging-n2o-supercooled/cold-pr-148K.yaml:172-231 (N2O), :52-111 (N2),
+  :112-171 (O2) and :232-282 (IC3H7OH); molecular weights from the elements
+  (N 14.007, O 15.999, C 12.011, H 1.008);
 * flash bounds and tolerances from examples/impinging-n2o-supercooled/cold-pr-148K-config.yaml:1-19;
 * molecular weight 44.013 kg/kmol, the value the reference records for N2O
   (results/real-fluid-v2-20260919/physical-model-manifest.json:147);
@@ -56,6 +58,37 @@ N2 = dict(
         [0.0, 0.0, 2.81166073, 0.00167067353, -6.79997428e-07, 1.32881379e-10,
          -1.02767442e-14, -869.811579, 6.6483805],
     ])
+
+O2 = dict(
+    name="O2", W=31.998, a=149772.3334866597, b=0.01982709144373723, omega=0.0222,
+    ranges=[148.0, 182.34, 200.0, 700.0, 3500.0],
+    nasa9=[
+        [-1008.7297701747248, 38.39770735944911, 2.905984455257836, 0.004775589822483856,
+         -2.042411776311955e-05, 4.147926112664399e-08, -2.4757854194367933e-11,
+         -1191.2736858521064, 7.404452100810184],
+        [0.0, 0.0, 3.487351092425565, 0.000171511121910552, -4.914758364368369e-07,
+         -3.668154124316966e-09, 1.714379649770826e-11, -1044.808865594206, 4.770321126998205],
+        [0.0, 0.0, 3.74403921, -0.00279740147, 9.80122558e-06, -1.03259643e-08,
+         3.79931247e-12, -1060.69827, 3.82132646],
+        [0.0, 0.0, 2.82012408, 0.00248211357, -1.51202094e-06, 4.48556201e-10,
+         -4.87305668e-14, -931.350148, 7.94914552],
+    ])
+
+IC3H7OH = dict(
+    name="IC3H7OH", W=60.096, a=1714219.955013869, b=0.06901149227230957, omega=0.6689,
+    ranges=[182.34, 300.0, 1490.0, 3500.0],
+    nasa9=[
+        [0.0, 0.0, 8.268209412358907, -0.08603907736461355, 0.000757315345210363,
+         -2.10122524775172e-06, 2.078637900786288e-09, -34964.21834756644, -3.480543450971361],
+        [0.0, 0.0, -1.25951086, 0.0499518902, -3.76786393e-05, 1.49318826e-08,
+         -2.3934462e-12, -34344.3869, 31.0096138],
+        [0.0, 0.0, 10.2736687, 0.0189903342, -6.50928762e-06, 9.8586399e-10,
+         -5.35101895e-14, -37781.2744, -29.2304676],
+    ])
+
+# The production gas of the reference's impingement case (cold-pr-148K.yaml:6-25):
+# air (N2, O2), N2O and isopropanol in one Peng-Robinson phase.
+AIR_N2O_IPA = (N2, O2, N2O, IC3H7OH)
 
 # Flash controls of the N2O case (cold-pr-148K-config.yaml:1-19).
 N2O_FLASH = dict(liquidTmin=148.0, liquidTc=309.52, Tmin=148.0, Tmax=3500.0,
@@ -122,6 +155,15 @@ def pure_model(sp=N2O, controls=N2O_FLASH, analytic_jacobian=1, scalar_recovery=
     for key in ("Tmin", "Tmax", "pmin", "pmax", "vtol", "etol", "mutol"):
         setattr(m, key, controls[key])
     m.enforceSpeciesTemperatureBounds = enforce_bounds
+    return m
+
+
+def mixture_model(species=AIR_N2O_IPA):
+    """A HEM model image whose gas table (phase 0) is the Peng-Robinson mixture of
+    `species`; used to evaluate mixture properties through the image's table."""
+    m = HemModel()
+    _fill_table(m.phase[0], list(species))
+    m.ns = len(species)
     return m
 
 
