@@ -91,6 +91,12 @@ IDEAL = {
 }
 
 
+MIXTURE = {
+    "properties_v3": ([_v, C.c_size_t, _v, _v, _v, C.c_int, C.c_int, _v, _v, _v, _v, C.c_char_p, C.c_size_t],
+                      C.c_int),
+}
+
+
 def load():
     """The loaded library with typed entry points (raises if it is absent)."""
     global _lib
@@ -99,7 +105,7 @@ def load():
             raise RuntimeError(f"{LIB_PATH} is missing: run __graft_entry__.build() (the CUDA library is required)")
         lib = C.CDLL(str(LIB_PATH))
         for table, prefix in ((TRANSPORT, "reactive_transport_"), (HEM, "reactive_gpu_hem_"),
-                              (IDEAL, "reactive_ideal_gas_")):
+                              (IDEAL, "reactive_ideal_gas_"), (MIXTURE, "reactive_b200_mixture_")):
             for name, (args, ret) in table.items():
                 fn = getattr(lib, prefix + name, None)
                 if fn is None:

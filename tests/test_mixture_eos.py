@@ -21,11 +21,12 @@ NS = 4
 D = C.POINTER(C.c_double)
 
 
-@pytest.fixture(scope="module")
-def libs(tmp_path_factory):
+def build_libs(directory):
+    """(host build of the library's evaluator, the reference's, the model image,
+    its gas table as a ReactiveB200Table)."""
     if not REF.exists():
         pytest.skip("oracle/_ref not built (make -C oracle)")
-    out = tmp_path_factory.mktemp("mix") / "libmixture_host.so"
+    out = Path(directory) / "libmixture_host.so"
     subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-fno-fast-math",
                     "-I", str(ROOT / "spuma-multiphysics_b200" / "csrc"),
                     str(ROOT / "tests" / "native" / "mixture_host_shim.cpp"), "-o", str(out)], check=True)
@@ -35,6 +36,11 @@ def libs(tmp_path_factory):
     table = Table()
     C.memmove(C.addressof(table), C.addressof(model.phase[0]), C.sizeof(Table))
     return ours, ref, image, table
+
+
+@pytest.fixture(scope="module")
+def libs(tmp_path_factory):
+    return build_libs(tmp_path_factory.mktemp("mix"))
 
 
 def evaluate(libs, T, value, Y, tp, choice=0, chem=1):
