@@ -167,6 +167,30 @@ def mixture_model(species=AIR_N2O_IPA):
     return m
 
 
+def production_model(species=AIR_N2O_IPA, condensable="N2O", controls=N2O_FLASH, analytic_jacobian=1,
+                     scalar_recovery=1, boundary_recovery=0, enforce_bounds=1):
+    """HEM model image of the reference's production configuration
+    (cold-pr-148K-config.yaml): the Peng-Robinson gas of `species` and one
+    condensed phase, the pure liquid of `condensable` (N2O), with the case's
+    bounds and tolerances."""
+    m = mixture_model(species)
+    k = [sp["name"] for sp in species].index(condensable)
+    _fill_table(m.phase[1], [species[k]])
+    m.nl = 1
+    m.condensable[0] = k
+    m.boundaryRecovery = boundary_recovery
+    m.scalarRecovery = scalar_recovery
+    m.analyticJacobian = analytic_jacobian
+    for i, sp in enumerate(species):
+        m.weights[i] = sp["W"]
+    m.liquidTmin[0] = controls["liquidTmin"]
+    m.liquidTc[0] = controls["liquidTc"]
+    for key in ("Tmin", "Tmax", "pmin", "pmax", "vtol", "etol", "mutol"):
+        setattr(m, key, controls[key])
+    m.enforceSpeciesTemperatureBounds = enforce_bounds
+    return m
+
+
 def model_bytes(model):
     return bytes(C.string_at(C.addressof(model), C.sizeof(model)))
 
