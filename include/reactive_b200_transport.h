@@ -114,6 +114,33 @@ int reactive_transport_set_capillary_v1(void* transport, const void* options);
 int reactive_transport_capillary_geometry_v1(void* transport, const double* cellColor,
     const double* fixedColor, double* surfaceEnergy, double* curvature, double* normalXYZ);
 int reactive_transport_capillary_profile_v1(void* transport, void* profile);
+/* Capillary-only entry points the solver references statically (so that a
+ * solver linked against this library resolves every symbol it names); each
+ * returns 1 with a message, as set_capillary_v1 does, and the solver reaches
+ * none of them without the capillary closure. Struct arguments are opaque here.
+ * src/reactiveTransport/reactiveCartesianTransport.h:34-35 (Cartesian descriptor),
+ * :44-49 (implicit geometry); reactiveTurbulence.h:69-81 (WALE PR properties);
+ * reactiveCapillaryResident.h:26-41 (resident capillary closure). */
+int reactive_transport_install_cartesian_v1(void* transport, const void* mesh);
+int reactive_transport_cartesian_info_v1(void* transport, void* info);
+int reactive_transport_set_implicit_v1(void* transport, const void* options);
+int reactive_transport_implicit_coefficients_v1(void* transport, double* output, const double* restore,
+    size_t count, size_t* required);
+int reactive_transport_set_wale_pr_model_v1(void* transport, const void* model);
+int reactive_transport_wale_pr_properties_v1(void* transport, const void* epoch, const double* q,
+    size_t qStride, const ReactiveThermoState* state);
+int reactive_transport_wale_pr_properties_v2(void* transport, const void* epoch, const double* q,
+    size_t qStride, const ReactiveThermoState* state, int statesUnchanged);
+int reactive_transport_wale_pr_profile_v1(void* transport, void* profile);
+int reactive_transport_capillary_resident_begin_v1(void* transport, size_t species, const double* q,
+    const double* liquid, const double* bulk, const ReactiveThermoState* states, const double* fixedColor,
+    double sigma, int equilibrium, int* fallback);
+int reactive_transport_capillary_resident_select_v1(void* transport, int iteration, void* view, int* fallback);
+int reactive_transport_capillary_resident_update_v1(void* transport, size_t count, double* residual,
+    int* fallback);
+int reactive_transport_capillary_resident_relax_v1(void* transport);
+int reactive_transport_capillary_resident_commit_v1(void* transport, ReactiveThermoState* states,
+    double* color, double* surfaceEnergy, double* curvature);
 
 /* ---- additive device-resident entry points (no reference counterpart; the
  * reference's resident path is advance_resident_v2 + download_conserved,

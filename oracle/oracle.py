@@ -11,6 +11,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF = HERE / "_ref"
+# the reference checkout (its sources feed the _ref/ builds and the fixture
+# scripts): $REFERENCE, by default the directory `reference` beside this repository
+REFERENCE = Path(os.environ.get("REFERENCE", HERE.parent.parent / "reference"))
 ORACLE_LIB = HERE / "liboracle.so"
 REF_TRANSPORT = REF / "libreactiveTransport_ref.so"
 REF_FLASH = REF / "libref_flash.so"

@@ -45,13 +45,16 @@ def build(force=False, verbose=False, extra=()):
         return LIB
     objdir = HERE / "_build"
     objdir.mkdir(exist_ok=True)
-    objects = []
     compile_flags = [f for f in FLAGS if f != "--shared"]
+    jobs = []
     for name, policy in SOURCES.items():
         obj = objdir / (name + ".o")
-        cmd = [nvcc(), *ARCH, *compile_flags, *policy, *extra, "-c", str(CSRC / name), "-o", str(obj)]
-        _run(cmd, verbose)
-        objects.append(str(obj))
+        jobs.append(([nvcc(), *ARCH, *compile_flags, *policy, *extra, "-c", str(CSRC / name), "-o", str(obj)], obj))
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        list(pool.map(lambda job: _run(job[0], verbose), jobs))
+    objects = [str(obj) for _, obj in jobs]
     _run([nvcc(), *ARCH, "--shared", *objects, "-o", str(LIB), "-lcudart", "-lpthread"], verbose)
     return LIB
 

@@ -46,7 +46,8 @@ def test_state_file_layout_and_round_trip(tmp_path):
 
 
 def test_reference_tool_reads_the_state_file(tmp_path):
-    tool = Path("/root/reference/tools/hem_checkpoint_batch.py")
+    from oracle import oracle
+    tool = oracle.REFERENCE / "tools" / "hem_checkpoint_batch.py"
     if not tool.is_file():
         pytest.skip("reference tree not present")
     spec = importlib.util.spec_from_file_location("hem_checkpoint_batch", tool)
