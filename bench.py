@@ -9,15 +9,20 @@ One step = CFL query, stage 0, HEM recovery of every cell, CFL recheck, stage 1,
 HEM recovery of every cell (both seeded with the step-start states), boundary
 ledger.
 
-Lines printed by rank 0 (one JSON object):
-  value   device-resident step, inputs resident in HBM, captured CUDA graph
-  e2e     the same steps through the reference-facing C ABI with host arrays
-          (upload_conserved / advance_resident_v2 / download_conserved /
-          reactive_gpu_hem_run_v1 per stage, as the reference solver calls it)
-  plain   the same device-resident kernels launched one by one (no graph)
+Keys of the one JSON line rank 0 prints:
+  value       FP64 device-resident step, inputs resident in HBM, one captured CUDA
+              graph per step (FP64 structured transport, work-queue FP64 flash)
+  mixed       the same step with FP32 transport arithmetic (compensated sums into
+              the FP64 state) and its per-field error against the FP64 run
+  plain_fp64  FP64, kernels launched one by one, flash one thread per cell
+  e2e         the same steps through the reference-facing C ABI with host arrays
+              (upload_conserved / advance_resident_v2 / download_conserved /
+              reactive_gpu_hem_run_v1 per stage, as the reference solver calls it)
+  roofline    the dominant kernel (the flash) against the measured FP64 FMA rate
 `--impl reference` times the reference's own CPU implementation (its transport
 built for the CPU, serial, and its flash compiled for the host on every core)
-on a bounded sample: one step of the same case at 40^3.
+on a bounded sample: the same case at 40^3, the same step window W+1..W+K;
+`same_window_40` puts the GPU's FP64 graph on that sample beside it.
 """
 import argparse
 import contextlib
@@ -47,6 +52,7 @@ UNIT = "Mcell-steps/s"
 FLOPS_PER_PHASE_EVAL = 525.1
 DRAM_BYTES_PER_PHASE_EVAL = 88.2
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
+REFERENCE_SAMPLE = 40  # cube size of the reference CPU arm's bounded sample
 
 
 def load_package():
@@ -61,12 +67,14 @@ def load_package():
     return sys.modules[name]
 
 
-def workload(n, precision="mixed (FP32 transport arithmetic, FP64 state and flash)"):
+def workload(n, precision="FP64 (state, transport and flash)"):
+    q_mb = 5 * 8 * n ** 3 / 1e6
     return {"workload": f"N2O impingement {n}^3 ({n ** 3:,} cells), 40 bar ambient, 2 liquid inlets, "
                         f"viscous + conduction + WALE, SSPRK2 + 2 HEM UV flashes per step, dt=1e-8 s",
             "cells": n ** 3, "faces": 3 * n * n * (n - 1) + 6 * n * n, "species": 1, "variables": 5,
-            "flux": "HLL", "precision": precision, "l2": "inputs larger than L2 (q alone 164 MB at 160^3; "
-                                                         "flash candidate records 8.6 GB)"}
+            "flux": "HLL", "precision": precision,
+            "l2": f"no flush: the step's inputs are larger than L2 (q alone {q_mb:.0f} MB, thermo states "
+                  f"{176 * n ** 3 / 1e6:.0f} MB)" if q_mb > 126 else "inputs smaller than L2 (not a timed headline)"}
 
 
 class ClockSampler:
@@ -214,6 +222,7 @@ class HostPath:
         assert self.lib.reactive_transport_set_wale_v1(self.t, C.byref(wale)) == 0
         self.version, self.attempt = 0, 0
         self.h2d = self.d2h = 0
+        self.library_s = 0.0
 
     def _pinned(self, shape, dtype):
         dtype = np.dtype(dtype)
@@ -256,8 +265,16 @@ class HostPath:
         if rc:
             raise RuntimeError(self.lib.reactive_transport_error(self.t).decode())
 
+    def _call(self, fn, *args):
+        """One library call, its wall time added to library_s."""
+        t0 = time.perf_counter()
+        try:
+            return fn(*args)
+        finally:
+            self.library_s += time.perf_counter() - t0
+
     def step(self, dt):
-        A, lib, t = self.A, self.lib, self.t
+        A, lib, t, call = self.A, self.lib, self.t, self._call
         # the step-start states stay untouched for the whole step; each flash
         # works in place on its own copy of them (ReactiveFoam.C:1011)
         start = self.states
@@ -265,14 +282,14 @@ class HostPath:
         dtc = C.c_double()
         tr0 = self._compact(start)
         prim = self._primitives(tr0)
-        self._check(lib.reactive_transport_stable_step_primitives(t, prim.ctypes.data_as(C.POINTER(A.Primitive)),
-                                                                  tr0.ctypes.data_as(C.POINTER(A.State)), .5, dt,
-                                                                  C.byref(dtc)))
+        self._check(call(lib.reactive_transport_stable_step_primitives, t,
+                         prim.ctypes.data_as(C.POINTER(A.Primitive)), tr0.ctypes.data_as(C.POINTER(A.State)), .5,
+                         dt, C.byref(dtc)))
         self.h2d += tr0.nbytes + prim.nbytes
         self.attempt += 1
-        self._check(lib.reactive_transport_begin_attempt(t, b"0" * 64, self.attempt))
+        self._check(call(lib.reactive_transport_begin_attempt, t, b"0" * 64, self.attempt))
         self.version += 1
-        self._check(lib.reactive_transport_upload_conserved(t, A.dptr(self.q), self.version))
+        self._check(call(lib.reactive_transport_upload_conserved, t, A.dptr(self.q), self.version))
         self.h2d += self.q.nbytes
         br = np.zeros(5)
         stage_states = None
@@ -284,15 +301,15 @@ class HostPath:
             self.version += 1
             after = A.Token(self.attempt, stage + 1, self.version)
             try:
-                self._check(lib.reactive_transport_advance_resident_v2(t, before, after, tr.ctypes.data_as(
-                    C.POINTER(A.State)), None, None, None, dt, A.dptr(br)))
-                self._check(lib.reactive_transport_download_conserved(t, after, A.dptr(self.q)))
+                self._check(call(lib.reactive_transport_advance_resident_v2, t, before, after,
+                                 tr.ctypes.data_as(C.POINTER(A.State)), None, None, None, dt, A.dptr(br)))
+                self._check(call(lib.reactive_transport_download_conserved, t, after, A.dptr(self.q)))
             finally:
                 copied.result()
             self.h2d += tr.nbytes
             self.d2h += self.q.nbytes
             self._energy()
-            ok, _ = self.hem.run(self.rho, self.e, out, success=self.ok)
+            ok, _ = call(self.hem.run, self.rho, self.e, out, self.ok)
             if not ok.all():
                 raise RuntimeError("HEM recovery failed")
             self.h2d += self.rho.nbytes + self.e.nbytes + out.nbytes
@@ -301,11 +318,11 @@ class HostPath:
                 stage_states = out
                 tr = self._compact(stage_states)  # reused by stage 1
                 prim = self._primitives(tr)
-                self._check(lib.reactive_transport_stable_step_primitives(
-                    t, prim.ctypes.data_as(C.POINTER(A.Primitive)), tr.ctypes.data_as(C.POINTER(A.State)), .5, dt,
-                    C.byref(dtc)))
+                self._check(call(lib.reactive_transport_stable_step_primitives, t,
+                                 prim.ctypes.data_as(C.POINTER(A.Primitive)), tr.ctypes.data_as(C.POINTER(A.State)),
+                                 .5, dt, C.byref(dtc)))
                 self.h2d += tr.nbytes + prim.nbytes
-        self._check(lib.reactive_transport_end_attempt(t, self.attempt, 1))
+        self._check(call(lib.reactive_transport_end_attempt, t, self.attempt, 1))
 
     def close(self):
         self._pool.shutdown()
@@ -376,11 +393,11 @@ def run_ours(args, rank, world):
     faces, volume = cases.cartesian_faces(n)
     init = cases.impingement(n, seed=2026 + rank)
     kw = dict(viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
-    # the headline form: mixed-precision structured transport + work-queue flash, one CUDA graph per step
-    mixed = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], precision="mixed",
-                 **kw)
-    # the same step in FP64 (graph-captured), and below its plain launch-by-launch form
-    flow = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], **kw)
+    case = (faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"])
+    # the headline form: FP64 structured transport + work-queue FP64 flash, one CUDA graph per step
+    flow = Flow(*case, **kw)
+    # the same step with FP32 transport arithmetic (compensated sums into the FP64 state)
+    mixed = Flow(*case, precision="mixed", **kw)
     setup_s = time.time() - t0
     lib = flow.lib
     rank_dev = int(os.environ.get("LOCAL_RANK", 0))
@@ -394,9 +411,10 @@ def run_ours(args, rank, world):
     def max_over_ranks_(x):
         return max_over_ranks(x, world, "cuda")
 
-    def timed_graph_steps(f, sample_clocks, snapshot=None):
+    def timed_graph_steps(f, sample_clocks, snapshot=None, steps=None):
         """W warm-up then K timed graph replays of flow f (CUDA events on its
         stream); `snapshot` (a list) receives the state the timed steps start from."""
+        steps = args.steps if steps is None else steps
         f.capture(DT)
         for _ in range(args.warmup):
             f.step(DT)
@@ -409,65 +427,63 @@ def run_ours(args, rank, world):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.nvtx.range_push("timed_step")
             a.record(f.stream)
-            for _ in range(args.steps):
+            for _ in range(steps):
                 f.step(DT)
             b.record(f.stream)
             barrier()
             torch.cuda.nvtx.range_pop()
         f.check(DT)
-        return max_over_ranks_(a.elapsed_time(b) / args.steps), clocks_
+        return max_over_ranks_(a.elapsed_time(b) / steps), clocks_
 
     # kernels launched per step: transport launches counted by the handle, plus
     # five per flash (inputs, queue, select, restart queue, restart select)
     stats0 = pkg._abi.Stats()
-    lib.reactive_transport_stats(mixed.transport, C.byref(stats0))
-    mixed.capture(DT)
+    lib.reactive_transport_stats(flow.transport, C.byref(stats0))
+    flow.capture(DT)
     stats1 = pkg._abi.Stats()
-    lib.reactive_transport_stats(mixed.transport, C.byref(stats1))
+    lib.reactive_transport_stats(flow.transport, C.byref(stats1))
     launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
-    tuned = {"mixed": mixed.autotune(), "fp64": flow.autotune()}
+    tuned = {"fp64": flow.autotune(), "mixed": mixed.autotune()}
     start = []
-    graph_ms, clocks = timed_graph_steps(mixed, True, start)
-    fp64_ms, _ = timed_graph_steps(flow, False)
+    graph_ms, clocks = timed_graph_steps(flow, True, start)
+    mixed_ms, _ = timed_graph_steps(mixed, False)
     # both runs took the same W + K steps from the same state
     mixed_errors = field_errors(mixed.conserved(), mixed.states(), flow.conserved(), flow.states())
+    mixed.close()
     # the flash alone (the headline's work-queue search) on exactly the states of
     # the timed steps: the headline flow goes back to the state its timed steps
     # started from and takes the same K steps again launch by launch (the same
     # kernels, so the same trajectory), with CUDA events on the flash's stream
     # around each step's first recovery and its work counters read around it
-    stream = mixed.stream
-    for dst, src in zip((mixed.qn, mixed.sn, mixed.tr), start):
+    stream = flow.stream
+    for dst, src in zip((flow.qn, flow.sn, flow.tr), start):
         dst.copy_(src)
     del start
     times, flash_phase_evals = [], 0.0
     for _ in range(args.steps):
-        mixed.stage0(DT)
-        mixed.hem.counters(stream.cuda_stream)
+        flow.stage0(DT)
+        flow.hem.counters(stream.cuda_stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push("flash_alone")
         e0.record(stream)
-        mixed._flash(mixed.q1, mixed.s1)
+        flow._flash(flow.q1, flow.s1)
         e1.record(stream)
         torch.cuda.nvtx.range_pop()
-        flash_phase_evals += mixed.hem.counters(stream.cuda_stream).phaseEvaluations
+        flash_phase_evals += flow.hem.counters(stream.cuda_stream).phaseEvaluations
         with torch.cuda.stream(stream):
-            mixed._launch_half(DT, 1)
+            flow._launch_half(DT, 1)
         times.append((e0, e1))
     stream.synchronize()
     flash_ms = statistics.mean(x.elapsed_time(y) for x, y in times)
     flash_phase_evals /= len(times)
-    mixed.check(DT)
-    mixed.close()
-    stream = flow.stream
+    flow.check(DT)
     # the reference's alternative search policy (closureSearch stableGasPrune,
     # ReactiveFoam.C:332-334): two-phase seeds skipped where the all-gas candidate
     # is stable; reported beside the headline, which uses the default search
     pruned_ms = None
     if not args.skip_plain:
         from spuma_multiphysics_b200.thermo_data import pure_model
-        pruned = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
-                      precision="mixed", model=pure_model(stable_gas_prune=1), **kw)
+        pruned = Flow(*case, model=pure_model(stable_gas_prune=1), **kw)
         pruned.autotune()
         pruned_ms, _ = timed_graph_steps(pruned, False)
         pruned.close()
@@ -475,24 +491,19 @@ def run_ours(args, rank, world):
     # (every candidate solved; results are the same bits)
     exhaustive_ms = None
     if not args.skip_plain:
-        full = Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], precision="mixed",
-                    **kw)
+        full = Flow(*case, **kw)
         full.two_phase_bound(False)
         full.autotune()
         exhaustive_ms, _ = timed_graph_steps(full, False)
         full.close()
-    stream = flow.stream
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cells = n ** 3
     value = world * cells / (graph_ms * 1e-3) / 1e6
 
-    # ---- plain launches, with CUDA events around every flash (dominant kernel)
+    # ---- plain launches: FP64, kernels one by one, the plain one-thread-per-cell flash
     plain_ms = None
-    plain_steps = min(args.steps, 3)  # about 2.9 s a step at 160^3
+    plain_steps = min(args.steps, 3)  # about 1.4 s a step at 160^3
     if not args.skip_plain:
-        flow.hem.counters(stream.cuda_stream)
-        ev = []
-        lib_t, t = flow.lib, flow.transport
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         a.record(stream)
         for _ in range(plain_steps):
@@ -507,17 +518,34 @@ def run_ours(args, rank, world):
         host = HostPath(pkg, faces, volume, flow, init["fixed_q"])
         host.step(DT)  # warm-up
         host.h2d = host.d2h = 0
+        host.library_s = 0.0
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             host.step(DT)
         barrier()
         e2e_s = max_over_ranks_((time.perf_counter() - t0) / args.e2e_steps)
+        library_s = host.library_s / args.e2e_steps
         e2e = {"value": world * cells / e2e_s / 1e6, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
                "h2d_bytes_per_step": host.h2d // args.e2e_steps, "d2h_bytes_per_step": host.d2h // args.e2e_steps,
-               "path": "reactive_transport_upload_conserved/advance_resident_v2/download_conserved + "
-                       "reactive_gpu_hem_run_v1, host arrays"}
+               "library_ms_per_step": library_s * 1e3, "caller_ms_per_step": (e2e_s - library_s) * 1e3,
+               "path": "the reference solver's calls with host arrays: stable_step_primitives, upload_conserved, "
+                       "2 x (advance_resident_v2, download_conserved, reactive_gpu_hem_run_v1); library = time "
+                       "inside those calls (their PCIe copies included), caller = the caller's own host "
+                       "bookkeeping (state compaction, primitives, energy)"}
         host.close()
+
+    # ---- the reference CPU arm's bounded sample, on the GPU: 40^3, same step window
+    same_window = None
+    if not args.skip_cpu:
+        fs, vs = cases.cartesian_faces(REFERENCE_SAMPLE)
+        i40 = cases.impingement(REFERENCE_SAMPLE, seed=2026)
+        f40 = Flow(fs, vs, i40["q"], i40["guess"], i40["fixed_q"], i40["fixed_guess"], **kw)
+        ms40, _ = timed_graph_steps(f40, False)
+        f40.close()
+        same_window = {"cells": REFERENCE_SAMPLE ** 3, "gpu_fp64_graph_ms_per_step": ms40,
+                       "gpu_fp64_graph_value": REFERENCE_SAMPLE ** 3 / (ms40 * 1e-3) / 1e6,
+                       "steps": f"{args.warmup + 1}-{args.warmup + args.steps}"}
 
     peaks = measured_peaks()
     fp64 = fp64_peak(lib, torch)
@@ -525,13 +553,13 @@ def run_ours(args, rank, world):
     if flash_ms:
         flops_per_eval = args.flops_per_phase_eval
         achieved = flops_per_eval * flash_phase_evals / (flash_ms * 1e-3) / 1e12 if flops_per_eval else None
-        roofline = {"bound": "fp64", "kernel": "HEM flash, one recovery of all cells (passSinglePhase + passQueue "
-                                                "+ selection + restarts): the first recovery of each timed step, "
-                                                "re-run from the timed steps' start state",
-                    "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                     "frac": achieved / fp64 if achieved else None,
-                    "peak_source": "measured in this run (FP64 FMA-chain probe)",
                     "traffic": args.dram_bytes_per_phase_eval * flash_phase_evals,
+                    "peak_source": "measured in this run (FP64 FMA-chain probe)",
+                    "kernel": "HEM flash, one recovery of all cells (passSinglePhase + passQueue + selection + "
+                              "restarts): the first recovery of each timed step, re-run from the timed steps' "
+                              "start state",
                     "traffic_note": "DRAM bytes per launch, ncu per-phase-evaluation figure x this launch's "
                                     "phase evaluations",
                     "ms_per_launch": flash_ms, "phase_evaluations_per_launch": flash_phase_evals,
@@ -548,43 +576,45 @@ def run_ours(args, rank, world):
         "ideal_gas_blast_64": adjoint_run(64, steps=50, every=10, probes=0)}
     cpu = None
     if rank == 0 and not args.skip_cpu:
-        cpu = cpu_reference(args, seconds_hint=20)
+        _, cpu = cpu_reference(args.warmup, args.cpu_steps, REFERENCE_SAMPLE)
+        same_window["reference_cpu_value"] = cpu["value"]
     clock = clocks.summary()
+    mixed_value = world * cells / (mixed_ms * 1e-3) / 1e6
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 state, f32 flux", "data": "synthetic (seeded N2O impingement initial state)",
-            "config": {**workload(n), "parallelism": f"{world} independent replicas (one per GPU)",
-                       "autotuned_launch_shapes": tuned},
-            "form": "mixed precision (FP32 gradients/WALE/face fluxes, compensated sums into the FP64 state), "
-                    "structured transport, work-queue FP64 flash with the two-phase admissibility bound "
-                    "(seeds that provably cannot converge are not solved; results bit-identical to the exhaustive "
-                    "search), one CUDA graph per step",
-            "mixed_field_error_vs_fp64": {"steps": args.warmup + args.steps, **mixed_errors},
-            "fp64_graph": {"ms_per_step": fp64_ms, "value": world * cells / (fp64_ms * 1e-3) / 1e6},
-            "stable_gas_prune_graph": None if pruned_ms is None else {
-                "ms_per_step": pruned_ms, "value": world * cells / (pruned_ms * 1e-3) / 1e6,
-                "search": "the reference's stableGasPrune closure search (not the headline)"},
-            "exhaustive_search_graph": None if exhaustive_ms is None else {
-                "ms_per_step": exhaustive_ms, "value": world * cells / (exhaustive_ms * 1e-3) / 1e6,
-                "form": "the headline step with the flash's two-phase admissibility bound off: every candidate "
-                        "of every cell solved (bit-identical results)"},
-            "plain_fp64": {"ms_per_step": plain_ms, "steps": plain_steps if plain_ms else None,
-                           "value": world * cells / (plain_ms * 1e-3) / 1e6 if plain_ms else None, "form": "FP64, kernels launched one by one, flash one thread per cell "
-                                               "running the whole candidate search (no work queue, no pruning)"},
-            "adjoint": adjoint,
-            "e2e": e2e, "roofline": roofline, "roofline_step_hbm": step_roofline, "cpu_baseline": cpu,
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N2O impingement initial state)",
+            "mixed": {"value": mixed_value, "ms_per_step": mixed_ms, "over_fp64_graph": mixed_value / value,
+                      "over_plain_fp64": graph_ms and plain_ms and plain_ms / mixed_ms,
+                      "field_error_vs_fp64": {"steps": args.warmup + args.steps, **mixed_errors}},
+            "plain_fp64": {"value": world * cells / (plain_ms * 1e-3) / 1e6 if plain_ms else None,
+                           "ms_per_step": plain_ms, "steps": plain_steps if plain_ms else None},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "same_window_40": same_window,
             "clocks": clock, "gpu_launches": launches_per_step * args.steps,
-            "fp64_peak_tflops": fp64, "setup_s": setup_s}
+            "config": {**workload(n, "FP64 (state, transport and flash)"),
+                       "parallelism": f"{world} independent replicas (one per GPU)",
+                       "autotuned_launch_shapes": tuned},
+            "form": "FP64 structured transport, work-queue FP64 flash with the two-phase admissibility bound, one "
+                    "CUDA graph per step; mixed = the same with FP32 transport arithmetic and compensated sums; "
+                    "plain_fp64 = kernels one by one, flash one thread per cell (no work queue, no bound)",
+            "roofline_step_hbm": step_roofline,
+            "stable_gas_prune_graph": None if pruned_ms is None else {
+                "ms_per_step": pruned_ms, "value": world * cells / (pruned_ms * 1e-3) / 1e6},
+            "exhaustive_search_graph": None if exhaustive_ms is None else {
+                "ms_per_step": exhaustive_ms, "value": world * cells / (exhaustive_ms * 1e-3) / 1e6},
+            "adjoint": adjoint, "fp64_peak_tflops": fp64, "setup_s": setup_s}
     flow.close()
     return line
 
 
-def cpu_reference(args, seconds_hint=20, n=40):
-    """One SSPRK2 + recovery step of the same case at 40^3 on the reference's CPU code:
-    its transport built for the CPU (serial by construction) and its flash compiled for
-    the host, threaded over all cores."""
+def cpu_reference(warmup, steps, n=40):
+    """The reference's own CPU code on the same case at n^3 (a bounded sample of
+    the 160^3 workload): its transport built for the CPU (serial by construction)
+    and its flash compiled for the host, threaded over all cores. The sample
+    advances `warmup` steps untimed and times the next `steps` steps, the same
+    step window (W+1 .. W+K) that the GPU arms time. Returns the per-step
+    samples and the baseline record."""
     sys.path.insert(0, str(ROOT / "tests"))
-    pkg = load_package()
+    load_package()
     from spuma_multiphysics_b200 import cases, thermo_data as td
     from oracle import oracle
     import rk_oracle
@@ -594,38 +624,38 @@ def cpu_reference(args, seconds_hint=20, n=40):
     image = td.model_bytes(td.pure_model())
     ref = rk_oracle.ReferenceFlow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
                                   VISCOSITY, CONDUCTIVITY, WALE_CW, image, threads=threads)
+    for _ in range(warmup):
+        ref.step(DT)
     samples = []
-    for _ in range(max(1, getattr(args, "cpu_steps", 1))):
+    for _ in range(steps):
         t0 = time.perf_counter()
         ref.step(DT)
         samples.append(time.perf_counter() - t0)
     ref.close()
     s = statistics.mean(samples)
-    return {"value": n ** 3 / s / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"one SSPRK2 step (2 transport stages + 2 recoveries of all cells) of the same case at "
-                      f"{n}^3 ({n ** 3:,} cells); transport serial (reference CPU build), flash on {threads} threads",
-            "seconds_per_step": s}
+    return samples, {"value": n ** 3 / s / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
+                     "sample": f"{n}^3 ({n ** 3:,} cells) sample of the same case, steps {warmup + 1}-{warmup + steps} "
+                               f"timed (the GPU arms' window); transport serial (reference CPU build), flash on "
+                               f"{threads} threads",
+                     "seconds_per_step": s}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    samples = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_reference(args)
-        if i >= args.warmup:
-            samples.append(r)
-    value = statistics.mean(r["value"] for r in samples)
-    cpu = dict(samples[0])
-    cpu["value"] = value
+    n = REFERENCE_SAMPLE
+    samples, cpu = cpu_reference(args.warmup, args.steps, n)
+    value = cpu["value"]
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(r["seconds_per_step"] for r in samples),
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(samples),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded N2O impingement initial state)", "impl": "reference",
-            "config": {**workload(args.size, "FP64 (the reference's CPU code)"),
-                       "parallelism": "reference CPU code on host cores"},
             "cpu_baseline": cpu, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                                         "d2h_bytes_per_step": 0}}
+                                         "d2h_bytes_per_step": 0},
+            "config": {**workload(n, "FP64 (the reference's CPU code)"),
+                       "sample_of": "the 160^3 impingement case (per-cell throughput; same physics, dt and step "
+                                    "window, 2 mm cells instead of 0.5 mm)",
+                       "parallelism": "reference CPU code on host cores"}}
 
 
 def run_flash_batch(args):
@@ -873,6 +903,8 @@ def main():
     p.add_argument("--skip-plain", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--cpu-steps", type=int, default=2,
+                   help="timed steps of the CPU baseline sample (after --warmup untimed steps)")
     p.add_argument("--flops-per-phase-eval", type=float, default=FLOPS_PER_PHASE_EVAL,
                    help="FP64 FLOPs per PR phase evaluation of the flash kernels (from an ncu capture)")
     p.add_argument("--dram-bytes-per-phase-eval", type=float, default=DRAM_BYTES_PER_PHASE_EVAL,

@@ -116,9 +116,11 @@ int reactive_gpu_hem_vjp_device_v3(void* hem, const double* conserved, size_t st
  * arrays like reactive_gpu_hem_run_device_v3 but needs no handle: its scratch is
  * one file-scope device array (about 9 MB, held by every GPU that loads this
  * library until the process exits) for at most 4,096 cells per call; larger
- * batches are rejected with an error. The first call on each device looks up the
- * array's address and should come before any stream capture. Calls share the
- * array: calls that overlap on the GPU race and must be serialised. */
+ * batches are rejected with an error. Every call looks up the array's address on
+ * the current device; the first call on each device also loads this library's
+ * device code there if needed and queries the flash kernel's occupancy, so make
+ * it before any stream capture. Calls share the array: calls that overlap on the
+ * GPU race and must be serialised. */
 int reactive_gpu_hem_run_static_v3(const void* model, size_t modelBytes, const double* conserved, size_t stride,
     size_t count, size_t variables, const ReactiveThermoState* seed, ReactiveThermoState* state,
     ReactiveTransportState* transport, int* success, void* stream, char* error, size_t errorSize);

@@ -18,7 +18,10 @@ extern "C" {
 
 /* Properties of `count` states. All pointers are device pointers:
  *   table  a ReactiveB200Table (the HEM model image's gas-table layout) with
- *          1 to 4 species;
+ *          1 to 4 species, uploaded by the caller; the host does not read it,
+ *          so the caller validates it first (a table with another layout or a
+ *          species count outside 1..4 gives status 1 per state, and a pointer
+ *          that is not a device allocation of the table's size faults);
  *   T      temperatures [K];
  *   value  densities [kg/m^3] for mode 0 (T, rho, Y), pressures [Pa] for mode 1
  *          (T, p, Y) on the root `choice` picks (0: the largest, as the reference

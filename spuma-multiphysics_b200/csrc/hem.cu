@@ -208,6 +208,10 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
         double eq = L.x.q, erm = L.rm, erp = L.rp, erT = L.rT;
         bool erv = L.rv;
         Eval* out = &v;
+        // A lane's own trial passes its kept gas-point terms (L.known); a helper's
+        // trial below passes none. The two agree bit for bit only because L.known
+        // is set solely in Q_SG_FINAL, never in a line-search state: a searching
+        // lane (tpSearch / fzSearch) has L.known false here.
         const GasPoint* kept = L.known ? &L.g : nullptr;
         int helpSlot = -1;
         if (nH > 0) {
@@ -1413,12 +1417,16 @@ int reactive_gpu_hem_run_counters_v3(void* raw, ReactiveGpuHemProfileV1* profile
 // at most kStaticHemCells cells (about 9 MB). Every GPU that loads this library
 // holds that array until the process exits.
 //
-// The array's device address is looked up with cudaGetSymbolAddress once per
-// device, on the first call made with that device current; make that first call
-// before capturing any stream. Every call uses the same array and finds the
-// previous call's contents there; the queue counters and work totals are cleared
-// at the start of each call. Calls that overlap on the GPU (two streams, two
-// host threads) race on the array: serialise them.
+// Every call looks up the array's device address with cudaGetSymbolAddress for
+// the current device (a cheap lookup, and never stale: after a cudaDeviceReset,
+// or under another context, the module is loaded again at a new address). The
+// first call on a device loads this library's device code there if it is not
+// loaded yet and queries the flash kernel's occupancy (kept per device): make
+// that first call before capturing any stream. Every call uses the same array
+// and finds the previous call's contents there; the queue counters and work
+// totals are cleared at the start of each call, and every candidate record a
+// call selects from is written by that call. Calls that overlap on the GPU (two
+// streams, two host threads) race on the array: serialise them.
 namespace rb200 {
 namespace {
 constexpr size_t kStaticHemCells = 4096;
@@ -1436,21 +1444,29 @@ constexpr size_t kStaticBytes = align256(kStaticTotals + NTOTALS * sizeof(unsign
 static __device__ __align__(256) unsigned char staticHemScratch[kStaticBytes];
 
 std::mutex staticHemMutex;
-void* staticHemAddress[64] = {};
+int staticHemBlocks[64] = {};  // work-queue grid per device ordinal (0: not yet queried)
 
-// Device address of the scratch array for the current device (looked up once).
+// Device address of the scratch array on the current device.
 unsigned char* staticScratch() {
+    void* ptr = nullptr;
+    check(cudaGetSymbolAddress(&ptr, staticHemScratch), "cudaGetSymbolAddress(static HEM scratch)");
+    require(ptr != nullptr, "Static HEM scratch has no device address");
+    return static_cast<unsigned char*>(ptr);
+}
+
+// Persistent work-queue grid for the current device (queried once per device).
+int staticQueueBlocks() {
     int device = 0;
     check(cudaGetDevice(&device), "cudaGetDevice");
-    require(device >= 0 && device < 64, "Device ordinal out of range for the static HEM scratch");
+    require(device >= 0 && device < 64, "Device ordinal out of range for the static HEM flash");
     std::lock_guard<std::mutex> lock(staticHemMutex);
-    if (!staticHemAddress[device]) {
-        void* ptr = nullptr;
-        check(cudaGetSymbolAddress(&ptr, staticHemScratch), "cudaGetSymbolAddress(static HEM scratch)");
-        require(ptr != nullptr, "Static HEM scratch has no device address");
-        staticHemAddress[device] = ptr;
+    if (!staticHemBlocks[device]) {
+        int perSm = 0, sms = 0;
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, passQueue, kPassThreads, 0), "occupancy");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attribute");
+        staticHemBlocks[device] = std::max(1, perSm) * std::max(1, sms);
     }
-    return static_cast<unsigned char*>(staticHemAddress[device]);
+    return staticHemBlocks[device];
 }
 
 __global__ void storeConstants(HemConst c, HemConst* dst) {
@@ -1487,11 +1503,7 @@ extern "C" int reactive_gpu_hem_run_static_v3(const void* model, size_t modelByt
         auto* counters = reinterpret_cast<unsigned*>(base + kStaticCounters);
         auto* totals = reinterpret_cast<unsigned long long*>(base + kStaticTotals);
         auto s = static_cast<cudaStream_t>(stream);
-        int perSm = 0, sms = 0, device = 0;
-        check(cudaGetDevice(&device), "cudaGetDevice");
-        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, passQueue, kPassThreads, 0), "occupancy");
-        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attribute");
-        const int blocks = std::max(1, perSm) * std::max(1, sms);
+        const int blocks = staticQueueBlocks();
         storeConstants<<<1, 1, 0, s>>>(hostConst, cst);
         check(cudaGetLastError(), "storeConstants");
         check(cudaMemsetAsync(counters, 0, NCOUNTERS * sizeof(unsigned), s), "clear counters");

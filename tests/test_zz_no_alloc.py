@@ -60,14 +60,19 @@ def _handle_call(hem, cons, n, seed, torch):
     return state.cpu().numpy().view(A.THERMO_DTYPE), transport.cpu().numpy(), ok.cpu().numpy()
 
 
-def test_static_flash_matches_handle_flash_on_two_calls():
+@pytest.mark.parametrize("prune", [0, 1])
+def test_static_flash_matches_handle_flash_on_two_calls(prune):
+    """Both closure searches: the reference's default, and stableGasPrune (its
+    two queue passes with the seed-cell compaction between them, whose second
+    pass solves only the cells the first pass left undecided)."""
     import torch
     fn = _bind(_lib.load())
-    image = td.model_bytes(td.pure_model())
-    for call, (n, seed_value) in enumerate([(MAX_CELLS, 101), (1500, 202)]):
+    model = td.pure_model(stable_gas_prune=prune)
+    image = td.model_bytes(model)
+    for call, (n, seed_value) in enumerate([(MAX_CELLS, 101 + prune), (1500, 202 + prune)]):
         cons, seed = _device_inputs(n, seed_value, torch)
         got_state, got_tr, got_ok = _static_call(fn, image, cons, n, seed, torch)
-        hem = GpuHem(capacity=n)
+        hem = GpuHem(model=model, capacity=n)
         ref_state, ref_tr, ref_ok = _handle_call(hem, cons, n, seed, torch)
         hem.close()
         assert np.array_equal(got_ok, ref_ok), f"call {call}: success flags differ"
@@ -78,6 +83,31 @@ def test_static_flash_matches_handle_flash_on_two_calls():
         assert np.array_equal(got_state[both].view(np.uint8), ref_state[both].view(np.uint8)), f"call {call}"
         assert np.array_equal(got_tr[both], ref_tr[both])
         assert np.max(np.abs(got_state["p"][both] / ref_state["p"][both] - 1)) <= 1e-9
+
+
+def test_static_flash_allocates_no_device_memory():
+    """After a first call (which may load the library's device code), a call
+    leaves the device's free memory unchanged: the entry point allocates nothing."""
+    import torch
+    fn = _bind(_lib.load())
+    image = td.model_bytes(td.pure_model())
+    n = 2048
+    cons, seed = _device_inputs(n, 303, torch)
+    state = torch.zeros_like(seed)
+    transport = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
+    ok = torch.zeros(n, dtype=torch.int32, device="cuda")
+    err = C.create_string_buffer(512)
+    stream = torch.cuda.current_stream().cuda_stream
+    args = (image, len(image), cons.data_ptr(), n, n, 5, seed.data_ptr(), state.data_ptr(), transport.data_ptr(),
+            ok.data_ptr(), stream, err, len(err))
+    assert fn(*args) == 0, err.value.decode()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        assert fn(*args) == 0, err.value.decode()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    assert int(ok.sum().item()) > 0.99 * n
 
 
 def test_static_flash_rejects_oversized_batch():
