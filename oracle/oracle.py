@@ -189,3 +189,56 @@ def cpu_threads():
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+# ---- the reference's CUDA scalar closure (oracle/_ref/libref_closure.so)
+CLOSURE_IN_DTYPE = np.dtype([("coeff", "<f8", (8,)), ("mix", "<f8", (3,)), ("W", "<f8"), ("b", "<f8"),
+                             ("r", "<f8"), ("rho", "<f8"), ("energy", "<f8"), ("T", "<f8"), ("lower", "<f8"),
+                             ("upper", "<f8"), ("tolerance", "<f8"), ("pmin", "<f8"), ("pmax", "<f8"),
+                             ("pr", "<i4"), ("enabled", "<i4")])
+CLOSURE_OUT_DTYPE = np.dtype([("p", "<f8"), ("T", "<f8"), ("energy", "<f8"), ("cv", "<f8"), ("success", "<i4"),
+                              ("iterations", "<i4")])
+_ref_closure = None
+
+
+def ref_closure_lib():
+    """The reference's scalar closure built for sm_100a (needs a GPU to run)."""
+    global _ref_closure
+    if _ref_closure is None:
+        path = REF / "libref_closure.so"
+        if not path.exists():
+            build()
+        lib = C.CDLL(str(path))
+        lib.reactive_closure_scalar_create_v1.argtypes = [C.c_size_t, C.c_char_p, C.c_size_t]
+        lib.reactive_closure_scalar_create_v1.restype = C.c_void_p
+        lib.reactive_closure_scalar_destroy_v1.argtypes = [C.c_void_p]
+        lib.reactive_closure_scalar_run_v1.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                                       C.c_char_p, C.c_size_t]
+        lib.reactive_closure_scalar_run_v1.restype = C.c_int
+        _ref_closure = lib
+    return _ref_closure
+
+
+def ref_closure_run(inputs):
+    """Run the reference's scalar closure kernel on CLOSURE_IN_DTYPE records (in
+    batches of its 65,536-record capacity); returns CLOSURE_OUT_DTYPE records."""
+    lib = ref_closure_lib()
+    err = C.create_string_buffer(1024)
+    cap = 65536
+    h = lib.reactive_closure_scalar_create_v1(cap, err, len(err))
+    if not h:
+        raise RuntimeError(err.value.decode())
+    inputs = np.ascontiguousarray(inputs, dtype=CLOSURE_IN_DTYPE)
+    out = np.zeros(len(inputs), dtype=CLOSURE_OUT_DTYPE)
+    profile = (C.c_char * 48)()
+    try:
+        for begin in range(0, len(inputs), cap):
+            chunk = inputs[begin:begin + cap]
+            res = out[begin:begin + cap]
+            rc = lib.reactive_closure_scalar_run_v1(h, chunk.ctypes.data, len(chunk), res.ctypes.data, profile, err,
+                                                    len(err))
+            if rc:
+                raise RuntimeError(err.value.decode())
+    finally:
+        lib.reactive_closure_scalar_destroy_v1(h)
+    return out
