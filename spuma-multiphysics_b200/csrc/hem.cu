@@ -158,10 +158,23 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
     L.known = false;
     Eval v;
     bool pending = false, exhausted = cells == 0;
+    // A short queue (fewer items than 32 per resident warp) is spread over the
+    // warps: a warp takes at most `cap` items per fetch, so a few long items (the
+    // frozen all-gas solves of cells inside the saturation dome late in a run) land
+    // in different warps whose other lanes, once the queue is drained, evaluate
+    // their line-search trials. Which lane runs an item changes no result.
+    const unsigned gridWarps = gridDim.x * (blockDim.x >> 5);
+    const unsigned cap = min(32u, max(1u, (total + gridWarps - 1) / gridWarps));
     for (;;) {
         for (int round = 0; round < 2; ++round) {
-            const bool need = L.st == Q_FREE && !exhausted;
-            const unsigned mask = __ballot_sync(0xffffffffu, need);
+            bool need = L.st == Q_FREE && !exhausted;
+            unsigned mask = __ballot_sync(0xffffffffu, need);
+            if (unsigned(__popc(mask)) > cap) {
+                unsigned rest = mask, take = 0;
+                for (unsigned i = 0; i < cap; ++i) { take |= rest & (0u - rest); rest &= rest - 1; }
+                mask = take;
+                need = (mask >> lane) & 1u;
+            }
             if (mask) {
                 unsigned base = 0;
                 if (lane == unsigned(__ffs(mask) - 1)) base = atomicAdd(counters + queueSlot, unsigned(__popc(mask)));
@@ -188,6 +201,10 @@ __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passQueue(
                     } else exhausted = true;
                 }
             }
+            // the item counter only grows: once one lane finds the queue drained, it
+            // is drained for every lane of the warp (capped fetches would otherwise
+            // discover it one lane at a time)
+            exhausted = __any_sync(0xffffffffu, exhausted);
             if (L.st != Q_FREE && !pending) pending = plan(C, L, v, records, n, stallLimitGas);
         }
         const bool any = __any_sync(0xffffffffu, pending);
