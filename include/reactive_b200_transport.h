@@ -159,6 +159,16 @@ int reactive_transport_stage_device_v3(void* transport, const double* qIn, doubl
 /* Writes the CFL step (or -1 when any face is invalid) to dt[0] on the device. */
 int reactive_transport_stable_step_device_v3(void* transport, const double* q,
     const ReactiveTransportState* state, double cfl, double maximum, double* dt, void* stream);
+/* The CFL query and the stage on the same device state in one call (no
+ * reference counterpart): the results are those of
+ * reactive_transport_stable_step_device_v3(q = qIn, state, cfl, maximum, dtOut)
+ * followed by reactive_transport_stage_device_v3(qIn, qOut, state, dt, stage,
+ * boundaryRate), bit for bit, with the cell primitives and (with WALE) the
+ * velocity gradients and eddy viscosities formed once for both. dt is the step
+ * taken; dtOut[0] receives the CFL step (or -1) on the device. */
+int reactive_transport_stage_cfl_device_v3(void* transport, const double* qIn, double* qOut,
+    const ReactiveTransportState* state, double dt, int stage, double* boundaryRate, double cfl,
+    double maximumStep, double* dtOut, void* stream);
 /* Structured Cartesian fast path of the device-resident entries (no reference
  * counterpart: the reference's Cartesian descriptor,
  * reactive_transport_install_cartesian_v1 in

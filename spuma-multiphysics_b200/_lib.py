@@ -46,6 +46,7 @@ TRANSPORT = {
     "fill_fixed_v3": ([_v, _v, _v, _v], C.c_int),
     "stage_device_v3": ([_v, _v, _v, _v, C.c_double, C.c_int, _v, _v], C.c_int),
     "stable_step_device_v3": ([_v, _v, _v, C.c_double, C.c_double, _v, _v], C.c_int),
+    "stage_cfl_device_v3": ([_v, _v, _v, _v, C.c_double, C.c_int, _v, C.c_double, C.c_double, _v, _v], C.c_int),
     "status_v3": ([_v, C.POINTER(C.c_uint), C.c_int, _v], C.c_int),
     "structured_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "precision_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),

@@ -551,10 +551,12 @@ struct Transport {
             waleProfile.cellsEvaluated += v.cells;
         }
     }
+    // gradientsReady: the gradients and eddy viscosities of `state` (and the
+    // primitives of qIn) were formed by the preceding launches on this stream.
     template <class R>
     void launchBoxStageT(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt, int stage,
-                         double* rate, R* grad, R* nut, cudaStream_t s) {
-        launchBoxGradientsT(state, grad, nut, s);
+                         double* rate, R* grad, R* nut, cudaStream_t s, bool gradientsReady = false) {
+        if (!gradientsReady) launchBoxGradientsT(state, grad, nut, s);
         if (rate) {
             bySpecies<LedgerK>(boxView(), qIn, state, static_cast<const R*>(grad), static_cast<const R*>(nut),
                                ledgerPartial, ledgerBlocks, s);
@@ -581,6 +583,14 @@ struct Transport {
                         double* rate, cudaStream_t s) {
         if (mixed) launchBoxStageT(qIn, qOut, state, dt, stage, rate, gradF, nutF, s);
         else launchBoxStageT(qIn, qOut, state, dt, stage, rate, v.grad, v.nut, s);
+    }
+    // The CFL query and then the stage on the same state: the CFL pass forms the
+    // gradients and eddy viscosities when WALE is on, and the stage reuses them.
+    void launchBoxStepStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt,
+                            int stage, double* rate, double cfl, double maximumStep, double* result, cudaStream_t s) {
+        launchBoxStep(state, cfl, maximumStep, result, s);
+        if (mixed) launchBoxStageT(qIn, qOut, state, dt, stage, rate, gradF, nutF, s, v.wale);
+        else launchBoxStageT(qIn, qOut, state, dt, stage, rate, v.grad, v.nut, s, v.wale);
     }
     void launchBoxStep(const ReactiveTransportState* state, double cfl, double maximumStep, double* result,
                        cudaStream_t s) {

@@ -186,10 +186,11 @@ class Flow:
         q_in, q_out, seed_out = (self.qn, self.q1, self.s1) if stage == 0 else (self.q1, self.qn, self.sn)
         if self.scalars:
             self._scalar_fields(self.sn if stage == 0 else self.s1)
-        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, q_in.data_ptr(), self.tr.data_ptr(), self.cfl,
-                                                                    dt, self.dt_cfl[stage:].data_ptr(), s))
-        _check(lib, t, lib.reactive_transport_stage_device_v3(t, q_in.data_ptr(), q_out.data_ptr(), self.tr.data_ptr(),
-                                                              dt, stage, self.boundary[stage].data_ptr(), s))
+        # the CFL query at q_in and the stage from q_in in one call (the results of
+        # stable_step_device_v3 then stage_device_v3, bit for bit)
+        _check(lib, t, lib.reactive_transport_stage_cfl_device_v3(
+            t, q_in.data_ptr(), q_out.data_ptr(), self.tr.data_ptr(), dt, stage, self.boundary[stage].data_ptr(),
+            self.cfl, dt, self.dt_cfl[stage:].data_ptr(), s))
         # both recoveries are seeded by the step-start states; the second one in place
         self._flash(q_out, seed_out, per_cell)
 
@@ -216,10 +217,9 @@ class Flow:
         lib, t, s = self.lib, self.transport, self.stream.cuda_stream
         if self.scalars:
             self._scalar_fields(self.sn)
-        _check(lib, t, lib.reactive_transport_stable_step_device_v3(t, self.qn.data_ptr(), self.tr.data_ptr(),
-                                                                    self.cfl, dt, self.dt_cfl.data_ptr(), s))
-        _check(lib, t, lib.reactive_transport_stage_device_v3(t, self.qn.data_ptr(), self.q1.data_ptr(),
-                                                              self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(), s))
+        _check(lib, t, lib.reactive_transport_stage_cfl_device_v3(
+            t, self.qn.data_ptr(), self.q1.data_ptr(), self.tr.data_ptr(), dt, 0, self.boundary[0].data_ptr(),
+            self.cfl, dt, self.dt_cfl.data_ptr(), s))
 
     def autotune(self):
         """Choose the launch shapes of this flow's transport and flash kernels by

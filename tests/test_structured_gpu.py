@@ -300,3 +300,65 @@ def test_host_entries_on_the_structured_box_match_the_face_graph(spec):
     assert box["dt"] == graph["dt"] and box["dt_prim"] == graph["dt_prim"]
     for key in ("br", "b0", "b1"):
         assert T.scaled_error(box[key][None], graph[key][None]) <= T.RHS_TOL
+
+
+@pytest.mark.parametrize("path", ["structured-fp64", "structured-mixed", "structured-hllc", "face-graph"])
+@pytest.mark.parametrize("spec", BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_cfl_stage_entry_equals_the_two_calls(spec, path):
+    """reactive_transport_stage_cfl_device_v3 (the CFL query and the stage in one
+    call) gives the CFL step, the staged state and the boundary ledger of
+    stable_step_device_v3 followed by stage_device_v3, bit for bit, for both stages."""
+    import torch
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    h = T.create(lib, 1, case, wale_cw=spec.get("wale"))
+    try:
+        if path == "face-graph":
+            assert L.reactive_transport_structured_v3(h, 0, None) == 0
+        elif path == "structured-mixed":
+            assert L.reactive_transport_precision_v3(h, 1, None) == 0
+        elif path == "structured-hllc":
+            assert L.reactive_transport_flux_v3(h, 1, None) == 0
+        stream = torch.cuda.current_stream().cuda_stream
+        nc, nv = case["nc"], case["nv"]
+        cells, fixed, nvar, nsp = (C.c_size_t() for _ in range(4))
+        assert L.reactive_transport_layout_v3(h, C.byref(cells), C.byref(fixed), C.byref(nvar), C.byref(nsp)) == 0
+        all_ = nc + fixed.value
+        q0 = torch.zeros((nv, all_), dtype=torch.float64, device="cuda")
+        q0[:, :nc] = torch.from_numpy(case["q"].T.copy()).cuda()
+        st = torch.zeros((all_, 7), dtype=torch.float64, device="cuda")
+        st[:nc] = torch.from_numpy(case["states"].view(np.float64).reshape(nc, 7)).cuda()
+        assert L.reactive_transport_fill_fixed_v3(h, q0.data_ptr(), st.data_ptr(), stream) == 0
+        dt = torch.zeros(1, dtype=torch.float64, device="cuda")
+        assert L.reactive_transport_stable_step_device_v3(h, q0.data_ptr(), st.data_ptr(), .23, .1, dt.data_ptr(),
+                                                          stream) == 0
+        torch.cuda.synchronize()
+        step = .1 * dt.item()
+        for stage in (0, 1):
+            outs = []
+            for combined in (False, True):
+                q_out = q0.clone() * 0.75  # stage 1 reads q_out as q^n
+                br = torch.zeros(nv, dtype=torch.float64, device="cuda")
+                d = torch.zeros(1, dtype=torch.float64, device="cuda")
+                if combined:
+                    rc = L.reactive_transport_stage_cfl_device_v3(h, q0.data_ptr(), q_out.data_ptr(), st.data_ptr(),
+                                                                  step, stage, br.data_ptr(), .23, .1, d.data_ptr(),
+                                                                  stream)
+                    assert rc == 0, lib.reactive_transport_error(h)
+                else:
+                    assert L.reactive_transport_stable_step_device_v3(h, q0.data_ptr(), st.data_ptr(), .23, .1,
+                                                                      d.data_ptr(), stream) == 0
+                    assert L.reactive_transport_stage_device_v3(h, q0.data_ptr(), q_out.data_ptr(), st.data_ptr(),
+                                                                step, stage, br.data_ptr(), stream) == 0
+                torch.cuda.synchronize()
+                outs.append((d.item(), q_out.cpu().numpy(), br.cpu().numpy()))
+            (d0, qa, ba), (d1, qb, bb) = outs
+            assert d0 == d1 and d0 > 0, (stage, d0, d1)
+            assert np.array_equal(qa, qb), stage
+            assert np.array_equal(ba, bb), stage
+        status = C.c_uint()
+        assert L.reactive_transport_status_v3(h, C.byref(status), 1, stream) == 0 and status.value == 0
+    finally:
+        lib.reactive_transport_destroy(h)
