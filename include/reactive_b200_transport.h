@@ -225,7 +225,8 @@ int reactive_transport_owned_cells_v3(void* transport, uint64_t begin, uint64_t 
 int reactive_transport_rate_vjp_v3(void* transport, const double* q, const ReactiveTransportState* state,
     const double* w, double* qBar, ReactiveTransportState* stateBar, void* stream);
 /* Launch-shape autotuner of the structured path (no reference counterpart).
- * Times the candidate block sizes of the stage (64, 96, 128 threads), gradient
+ * Times the candidates of the stage kernel (0: the shared-memory tiled form; or
+ * the per-cell form with 64, 96 (the default), 128 threads a block), gradient
  * (64, 128, 256) and CFL (64, 128, 256) kernels on this handle's problem (q and
  * state as stage_device_v3 takes them; neither is modified) and keeps the
  * fastest for later launches; results do not depend on the choice. Synchronous;
@@ -233,6 +234,12 @@ int reactive_transport_rate_vjp_v3(void* transport, const double* q, const React
  * a graph. chosen (may be NULL) receives {stage, gradient, CFL} block sizes. */
 int reactive_transport_autotune_v3(void* transport, const double* q, const ReactiveTransportState* state,
     void* stream, unsigned* chosen);
+/* Query (request NULL) or set the structured path's launch shapes {stage, gradient,
+ * CFL} (no reference counterpart): stage 0 is the shared-memory tiled stage
+ * kernel, 64/96/128 the per-cell kernel's block size; gradient and CFL block
+ * sizes 64/128/256. Results do not depend on them. active (may be NULL)
+ * receives the shapes in use. */
+int reactive_transport_launch_shapes_v3(void* transport, const unsigned* request, unsigned* active);
 /* Device-resident refresh of the WALE scalar fields for the device stage
  * entries (no reference counterpart: the reference fills them from the host or
  * from its own PR property pass). Stream-ordered and allocation-free, so it can

@@ -52,6 +52,7 @@ TRANSPORT = {
     "precision_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "flux_v3": ([_v, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "autotune_v3": ([_v, _v, _v, _v, C.POINTER(C.c_uint)], C.c_int),
+    "launch_shapes_v3": ([_v, _v, C.POINTER(C.c_uint)], C.c_int),
     "rate_vjp_v3": ([_v, _v, _v, _v, _v, _v, _v], C.c_int),
     "owned_cells_v3": ([_v, C.c_uint64, C.c_uint64], C.c_int),
 }

@@ -483,6 +483,262 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
     }
 }
 
+// ---------------------------------------------------------------------------
+// The stage kernel with its face stencils staged through shared memory.
+//
+// A block owns a kTileX x kTileY tile of an x-y plane and marches a chunk of
+// kTileZ planes in z. Per plane, the flux inputs of the tile's cells and of a
+// one-cell halo ring in x and y are loaded once into shared memory (SoA, in the
+// arithmetic type R); every x and y face of the tile's cells is then evaluated
+// ONCE into shared memory by one thread, instead of once by each of its two
+// cells; each column's z face is evaluated by the column's thread and carried in
+// registers to the next plane as that cell's lower face. Each own cell then sums
+// its faces in its face-graph incidence order (-z, -y, -x, +x, +y, +z, then the
+// box sides), so the stage results are bitwise those of cartRates.
+#ifndef RB200_TILE_Y
+#define RB200_TILE_Y 4
+#endif
+#ifndef RB200_TILE_MINBLOCKS
+#define RB200_TILE_MINBLOCKS 3
+#endif
+constexpr int kTileX = 32, kTileY = RB200_TILE_Y, kTileZ = 16;
+
+template <int NS, bool SGS> struct TileLayout {
+    static constexpr int NQ = NS + 4;
+    // flux inputs: q, u, p, T, rho, c, [cp, h], gradient, eddy viscosity
+    static constexpr int Q = 0, U = NQ, P = U + 3, T = P + 1, RHO = T + 1, C = RHO + 1, CP = C + 1,
+                         H = CP + (SGS ? 1 : 0), G = H + (SGS ? NS : 0), NUT = G + 9, FIELDS = NUT + 1;
+    static constexpr int PX = kTileX + 2, PY = kTileY + 2, SLOTS = PX * PY;
+    static constexpr int FX = (kTileX + 1) * kTileY, FY = kTileX * (kTileY + 1);
+    template <class R> static constexpr size_t bytes() {
+        return sizeof(R) * (size_t(FIELDS) * SLOTS + size_t(FX + FY) * NQ);
+    }
+};
+
+// One cell's flux inputs, rounded to R once (as asCell), with its gradient and
+// eddy viscosity, into shared-memory slot `slot`.
+template <int NS, class R, bool SGS>
+__device__ __forceinline__ void stageTileCell(const CartView& v, const double* __restrict__ q,
+                                              const ReactiveTransportState* __restrict__ st,
+                                              const R* __restrict__ grad, const R* __restrict__ nut, size_t c,
+                                              R* plane, int slot, bool viscous) {
+    using Lay = TileLayout<NS, SGS>;
+    constexpr int S = Lay::SLOTS;
+    CellData d;
+    loadCell<NS, SGS>(v, q, st, c, d, true);
+    const CellT<R> t = asCell<NS, R, SGS>(d);
+#pragma unroll
+    for (int k = 0; k < Lay::NQ; ++k) plane[(Lay::Q + k) * S + slot] = t.q[k];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) plane[(Lay::U + a) * S + slot] = t.u[a];
+    plane[Lay::P * S + slot] = t.p;
+    plane[Lay::T * S + slot] = t.T;
+    plane[Lay::RHO * S + slot] = t.rho;
+    plane[Lay::C * S + slot] = t.c;
+    if constexpr (SGS) {
+        plane[Lay::CP * S + slot] = t.cp;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) plane[(Lay::H + k) * S + slot] = t.h[k];
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) plane[(Lay::G + j) * S + slot] = viscous ? grad[size_t(j) * v.cells + c] : R(0);
+    plane[Lay::NUT * S + slot] = v.wale ? nut[c] : R(0);
+}
+
+template <int NS, class R, bool SGS>
+__device__ __forceinline__ void tileCell(const R* plane, int slot, CellT<R>& t, R* g, R& nu) {
+    using Lay = TileLayout<NS, SGS>;
+    constexpr int S = Lay::SLOTS;
+#pragma unroll
+    for (int k = 0; k < Lay::NQ; ++k) t.q[k] = plane[(Lay::Q + k) * S + slot];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) t.u[a] = plane[(Lay::U + a) * S + slot];
+    t.p = plane[Lay::P * S + slot];
+    t.T = plane[Lay::T * S + slot];
+    t.rho = plane[Lay::RHO * S + slot];
+    t.c = plane[Lay::C * S + slot];
+    t.cv = R(0);
+    if constexpr (SGS) {
+        t.cp = plane[Lay::CP * S + slot];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) t.h[k] = plane[(Lay::H + k) * S + slot];
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) g[j] = plane[(Lay::G + j) * S + slot];
+    nu = plane[Lay::NUT * S + slot];
+}
+
+// The same inputs for a cell read straight from global memory (the column's
+// next plane, and the plane below a chunk's first).
+template <int NS, class R, bool SGS>
+__device__ __forceinline__ void globalCell(const CartView& v, const double* __restrict__ q,
+                                           const ReactiveTransportState* __restrict__ st, const R* __restrict__ grad,
+                                           const R* __restrict__ nut, size_t c, bool viscous, CellT<R>& t, R* g,
+                                           R& nu) {
+    CellData d;
+    loadCell<NS, SGS>(v, q, st, c, d, true);
+    t = asCell<NS, R, SGS>(d);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) g[j] = viscous ? grad[size_t(j) * v.cells + c] : R(0);
+    nu = v.wale ? nut[c] : R(0);
+}
+
+template <int NS, class R, bool SGS = false>
+__global__ void __launch_bounds__(kTileX * kTileY, RB200_TILE_MINBLOCKS) cartRatesTile(CartView v, const double* __restrict__ q,
+                                                                const ReactiveTransportState* __restrict__ st,
+                                                                const R* __restrict__ grad,
+                                                                const R* __restrict__ nut, double* out,
+                                                                size_t outStride, int mode, double dt,
+                                                                unsigned* error) {
+    using Lay = TileLayout<NS, SGS>;
+    constexpr int NQ = Lay::NQ, S = Lay::SLOTS, PX = Lay::PX;
+    constexpr bool fp64 = sizeof(R) == sizeof(double);
+    extern __shared__ __align__(16) unsigned char tileMemory[];
+    R* plane = reinterpret_cast<R*>(tileMemory);
+    R* fx = plane + size_t(Lay::FIELDS) * S;   // x faces: [ly][lx], lx = 0..kTileX (face lx-1 | lx)
+    R* fy = fx + size_t(Lay::FX) * NQ;         // y faces: [ly][lx], ly = 0..kTileY (face ly-1 | ly)
+    const bool viscous = v.viscosity > 0 || v.wale;
+    const int tid = threadIdx.x, tx = tid % kTileX, ty = tid / kTileX;
+    const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z0 = blockIdx.z * kTileZ;
+    const int z1 = min(z0 + kTileZ, v.nz);
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool inside = gx < v.nx && gy < v.ny;
+    auto cellAt = [&](int x, int y, int z) { return size_t(x) + size_t(v.nx) * (size_t(y) + size_t(v.ny) * z); };
+    auto own = [&](int x, int y, int z) {
+        if (x < 0 || y < 0 || x >= v.nx || y >= v.ny || z < 0 || z >= v.nz) return false;
+        const size_t c = cellAt(x, y, z);
+        return c >= v.ownBegin && c < v.ownEnd;
+    };
+    bool bad = false, faceBad = false;
+    R down[NQ];  // the column's lower z face (the face between this plane and the one below)
+#pragma unroll
+    for (int kk = 0; kk < NQ; ++kk) down[kk] = R(0);
+    if (inside && z0 > 0 && z0 < z1 && (own(gx, gy, z0 - 1) || own(gx, gy, z0))) {
+        CellT<R> lo, hi;
+        R gl[9], gh[9], nl, nh;
+        globalCell<NS, R, SGS>(v, q, st, grad, nut, cellAt(gx, gy, z0 - 1), viscous, lo, gl, nl);
+        globalCell<NS, R, SGS>(v, q, st, grad, nut, cellAt(gx, gy, z0), viscous, hi, gh, nh);
+        faceFluxCart<NS, R, SGS>(v, 2, 1.0, v.area[2], v.dist[2], .5, 0, true, lo, hi, gl, gh, nl, nh, down, bad,
+                                 faceBad);
+    }
+    for (int z = z0; z < z1; ++z) {
+        __syncthreads();  // the previous plane's readers are done
+        // stage the plane: the tile's own slots, then the halo ring
+        if (inside)
+            stageTileCell<NS, R, SGS>(v, q, st, grad, nut, cellAt(gx, gy, z), plane, (ty + 1) * PX + tx + 1,
+                                      viscous);
+        constexpr int ring = 2 * kTileX + 2 * kTileY;
+        for (int h = tid; h < ring; h += kTileX * kTileY) {
+            int lx, ly;
+            if (h < kTileX) { lx = h; ly = -1; }
+            else if (h < 2 * kTileX) { lx = h - kTileX; ly = kTileY; }
+            else if (h < 2 * kTileX + kTileY) { lx = -1; ly = h - 2 * kTileX; }
+            else { lx = kTileX; ly = h - 2 * kTileX - kTileY; }
+            const int x = x0 + lx, y = y0 + ly;
+            if (x >= 0 && y >= 0 && x < v.nx && y < v.ny)
+                stageTileCell<NS, R, SGS>(v, q, st, grad, nut, cellAt(x, y, z), plane, (ly + 1) * PX + lx + 1,
+                                          viscous);
+        }
+        __syncthreads();
+        // every x and y face of the tile's own cells, once
+        for (int f = tid; f < Lay::FX + Lay::FY; f += kTileX * kTileY) {
+            const bool xFace = f < Lay::FX;
+            const int idx = xFace ? f : f - Lay::FX;
+            const int lx = xFace ? idx % (kTileX + 1) : idx % kTileX;
+            const int ly = xFace ? idx / (kTileX + 1) : idx / kTileX;
+            // lower cell (ax, ay) and upper cell (bx, by) in tile coordinates
+            const int ax = xFace ? lx - 1 : lx, ay = xFace ? ly : ly - 1;
+            const int bx = lx, by = ly;
+            const bool lowerOwn = ax >= 0 && ay >= 0 && own(x0 + ax, y0 + ay, z);
+            const bool upperOwn = bx < kTileX && by < kTileY && own(x0 + bx, y0 + by, z);
+            const bool exists = x0 + ax >= 0 && y0 + ay >= 0 && x0 + bx < v.nx && y0 + by < v.ny;
+            R* F = (xFace ? fx : fy) + size_t(idx) * NQ;
+            if (!exists || !(lowerOwn || upperOwn)) continue;
+            CellT<R> L, Rt;
+            R gL[9], gR[9], nL, nR;
+            tileCell<NS, R, SGS>(plane, (ay + 1) * PX + ax + 1, L, gL, nL);
+            tileCell<NS, R, SGS>(plane, (by + 1) * PX + bx + 1, Rt, gR, nR);
+            R flux[NQ];
+            const int axis = xFace ? 0 : 1;
+            faceFluxCart<NS, R, SGS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, L, Rt, gL, gR, nL, nR,
+                                     flux, bad, faceBad);
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) F[kk] = flux[kk];
+        }
+        // the column's upper z face
+        const int slot = (ty + 1) * PX + tx + 1;
+        R up[NQ];
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) up[kk] = R(0);
+        const bool hasUp = z + 1 < v.nz;
+        if (inside && hasUp && (own(gx, gy, z) || own(gx, gy, z + 1))) {
+            CellT<R> lo, hi;
+            R gl[9], gh[9], nl, nh;
+            tileCell<NS, R, SGS>(plane, slot, lo, gl, nl);
+            globalCell<NS, R, SGS>(v, q, st, grad, nut, cellAt(gx, gy, z + 1), viscous, hi, gh, nh);
+            faceFluxCart<NS, R, SGS>(v, 2, 1.0, v.area[2], v.dist[2], .5, 0, true, lo, hi, gl, gh, nl, nh, up, bad,
+                                     faceBad);
+        }
+        __syncthreads();
+        if (inside && own(gx, gy, z)) {
+            const size_t c = cellAt(gx, gy, z);
+            const double iv = v.invV[c];
+            R rate[NQ], comp[NQ];
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) rate[kk] = comp[kk] = R(0);
+            auto add = [&](const R* F, double sign) {
+#pragma unroll
+                for (int kk = 0; kk < NQ; ++kk) {
+                    if constexpr (fp64) rate[kk] += sign * F[kk] * iv;
+                    else twoSum(rate[kk], comp[kk], sign > 0 ? F[kk] : -F[kk]);
+                }
+            };
+            // internal faces in incidence order: -z, -y, -x, +x, +y, +z
+            if (z > 0) add(down, 1);
+            if (gy > 0) add(fy + size_t(ty * kTileX + tx) * NQ, 1);
+            if (gx > 0) add(fx + size_t(ty * (kTileX + 1) + tx) * NQ, 1);
+            if (gx + 1 < v.nx) add(fx + size_t(ty * (kTileX + 1) + tx + 1) * NQ, -1);
+            if (gy + 1 < v.ny) add(fy + size_t((ty + 1) * kTileX + tx) * NQ, -1);
+            if (hasUp) add(up, -1);
+            // box sides (-x, +x, -y, +y, -z, +z)
+            CellT<R> me;
+            R gMe[9], nuMe;
+            tileCell<NS, R, SGS>(plane, slot, me, gMe, nuMe);
+            CellData C;
+            const bool boundary = gx == 0 || gy == 0 || z == 0 || gx + 1 == v.nx || gy + 1 == v.ny || z + 1 == v.nz;
+            if (boundary) loadCell<NS, SGS>(v, q, st, c, C, true);
+#pragma unroll
+            for (int side = 0; side < 6; ++side) {
+                if (hasNeighbour(v, side, gx, gy, z)) continue;
+                const int axis = side >> 1;
+                const ReactiveTransportFace& f = sideFace(v, side, gx, gy, z);
+                CellData Rd;
+                boundaryRight<NS, SGS>(v, q, st, f, axis, C, Rd, true);
+                R flux[NQ];
+                faceFluxCart<NS, R, SGS>(v, axis, (side & 1) ? 1.0 : -1.0, f.area, f.distance, f.ownerWeight, f.kind,
+                                         false, me, asCell<NS, R, SGS>(Rd), gMe, gMe, nuMe, nuMe, flux, bad, faceBad);
+                add(flux, -1);
+            }
+            // the cell's own conserved variables in FP64 for the update
+            double qc[NQ];
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) qc[kk] = q[size_t(kk) * v.all + c];
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) {
+                const double r = fp64 ? double(rate[kk]) : (double(rate[kk]) + double(comp[kk])) * iv;
+                const size_t o = size_t(kk) * outStride + c;
+                if (mode == 0) out[o] = r;
+                else if (mode == 1) out[o] = qc[kk] + dt * r;
+                else out[o] = .5 * out[o] + .5 * (qc[kk] + dt * r);
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) down[kk] = up[kk];
+    }
+    if (bad) atomicOr(error, 1u);
+    if (faceBad) atomicOr(error, 2u);
+}
+
 // Wave/diffusion speed of one face (faceSpeeds of the face graph); -1 when invalid.
 template <bool SGS = false>
 __device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, double sgn, double dist, double w,

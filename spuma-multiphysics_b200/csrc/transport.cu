@@ -503,7 +503,10 @@ struct Transport {
     // times the candidates on the handle's own problem and keeps the fastest;
     // the results do not depend on them).
     struct BoxLaunch {
-        unsigned rates = 128, gradients = 256, steps = 256;
+        // rates 0 selects the shared-memory tiled stage kernel; the per-cell kernel
+        // with 96 threads a block is the default (the faster of the two on the
+        // 160^3 box on B200, FP64 and mixed; the autotuner times both)
+        unsigned rates = 96, gradients = 256, steps = 256;
     } launch;
     template <int NS> struct GradientsK {
         template <class R>
@@ -513,10 +516,36 @@ struct Transport {
         }
     };
     template <int NS> struct RatesK {
+        // block 0: the shared-memory tiled kernel; otherwise the per-cell kernel
+        // with that many threads a block (the two give the same bits)
+        template <class R, bool SGS>
+        static void tiled(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
+                          const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
+                          cudaStream_t s) {
+            const size_t bytes = TileLayout<NS, SGS>::template bytes<R>();
+            static thread_local int configured = -1;
+            int device = 0;
+            check(cudaGetDevice(&device), "cudaGetDevice");
+            if (configured != device) {
+                check(cudaFuncSetAttribute(cartRatesTile<NS, R, SGS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(bytes)),
+                      "tiled stage shared memory");
+                configured = device;
+            }
+            const dim3 grid((b.nx + kTileX - 1) / kTileX, (b.ny + kTileY - 1) / kTileY,
+                            (b.nz + kTileZ - 1) / kTileZ);
+            cartRatesTile<NS, R, SGS><<<grid, kTileX * kTileY, bytes, s>>>(b, q, st, grad, nut, out, stride, mode, dt,
+                                                                         error);
+        }
         template <class R>
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                         const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
                         unsigned block, cudaStream_t s) {
+            if (block == 0) {
+                if (b.sgs) tiled<R, true>(b, q, st, grad, nut, out, stride, mode, dt, error, s);
+                else tiled<R, false>(b, q, st, grad, nut, out, stride, mode, dt, error, s);
+                return;
+            }
             if (b.sgs)
                 cartRates<NS, R, true><<<gridFor(b.cells, block), block, 0, s>>>(b, q, st, grad, nut, out, stride,
                                                                                mode, dt, error);
@@ -672,7 +701,7 @@ struct Transport {
             if (mixed) launchBoxGradientsT(state, gradF, nutF, s);
             else launchBoxGradientsT(state, v.grad, v.nut, s);
         });
-        pick(launch.rates, {64u, 96u, 128u}, [&] { launchBoxStage(q, out, state, 1e-30, 0, nullptr, s); });
+        pick(launch.rates, {0u, 64u, 96u, 128u}, [&] { launchBoxStage(q, out, state, 1e-30, 0, nullptr, s); });
         pick(launch.steps, {64u, 128u, 256u}, [&] { launchBoxStep(state, .5, 1.0, reduceScratch + reduceBlocks, s); });
         check(cudaEventDestroy(a), "event");
         check(cudaEventDestroy(b), "event");

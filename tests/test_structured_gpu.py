@@ -362,3 +362,48 @@ def test_cfl_stage_entry_equals_the_two_calls(spec, path):
         assert L.reactive_transport_status_v3(h, C.byref(status), 1, stream) == 0 and status.value == 0
     finally:
         lib.reactive_transport_destroy(h)
+
+
+TILE_BOXES = BOXES + [
+    dict(dims=(70, 9, 37), ns=1, kinds="mixed", viscous=True, conduction=True, wale=.325),
+    dict(dims=(33, 6, 17), ns=2, kinds=(1, 2, 3, 1, 2, 1), viscous=True, conduction=True),
+]
+
+
+@pytest.mark.parametrize("path", ["fp64", "mixed", "hllc"])
+@pytest.mark.parametrize("spec", TILE_BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_tiled_stage_kernel_equals_per_cell_kernel(spec, path):
+    """The shared-memory tiled stage kernel (launch shape 0: each x and y face
+    evaluated once per plane into shared memory, z faces carried down the
+    column) gives the per-cell kernel's stage results bit for bit: both stages,
+    the CFL step and the boundary ledger, across tiles and z-chunks."""
+    import torch
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    h = T.create(lib, 1, case, wale_cw=spec.get("wale"))
+    try:
+        if path == "mixed":
+            assert L.reactive_transport_precision_v3(h, 1, None) == 0
+        elif path == "hllc":
+            assert L.reactive_transport_flux_v3(h, 1, None) == 0
+        stream = torch.cuda.current_stream().cuda_stream
+        runs = []
+        for stage_shape in (0, 128):
+            shapes = (C.c_uint * 3)(stage_shape, 256, 256)
+            active = (C.c_uint * 3)()
+            assert L.reactive_transport_launch_shapes_v3(h, shapes, active) == 0
+            assert list(active) == [stage_shape, 256, 256]
+            runs.append(_stage_pair(L, h, case, stream, torch))
+        tiled, per_cell = runs
+        assert tiled["status"] == per_cell["status"]
+        assert tiled["dt"] == per_cell["dt"]
+        assert np.array_equal(tiled["q1"], per_cell["q1"])
+        assert np.array_equal(tiled["qn"], per_cell["qn"])
+        assert np.array_equal(tiled["br0"], per_cell["br0"]) and np.array_equal(tiled["br1"], per_cell["br1"])
+        assert tiled["tail"] and per_cell["tail"]
+        bad = (C.c_uint * 3)(32, 256, 256)
+        assert L.reactive_transport_launch_shapes_v3(h, bad, None) == 1
+    finally:
+        lib.reactive_transport_destroy(h)
