@@ -134,7 +134,9 @@ class Flow:
         self.tr = torch.zeros((all_, 7), **f64)
         self.sn = torch.from_numpy(state0.view(np.uint8).copy()).to(dev)   # step-start thermo (seeds)
         self.s1 = torch.zeros_like(self.sn)                                   # stage-1 thermo
-        self.success = torch.zeros(self.cells, dtype=torch.int32, device=dev)
+        # per-cell success flags of each stage's recovery (a failure in either fails the step)
+        self.success_stages = torch.zeros((2, self.cells), dtype=torch.int32, device=dev)
+        self.success = self.success_stages[1]
         self.boundary = torch.zeros((2, self.nv), **f64)
         self.dt_cfl = torch.zeros(2, **f64)
         self.stream = torch.cuda.Stream(device=dev)
@@ -157,6 +159,8 @@ class Flow:
         self.graph = None
         self.graph_dt = None
         self.steps = 0
+        self.retries = 0           # dt halvings taken by advance()
+        self.last_failure = None   # why advance()'s last failed attempt failed
 
     # ------------------------------------------------------------------ step
     _CP_OFFSET = A.THERMO_DTYPE.fields["cp"][1]
@@ -170,13 +174,14 @@ class Flow:
         _check(lib, t, lib.reactive_transport_wale_scalar_fields_device_v3(
             t, thermo.data_ptr() + self._CP_OFFSET, None, fixed_cp, None, self._THERMO_DOUBLES, 1, s))
 
-    def _flash(self, q, out, per_cell=False):
+    def _flash(self, q, out, per_cell=False, stage=0):
         """Recovery of the own cells of q (SoA, stride cells+fixed) seeded by the
         step-start states, into `out` and the transport states."""
         b, e = self.own
         size = A.THERMO_DTYPE.itemsize
+        success = self.success_stages[stage]
         self.hem.run_device(q.data_ptr() + 8 * b, self.qn.shape[1], e - b, self.nv, self.sn.data_ptr() + size * b,
-                            out.data_ptr() + size * b, self.tr.data_ptr() + 56 * b, self.success.data_ptr() + 4 * b,
+                            out.data_ptr() + size * b, self.tr.data_ptr() + 56 * b, success.data_ptr() + 4 * b,
                             self.stream.cuda_stream, per_cell)
 
     def _launch_half(self, dt, stage, per_cell=False):
@@ -192,7 +197,7 @@ class Flow:
             t, q_in.data_ptr(), q_out.data_ptr(), self.tr.data_ptr(), dt, stage, self.boundary[stage].data_ptr(),
             self.cfl, dt, self.dt_cfl[stage:].data_ptr(), s))
         # both recoveries are seeded by the step-start states; the second one in place
-        self._flash(q_out, seed_out, per_cell)
+        self._flash(q_out, seed_out, per_cell, stage)
 
     def _launch_step(self, dt, per_cell=False):
         self._launch_half(dt, 0, per_cell)
@@ -265,6 +270,87 @@ class Flow:
                 self._launch_step(dt, per_cell)
         self.steps += 1
 
+    def _failure(self, dt, totals0=None):
+        """Why the last step failed, or None (synchronises): a recovery that
+        failed in any own cell at either stage, a CFL step (at the step start or at
+        RK1) that does not admit dt, a transport status bit (WALE / HLLC / scalar
+        field), or, with totals0 (the step-start totals), the boundary-corrected
+        mass and total-energy balances of the reference driver
+        (src/reactiveFoam/ReactiveFoam.C:1458-1470: mass within 1e-7 of the mass,
+        energy within 1e-9 of the energy scale)."""
+        self.stream.synchronize()
+        status = C.c_uint()
+        _check(self.lib, self.transport,
+               self.lib.reactive_transport_status_v3(self.transport, C.byref(status), 1, self.stream.cuda_stream))
+        own = slice(self.own[0], self.own[1])
+        failed = int((self.success_stages[:, own] == 0).any(dim=0).sum().item())
+        if failed:
+            return f"HEM recovery failed in {failed} cells"
+        cfl = self.dt_cfl.min().item()
+        if not (cfl > 0 and dt <= cfl * (1 + 1e-10)):
+            return f"dt={dt} exceeds the wave/diffusion CFL step {cfl}"
+        if status.value & 7:
+            return f"transport status {status.value}"
+        if totals0 is not None:
+            totals = self._totals()
+            ledger = torch.from_numpy(self.ledger(dt)).to(self.device)
+            balance = totals - totals0 + ledger
+            mass0 = float(totals0[:self.nv - 4].sum())
+            energy_scale = max(float(self._energy_magnitude()), mass0 * 1e5)
+            mass_error = abs(float(balance[:self.nv - 4].sum())) / mass0
+            energy_error = abs(float(balance[self.nv - 1])) / energy_scale
+            if not (np.isfinite(mass_error) and np.isfinite(energy_error) and mass_error < 1e-7
+                    and energy_error < 1e-9):
+                return f"boundary-corrected balance failed (mass {mass_error:.3e}, energy {energy_error:.3e})"
+        return None
+
+    def _totals(self):
+        """Volume integrals of the own cells' conserved variables (device, FP64)."""
+        b, e = self.own
+        if not hasattr(self, "_volume_device"):
+            self._volume_device = torch.from_numpy(self.volume).to(self.device)
+        with torch.cuda.stream(self.stream):
+            return (self.qn[:, b:e] * self._volume_device[b:e]).sum(dim=1)
+
+    def _energy_magnitude(self):
+        b, e = self.own
+        with torch.cuda.stream(self.stream):
+            return (self.qn[self.nv - 1, b:e].abs() * self._volume_device[b:e]).sum()
+
+    def advance(self, dt, max_retries=12, graph=True, balance=True):
+        """One accepted step with the reference driver's failure handling
+        (src/reactiveFoam/ReactiveFoam.C:1434-1494): the step-start conserved and
+        thermodynamic states are kept on the device; a step that fails (see
+        _failure; balance=False skips the balance check) is rolled back to them
+        and retried with half the step, at most max_retries times (and not below
+        1e-15 s). Returns the dt taken. When the retries run out the state is the
+        step-start state again and FlowError is raised. The retries launch the
+        kernels one by one (the captured graph holds the caller's dt)."""
+        if not hasattr(self, "_saved"):
+            self._saved = [torch.empty_like(self.qn), torch.empty_like(self.sn), torch.empty_like(self.tr)]
+        with torch.cuda.stream(self.stream):
+            for dst, src in zip(self._saved, (self.qn, self.sn, self.tr)):
+                dst.copy_(src)
+        totals0 = self._totals() if balance else None
+        steps0 = self.steps
+        attempt_dt = dt
+        for retry in range(max_retries + 1):
+            self.step(attempt_dt, graph=graph and attempt_dt == dt)
+            reason = self._failure(attempt_dt, totals0)
+            if reason is None:
+                return attempt_dt
+            with torch.cuda.stream(self.stream):
+                for dst, src in zip((self.qn, self.sn, self.tr), self._saved):
+                    dst.copy_(src)
+            self.steps = steps0
+            self.last_failure = reason
+            if retry == max_retries or attempt_dt * .5 <= 1e-15:
+                break
+            self.retries += 1
+            attempt_dt *= .5
+        self.stream.synchronize()
+        raise FlowError(f"step failed after {max_retries} retries with dt halved to {attempt_dt}: {reason}")
+
     def check(self, dt):
         """Host check after a run of steps: every flash succeeded, dt within CFL,
         no WALE failure (synchronises)."""
@@ -272,7 +358,7 @@ class Flow:
         status = C.c_uint()
         _check(self.lib, self.transport,
                self.lib.reactive_transport_status_v3(self.transport, C.byref(status), 1, self.stream.cuda_stream))
-        failed = int((self.success[self.own[0]:self.own[1]] == 0).sum().item())
+        failed = int((self.success_stages[:, self.own[0]:self.own[1]] == 0).any(dim=0).sum().item())
         cfl = self.dt_cfl.min().item()
         if status.value & 1:
             raise FlowError("WALE gradient/viscosity/traction became non-finite")

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from spuma_multiphysics_b200 import cases, thermo_data as td
-from spuma_multiphysics_b200.flow import Flow, field_errors
+from spuma_multiphysics_b200.flow import Flow, FlowError, field_errors
 import rk_oracle
 
 pytestmark = pytest.mark.gpu
@@ -106,3 +106,65 @@ def test_autotune_keeps_results():
         flow.close()
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1].view(np.uint8), runs[1][1].view(np.uint8))
+
+
+def _case_flow(n=12, **extra):
+    faces, volume, init = small_case(n)
+    kw = dict(viscosity=1.821e-5, conductivity=0.02587, wale_cw=0.325)
+    kw.update(extra)
+    return Flow(faces, volume, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"], **kw)
+
+
+def test_advance_halves_dt_until_the_step_is_admitted():
+    """A step 3.2 times the CFL step fails (CFL, and recoveries of the wrecked
+    stage states), is rolled back to the step-start state and retried with dt/2
+    and dt/4 (the reference driver's retry loop, ReactiveFoam.C:1434-1494); the
+    accepted step equals a direct step of dt/4 bit for bit."""
+    import torch
+    probe = _case_flow()
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert probe.lib.reactive_transport_stable_step_device_v3(probe.transport, probe.qn.data_ptr(),
+                                                              probe.tr.data_ptr(), probe.cfl, 1.0, out.data_ptr(),
+                                                              probe.stream.cuda_stream) == 0
+    probe.stream.synchronize()
+    cfl = out.item()
+    probe.close()
+    assert 0 < cfl < 1e-6
+    big = 3.2 * cfl
+    flow, ref = _case_flow(), _case_flow()
+    try:
+        taken = flow.advance(big)
+        assert taken == big / 4
+        assert flow.retries == 2 and flow.steps == 1
+        assert "CFL" in flow.last_failure or "recovery" in flow.last_failure
+        ref.step(big / 4, graph=False)
+        ref.check(big / 4)
+        assert np.array_equal(flow.conserved(), ref.conserved())
+        assert flow.states().tobytes() == ref.states().tobytes()
+        # an admitted step is taken once, with no retry
+        assert flow.advance(big / 4) == big / 4 and flow.retries == 2 and flow.steps == 2
+    finally:
+        flow.close()
+        ref.close()
+
+
+def test_advance_gives_up_after_the_retries_and_restores_the_step_start():
+    """One cell whose conserved energy no state can recover (set on the host
+    before the step) fails every attempt: after 12 halvings FlowError is raised
+    and the conserved and thermodynamic states are the step-start ones again."""
+    import torch
+    flow = _case_flow()
+    try:
+        c = 5
+        flow.qn[4, c] = -1e12  # internal energy far below any PR state: the recovery fails
+        torch.cuda.synchronize()
+        q0, s0 = flow.conserved(), flow.states().copy()
+        with pytest.raises(FlowError, match="retries"):
+            flow.advance(1e-9, max_retries=12)
+        assert flow.retries == 12
+        assert "recovery failed" in flow.last_failure
+        assert np.array_equal(flow.conserved(), q0)
+        assert flow.states().tobytes() == s0.tobytes()
+        assert flow.steps == 0
+    finally:
+        flow.close()
