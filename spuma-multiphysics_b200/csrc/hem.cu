@@ -18,6 +18,7 @@
 #include "hem_flash.cuh"
 #include "hem_common.cuh"
 #include "hem_queue.cuh"
+#include "hem_mixture.h"
 #include "common.cuh"
 #include "../../include/reactive_b200_hem.h"
 
@@ -701,6 +702,8 @@ struct HemDevice {
     int domeBuilt = 0;  // grid points of the two-phase bound (0: none for this model)
     size_t bytes = 0;
     std::vector<void*> blocks;
+    // a model image beyond the pure fluid: the multi-species flash (hem_mixture.cu)
+    MixtureFlash* mixture = nullptr;
 
     template <class T> T* alloc(size_t n) {
         void* p = nullptr;
@@ -710,6 +713,7 @@ struct HemDevice {
         return static_cast<T*>(p);
     }
     ~HemDevice() {
+        if (mixture) mixtureDestroy(mixture);
         if (stream) cudaStreamSynchronize(stream);
         if (down) cudaStreamSynchronize(down);
         for (void* p : blocks) cudaFree(p);
@@ -870,11 +874,19 @@ void* create(const void* raw, size_t bytes, size_t capacity, bool hostPath, char
         std::memcpy(&m, raw, sizeof(m));
         std::unique_ptr<HemDevice> d(new HemDevice);
         const std::string why = validateAndDerive(m, d->hostConst);
-        require(why.empty(), why.c_str());
         int count = 0;
         check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
         require(count > 0, "No CUDA device");
         check(cudaGetDevice(&d->device), "cudaGetDevice");
+        if (!why.empty()) {
+            // not the pure-fluid scope: the multi-species flash, if the image is within its scope
+            std::string whyMixture;
+            d->mixture = mixtureCreate(m, capacity, d->device, whyMixture);
+            if (!d->mixture) throw std::runtime_error(why + "; " + whyMixture);
+            d->capacity = capacity;
+            d->bytes = mixtureDeviceBytes(d->mixture);
+            return d.release();
+        }
         check(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         d->capacity = capacity;
         d->cst = d->alloc<HemConst>(1);
@@ -1127,6 +1139,14 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count && count <= d.capacity, "CUDA HEM batch exceeds capacity");
         rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+        if (d.mixture) {
+            ReactiveGpuHemProfileV1 p{};
+            p.abiVersion = 1;
+            p.structBytes = sizeof(p);
+            rb200::mixtureRun(d.mixture, q, energy, count, states, success, p);
+            *profile = p;
+            return 0;
+        }
         d.ensureHostPath();
         const auto begin = std::chrono::steady_clock::now();
         // Pipelined in chunks: the uploads of later chunks (copy stream up) and
@@ -1241,6 +1261,7 @@ int reactive_gpu_hem_run_resident_v1(void* raw, const double* q, const double* e
                            && profile->structBytes == sizeof(*profile),
                        "Invalid resident CUDA HEM batch arguments");
         auto& d = *static_cast<HemDevice*>(raw);
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count && count <= d.capacity, "Resident CUDA HEM batch exceeds capacity");
         rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
@@ -1299,6 +1320,7 @@ int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t st
                            && variables >= 5,
                        "Invalid device HEM batch arguments");
         auto& d = *static_cast<HemDevice*>(raw);
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count <= d.capacity, "Device HEM batch exceeds capacity");
         auto s = static_cast<cudaStream_t>(stream);
@@ -1318,6 +1340,7 @@ int reactive_gpu_hem_two_phase_bound_v3(void* raw, int request, int* active, cha
     try {
         rb200::require(raw && request >= -1 && request <= 1, "Invalid two-phase bound request");
         auto& d = *static_cast<HemDevice*>(raw);
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(request != 1 || d.domeBuilt, "This model has no two-phase bound (see the header)");
         if (request >= 0) {
@@ -1343,6 +1366,7 @@ int reactive_gpu_hem_vjp_device_v3(void* raw, const double* conserved, size_t st
                            && barStride >= count && variables == 5,
                        "Invalid HEM VJP arguments (pure fluid: variables = 5)");
         auto& d = *static_cast<HemDevice*>(raw);
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         auto s = static_cast<cudaStream_t>(stream);
         rb200::hemStateVjp<<<rb200::gridFor(count, 128), 128, 0, s>>>(d.cst, conserved, stride, count, state,
@@ -1362,6 +1386,7 @@ int reactive_gpu_hem_autotune_v3(void* raw, const double* conserved, size_t stri
         rb200::require(raw && conserved && seed && count && stride >= count && variables >= 5,
                        "Invalid HEM autotune arguments");
         auto& d = *static_cast<HemDevice*>(raw);
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count <= d.capacity, "CUDA HEM batch exceeds capacity");
         rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
@@ -1406,6 +1431,7 @@ int reactive_gpu_hem_run_counters_v3(void* raw, ReactiveGpuHemProfileV1* profile
     try {
         rb200::require(raw && profile, "Invalid HEM counter query");
         auto& d = *static_cast<HemDevice*>(raw);
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         ReactiveGpuHemProfileV1 p{};
         p.abiVersion = 1;

@@ -1,0 +1,24 @@
+// Host interface of the multi-species HEM flash (hem_mixture.cu) for the
+// reactive_gpu_hem_* entry points in hem.cu.
+#pragma once
+#include <cstddef>
+#include <string>
+#include "../../include/reactive_b200_types.h"
+
+namespace rb200 {
+
+struct MixtureFlash;
+
+// A handle for a model image outside the pure-fluid scope: a Peng-Robinson gas of
+// 1 to 4 species with 0 to 2 pure condensed liquids. Returns nullptr and the
+// reason when the image is invalid or outside this build's scope.
+MixtureFlash* mixtureCreate(const ReactiveB200HemModel& model, size_t capacity, int device, std::string& why);
+void mixtureDestroy(MixtureFlash* flash);
+size_t mixtureDeviceBytes(const MixtureFlash* flash);
+// The reference's run_v1 contract on host arrays: q cell-major (count x ns species
+// densities), energy the internal energy density, states the seeds in and the
+// results out (a failed cell keeps its seed), success per cell. Synchronous.
+void mixtureRun(MixtureFlash* flash, const double* q, const double* energy, size_t count,
+                ReactiveThermoState* states, int* success, ReactiveGpuHemProfileV1& profile);
+
+}  // namespace rb200

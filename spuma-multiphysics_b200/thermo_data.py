@@ -191,6 +191,37 @@ def production_model(species=AIR_N2O_IPA, condensable="N2O", controls=N2O_FLASH,
     return m
 
 
+def two_liquid_model(species=AIR_N2O_IPA, condensables=("N2O", "IC3H7OH"), controls=N2O_FLASH, scalar_recovery=1,
+                     boundary_recovery=1, stable_gas_prune=0, enforce_bounds=1):
+    """HEM model image with two condensed phases: the Peng-Robinson gas of
+    `species` and the pure liquids of `condensables` (N2O and isopropanol, the
+    configuration the reference's captured recovery inputs were taken with),
+    the boundary recovery on, and the Newton Jacobian by finite differences
+    (analyticJacobian 0). N2O's liquid range is the case's; isopropanol's runs
+    from the start of its NASA data to its Peng-Robinson critical temperature."""
+    m = mixture_model(species)
+    names = [sp["name"] for sp in species]
+    for i, name in enumerate(condensables):
+        k = names.index(name)
+        _fill_table(m.phase[i + 1], [species[k]])
+        m.condensable[i] = k
+        if name == "N2O":
+            m.liquidTmin[i], m.liquidTc[i] = controls["liquidTmin"], controls["liquidTc"]
+        else:
+            m.liquidTmin[i], m.liquidTc[i] = species[k]["ranges"][0], critical_point(species[k])[0]
+    m.nl = len(condensables)
+    m.boundaryRecovery = boundary_recovery
+    m.scalarRecovery = scalar_recovery
+    m.analyticJacobian = 0
+    m.stableGasPrune = stable_gas_prune
+    for i, sp in enumerate(species):
+        m.weights[i] = sp["W"]
+    for key in ("Tmin", "Tmax", "pmin", "pmax", "vtol", "etol", "mutol"):
+        setattr(m, key, controls[key])
+    m.enforceSpeciesTemperatureBounds = enforce_bounds
+    return m
+
+
 def model_bytes(model):
     return bytes(C.string_at(C.addressof(model), C.sizeof(model)))
 
