@@ -99,7 +99,7 @@ int reactive_transport_wale_primitives_v1(void* transport, const ReactiveTranspo
  * message, as the reference's own CPU build does for its CUDA-only paths
  * (src/reactiveTransport/reactiveTransport.cpp:1613-1630):
  * src/reactiveTransport/reactiveTransport.h:93-102 (NASA-generated gas properties),
- * :48-54 (capillary), src/reactiveTransport/reactiveTurbulence.h:47-85 (WALE PR properties). */
+ * src/reactiveTransport/reactiveTurbulence.h:47-85 (WALE PR properties). */
 int reactive_transport_set_gas_thermo(void* transport, const ReactiveGasThermoSpecies* species,
     size_t count, const ReactiveGasThermoRegion* regions, size_t regionCount,
     const int64_t* liquidSpecies, size_t liquids);
@@ -110,14 +110,30 @@ int reactive_transport_rhs_gas(void* transport, const double* q, const ReactiveT
     const ReactiveGasPartition* partition, double* rhs, double* boundaryRate);
 int reactive_transport_gas_properties_resident(void* transport, const ReactiveTransportState* state,
     const ReactiveGasPartition* partition, double* gasY, double* gasH);
-int reactive_transport_set_capillary_v1(void* transport, const void* options);
+/* The diffuse capillary closure on the face graph (src/reactiveTransport/
+ * reactiveTransport.h:48-54, reactiveTransport.cpp:859-962): a resolved material
+ * color with its Green-Gauss interface geometry
+ * (src/reactiveInterface/reactiveUnstructuredInterface.h) and the balanced
+ * contact-preserving HLLC face core (reactiveBalancedCapillary.h:55-142). Install
+ * once before stepping, on a non-mechanical model with one frozen liquid
+ * inventory (variables = species + 5). Each geometry call replaces the cell and
+ * fixed colors (each in [0, 1]) and rebuilds the gradient, normal, area density,
+ * curvature and surface energy sigma |grad c| [J/m^3]; curvature and normalXYZ
+ * (packed XYZ per cell) may be NULL. An identical request without normalXYZ
+ * returns the published outputs without device work. Every stage then consumes
+ * this exact geometry; a face whose balanced flux cannot be formed fails the host
+ * entries with "Invalid capillary face flux" and sets bit 3 of the device status
+ * word. The capillary model keeps the face graph (the structured box path needs
+ * variables = species + 4). */
+int reactive_transport_set_capillary_v1(void* transport, const ReactiveCapillaryOptionsV1* options);
 int reactive_transport_capillary_geometry_v1(void* transport, const double* cellColor,
     const double* fixedColor, double* surfaceEnergy, double* curvature, double* normalXYZ);
-int reactive_transport_capillary_profile_v1(void* transport, void* profile);
-/* Capillary-only entry points the solver references statically (so that a
- * solver linked against this library resolves every symbol it names); each
- * returns 1 with a message, as set_capillary_v1 does, and the solver reaches
- * none of them without the capillary closure. Struct arguments are opaque here.
+int reactive_transport_capillary_profile_v1(void* transport, ReactiveCapillaryProfileV1* profile);
+/* Entry points of the Cartesian implicit surface geometry, the WALE PR
+ * properties and the resident capillary-flash loop, which the solver references
+ * statically (so that a solver linked against this library resolves every
+ * symbol it names); each returns 1 with a message, and the solver reaches them
+ * only with those options selected. Struct arguments are opaque here.
  * src/reactiveTransport/reactiveCartesianTransport.h:34-35 (Cartesian descriptor),
  * :44-49 (implicit geometry); reactiveTurbulence.h:69-81 (WALE PR properties);
  * reactiveCapillaryResident.h:26-41 (resident capillary closure). */
@@ -254,7 +270,8 @@ int reactive_transport_wale_scalar_fields_device_v3(void* transport, const doubl
     const double* fixedCp, const double* fixedH, size_t cpStride, size_t hStride, void* stream);
 /* Device status word: bit 0 = WALE gradient/viscosity/traction non-finite,
  * bit 1 = an HLLC face could not be formed, bit 2 = an invalid WALE scalar
- * field from wale_scalar_fields_device_v3. Reading
+ * field from wale_scalar_fields_device_v3, bit 3 = a capillary face flux or
+ * liquid inventory that could not be formed. Reading
  * it synchronises the handle's work on `stream`; clear=1 resets it afterwards. */
 int reactive_transport_status_v3(void* transport, unsigned* status, int clear, void* stream);
 

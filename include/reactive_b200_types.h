@@ -13,6 +13,7 @@
  *   ReactiveTransportOptionsV21/ProfileV21  src/reactiveTransport/reactiveTransportV21.h:4-16
  *   ReactiveWaleOptionsV1 / ProfileV1       src/reactiveTransport/reactiveTurbulence.h:12-19
  *   ReactiveWaleScalarOptionsV1 / ProfileV1 src/reactiveTransport/reactiveTurbulence.h:28-35
+ *   ReactiveCapillaryOptionsV1 / ProfileV1  src/reactiveTransport/reactiveTransport.h:38-47
  *   ReactiveGasThermoSpecies/Region/Partition src/reactiveThermo/reactiveGasThermo.h:12-21
  *   ReactiveThermoState                     src/reactiveThermo/reactiveThermo.h:11-19
  *   ReactiveGpuHemProfileV1                 src/reactiveThermo/reactiveGpuHem.h:14-21
@@ -110,6 +111,22 @@ typedef struct ReactiveWaleScalarProfileV1 {
     uint64_t fieldUploads, fieldUploadBytes, workspaceBytes;
 } ReactiveWaleScalarProfileV1;
 
+/* The diffuse capillary closure: surface tension sigma [N/m], the capillary
+ * wave Courant number (0, 1], the geometry threshold on |grad c| * V^(1/3)
+ * below which a cell has no interface normal, and the species whose liquid
+ * inventory is conserved variable species+4. */
+typedef struct ReactiveCapillaryOptionsV1 {
+    uint32_t abiVersion, structBytes;
+    double sigma, capillaryCfl, geometryEpsilon;
+    int64_t condensableSpecies;
+} ReactiveCapillaryOptionsV1;
+
+typedef struct ReactiveCapillaryProfileV1 {
+    uint32_t abiVersion, structBytes;
+    uint64_t geometryBuilds, geometryCells, geometryKernels, faceFluxBuilds;
+    uint64_t colorUploadBytes, geometryDownloadBytes, capillaryWorkspaceBytes;
+} ReactiveCapillaryProfileV1;
+
 typedef struct ReactiveGasThermoSpecies {
     uint64_t regionOffset, regionCount;
     double gasConstant;
@@ -196,6 +213,8 @@ static_assert(sizeof(ReactiveTransportState) == 56, "state layout");
 static_assert(sizeof(ReactiveThermoState) == 176, "thermo state layout");
 static_assert(sizeof(ReactiveWaleScalarOptionsV1) == 24, "WALE scalar options layout");
 static_assert(sizeof(ReactiveWaleScalarProfileV1) == 32, "WALE scalar profile layout");
+static_assert(sizeof(ReactiveCapillaryOptionsV1) == 40, "capillary options layout");
+static_assert(sizeof(ReactiveCapillaryProfileV1) == 64, "capillary profile layout");
 static_assert(sizeof(ReactiveGpuHemOutputV1) == 184, "HEM output layout");
 static_assert(sizeof(ReactiveB200HemModel) == 47448, "HEM model image layout");
 static_assert(offsetof(ReactiveB200HemModel, stableGasPrune) == 45004, "HEM model image layout");

@@ -83,6 +83,17 @@ class WaleScalarProfile(C.Structure):
         (n, C.c_uint64) for n in ("fieldUploads", "fieldUploadBytes", "workspaceBytes")]
 
 
+class CapillaryOptions(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32), ("sigma", C.c_double),
+                ("capillaryCfl", C.c_double), ("geometryEpsilon", C.c_double), ("condensableSpecies", C.c_int64)]
+
+
+class CapillaryProfile(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32)] + [
+        (n, C.c_uint64) for n in ("geometryBuilds", "geometryCells", "geometryKernels", "faceFluxBuilds",
+                                  "colorUploadBytes", "geometryDownloadBytes", "capillaryWorkspaceBytes")]
+
+
 class ThermoState(C.Structure):
     _fields_ = [(k, C.c_double) for k in (
         "p", "T", "rho", "e", "entropy", "soundFrozen", "soundEquilibrium",

@@ -42,6 +42,9 @@ TRANSPORT = {
     "wale_scalar_profile_v1": ([_v, C.POINTER(A.WaleScalarProfile)], C.c_int),
     "wale_scalar_fields_v1": ([_v, _d, _d, _d, _d], C.c_int),
     "wale_scalar_fields_device_v3": ([_v, _v, _v, _v, _v, C.c_size_t, C.c_size_t, _v], C.c_int),
+    "set_capillary_v1": ([_v, C.POINTER(A.CapillaryOptions)], C.c_int),
+    "capillary_geometry_v1": ([_v, _d, _d, _d, _d, _d], C.c_int),
+    "capillary_profile_v1": ([_v, C.POINTER(A.CapillaryProfile)], C.c_int),
     "layout_v3": ([_v, C.POINTER(C.c_size_t)] * 1 + [C.POINTER(C.c_size_t)] * 3, C.c_int),
     "fill_fixed_v3": ([_v, _v, _v, _v], C.c_int),
     "stage_device_v3": ([_v, _v, _v, _v, C.c_double, C.c_int, _v, _v], C.c_int),

@@ -77,6 +77,13 @@ struct Transport {
     ReactiveWaleProfileV1 waleProfile{1, sizeof(ReactiveWaleProfileV1), 0, 0, 0, 0};
     ReactiveWaleScalarProfileV1 waleScalarProfile{1, sizeof(ReactiveWaleScalarProfileV1), 0, 0, 0};
     bool scalarCp = false, scalarH = false;  // WALE scalar fields present for the next stage
+    // diffuse capillary closure: the published geometry and the host copies of
+    // its inputs and outputs that let an identical request skip the device
+    ReactiveCapillaryProfileV1 capillaryProfile{1, sizeof(ReactiveCapillaryProfileV1), 0, 0, 0, 0, 0, 0, 0};
+    bool colorReady = false, geometryShadowValid = false;
+    std::vector<double> colorShadow, fixedColorShadow, energyShadow, curvatureShadow;
+    uint64_t geometryBuildsSkipped = 0;
+    double* colorDevice = nullptr;  // cells + fixed
     std::string physicalHash;
     uint64_t attemptId = 0, lastAttempt = 0, tokenStage = 0;
     bool attemptOpen = false;
@@ -721,6 +728,7 @@ struct Transport {
 
     // ------------------------------------------------------- reference contract
     void prepareResident(const ReactiveTransportState* states, const double* gasY, const double* gasH, bool transport) {
+        requireCapillaryGeometry();
         requireScalarFields(transport);
         if (!structured) ensureGraphScalarWork();
         uploadState(states);
@@ -743,14 +751,19 @@ struct Transport {
                 cellGradients<<<gridFor(v.cells, 256), 256, 0, stream>>>(g);
                 launched();
             }
+            if (v.capillary) check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
             faceWork<<<gridFor(v.faces, 128), 128, 0, stream>>>(g);
             launched();
             ++deviceProfile.transportFaceLaunches;
-            if (v.wale) {
+            if (v.wale || v.capillary) {
                 unsigned status = 0;
                 download(&status, flags, 1);
                 finish();
-                require(!status, "Nonfinite WALE traction/energy flux; stage remains uncommitted");
+                if (v.capillary) {
+                    require(!(status & kCapillaryBit), "Invalid capillary face flux");
+                    capillaryProfile.faceFluxBuilds += cfg.faces;
+                }
+                require(!(status & ~kCapillaryBit), "Nonfinite WALE traction/energy flux; stage remains uncommitted");
             }
         } else launchSpeeds(stateDevice, stream);
     }
@@ -845,6 +858,90 @@ struct Transport {
         stageDt = dt;
         ++stats.stages;
     }
+    // Diffuse capillary closure (src/reactiveTransport/reactiveTransport.cpp:859-886).
+    void setCapillary(const ReactiveCapillaryOptionsV1& options) {
+        require(options.abiVersion == 1 && options.structBytes == sizeof(options) && std::isfinite(options.sigma)
+                    && options.sigma > 0 && std::isfinite(options.capillaryCfl) && options.capillaryCfl > 0
+                    && options.capillaryCfl <= 1 && std::isfinite(options.geometryEpsilon)
+                    && options.geometryEpsilon >= 0 && options.geometryEpsilon < 1,
+                "Invalid capillary options ABI/model");
+        require(!v.capillary && !attemptOpen && !stats.stages && !highestVersion,
+                "Capillary model must be installed once before stepping");
+        require(!cfg.mechanical && cfg.variables == cfg.species + 5 && options.condensableSpecies >= 0
+                    && size_t(options.condensableSpecies) < cfg.species,
+                "Capillary model needs one mapped conserved liquid inventory");
+        const size_t before = arena.bytes;
+        // one block: color (all), gradient and normal (3 x cells each), area
+        // density, curvature and surface energy (cells each)
+        double* block = arena.get<double>(v.all + product(cfg.cells, 9));
+        check(cudaMemsetAsync(block, 0, (v.all + product(cfg.cells, 9)) * sizeof(double), stream), "memset");
+        colorDevice = block;
+        v.color = block;
+        v.cGrad = block + v.all;
+        v.cNormal = v.cGrad + 3 * cfg.cells;
+        v.cArea = v.cNormal + 3 * cfg.cells;
+        v.cCurv = v.cArea + cfg.cells;
+        v.cEnergy = v.cCurv + cfg.cells;
+        v.capError = flags;
+        v.sigma = options.sigma;
+        v.capCfl = options.capillaryCfl;
+        v.geomEps = options.geometryEpsilon;
+        v.capSpecies = size_t(options.condensableSpecies);
+        v.capillary = true;
+        finish();
+        capillaryProfile.capillaryWorkspaceBytes = arena.bytes - before + sizeof(uint32_t);
+    }
+    // src/reactiveTransport/reactiveTransport.cpp:887-962 (diffuse geometry).
+    void capillaryGeometry(const double* cellColor, const double* fixedColor, double* energy, double* curvature,
+                           double* normal) {
+        require(v.capillary && cellColor && energy && (!cfg.fixed || fixedColor),
+                "Missing capillary model, color or surface-energy output");
+        const auto unit = [](double c) { return std::isfinite(c) && c >= 0 && c <= 1; };
+        require(firstFailure(cfg.cells, [&](size_t c) { return unit(cellColor[c]); }) == cfg.cells,
+                "Invalid material color");
+        for (size_t c = 0; c < cfg.fixed; ++c) require(unit(fixedColor[c]), "Invalid fixed material color");
+        const auto same = [](const std::vector<double>& shadow, const double* x, size_t n) {
+            return shadow.size() == n && (n == 0 || std::memcmp(shadow.data(), x, n * sizeof(double)) == 0);
+        };
+        if (!normal && colorReady && geometryShadowValid && (!curvature || !curvatureShadow.empty())
+            && same(colorShadow, cellColor, cfg.cells) && same(fixedColorShadow, fixedColor, cfg.fixed)) {
+            std::memcpy(energy, energyShadow.data(), cfg.cells * sizeof(double));
+            if (curvature) std::memcpy(curvature, curvatureShadow.data(), cfg.cells * sizeof(double));
+            ++geometryBuildsSkipped;
+            return;
+        }
+        geometryShadowValid = false;
+        colorReady = false;
+        check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
+        upload(colorDevice, cellColor, cfg.cells);
+        upload(colorDevice + cfg.cells, fixedColor, cfg.fixed);
+        const uint64_t previousKernels = stats.kernelLaunches;
+        const unsigned blocks = unsigned(std::min<size_t>((cfg.cells + 255) / 256, 148 * 16));
+        interfaceGradient<<<blocks, 256, 0, stream>>>(v);
+        launched();
+        interfaceCurvature<<<blocks, 256, 0, stream>>>(v);
+        launched();
+        download(energy, v.cEnergy, cfg.cells);
+        if (curvature) download(curvature, v.cCurv, cfg.cells);
+        if (normal) download(normal, v.cNormal, product(cfg.cells, 3));
+        unsigned status = 0;
+        download(&status, flags, 1);
+        finish();
+        require(!(status & kCapillaryBit), "Invalid capillary geometry");
+        colorReady = true;
+        ++capillaryProfile.geometryBuilds;
+        colorShadow.assign(cellColor, cellColor + cfg.cells);
+        fixedColorShadow.assign(fixedColor, fixedColor + cfg.fixed);
+        energyShadow.assign(energy, energy + cfg.cells);
+        if (curvature) curvatureShadow.assign(curvature, curvature + cfg.cells);
+        else curvatureShadow.clear();
+        geometryShadowValid = true;
+        capillaryProfile.geometryCells += cfg.cells;
+        capillaryProfile.geometryKernels += stats.kernelLaunches - previousKernels;
+        capillaryProfile.colorUploadBytes += (cfg.cells + cfg.fixed) * sizeof(double);
+        capillaryProfile.geometryDownloadBytes +=
+            cfg.cells * sizeof(double) * (1 + (curvature ? 1 : 0) + (normal ? 3 : 0));
+    }
     void installWale(const ReactiveWaleOptionsV1& options) {
         require(options.abiVersion == 1 && options.structBytes == sizeof(options), "Invalid WALE options ABI");
         require(!v.wale && !highestVersion && !stats.stages && !stats.stepQueries && profile.conservedUploads == 0
@@ -869,8 +966,10 @@ struct Transport {
         require(std::isfinite(options.turbulentPrandtl) && std::isfinite(options.turbulentSchmidt)
                     && options.turbulentPrandtl >= 0 && options.turbulentSchmidt >= 0,
                 "Invalid turbulent Prandtl/Schmidt number");
-        require(options.turbulentSchmidt == 0 || cfg.variables == cfg.species + 4,
-                "WALE total-species mixing requires equilibrium phase partition; frozen inventories are unsupported");
+        require(options.turbulentSchmidt == 0 || cfg.variables == cfg.species + 4
+                    || (v.capillary && cfg.variables == cfg.species + 5 && v.capSpecies < cfg.species),
+                "WALE total-species mixing requires equilibrium phase partition or a mapped capillary liquid "
+                "inventory; frozen non-capillary inventories are unsupported");
         const size_t before = arena.bytes;
         if (options.turbulentPrandtl > 0) v.mixCp = arena.get<double>(v.all);
         if (options.turbulentSchmidt > 0) {
@@ -959,6 +1058,9 @@ struct Transport {
         ++waleScalarProfile.fieldUploads;
     }
     // Stage / CFL preconditions (src/reactiveTransport/reactiveTransport.cpp:1395-1397, 1415-1416).
+    void requireCapillaryGeometry() const {
+        require(!v.capillary || colorReady, "Capillary geometry must be uploaded for this stage");
+    }
     void requireScalarFields(bool transport) const {
         if (!v.sgs) return;
         if (transport)

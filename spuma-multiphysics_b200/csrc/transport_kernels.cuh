@@ -60,7 +60,22 @@ struct GraphView {
     const double* spH = nullptr;                     // SoA ns x all, effective species enthalpies
     double* sgsWork = nullptr;                       // SoA 3 x faces: diffusion, sumJ, carrier flux
     int* sgsCarrier = nullptr;                       // faces
+    // capillary closure: a resolved material color (cells + fixed) with its
+    // diffuse interface geometry and the balanced HLLC face core; the conserved
+    // vector carries the liquid inventory of species capSpecies at ns + 4
+    bool capillary = false;
+    size_t capSpecies = 0;
+    double sigma = 0, capCfl = 0, geomEps = 0;
+    const double* color = nullptr;                   // all
+    double* cGrad = nullptr;                         // cells x 3 (packed per cell)
+    double* cNormal = nullptr;                       // cells x 3, from color 1 towards color 0
+    double* cArea = nullptr;                         // cells: |grad color|
+    double* cCurv = nullptr;                         // cells
+    double* cEnergy = nullptr;                       // cells: sigma |grad color|
+    unsigned* capError = nullptr;                    // bit kCapillaryBit on failure
 };
+
+constexpr unsigned kCapillaryBit = 8u;
 
 // The species-mixing record of one face (zero diffusion: no mixing flux).
 struct SgsFace {
@@ -184,6 +199,204 @@ __global__ void faceSpeeds(GraphView v) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Capillary closure (src/reactiveInterface/reactiveUnstructuredInterface.h and
+// reactiveBalancedCapillary.h): the color's Green-Gauss gradient, interface
+// normal, area density and curvature on the face graph, and the face core in
+// which the pressure jump sigma kappa (c_L - c_R) enters a contact-preserving
+// HLLC solver through pi = p - sigma kappa c and the shared surface stress
+// sigma |grad c| (I - n n) restores the momentum and energy fluxes.
+__device__ __forceinline__ bool unitColor(double c) { return isfinite(c) && c >= 0 && c <= 1; }
+__device__ __forceinline__ double capOtherColor(const GraphView& v, const ReactiveTransportFace& f) {
+    if (f.neighbour >= 0) return v.color[size_t(f.neighbour)];
+    if (f.kind == 3) return v.color[v.cells + size_t(f.fixed)];
+    return v.color[size_t(f.owner)];
+}
+__device__ __forceinline__ double capFaceColor(const GraphView& v, const ReactiveTransportFace& f) {
+    return f.ownerWeight * v.color[size_t(f.owner)] + (1 - f.ownerWeight) * capOtherColor(v, f);
+}
+// The interface normal at a face: the weighted cell normals, normalised when
+// nonzero (boundary faces take the owner's).
+__device__ __forceinline__ void capFaceNormal(const GraphView& v, const ReactiveTransportFace& f, double out[3]) {
+    const size_t l = size_t(f.owner), r = f.neighbour >= 0 ? size_t(f.neighbour) : l;
+    double mag2 = 0;
+    for (int d = 0; d < 3; ++d) {
+        out[d] = f.ownerWeight * v.cNormal[3 * l + d] + (1 - f.ownerWeight) * v.cNormal[3 * r + d];
+        mag2 += out[d] * out[d];
+    }
+    if (mag2 > 0) {
+        const double inv = 1 / sqrt(mag2);
+        for (int d = 0; d < 3; ++d) out[d] *= inv;
+    }
+}
+
+// Gradient of the color (face values less the cell's, so a uniform color has
+// none), its magnitude (the interface area density) and the unit normal where
+// |grad c| times the cell size exceeds the geometry threshold.
+__global__ void interfaceGradient(GraphView v) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        bool ok = unitColor(v.color[c]);
+        double g[3] = {0, 0, 0};
+        for (int64_t j = v.row[c]; ok && j < v.row[c + 1]; ++j) {
+            const int64_t e = v.incidence[j];
+            const ReactiveTransportFace& f = v.face[size_t(e < 0 ? -e - 1 : e - 1)];
+            const double orientation = e < 0 ? 1.0 : -1.0;
+            const double cf = capFaceColor(v, f);
+            if (!unitColor(cf)) { ok = false; break; }
+            for (int d = 0; d < 3; ++d) g[d] += (cf - v.color[c]) * orientation * f.area * f.normal[d];
+        }
+        double mag2 = 0;
+        for (int d = 0; ok && d < 3; ++d) {
+            g[d] *= v.invV[c];
+            mag2 += g[d] * g[d];
+            if (!isfinite(g[d])) ok = false;
+            v.cGrad[3 * c + d] = g[d];
+        }
+        if (ok) {
+            const double mag = sqrt(mag2);
+            if (!isfinite(mag) || mag < 0) ok = false;
+            else {
+                v.cArea[c] = mag;
+                const bool active = mag * cbrt(1 / v.invV[c]) > v.geomEps;
+                for (int d = 0; d < 3; ++d) v.cNormal[3 * c + d] = active ? -g[d] / mag : 0;
+            }
+        }
+        if (!ok) atomicOr(v.capError, kCapillaryBit);
+    }
+}
+
+// Curvature as the divergence of the interface normal (face normals less the
+// cell's) and the surface energy density sigma |grad c|.
+__global__ void interfaceCurvature(GraphView v) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        double sum = 0;
+        for (int64_t j = v.row[c]; j < v.row[c + 1]; ++j) {
+            const int64_t e = v.incidence[j];
+            const ReactiveTransportFace& f = v.face[size_t(e < 0 ? -e - 1 : e - 1)];
+            const double orientation = e < 0 ? 1.0 : -1.0;
+            double nf[3];
+            capFaceNormal(v, f, nf);
+            for (int d = 0; d < 3; ++d) sum += (nf[d] - v.cNormal[3 * c + d]) * orientation * f.area * f.normal[d];
+        }
+        const double kappa = sum * v.invV[c];
+        if (!isfinite(kappa)) atomicOr(v.capError, kCapillaryBit);
+        else v.cCurv[c] = kappa;
+        v.cEnergy[c] = v.sigma * v.cArea[c];
+    }
+}
+
+struct CapSide {
+    double rho, u[3], p, sound, E, color;
+};
+struct CapResult {
+    double advL, advR, contact, pMom, pEnergy, capEnergy, capMom[3];
+};
+
+// The balanced capillary core of one face (left = owner side), false when it
+// cannot be formed. curvature, colorFace and the surface stress come from the
+// shared face geometry.
+__device__ inline bool capillaryCore(const CapSide& L, const CapSide& R, const double n[3], double curvature,
+                                     double sigma, double colorFace, const double stress[9], CapResult& o) {
+    auto valid = [](const CapSide& s) {
+        if (!isfinite(s.rho) || s.rho <= 0 || !isfinite(s.p) || s.p <= 0 || !isfinite(s.sound) || s.sound <= 0
+            || !isfinite(s.E) || !unitColor(s.color))
+            return false;
+        for (int d = 0; d < 3; ++d)
+            if (!isfinite(s.u[d])) return false;
+        return true;
+    };
+    if (!valid(L) || !valid(R) || !isfinite(curvature) || !isfinite(sigma) || sigma < 0 || !unitColor(colorFace))
+        return false;
+    double n2 = 0, unL = 0, unR = 0;
+    for (int d = 0; d < 3; ++d) {
+        if (!isfinite(n[d])) return false;
+        n2 += n[d] * n[d];
+        unL += L.u[d] * n[d];
+        unR += R.u[d] * n[d];
+    }
+    if (!isfinite(n2) || fabs(n2 - 1) > 1e-10) return false;
+    for (int j = 0; j < 9; ++j)
+        if (!isfinite(stress[j])) return false;
+    const double piL = L.p - sigma * curvature * L.color, piR = R.p - sigma * curvature * R.color;
+    if (!isfinite(piL) || !isfinite(piR)) return false;
+    const double sl = dmin(0, dmin(unL - L.sound, unR - R.sound)), sr = dmax(0, dmax(unL + L.sound, unR + R.sound));
+    const double den = L.rho * (sl - unL) - R.rho * (sr - unR);
+    if (!isfinite(den) || den == 0 || !isfinite(sl) || !isfinite(sr) || sr <= sl) return false;
+    const double star = (piR - piL + L.rho * unL * (sl - unL) - R.rho * unR * (sr - unR)) / den;
+    o = CapResult{};
+    double mass;
+    if (!isfinite(star) || star <= sl || star >= sr) {
+        // waves outrunning the estimated bounds: the HLL coefficients
+        const double inv = 1 / (sr - sl);
+        o.contact = (sr * unL - sl * unR) * inv;
+        o.advL = sr * (unL - sl) * inv;
+        o.advR = sl * (sr - unR) * inv;
+        mass = o.advL * L.rho + o.advR * R.rho;
+        o.pMom = (sr * piL - sl * piR) * inv;
+        o.pEnergy = (sr * piL * unL - sl * piR * unR) * inv;
+    } else {
+        const bool useLeft = star >= 0;
+        const CapSide& side = useLeft ? L : R;
+        const double un = useLeft ? unL : unR, wave = useLeft ? sl : sr, pi = useLeft ? piL : piR;
+        const bool supersonic = (useLeft && sl >= 0) || (!useLeft && sr <= 0);
+        o.contact = supersonic ? un : star;
+        if (supersonic) {
+            mass = side.rho * un;
+            o.pMom = pi;
+            o.pEnergy = pi * un;
+        } else {
+            const double rhoStar = side.rho * (wave - un) / (wave - star);
+            const double piStar = pi + side.rho * (wave - un) * (star - un);
+            const double eStar = ((wave - un) * side.E - pi * un + piStar * star) / (wave - star);
+            mass = rhoStar * star;
+            o.pMom = piStar + mass * (star - un);
+            o.pEnergy = star * (eStar + piStar) - mass * side.E / side.rho;
+        }
+        if (useLeft) o.advL = mass / L.rho;
+        else o.advR = mass / R.rho;
+    }
+    // the surface traction and its work with one shared face velocity (the
+    // average tangential velocity plus the contact speed along n)
+    double faceVelocity[3], averageNormal = 0;
+    for (int d = 0; d < 3; ++d) {
+        faceVelocity[d] = 0.5 * (L.u[d] + R.u[d]);
+        averageNormal += faceVelocity[d] * n[d];
+    }
+    for (int d = 0; d < 3; ++d) faceVelocity[d] += (o.contact - averageNormal) * n[d];
+    o.capEnergy = 0;
+    for (int i = 0; i < 3; ++i) {
+        double traction = 0;
+        for (int j = 0; j < 3; ++j) traction += stress[3 * i + j] * n[j];
+        o.capMom[i] = sigma * curvature * colorFace * n[i] - traction;
+        o.capEnergy += faceVelocity[i] * o.capMom[i];
+    }
+    const double advective = o.advL * L.E + o.advR * R.E;
+    const double total = advective + o.pEnergy + o.capEnergy;
+    if (!isfinite(mass) || !isfinite(o.pMom) || !isfinite(o.pEnergy) || !isfinite(o.capEnergy) || !isfinite(total))
+        return false;
+    for (int d = 0; d < 3; ++d) {
+        const double momentum = o.advL * L.rho * L.u[d] + o.advR * R.rho * R.u[d] + o.pMom * n[d] + o.capMom[d];
+        if (!isfinite(momentum) || !isfinite(o.capMom[d])) return false;
+    }
+    return true;
+}
+
+// The shared face geometry of face f: curvature, color and surface stress.
+__device__ inline bool capillaryFaceGeometry(const GraphView& v, const ReactiveTransportFace& f, double& curvature,
+                                             double& colorFace, double stress[9]) {
+    const size_t l = size_t(f.owner), r = f.neighbour >= 0 ? size_t(f.neighbour) : l;
+    if (!isfinite(v.sigma) || v.sigma < 0) return false;
+    const double w = f.ownerWeight;
+    curvature = w * v.cCurv[l] + (1 - w) * v.cCurv[r];
+    colorFace = capFaceColor(v, f);
+    double ni[3];
+    capFaceNormal(v, f, ni);
+    const double scale = v.sigma * (w * v.cArea[l] + (1 - w) * v.cArea[r]);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) stress[3 * i + j] = scale * ((i == j ? 1.0 : 0.0) - ni[i] * ni[j]);
+    return isfinite(curvature) && unitColor(colorFace) && isfinite(scale);
+}
+
 __global__ void faceWork(GraphView v) {
     for (size_t fi = blockIdx.x * size_t(blockDim.x) + threadIdx.x; fi < v.faces;
          fi += size_t(blockDim.x) * gridDim.x) {
@@ -204,6 +417,29 @@ __global__ void faceWork(GraphView v) {
         out[FW_P_MOM] = (right * sl.p - left * sr.p) * invWave;
         out[FW_P_ENERGY] = (right * sl.p * unL - left * sr.p * unR) * invWave;
         double traction[3] = {0, 0, 0}, energy = 0;
+        CapResult cap{};
+        if (v.capillary) {
+            CapSide cl, cr;
+            cl.rho = sl.rho; cr.rho = sr.rho;
+            cl.p = sl.p; cr.p = sr.p;
+            cl.sound = aL; cr.sound = aR;
+            cl.E = v.q[(v.ns + 3) * v.all + l];
+            cr.E = v.q[(v.ns + 3) * v.all + r];
+            cl.color = v.color[l]; cr.color = v.color[r];
+            for (int d = 0; d < 3; ++d) { cl.u[d] = ul[d]; cr.u[d] = ur[d]; }
+            double curvature, colorFace, stress[9];
+            if (!capillaryFaceGeometry(v, f, curvature, colorFace, stress)
+                || !capillaryCore(cl, cr, f.normal, curvature, v.sigma, colorFace, stress, cap)) {
+                atomicOr(v.capError, kCapillaryBit);
+                cap = CapResult{};
+            }
+            out[FW_VELOCITY] = cap.contact;
+            out[FW_ADV_L] = cap.advL;
+            out[FW_ADV_R] = cap.advR;
+            out[FW_P_MOM] = cap.pMom;
+            out[FW_P_ENERGY] = cap.pEnergy;
+            energy += cap.capEnergy;
+        }
         if (v.viscosity > 0 || v.wale) {
             double g[9];
             for (int j = 0; j < 9; ++j) {
@@ -283,6 +519,18 @@ __global__ void faceWork(GraphView v) {
                 energy += J * (hk - hc);
             }
         }
+        if (v.capillary) {
+            // the liquid inventory of each side lies within its species' density
+            const size_t sk = v.capSpecies, lk = v.ns + 4;
+            const double slq = v.q[sk * v.all + l], srq = v.q[sk * v.all + r];
+            const double ml = v.q[lk * v.all + l], mr = v.q[lk * v.all + r];
+            if (!isfinite(slq) || !isfinite(srq) || !isfinite(ml) || !isfinite(mr) || slq < 0 || srq < 0 || ml < 0
+                || mr < 0 || ml > slq || mr > srq)
+                atomicOr(v.capError, kCapillaryBit);
+            // the viscous work above used the viscous traction only; the shared
+            // capillary momentum flux joins the face traction here
+            for (int d = 0; d < 3; ++d) traction[d] -= cap.capMom[d];
+        }
         if (v.sgs && v.sc > 0) {
             v.sgsWork[fi] = sg.diffusion;
             v.sgsWork[v.faces + fi] = sg.sumJ;
@@ -338,6 +586,25 @@ __device__ __forceinline__ double faceFluxK(const GraphView& v, const ReactiveTr
             }
         }
         flux += diffusion;
+    } else if (v.capillary && k == ns + 4) {
+        // the liquid inventory moves with its species' turbulent mixing flux
+        // in proportion to its liquid fraction on each side
+        if (sg.diffusion != 0) {
+            const size_t sk = v.capSpecies;
+            const double sl = v.q[sk * v.all + l], sr = v.q[sk * v.all + r];
+            const double ml = v.q[(ns + 4) * v.all + l], mr = v.q[(ns + 4) * v.all + r];
+            if (sl < 0 || sr < 0 || ml < 0 || mr < 0 || ml > sl || mr > sr) atomicOr(v.capError, kCapillaryBit);
+            else {
+                double species;
+                if (int(sk) == sg.carrier) species = sg.carrierFlux;
+                else {
+                    const double yl = v.q[sk * v.all + l] / sg.rhoL, yr = v.q[sk * v.all + r] / sg.rhoR;
+                    species = sg.diffusion * (yr - yl) - (f.ownerWeight * yl + (1 - f.ownerWeight) * yr) * sg.sumJ;
+                }
+                const double fl = sl > 0 ? ml / sl : 0, fr = sr > 0 ? mr / sr : 0;
+                flux += (f.ownerWeight * fl + (1 - f.ownerWeight) * fr) * species;
+            }
+        }
     } else if (k < ns + 3) flux -= wk[FW_TRACTION_X + (k - ns)];
     else if (k == ns + 3) flux += wk[FW_ENERGY];
     return flux * f.area;
@@ -414,6 +681,13 @@ __global__ void cellSteps(GraphView v, double cfl, double maximumStep) {
             denominator += v.face[fi].area * speed;
         }
         double step = denominator > 0 ? dmin(maximumStep, cfl / (v.invV[c] * denominator)) : maximumStep;
+        if (v.capillary && v.sigma > 0) {
+            // capillary waves: dt <= capCfl sqrt(rho V / (pi sigma)) where the interface is resolved
+            const double volume = 1 / v.invV[c];
+            if (v.cArea[c] * cbrt(volume) > v.geomEps)
+                step = dmin(step, v.capCfl * sqrt(v.state[c].rho * volume / (3.141592653589793238462643383279502884
+                                                                              * v.sigma)));
+        }
         if (bad || !isfinite(denominator) || denominator < 0) step = -1;
         v.step[c] = step;
     }
