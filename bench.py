@@ -23,6 +23,9 @@ Keys of the one JSON line rank 0 prints:
 built for the CPU, serial, and its flash compiled for the host on every core)
 on a bounded sample: the same case at 40^3, the same step window W+1..W+K;
 `same_window_40` puts the GPU's FP64 graph on that sample beside it.
+With N > 1 ranks (torchrun) the case is split into z-slabs, one per GPU, with a
+halo exchange over NCCL after each recovery (strong scaling);
+`--decompose replicas` runs N independent copies instead (weak scaling).
 """
 import argparse
 import contextlib
@@ -45,12 +48,13 @@ METRIC = "Mcell-steps/s at 160³, plain FP64 vs mixed/batched; adjoint/forward t
 UNIT = "Mcell-steps/s"
 # Per-unit figures of the dominant kernel (the flash: its one-thread-per-cell
 # single-phase pass, with the work queue for the cells the two-phase bound keeps),
-# from an ncu capture of one recovery of the 40^3 impingement step (the command is
-# in profiles/passSinglePhase_flops_impingement40.md): FP64 FLOPs = 2 DFMA + DADD +
-# DMUL thread instructions, and DRAM read+write bytes, each per PR phase
-# evaluation (the device counter the flash reports).
+# each per PR phase evaluation (the device counter the flash reports), from ncu
+# captures of one recovery of the impingement flow: FP64 FLOPs = 2 DFMA + DADD +
+# DMUL thread instructions (40^3, steps 4-5; 516.8 at 80^3, steps 21-22), and DRAM
+# read+write bytes (80^3, steps 21-22: more cells than resident threads, as at
+# 160^3, so the pass's stack frames do not stay in L2).
 FLOPS_PER_PHASE_EVAL = 525.1
-DRAM_BYTES_PER_PHASE_EVAL = 88.2
+DRAM_BYTES_PER_PHASE_EVAL = 166.2
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
 REFERENCE_SAMPLE = 40  # cube size of the reference CPU arm's bounded sample
 
@@ -331,10 +335,10 @@ class HostPath:
 
 def run_slab(args, rank, world):
     """The 160^3 case decomposed into z-slabs over the ranks (strong scaling):
-    each rank steps its own layers plus two halo layers (mixed precision,
-    each half step a captured graph), with the halo exchange over NCCL after
-    each recovery; the CFL minimum over ranks is checked after the run. One
-    rank runs the undivided box through the same code."""
+    each rank steps its own layers plus two halo layers (the headline's FP64
+    form, each half step a captured graph), with the halo exchange over NCCL
+    after each recovery; the CFL minimum over ranks is checked after the run.
+    One rank runs the undivided box through the same code."""
     import torch
     load_package()
     from spuma_multiphysics_b200 import cases
@@ -343,8 +347,17 @@ def run_slab(args, rank, world):
     n = args.size
     init = cases.impingement(n, seed=2026)
     slab = SlabFlow(n, rank, world, init["q"], init["guess"], init["fixed_q"], init["fixed_guess"],
-                    precision="mixed", viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
+                    viscosity=VISCOSITY, conductivity=CONDUCTIVITY, wale_cw=WALE_CW)
     f = slab.flow
+    pkg = load_package()
+    stats0 = pkg._abi.Stats()
+    f.lib.reactive_transport_stats(f.transport, C.byref(stats0))
+    slab.capture(DT)
+    stats1 = pkg._abi.Stats()
+    f.lib.reactive_transport_stats(f.transport, C.byref(stats1))
+    # transport launches counted by the handle while capturing both half steps,
+    # plus five per flash (inputs, queue, select, restart queue, restart select)
+    launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
 
     def barrier():
         if world > 1:
@@ -372,12 +385,12 @@ def run_slab(args, rank, world):
     L = slab.layout
     line = {"metric": METRIC, "value": n ** 3 / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f64 state, f32 flux", "data": "synthetic",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {**workload(n), "parallelism": f"z-slabs x{world} (own layers + 2 halo layers, "
                                                      f"NCCL halo exchange after each recovery)",
                        "own_layers_rank0": L.z1 - L.z0},
             "e2e": None, "roofline": None, "cpu_baseline": None, "clocks": sampler.summary(),
-            "gpu_launches": None}
+            "gpu_launches": launches_per_step * args.steps}
     slab.close()
     return line
 
@@ -920,8 +933,9 @@ def main():
                    help="run the ideal-gas blast box adjoint check on this cube size")
     p.add_argument("--adjoint-steps", type=int, default=50)
     p.add_argument("--skip-adjoint", action="store_true")
-    p.add_argument("--decompose", choices=("replicas", "slab"), default="replicas",
-                   help="N > 1: independent replicas (weak scaling) or the case split into z-slabs (strong scaling)")
+    p.add_argument("--decompose", choices=("auto", "replicas", "slab"), default="auto",
+                   help="N > 1: the case split into z-slabs with a halo exchange (strong scaling; the default) "
+                        "or independent replicas (weak scaling); N = 1 runs the undivided case")
     args = p.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -941,7 +955,7 @@ def main():
         else:
             if args.impl == "reference":
                 line = run_reference(args, rank, world)
-            elif args.decompose == "slab":
+            elif args.decompose == "slab" or (args.decompose == "auto" and world > 1):
                 line = run_slab(args, rank, world)
             else:
                 line = run_ours(args, rank, world)

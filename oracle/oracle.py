@@ -126,6 +126,10 @@ def ref_flash_lib():
         lib.ref_flash_recover.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _v, C.POINTER(C.c_int),
                                           C.POINTER(C.c_uint64), C.c_int, C.c_int]
         lib.ref_flash_recover.restype = C.c_int
+        lib.ref_flash_recover_capillary.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _d, _d,
+                                                    C.POINTER(C.c_int), _v, C.POINTER(C.c_int),
+                                                    C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.c_int]
+        lib.ref_flash_recover_capillary.restype = C.c_int
         lib.ref_pr_evaluate_tp.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _d,
                                            C.POINTER(C.c_int)]
         lib.ref_pr_evaluate_trho.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, _d,
@@ -182,6 +186,26 @@ def ref_flash_recover(model_image, q, energy, guess, threads=1, use_cache=True):
     if rc:
         raise RuntimeError("reference flash rejected the model image")
     return out, success, counters
+
+
+def ref_flash_recover_capillary(model_image, q, energy, guess, color, jump, equilibrium, threads=1):
+    """The reference's capillary recovery (recoverCapillary) on the host:
+    (states, success, status, counters[count,7]); a failed cell keeps its seed."""
+    count = len(energy)
+    out = np.zeros(count, dtype=guess.dtype)
+    success = np.zeros(count, dtype=np.int32)
+    status = np.zeros(count, dtype=np.int32)
+    counters = np.zeros((count, 7), dtype=np.uint64)
+    eq = np.ascontiguousarray(equilibrium, dtype=np.int32)
+    rc = ref_flash_lib().ref_flash_recover_capillary(
+        model_image, count, _p(np.ascontiguousarray(q, dtype=np.float64)),
+        _p(np.ascontiguousarray(energy, dtype=np.float64)), guess.ctypes.data_as(_v),
+        _p(np.ascontiguousarray(color, dtype=np.float64)), _p(np.ascontiguousarray(jump, dtype=np.float64)),
+        eq.ctypes.data_as(C.POINTER(C.c_int)), out.ctypes.data_as(_v), success.ctypes.data_as(C.POINTER(C.c_int)),
+        status.ctypes.data_as(C.POINTER(C.c_int)), counters.ctypes.data_as(C.POINTER(C.c_uint64)), int(threads))
+    if rc:
+        raise RuntimeError("reference flash rejected the model image")
+    return out, success, status, counters
 
 
 def cpu_threads():

@@ -12,6 +12,9 @@
 //                                (reactiveDeviceFlash.h:564) with the pure-liquid
 //                                reported-phase cache that the reference CUDA kernel
 //                                builds (reactiveGpuHem.cuh:31-36), threads optional
+//   ref_flash_recover_capillary  ReactiveDeviceFlash::recoverCapillary per cell
+//                                (reactiveDeviceFlash.h:572-588): per-cell color,
+//                                pressure jump and equilibrium flag; status per cell
 //   ref_pr_evaluate_tp / _trho   ReactiveDevicePR::evaluateTPTrusted / evaluateTrhoTrusted
 //                                (reactiveDevicePR.h:575, :474) for EOS unit checks
 //   ref_pr_mix_tp / _trho        the same for a mixture table with mass fractions Y
@@ -62,6 +65,52 @@ int ref_flash_recover(const void* image, size_t count, const double* q, const do
                 ReactiveDeviceFlash::recover(*m, in, useCache ? cache : nullptr);
             out[c] = o.success ? o.state : guess[c];
             success[c] = o.success;
+            if (counters) {
+                uint64_t* k = counters + 7 * c;
+                k[0] = o.counters.phases; k[1] = o.counters.residuals; k[2] = o.counters.candidates;
+                k[3] = o.counters.stable; k[4] = o.counters.failures;
+                k[5] = o.counters.analyticJacobians; k[6] = o.counters.finiteDifferenceJacobians;
+            }
+        }
+    };
+    if (threads <= 1) worker();
+    else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+    }
+    delete m;
+    return 0;
+}
+
+// The capillary batch: color[c], jump[c], equilibrium[c] per cell; a failed
+// cell keeps its seed in out; status[c] is the reference's Output.status
+// (0 success, 1 no candidate, 2 invalid capillary input).
+int ref_flash_recover_capillary(const void* image, size_t count, const double* q, const double* energy,
+                                const ReactiveThermoState* guess, const double* color, const double* jump,
+                                const int* equilibrium, ReactiveThermoState* out, int* success, int* status,
+                                uint64_t* counters, int threads) {
+    Model* m = new Model;
+    std::memcpy(m, image, sizeof(Model));
+    if (!ReactiveDeviceFlash::validModel(*m)) { delete m; return 1; }
+    Cache cache[2]{};
+    for (int i = 0; i < m->nl && i < 2; ++i)
+        ReactiveDevicePRPurePhaseCache::buildPureReportedPhaseCache(m->phase[i + 1], cache[i]);
+    const int ns = m->ns;
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const size_t c = next.fetch_add(1);
+            if (c >= count) break;
+            ReactiveDeviceFlash::Input in{};
+            for (int k = 0; k < ns; ++k) in.q[k] = q[c * ns + k];
+            in.energy = energy[c];
+            in.guess = guess[c];
+            const ReactiveDeviceFlash::Output o =
+                ReactiveDeviceFlash::recoverCapillary(*m, in, color[c], jump[c], equilibrium[c] != 0, cache);
+            out[c] = o.success ? o.state : guess[c];
+            success[c] = o.success;
+            status[c] = o.status;
             if (counters) {
                 uint64_t* k = counters + 7 * c;
                 k[0] = o.counters.phases; k[1] = o.counters.residuals; k[2] = o.counters.candidates;
