@@ -29,12 +29,20 @@ void reactive_gpu_hem_destroy_v1(void* hem);
  * cell, energy the internal energy density, state the seed in / the result out. */
 int reactive_gpu_hem_run_v1(void* hem, const double* q, const double* energy, size_t count,
     ReactiveThermoState* state, int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);
-/* src/reactiveThermo/reactiveGpuHem.h:63-65, :72-84: the capillary batches. This build runs them
- * for UV phase equilibrium without a pressure jump (capillary NULL for the resident form, or every
- * entry with pressureJump = 0 and equilibrium = 1), which is the plain flash of run_v1; a pressure
- * jump or the frozen partition returns 1 with a message. run_resident_v1: device pointers indexed
- * by global cell, order[0..count) names the cells, each result (state, success) goes to
- * output[cell], a failed cell returns its seed; synchronous, batch totals in *profile.
+/* src/reactiveThermo/reactiveGpuHem.h:56-65, :72-84: the capillary batches. energy is the bulk
+ * internal energy density (kinetic and surface energy removed); each cell's color in [0, 1],
+ * pressure jump sigma*kappa [Pa] and equilibrium flag select the reference's capillary recovery
+ * (recoverCapillary, reactiveDeviceFlash.h:572-588): the gas phase at p - color*jump, the liquid at
+ * p + (1 - color)*jump, p the returned mechanical pressure; UV equilibrium with the boundary search,
+ * or (equilibrium 0) the frozen partition at the seed's liquid masses; a nonzero jump needs one
+ * pure liquid (else the cell fails). run_v2 rejects the batch ("Invalid CUDA HEM capillary cell
+ * input") for a color outside [0, 1], a non-finite jump or an equilibrium flag other than 0/1.
+ * These run on the multi-species engine, one thread per cell (for a pure-fluid handle, one made
+ * from the same image); a pure-fluid image with analyticJacobian = 1 takes only equilibrium batches
+ * without a jump, on its fast path (the plain UV flash), and returns 1 with a message otherwise.
+ * run_resident_v1: device pointers indexed by global cell, order[0..count) names the cells, each
+ * result (state, success) goes to output[cell] (reserved untouched), a failed cell returns its
+ * seed; capillary may be NULL for the plain flash; synchronous, batch totals in *profile.
  * src/reactiveThermo/reactiveGpuHem.h:66-71 (primitive initialisation) returns 1 with a message. */
 int reactive_gpu_hem_run_v2(void* hem, const double* q, const double* energy,
     const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* state, int* success,

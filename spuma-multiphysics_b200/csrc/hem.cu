@@ -704,6 +704,21 @@ struct HemDevice {
     std::vector<void*> blocks;
     // a model image beyond the pure fluid: the multi-species flash (hem_mixture.cu)
     MixtureFlash* mixture = nullptr;
+    // a pure-fluid handle's capillary batches (pressure jumps, the frozen
+    // partition, the capillary boundary search): the same engine on the same
+    // image, created by the first such batch when the image is in its scope
+    std::unique_ptr<ReactiveB200HemModel> image;
+    MixtureFlash* capillaryEngine = nullptr;
+    MixtureFlash* capillaryFlash() {
+        if (mixture) return mixture;
+        if (!capillaryEngine && image) {
+            std::string why;
+            capillaryEngine = mixtureCreate(*image, capacity, device, why);
+            if (!capillaryEngine) image.reset();  // outside its scope (an analytic-Jacobian image)
+            else bytes += mixtureDeviceBytes(capillaryEngine);
+        }
+        return capillaryEngine;
+    }
 
     template <class T> T* alloc(size_t n) {
         void* p = nullptr;
@@ -714,6 +729,7 @@ struct HemDevice {
     }
     ~HemDevice() {
         if (mixture) mixtureDestroy(mixture);
+        if (capillaryEngine) mixtureDestroy(capillaryEngine);
         if (stream) cudaStreamSynchronize(stream);
         if (down) cudaStreamSynchronize(down);
         for (void* p : blocks) cudaFree(p);
@@ -889,6 +905,7 @@ void* create(const void* raw, size_t bytes, size_t capacity, bool hostPath, char
         }
         check(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         d->capacity = capacity;
+        d->image.reset(new ReactiveB200HemModel(m));
         d->cst = d->alloc<HemConst>(1);
         d->in = d->alloc<CellInput>(capacity);
         d->rec = d->alloc<CandRecord>(7 * capacity);
@@ -1143,7 +1160,7 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
             ReactiveGpuHemProfileV1 p{};
             p.abiVersion = 1;
             p.structBytes = sizeof(p);
-            rb200::mixtureRun(d.mixture, q, energy, count, states, success, p);
+            rb200::mixtureRun(d.mixture, q, energy, count, nullptr, states, success, p);
             *profile = p;
             return 0;
         }
@@ -1224,21 +1241,52 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
     }
 }
 
+// src/reactiveTransport/reactiveGpuHem.cuh:354-358, 227-241: the capillary
+// batch. Every cell is the reference's capillary recovery (recoverCapillary):
+// the gas at p - color*jump, the liquid at p + (1 - color)*jump, UV equilibrium
+// with the boundary search, or the frozen partition at the seed's liquid masses.
+// It runs on the multi-species engine (hem_mixture.cu), for a pure-fluid handle
+// one made from the same image. A pure-fluid image with the analytic Jacobian
+// (outside that engine's scope) takes equilibrium batches without a jump on its
+// own fast path (the plain UV flash) and refuses the rest.
 int reactive_gpu_hem_run_v2(void* raw, const double* q, const double* energy,
                             const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* states,
                             int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t size) {
-    // without a pressure jump and in equilibrium the capillary batch is the plain UV flash
-    if (!capillary && count) {
-        if (error && size) std::snprintf(error, size, "Null capillary input");
+    try {
+        rb200::require(capillary != nullptr, "Null CUDA HEM capillary input");
+        rb200::require(raw && q && energy && states && success && profile && profile->abiVersion == 1
+                           && profile->structBytes == sizeof(*profile),
+                       "Invalid CUDA HEM batch arguments");
+        auto& d = *static_cast<HemDevice*>(raw);
+        bool plain = true;
+        for (size_t c = 0; c < count; ++c) {
+            const auto& in = capillary[c];
+            rb200::require(std::isfinite(in.color) && in.color >= 0 && in.color <= 1 && std::isfinite(in.pressureJump)
+                               && (in.equilibrium == 0 || in.equilibrium == 1),
+                           "Invalid CUDA HEM capillary cell input");
+            plain = plain && in.pressureJump == 0.0 && in.equilibrium == 1;
+        }
+        rb200::MixtureFlash* engine = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(d.entry);
+            rb200::require(count && count <= d.capacity, "CUDA HEM batch exceeds capacity");
+            rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+            engine = d.capillaryFlash();
+            if (engine) {
+                ReactiveGpuHemProfileV1 p{};
+                p.abiVersion = 1;
+                p.structBytes = sizeof(p);
+                rb200::mixtureRun(engine, q, energy, count, capillary, states, success, p);
+                *profile = p;
+                return 0;
+            }
+        }
+        rb200::require(plain, "Capillary pressure jumps and the frozen partition need a model image with "
+                              "analyticJacobian = 0 on this build");
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
         return 1;
     }
-    for (size_t c = 0; c < count; ++c)
-        if (!(capillary[c].pressureJump == 0.0 && capillary[c].equilibrium == 1)) {
-            if (error && size)
-                std::snprintf(error, size, "Capillary pressure jumps and the frozen partition are not part of this "
-                                           "B200 build");
-            return 1;
-        }
     return reactive_gpu_hem_run_v1(raw, q, energy, count, states, success, profile, error, size);
 }
 int reactive_gpu_hem_initialize_tp_v1(void*, double*, double*, const ReactiveGpuHemCapillaryInputV2*, size_t,
@@ -1261,10 +1309,20 @@ int reactive_gpu_hem_run_resident_v1(void* raw, const double* q, const double* e
                            && profile->structBytes == sizeof(*profile),
                        "Invalid resident CUDA HEM batch arguments");
         auto& d = *static_cast<HemDevice*>(raw);
-        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count && count <= d.capacity, "Resident CUDA HEM batch exceeds capacity");
         rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+        // the capillary recovery (and every batch of a multi-species handle) on the
+        // multi-species engine; a pure-fluid image outside its scope keeps the fast path
+        rb200::MixtureFlash* engine = d.mixture ? d.mixture : (capillary ? d.capillaryFlash() : nullptr);
+        if (engine) {
+            ReactiveGpuHemProfileV1 p{};
+            p.abiVersion = 1;
+            p.structBytes = sizeof(p);
+            rb200::mixtureRunResident(engine, q, energy, seed, capillary, order, count, output, p);
+            *profile = p;
+            return 0;
+        }
         d.ensureHostPath();  // gathered seeds, results and flags
         const auto begin = std::chrono::steady_clock::now();
         cudaStream_t s = d.stream;
@@ -1320,7 +1378,7 @@ int reactive_gpu_hem_run_device_v3(void* raw, const double* conserved, size_t st
                            && variables >= 5,
                        "Invalid device HEM batch arguments");
         auto& d = *static_cast<HemDevice*>(raw);
-        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1, run_v2 and run_resident_v1 only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count <= d.capacity, "Device HEM batch exceeds capacity");
         auto s = static_cast<cudaStream_t>(stream);
@@ -1340,7 +1398,7 @@ int reactive_gpu_hem_two_phase_bound_v3(void* raw, int request, int* active, cha
     try {
         rb200::require(raw && request >= -1 && request <= 1, "Invalid two-phase bound request");
         auto& d = *static_cast<HemDevice*>(raw);
-        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1, run_v2 and run_resident_v1 only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(request != 1 || d.domeBuilt, "This model has no two-phase bound (see the header)");
         if (request >= 0) {
@@ -1366,7 +1424,7 @@ int reactive_gpu_hem_vjp_device_v3(void* raw, const double* conserved, size_t st
                            && barStride >= count && variables == 5,
                        "Invalid HEM VJP arguments (pure fluid: variables = 5)");
         auto& d = *static_cast<HemDevice*>(raw);
-        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1, run_v2 and run_resident_v1 only");
         std::lock_guard<std::mutex> lock(d.entry);
         auto s = static_cast<cudaStream_t>(stream);
         rb200::hemStateVjp<<<rb200::gridFor(count, 128), 128, 0, s>>>(d.cst, conserved, stride, count, state,
@@ -1386,7 +1444,7 @@ int reactive_gpu_hem_autotune_v3(void* raw, const double* conserved, size_t stri
         rb200::require(raw && conserved && seed && count && stride >= count && variables >= 5,
                        "Invalid HEM autotune arguments");
         auto& d = *static_cast<HemDevice*>(raw);
-        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1, run_v2 and run_resident_v1 only");
         std::lock_guard<std::mutex> lock(d.entry);
         rb200::require(count <= d.capacity, "CUDA HEM batch exceeds capacity");
         rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
@@ -1431,7 +1489,7 @@ int reactive_gpu_hem_run_counters_v3(void* raw, ReactiveGpuHemProfileV1* profile
     try {
         rb200::require(raw && profile, "Invalid HEM counter query");
         auto& d = *static_cast<HemDevice*>(raw);
-        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1 (host arrays) only");
+        rb200::require(!d.mixture, "The multi-species flash runs through reactive_gpu_hem_run_v1, run_v2 and run_resident_v1 only");
         std::lock_guard<std::mutex> lock(d.entry);
         ReactiveGpuHemProfileV1 p{};
         p.abiVersion = 1;

@@ -3,8 +3,10 @@
 // isopropanol model of the reference's production case), one thread per cell.
 //
 // The search restates the reference device flash
-// (src/reactiveThermo/reactiveDeviceFlash.h) for models without solids and
-// without capillarity, with the finite-difference Jacobian (analyticJacobian 0):
+// (src/reactiveThermo/reactiveDeviceFlash.h) for models without solids, with the
+// finite-difference Jacobian (analyticJacobian 0), including its capillary form
+// (recoverCapillary, :572-588: the phases at their own pressures across a fixed
+// jump, the boundary search in every equilibrium batch, the frozen partition):
 //   * phase sums of one evaluation at (p, T) with given liquid masses, the gas
 //     phase from the remaining species and, on request, virtual liquids for the
 //     chemical potentials (evaluate, :210-262);
@@ -56,6 +58,11 @@ struct Tally {
     unsigned long long phases = 0, residuals = 0, candidates = 0, stable = 0, failures = 0, fd = 0;
 };
 
+// One cell's recovery: its inputs, the search mode and, for a capillary batch,
+// the interface color and the pressure jump sigma*kappa held fixed during the
+// solve (src/reactiveThermo/reactiveDeviceFlash.h:146-153): the gas phase is
+// evaluated at p - color*jump and the liquids at p + (1 - color)*jump, p the
+// volume-averaged mechanical pressure.
 struct MixCell {
     const ReactiveB200HemModel& m;
     double q[kNs];
@@ -63,6 +70,7 @@ struct MixCell {
     ReactiveThermoState guess;
     bool adaptive;
     Tally& n;
+    double color = 0, jump = 0;
 };
 
 __device__ __forceinline__ bool fin(double x) { return x == x && fabs(x) <= 1.79769313486231570815e308; }
@@ -88,6 +96,8 @@ __device__ __forceinline__ bool isCondensable(const ReactiveB200HemModel& m, int
     return false;
 }
 __device__ __forceinline__ double energyScale(const MixEval& v) { return fmax(1e5 * v.s.rho, v.cpD * v.s.T); }
+__device__ __forceinline__ double gasPressure(const MixCell& c, double p) { return p - c.color * c.jump; }
+__device__ __forceinline__ double liquidPressure(const MixCell& c, double p) { return p + (1 - c.color) * c.jump; }
 
 // The gas mixture at (p, T, Y) on its gas root; species outside their NASA
 // range invalidate the state when the model enforces the ranges.
@@ -155,11 +165,12 @@ __device__ __noinline__ bool evaluate(MixCell& c, const double* mass, double p, 
     double mg = 0;
     for (int k = 0; k < m.ns; ++k) mg += gas[k];
     s.gasMass = mg;
+    const double pg = gasPressure(c, p), pl = liquidPressure(c, p);
     if (mg > 0) {
         for (int k = 0; k < m.ns; ++k) gas[k] /= mg;
         mix::Props prop;
-        if (gasPhase(c, p, T, gas, virt, prop) != mix::OK) return false;
-        addPhase(v, mg, prop, p);
+        if (gasPhase(c, pg, T, gas, virt, prop) != mix::OK) return false;
+        addPhase(v, mg, prop, pg);
         s.alphaGas = mg / prop.rho;
         s.rhoGas = prop.rho;
         if (virt)
@@ -169,7 +180,7 @@ __device__ __noinline__ bool evaluate(MixCell& c, const double* mass, double p, 
         s.liquidMass[i] = mass[i];
         if (!(mass[i] > 0 || (virt && c.q[m.condensable[i]] > 0))) continue;
         mix::Props prop;
-        const int status = liquidPhase(c, i, p, T, virt, prop);
+        const int status = liquidPhase(c, i, pl, T, virt, prop);
         if (status != mix::OK) {
             if (mass[i] > 0 || !unavailable(status)) return false;
             v.muLiq[i] = HUGE_VAL;
@@ -177,7 +188,7 @@ __device__ __noinline__ bool evaluate(MixCell& c, const double* mass, double p, 
         }
         if (virt) v.muLiq[i] = prop.mu[0] / (kRu * T);
         if (mass[i] > 0) {
-            addPhase(v, mass[i], prop, p);
+            addPhase(v, mass[i], prop, pl);
             s.rhoLiquid[i] = prop.rho;
             s.alphaLiquid[i] = mass[i] / prop.rho;
             s.activeLiquids |= 1 << i;
@@ -244,7 +255,8 @@ __device__ bool solveDense(const double a0[4][4], const double* rhs, int n, doub
 }
 
 // The scalar all-gas energy residual at (T, rho): properties at (T, rho), then
-// the gas root at the resulting pressure must be that density.
+// the gas root at the resulting pressure must be that density. p is the
+// mechanical pressure, the gas's plus color*jump.
 __device__ __noinline__ bool gasProbe(MixCell& c, double T, double& F, double& cv, double& p, double* cp) {
     const double rho = density(c);
     double Y[kNs] = {0, 0, 0, 0};
@@ -252,10 +264,11 @@ __device__ __noinline__ bool gasProbe(MixCell& c, double T, double& F, double& c
     ++c.n.phases;
     mix::Props prop;
     if (mix::trho(c.m.phase[0], T, rho, Y, false, prop) != mix::OK) return false;
-    p = prop.p;
+    const double gasP = prop.p;
+    p = gasP + c.color * c.jump;
     if (!inBounds(c.m, p, T)) return false;
     mix::Props gas;
-    if (gasPhase(c, prop.p, T, Y, false, gas) != mix::OK || fabs(gas.rho - rho) > 1e-8 * rho) return false;
+    if (gasPhase(c, gasP, T, Y, false, gas) != mix::OK || fabs(gas.rho - rho) > 1e-8 * rho) return false;
     F = rho * prop.e - c.energy;
     cv = rho * prop.cv;
     if (cp) *cp = prop.cp;
@@ -552,7 +565,7 @@ __device__ __noinline__ double tangent(MixCell& c, double p, double T, const int
     for (int k = 0; k < m.ns; ++k) { Y[k] = mole[k] * m.weights[k]; sum += Y[k]; }
     for (int k = 0; k < m.ns; ++k) Y[k] /= sum;
     mix::Props prop;
-    const int status = gasPhase(c, p, T, Y, false, prop);
+    const int status = gasPhase(c, gasPressure(c, p), T, Y, false, prop);
     if (status != mix::OK) return unavailable(status) ? HUGE_VAL : nan("");
     double reference = 0, W = 0;
     for (int i = 0; i < n; ++i) reference += mole[m.condensable[present[i]]] * mu[present[i]];
@@ -582,7 +595,7 @@ __device__ __noinline__ bool stableCandidate(MixCell& c, const MixEval& v) {
         if (v.s.liquidMass[i] > 0) {
             present[np++] = i;
             mix::Props prop;
-            if (liquidPhase(c, i, p, T, true, prop) != mix::OK) return false;
+            if (liquidPhase(c, i, liquidPressure(c, p), T, true, prop) != mix::OK) return false;
             mu[i] = prop.mu[0] / (kRu * T);
         }
     if (!np) return false;
@@ -700,18 +713,19 @@ __device__ __noinline__ bool searchCandidates(MixCell& c, MixEval& best) {
     return have;
 }
 
-// The recovery of one cell: the candidate search; with the boundary recovery a
-// second search in log vapour fractions when the first found nothing or left a
-// condensable almost entirely liquid beside a gas phase, the larger entropy
-// (the first search on a tie) kept.
-__device__ bool recoverCell(MixCell& c, MixEval& result) {
+// The recovery of one cell: the candidate search; with the boundary recovery (or
+// in a capillary batch, whose transported trace inventories can defeat the
+// reference seeds) a second search in log vapour fractions when the first found
+// nothing or left a condensable almost entirely liquid beside a gas phase, the
+// larger entropy (the first search on a tie) kept.
+__device__ bool recoverCell(MixCell& c, MixEval& result, bool capillaryBoundary) {
     const ReactiveB200HemModel& m = c.m;
     if (m.ns <= 0 || m.ns > kNs || m.nl < 0 || m.nl > kLiq || !fin(c.energy) || !(density(c) > 0)) return false;
     for (int k = 0; k < m.ns; ++k)
         if (!fin(c.q[k]) || c.q[k] < 0) return false;
     MixEval reference;
     const bool have = searchCandidates(c, reference);
-    if (!m.boundaryRecovery) {
+    if (!m.boundaryRecovery && !capillaryBoundary) {
         if (have) result = reference;
         return have;
     }
@@ -732,29 +746,64 @@ __device__ bool recoverCell(MixCell& c, MixEval& result) {
     return true;
 }
 
-enum : int { M_PHASES, M_RESIDUALS, M_CANDIDATES, M_STABLE, M_FD, M_COUNT };
+enum : int { M_PHASES, M_RESIDUALS, M_CANDIDATES, M_STABLE, M_FD, M_SUCCEEDED, M_COUNT };
 
+// A capillary cell input the reference's recoverCapillary accepts
+// (src/reactiveThermo/reactiveDeviceFlash.h:572-588): a color in [0, 1], a
+// finite jump, and a nonzero jump only with one pure liquid.
+__device__ __forceinline__ bool capillaryAccepted(const ReactiveB200HemModel& m, double color, double jump) {
+    return fin(color) && color >= 0 && color <= 1 && fin(jump) && (jump == 0 || (m.nl == 1 && m.condensedKind[0] == 0));
+}
+
+// One thread per cell. `order` (optional) names the cells: thread item i works on
+// cell order[i], and every per-cell array is indexed by that cell. With
+// `capillary` each cell is the reference's capillary recovery: UV equilibrium
+// with the boundary search, or (equilibrium = 0) the frozen partition at the
+// seed's liquid masses. Results go to out/success, or to outputs[cell] for the
+// resident form; a failed cell gets its seed.
 __global__ void __launch_bounds__(kBlock) mixtureFlashKernel(const ReactiveB200HemModel* __restrict__ model,
                                                             const double* __restrict__ q,
                                                             const double* __restrict__ energy, size_t count,
                                                             const ReactiveThermoState* __restrict__ seed,
-                                                            ReactiveThermoState* __restrict__ out, int* success,
+                                                            const ReactiveGpuHemCapillaryInputV2* capillary,
+                                                            const uint32_t* order, ReactiveThermoState* out,
+                                                            int* success, ReactiveGpuHemOutputV1* outputs,
                                                             unsigned long long* totals) {
     const ReactiveB200HemModel& m = *model;
     Tally n;
+    unsigned long long succeeded = 0;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(blockDim.x) * gridDim.x) {
-        MixCell c{m, {0, 0, 0, 0}, energy[i], seed[i], false, n};
-        for (int k = 0; k < m.ns && k < kNs; ++k) c.q[k] = q[i * size_t(m.ns) + k];
+        const size_t cell = order ? size_t(order[i]) : i;
+        MixCell c{m, {0, 0, 0, 0}, energy[cell], seed[cell], false, n};
+        for (int k = 0; k < m.ns && k < kNs; ++k) c.q[k] = q[cell * size_t(m.ns) + k];
         MixEval result;
-        const bool ok = recoverCell(c, result);
-        out[i] = ok ? result.s : c.guess;
-        success[i] = ok ? 1 : 0;
+        bool ok;
+        if (capillary) {
+            const ReactiveGpuHemCapillaryInputV2 in = capillary[cell];
+            c.color = in.color;
+            c.jump = in.pressureJump;
+            if (!capillaryAccepted(m, c.color, c.jump)) ok = false;
+            else if (in.equilibrium) ok = recoverCell(c, result, true);
+            else {
+                const double mass[kLiq] = {c.guess.liquidMass[0], c.guess.liquidMass[1]};
+                ok = frozen(c, mass, result, 0);
+            }
+        } else ok = recoverCell(c, result, false);
+        const ReactiveThermoState& st = ok ? result.s : c.guess;
+        if (out) out[cell] = st;
+        if (success) success[cell] = ok ? 1 : 0;
+        if (outputs) {
+            outputs[cell].state = st;
+            outputs[cell].success = ok ? 1 : 0;
+        }
+        succeeded += ok ? 1 : 0;
     }
     atomicAdd(totals + M_PHASES, n.phases);
     atomicAdd(totals + M_RESIDUALS, n.residuals);
     atomicAdd(totals + M_CANDIDATES, n.candidates);
     atomicAdd(totals + M_STABLE, n.stable);
     atomicAdd(totals + M_FD, n.fd);
+    atomicAdd(totals + M_SUCCEEDED, succeeded);
 }
 
 bool finiteHost(double x) { return x == x && std::fabs(x) <= 1.79769313486231570815e308; }
@@ -813,6 +862,7 @@ struct MixtureFlash {
     ReactiveThermoState* seed = nullptr;
     ReactiveThermoState* out = nullptr;
     int* success = nullptr;
+    ReactiveGpuHemCapillaryInputV2* capillary = nullptr;  // allocated by the first capillary batch
     unsigned long long* totals = nullptr;
     template <class T> T* alloc(size_t n) {
         void* p = nullptr;
@@ -851,22 +901,29 @@ MixtureFlash* mixtureCreate(const ReactiveB200HemModel& m, size_t capacity, int 
 void mixtureDestroy(MixtureFlash* f) { delete f; }
 size_t mixtureDeviceBytes(const MixtureFlash* f) { return f ? f->bytes : 0; }
 
-void mixtureRun(MixtureFlash* f, const double* q, const double* energy, size_t count, ReactiveThermoState* states,
-                int* success, ReactiveGpuHemProfileV1& p) {
+void mixtureRun(MixtureFlash* f, const double* q, const double* energy, size_t count,
+                const ReactiveGpuHemCapillaryInputV2* capillary, ReactiveThermoState* states, int* success,
+                ReactiveGpuHemProfileV1& p) {
     require(count && count <= f->capacity, "CUDA HEM batch exceeds capacity");
     check(cudaSetDevice(f->device), "cudaSetDevice");
     const auto begin = std::chrono::steady_clock::now();
     cudaStream_t s = f->stream;
+    if (capillary && !f->capillary) f->capillary = f->alloc<ReactiveGpuHemCapillaryInputV2>(f->capacity);
     cudaEvent_t a, b;
     check(cudaEventCreate(&a), "event");
     check(cudaEventCreate(&b), "event");
     check(cudaMemcpyAsync(f->q, q, count * size_t(f->ns) * sizeof(double), cudaMemcpyHostToDevice, s), "H2D q");
     check(cudaMemcpyAsync(f->energy, energy, count * sizeof(double), cudaMemcpyHostToDevice, s), "H2D e");
     check(cudaMemcpyAsync(f->seed, states, count * sizeof(ReactiveThermoState), cudaMemcpyHostToDevice, s), "H2D seed");
+    if (capillary)
+        check(cudaMemcpyAsync(f->capillary, capillary, count * sizeof(ReactiveGpuHemCapillaryInputV2),
+                              cudaMemcpyHostToDevice, s),
+              "H2D capillary");
     check(cudaMemsetAsync(f->totals, 0, M_COUNT * sizeof(unsigned long long), s), "memset");
     check(cudaEventRecord(a, s), "event");
-    mixtureFlashKernel<<<gridFor(count, kBlock), kBlock, 0, s>>>(f->model, f->q, f->energy, count, f->seed, f->out,
-                                                                  f->success, f->totals);
+    mixtureFlashKernel<<<gridFor(count, kBlock), kBlock, 0, s>>>(f->model, f->q, f->energy, count, f->seed,
+                                                                  capillary ? f->capillary : nullptr, nullptr, f->out,
+                                                                  f->success, nullptr, f->totals);
     check(cudaGetLastError(), "mixture flash");
     check(cudaEventRecord(b, s), "event");
     check(cudaMemcpyAsync(states, f->out, count * sizeof(ReactiveThermoState), cudaMemcpyDeviceToHost, s), "D2H");
@@ -880,17 +937,56 @@ void mixtureRun(MixtureFlash* f, const double* q, const double* energy, size_t c
     cudaEventDestroy(b);
     p.batches = 1;
     p.submitted = count;
-    p.succeeded = 0;
-    for (size_t c = 0; c < count; ++c) p.succeeded += success[c] != 0;
+    p.succeeded = t[M_SUCCEEDED];
     p.deviceFailures = count - p.succeeded;
     p.phaseEvaluations = t[M_PHASES];
     p.residualEvaluations = t[M_RESIDUALS];
     p.flashCandidates = t[M_CANDIDATES];
     p.stableCandidates = t[M_STABLE];
     p.finiteDifferenceJacobians = t[M_FD];
-    p.transferBytes = count * ((f->ns + 1) * sizeof(double) + 2 * sizeof(ReactiveThermoState) + sizeof(int));
+    p.transferBytes = count * ((f->ns + 1) * sizeof(double) + 2 * sizeof(ReactiveThermoState) + sizeof(int)
+                               + (capillary ? sizeof(ReactiveGpuHemCapillaryInputV2) : 0));
     p.deviceBytes = f->bytes;
     p.hostBytes = count * sizeof(ReactiveThermoState);
+    p.kernelSeconds = kernel / 1000.;
+    p.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+    p.copySeconds = std::max(0.0, p.wallSeconds - p.kernelSeconds);
+}
+
+void mixtureRunResident(MixtureFlash* f, const double* q, const double* energy, const ReactiveThermoState* seed,
+                        const ReactiveGpuHemCapillaryInputV2* capillary, const uint32_t* order, size_t count,
+                        ReactiveGpuHemOutputV1* output, ReactiveGpuHemProfileV1& p) {
+    require(count && count <= f->capacity, "Resident CUDA HEM batch exceeds capacity");
+    check(cudaSetDevice(f->device), "cudaSetDevice");
+    const auto begin = std::chrono::steady_clock::now();
+    cudaStream_t s = f->stream;
+    cudaEvent_t a, b;
+    check(cudaEventCreate(&a), "event");
+    check(cudaEventCreate(&b), "event");
+    check(cudaMemsetAsync(f->totals, 0, M_COUNT * sizeof(unsigned long long), s), "memset");
+    check(cudaEventRecord(a, s), "event");
+    mixtureFlashKernel<<<gridFor(count, kBlock), kBlock, 0, s>>>(f->model, q, energy, count, seed, capillary, order,
+                                                                  nullptr, nullptr, output, f->totals);
+    check(cudaGetLastError(), "mixture flash");
+    check(cudaEventRecord(b, s), "event");
+    unsigned long long t[M_COUNT] = {};
+    check(cudaMemcpyAsync(t, f->totals, sizeof(t), cudaMemcpyDeviceToHost, s), "D2H totals");
+    check(cudaStreamSynchronize(s), "sync");
+    float kernel = 0;
+    cudaEventElapsedTime(&kernel, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    p.batches = 1;
+    p.submitted = count;
+    p.succeeded = t[M_SUCCEEDED];
+    p.deviceFailures = count - p.succeeded;
+    p.phaseEvaluations = t[M_PHASES];
+    p.residualEvaluations = t[M_RESIDUALS];
+    p.flashCandidates = t[M_CANDIDATES];
+    p.stableCandidates = t[M_STABLE];
+    p.finiteDifferenceJacobians = t[M_FD];
+    p.transferBytes = sizeof(t);
+    p.deviceBytes = f->bytes;
     p.kernelSeconds = kernel / 1000.;
     p.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
     p.copySeconds = std::max(0.0, p.wallSeconds - p.kernelSeconds);

@@ -60,6 +60,44 @@ class GpuHem:
             raise HemError(err.value.decode())
         return success, prof
 
+    def run_capillary(self, q, energy, capillary, states, success=None):
+        """The capillary batch (reactive_gpu_hem_run_v2) on host arrays: energy is the
+        bulk internal energy density (kinetic and surface energy removed), capillary
+        (CAPILLARY_DTYPE) each cell's color, pressure jump sigma*kappa and
+        equilibrium flag (0: the frozen partition at the seed's liquid masses).
+        states are seeds in, results out for successful cells.
+        Returns (success int32 array, profile)."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        energy = np.ascontiguousarray(energy, dtype=np.float64)
+        capillary = np.ascontiguousarray(capillary, dtype=A.CAPILLARY_DTYPE)
+        assert states.dtype == A.THERMO_DTYPE and states.flags.c_contiguous
+        n = len(energy)
+        if success is None:
+            success = np.zeros(n, dtype=np.int32)
+        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+        err = C.create_string_buffer(1024)
+        rc = self.lib.reactive_gpu_hem_run_v2(self.handle, A.dptr(q), A.dptr(energy),
+                                              capillary.ctypes.data_as(C.c_void_p), n,
+                                              states.ctypes.data_as(C.c_void_p),
+                                              success.ctypes.data_as(C.POINTER(C.c_int)), C.byref(prof), err, len(err))
+        if rc:
+            raise HemError(err.value.decode())
+        return success, prof
+
+    def run_resident(self, q, energy, seed, capillary, order, count, output):
+        """The device-resident batch (reactive_gpu_hem_run_resident_v1): device
+        pointers or torch tensors indexed by cell; order[0..count) names the cells
+        and each result goes to output[cell] (HEM_OUTPUT_DTYPE records).
+        Returns the profile."""
+        ptr = lambda t: None if t is None else (t if isinstance(t, int) else t.data_ptr())
+        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+        err = C.create_string_buffer(1024)
+        rc = self.lib.reactive_gpu_hem_run_resident_v1(self.handle, ptr(q), ptr(energy), ptr(seed), ptr(capillary),
+                                                       ptr(order), count, ptr(output), C.byref(prof), err, len(err))
+        if rc:
+            raise HemError(err.value.decode())
+        return prof
+
     def run_device(self, conserved, stride, count, variables, seed, state=None, transport=None, success=None,
                    stream=0, per_cell=False):
         """Device batch: all arguments are device pointers (ints) or torch tensors.
