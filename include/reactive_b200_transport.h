@@ -129,14 +129,13 @@ int reactive_transport_set_capillary_v1(void* transport, const ReactiveCapillary
 int reactive_transport_capillary_geometry_v1(void* transport, const double* cellColor,
     const double* fixedColor, double* surfaceEnergy, double* curvature, double* normalXYZ);
 int reactive_transport_capillary_profile_v1(void* transport, ReactiveCapillaryProfileV1* profile);
-/* Entry points of the Cartesian implicit surface geometry, the WALE PR
- * properties and the resident capillary-flash loop, which the solver references
- * statically (so that a solver linked against this library resolves every
- * symbol it names); each returns 1 with a message, and the solver reaches them
- * only with those options selected. Struct arguments are opaque here.
+/* Entry points of the Cartesian implicit surface geometry and the WALE PR
+ * properties, which the solver references statically (so that a solver linked
+ * against this library resolves every symbol it names); each returns 1 with a
+ * message, and the solver reaches them only with those options selected. Struct
+ * arguments are opaque here.
  * src/reactiveTransport/reactiveCartesianTransport.h:34-35 (Cartesian descriptor),
- * :44-49 (implicit geometry); reactiveTurbulence.h:69-81 (WALE PR properties);
- * reactiveCapillaryResident.h:26-41 (resident capillary closure). */
+ * :44-49 (implicit geometry); reactiveTurbulence.h:69-81 (WALE PR properties). */
 int reactive_transport_install_cartesian_v1(void* transport, const void* mesh);
 int reactive_transport_cartesian_info_v1(void* transport, void* info);
 int reactive_transport_set_implicit_v1(void* transport, const void* options);
@@ -148,10 +147,33 @@ int reactive_transport_wale_pr_properties_v1(void* transport, const void* epoch,
 int reactive_transport_wale_pr_properties_v2(void* transport, const void* epoch, const double* q,
     size_t qStride, const ReactiveThermoState* state, int statesUnchanged);
 int reactive_transport_wale_pr_profile_v1(void* transport, void* profile);
+/* The resident capillary closure (src/reactiveTransport/reactiveCapillaryResident.h:26-41,
+ * reactiveTransport.cpp:963-1127): the outer iteration between the capillary HEM
+ * flash and the diffuse geometry with every per-cell array on the device; the
+ * caller keeps the iteration control (src/reactiveFoam/reactiveCapillary.H:54-115).
+ * begin: q (`species` = the transport's species masses per cell), the
+ * transported liquid inventory, the bulk energy (kinetic removed, surface energy
+ * not), the incoming states and the fixed colors; builds the seeds (each state
+ * carrying its cell's liquid inventory), their color and geometry.
+ * select: snapshots the iteration's color, jump and surface energy, and fills the
+ * view for reactive_gpu_hem_run_resident_v1: the bulk energy less the surface
+ * energy, the capillary records, and `order` with the cells to flash first (all
+ * at iteration 0, later those whose color, jump or surface energy changed
+ * bitwise since their last flash; heavy-first by the HEM bucket key), `count` of them.
+ * update (after a fully successful flash of `count` cells): records the flashed
+ * inputs, the candidate color from the flashed states, its geometry, and the
+ * residual max(|dc|, |dE_s| / max(|E_bulk|, 1e5 rho), |dJ| / max(p, 1)).
+ * relax: the color becomes 0.5 (before + candidate), geometry rebuilt.
+ * commit: downloads the states, color, surface energy and curvature; a later
+ * identical geometry request reuses that geometry.
+ * A nonzero *fallback means an input the host closure would reject (a color
+ * that does not close, a non-finite value): nothing host-side changed and the
+ * caller reruns the closure on the host path. Out-of-order calls return 1. */
 int reactive_transport_capillary_resident_begin_v1(void* transport, size_t species, const double* q,
     const double* liquid, const double* bulk, const ReactiveThermoState* states, const double* fixedColor,
     double sigma, int equilibrium, int* fallback);
-int reactive_transport_capillary_resident_select_v1(void* transport, int iteration, void* view, int* fallback);
+int reactive_transport_capillary_resident_select_v1(void* transport, int iteration,
+    ReactiveCapillaryResidentViewV1* view, int* fallback);
 int reactive_transport_capillary_resident_update_v1(void* transport, size_t count, double* residual,
     int* fallback);
 int reactive_transport_capillary_resident_relax_v1(void* transport);

@@ -14,6 +14,7 @@
  *   ReactiveWaleOptionsV1 / ProfileV1       src/reactiveTransport/reactiveTurbulence.h:12-19
  *   ReactiveWaleScalarOptionsV1 / ProfileV1 src/reactiveTransport/reactiveTurbulence.h:28-35
  *   ReactiveCapillaryOptionsV1 / ProfileV1  src/reactiveTransport/reactiveTransport.h:38-47
+ *   ReactiveCapillaryResidentViewV1         src/reactiveTransport/reactiveCapillaryResident.h:17-22
  *   ReactiveGasThermoSpecies/Region/Partition src/reactiveThermo/reactiveGasThermo.h:12-21
  *   ReactiveThermoState                     src/reactiveThermo/reactiveThermo.h:11-19
  *   ReactiveGpuHemProfileV1                 src/reactiveThermo/reactiveGpuHem.h:14-21
@@ -167,6 +168,21 @@ typedef struct ReactiveGpuHemOutputV1 {
     ReactiveThermoState state; int success, reserved;
 } ReactiveGpuHemOutputV1;
 
+/* The device view of one resident capillary iteration
+ * (src/reactiveTransport/reactiveCapillaryResident.h:17-22): DEVICE pointers for
+ * reactive_gpu_hem_run_resident_v1 (the first `count` entries of `order` are the
+ * cells to flash). */
+typedef struct ReactiveCapillaryResidentViewV1 {
+    uint32_t abiVersion, structBytes;
+    const double* q;
+    const double* energy;
+    const ReactiveThermoState* seed;
+    const ReactiveGpuHemCapillaryInputV2* capillary;
+    const uint32_t* order;
+    ReactiveGpuHemOutputV1* output;
+    size_t count;
+} ReactiveCapillaryResidentViewV1;
+
 /* The HEM model image. The reference passes an opaque 47,448-byte POD image
  * (src/reactiveThermo/reactiveDeviceFlash.h:39-53, static_assert at :52);
  * this is the same layout so an exported image can be handed over unchanged. */
@@ -215,6 +231,7 @@ static_assert(sizeof(ReactiveWaleScalarOptionsV1) == 24, "WALE scalar options la
 static_assert(sizeof(ReactiveWaleScalarProfileV1) == 32, "WALE scalar profile layout");
 static_assert(sizeof(ReactiveCapillaryOptionsV1) == 40, "capillary options layout");
 static_assert(sizeof(ReactiveCapillaryProfileV1) == 64, "capillary profile layout");
+static_assert(sizeof(ReactiveCapillaryResidentViewV1) == 64, "resident capillary view layout");
 static_assert(sizeof(ReactiveGpuHemOutputV1) == 184, "HEM output layout");
 static_assert(sizeof(ReactiveB200HemModel) == 47448, "HEM model image layout");
 static_assert(offsetof(ReactiveB200HemModel, stableGasPrune) == 45004, "HEM model image layout");

@@ -94,6 +94,11 @@ class CapillaryProfile(C.Structure):
                                   "colorUploadBytes", "geometryDownloadBytes", "capillaryWorkspaceBytes")]
 
 
+class CapillaryResidentView(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32)] + [
+        (n, C.c_void_p) for n in ("q", "energy", "seed", "capillary", "order", "output")] + [("count", C.c_size_t)]
+
+
 class ThermoState(C.Structure):
     _fields_ = [(k, C.c_double) for k in (
         "p", "T", "rho", "e", "entropy", "soundFrozen", "soundEquilibrium",

@@ -45,6 +45,12 @@ TRANSPORT = {
     "set_capillary_v1": ([_v, C.POINTER(A.CapillaryOptions)], C.c_int),
     "capillary_geometry_v1": ([_v, _d, _d, _d, _d, _d], C.c_int),
     "capillary_profile_v1": ([_v, C.POINTER(A.CapillaryProfile)], C.c_int),
+    "capillary_resident_begin_v1": ([_v, C.c_size_t, _d, _d, _d, _v, _d, C.c_double, C.c_int, C.POINTER(C.c_int)],
+                                    C.c_int),
+    "capillary_resident_select_v1": ([_v, C.c_int, C.POINTER(A.CapillaryResidentView), C.POINTER(C.c_int)], C.c_int),
+    "capillary_resident_update_v1": ([_v, C.c_size_t, _d, C.POINTER(C.c_int)], C.c_int),
+    "capillary_resident_relax_v1": ([_v], C.c_int),
+    "capillary_resident_commit_v1": ([_v, _v, _d, _d, _d], C.c_int),
     "layout_v3": ([_v, C.POINTER(C.c_size_t)] * 1 + [C.POINTER(C.c_size_t)] * 3, C.c_int),
     "fill_fixed_v3": ([_v, _v, _v, _v], C.c_int),
     "stage_device_v3": ([_v, _v, _v, _v, C.c_double, C.c_int, _v, _v], C.c_int),

@@ -7,6 +7,8 @@
 // src/reactiveTransport/reactiveTransport.h:48-141. Execution is CUDA only:
 // backend 0 (the reference's serial CPU loop) is rejected, never emulated.
 #include "cartesian_kernels.cuh"
+#include "capillary_resident.cuh"
+#include <cub/device/device_radix_sort.cuh>
 #include "../../include/reactive_b200_transport.h"
 
 #include <algorithm>
@@ -84,6 +86,25 @@ struct Transport {
     std::vector<double> colorShadow, fixedColorShadow, energyShadow, curvatureShadow;
     uint64_t geometryBuildsSkipped = 0;
     double* colorDevice = nullptr;  // cells + fixed
+    // the resident capillary closure's device buffers (allocated by its first begin)
+    struct CapillaryResident {
+        size_t cells = 0, species = 0, sortBytes = 0;
+        double sigma = 0;
+        int equilibrium = 1;
+        bool ready = false;
+        double *q = nullptr, *bulk = nullptr, *energy = nullptr, *color = nullptr, *jump = nullptr;
+        double *colorBefore = nullptr, *jumpBefore = nullptr, *energyBefore = nullptr;
+        double *flashedColor = nullptr, *flashedJump = nullptr, *flashedEnergy = nullptr;
+        ReactiveThermoState* seed = nullptr;
+        ReactiveGpuHemOutputV1* output = nullptr;
+        ReactiveGpuHemCapillaryInputV2* capillary = nullptr;
+        uint16_t *keys = nullptr, *sortedKeys = nullptr;
+        uint32_t *cells32 = nullptr, *order = nullptr;
+        void* sortTemp = nullptr;
+        unsigned long long* scalars = nullptr;  // [0] dirty count, [1] residual bits
+        unsigned* flags = nullptr;
+        std::vector<double> fixedColor;
+    } resident;
     std::string physicalHash;
     uint64_t attemptId = 0, lastAttempt = 0, tokenStage = 0;
     bool attemptOpen = false;
@@ -941,6 +962,217 @@ struct Transport {
         capillaryProfile.colorUploadBytes += (cfg.cells + cfg.fixed) * sizeof(double);
         capillaryProfile.geometryDownloadBytes +=
             cfg.cells * sizeof(double) * (1 + (curvature ? 1 : 0) + (normal ? 3 : 0));
+    }
+    // ------------------------------------------- resident capillary closure
+    // (src/reactiveTransport/reactiveTransport.cpp:963-1127)
+    unsigned residentGrid(size_t n) const { return unsigned(std::min<size_t>(65535, (n + 255) / 256)); }
+    // All buffers or none: a budget or allocation failure frees what this call
+    // allocated, so a retry starts from the same state.
+    void residentAllocate(size_t species) {
+        const size_t n = cfg.cells;
+        if (resident.cells == n && resident.species == species) return;
+        require(!resident.cells, "Resident capillary species count changed");
+        require(species == cfg.species && n <= size_t(std::numeric_limits<int>::max()),
+                "Resident capillary species/count exceeds the transport or sort layout");
+        CapillaryResident r;
+        std::vector<void*> fresh;
+        uint64_t freshBytes = 0;
+        auto get = [&](size_t bytes) -> void* {
+            require(double(arena.bytes) + double(freshBytes) + double(bytes) <= arena.limit,
+                    "Resident capillary closure exceeds the transport workspace budget");
+            void* p = nullptr;
+            check(cudaMalloc(&p, std::max<size_t>(bytes, 1)), "cudaMalloc");
+            fresh.push_back(p);
+            freshBytes += bytes;
+            return p;
+        };
+        try {
+            r.cells = n;
+            r.species = species;
+            r.q = static_cast<double*>(get(product(product(n, species), sizeof(double))));
+            double** arrays[] = {&r.bulk, &r.energy, &r.color, &r.jump, &r.colorBefore, &r.jumpBefore,
+                                 &r.energyBefore, &r.flashedColor, &r.flashedJump, &r.flashedEnergy};
+            for (double** a : arrays) *a = static_cast<double*>(get(product(n, sizeof(double))));
+            r.seed = static_cast<ReactiveThermoState*>(get(product(n, sizeof(ReactiveThermoState))));
+            r.output = static_cast<ReactiveGpuHemOutputV1*>(get(product(n, sizeof(ReactiveGpuHemOutputV1))));
+            r.capillary = static_cast<ReactiveGpuHemCapillaryInputV2*>(
+                get(product(n, sizeof(ReactiveGpuHemCapillaryInputV2))));
+            r.keys = static_cast<uint16_t*>(get(product(n, sizeof(uint16_t))));
+            r.sortedKeys = static_cast<uint16_t*>(get(product(n, sizeof(uint16_t))));
+            r.cells32 = static_cast<uint32_t*>(get(product(n, sizeof(uint32_t))));
+            r.order = static_cast<uint32_t*>(get(product(n, sizeof(uint32_t))));
+            r.scalars = static_cast<unsigned long long*>(get(2 * sizeof(unsigned long long)));
+            r.flags = static_cast<unsigned*>(get(sizeof(unsigned)));
+            check(cub::DeviceRadixSort::SortPairs(nullptr, r.sortBytes, r.keys, r.sortedKeys, r.cells32, r.order,
+                                                  int(n), 0, 9, stream),
+                  "sort size");
+            r.sortTemp = get(std::max<size_t>(r.sortBytes, 1));
+            capres::identity<<<residentGrid(n), 256, 0, stream>>>(n, r.cells32);
+            launched();
+            check(cudaMemsetAsync(r.output, 0, product(n, sizeof(ReactiveGpuHemOutputV1)), stream), "memset");
+            finish();
+        } catch (...) {
+            cudaStreamSynchronize(stream);
+            for (void* p : fresh) cudaFree(p);
+            throw;
+        }
+        arena.blocks.insert(arena.blocks.end(), fresh.begin(), fresh.end());
+        arena.bytes += freshBytes;
+        arena.peak = std::max(arena.peak, arena.bytes);
+        capillaryProfile.capillaryWorkspaceBytes += freshBytes;
+        resident = std::move(r);
+    }
+    void residentClearFlags() {
+        check(cudaMemsetAsync(resident.flags, 0, sizeof(unsigned), stream), "memset");
+        check(cudaMemsetAsync(resident.scalars, 0, 2 * sizeof(unsigned long long), stream), "memset");
+    }
+    unsigned residentFlags(unsigned long long* scalars = nullptr) {
+        unsigned f = 0;
+        download(&f, resident.flags, 1);
+        if (scalars) download(scalars, resident.scalars, 2);
+        finish();
+        return f;
+    }
+    // The diffuse geometry of the device color and the jump sigma*kappa.
+    void residentGeometry() {
+        auto& r = resident;
+        const size_t n = cfg.cells;
+        geometryShadowValid = false;
+        colorReady = false;
+        check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
+        check(cudaMemcpyAsync(colorDevice, r.color, n * sizeof(double), cudaMemcpyDeviceToDevice, stream), "D2D");
+        ++deviceCopies;
+        upload(colorDevice + n, r.fixedColor.data(), cfg.fixed);
+        const unsigned blocks = unsigned(std::min<size_t>((n + 255) / 256, 148 * 16));
+        interfaceGradient<<<blocks, 256, 0, stream>>>(v);
+        launched();
+        interfaceCurvature<<<blocks, 256, 0, stream>>>(v);
+        launched();
+        capres::pressureJump<<<residentGrid(n), 256, 0, stream>>>(n, r.sigma, v.cCurv, r.jump);
+        check(cudaGetLastError(), "kernel launch");
+        unsigned status = 0;
+        download(&status, flags, 1);
+        finish();
+        require(!(status & kCapillaryBit), "Invalid capillary geometry");
+        colorReady = true;
+        ++capillaryProfile.geometryBuilds;
+        capillaryProfile.geometryCells += n;
+        capillaryProfile.geometryKernels += 2;
+        capillaryProfile.colorUploadBytes += cfg.fixed * sizeof(double);
+    }
+    void residentBegin(size_t species, const double* hq, const double* liquid, const double* bulk,
+                       const ReactiveThermoState* states, const double* fixedColor, double sigma, int equilibrium,
+                       int* fallback) {
+        require(v.capillary, "Resident capillary closure needs CUDA diffuse geometry");
+        require(species > 0 && hq && liquid && bulk && states && fallback && (!cfg.fixed || fixedColor)
+                    && std::isfinite(sigma) && (equilibrium == 0 || equilibrium == 1),
+                "Invalid resident capillary input");
+        for (size_t c = 0; c < cfg.fixed; ++c)
+            require(std::isfinite(fixedColor[c]) && fixedColor[c] >= 0 && fixedColor[c] <= 1,
+                    "Invalid fixed material color");
+        residentAllocate(species);
+        auto& r = resident;
+        const size_t n = cfg.cells;
+        r.sigma = sigma;
+        r.equilibrium = equilibrium;
+        r.ready = false;
+        r.fixedColor.assign(fixedColor, fixedColor + cfg.fixed);
+        residentClearFlags();
+        upload(r.q, hq, product(n, species));
+        upload(r.bulk, bulk, n);
+        upload(r.seed, states, n);
+        upload(r.energy, liquid, n);  // the liquid inventory, folded into the seeds below
+        capres::seedStates<<<residentGrid(n), 256, 0, stream>>>(n, r.seed, r.energy, r.color, r.flags);
+        check(cudaGetLastError(), "kernel launch");
+        if ((*fallback = residentFlags() != 0)) return;
+        residentGeometry();
+        r.ready = true;
+    }
+    void residentSelect(int iteration, ReactiveCapillaryResidentViewV1& view, int* fallback) {
+        auto& r = resident;
+        const size_t n = cfg.cells;
+        require(r.ready && fallback && view.abiVersion == 1 && view.structBytes == sizeof(view),
+                "Resident capillary select out of order");
+        residentClearFlags();
+        capres::selectDirty<<<unsigned((n + 255) / 256), 256, 0, stream>>>(
+            n, iteration == 0, r.equilibrium, int(r.species), r.q, r.seed, r.bulk, r.color, r.jump, v.cEnergy,
+            r.colorBefore, r.jumpBefore, r.energyBefore, r.flashedColor, r.flashedJump, r.flashedEnergy, r.energy,
+            r.capillary, r.keys, r.scalars, r.flags);
+        check(cudaGetLastError(), "kernel launch");
+        size_t bytes = r.sortBytes;
+        check(cub::DeviceRadixSort::SortPairs(r.sortTemp, bytes, r.keys, r.sortedKeys, r.cells32, r.order, int(n), 0,
+                                              9, stream),
+              "sort");
+        unsigned long long scalars[2] = {0, 0};
+        if ((*fallback = residentFlags(scalars) != 0)) {
+            r.ready = false;
+            return;
+        }
+        view.q = r.q;
+        view.energy = r.energy;
+        view.seed = r.seed;
+        view.capillary = r.capillary;
+        view.order = r.order;
+        view.output = r.output;
+        view.count = size_t(scalars[0]);
+    }
+    void residentUpdate(size_t count, double* residual, int* fallback) {
+        auto& r = resident;
+        const size_t n = cfg.cells;
+        require(r.ready && residual && fallback && count <= n, "Resident capillary update out of order");
+        residentClearFlags();
+        if (count) {
+            capres::recordFlashed<<<residentGrid(count), 256, 0, stream>>>(count, r.order, r.colorBefore,
+                                                                          r.jumpBefore, r.energyBefore, r.flashedColor,
+                                                                          r.flashedJump, r.flashedEnergy);
+            check(cudaGetLastError(), "kernel launch");
+        }
+        capres::candidateColor<<<residentGrid(n), 256, 0, stream>>>(n, r.output, r.color, r.flags);
+        check(cudaGetLastError(), "kernel launch");
+        if ((*fallback = residentFlags() != 0)) {
+            r.ready = false;
+            return;
+        }
+        residentGeometry();
+        capres::closureResidual<<<unsigned((n + 255) / 256), 256, 0, stream>>>(
+            n, r.color, r.colorBefore, v.cEnergy, r.energyBefore, r.jump, r.jumpBefore, r.bulk, r.output,
+            r.scalars + 1, r.flags);
+        check(cudaGetLastError(), "kernel launch");
+        unsigned long long scalars[2] = {0, 0};
+        if ((*fallback = residentFlags(scalars) != 0)) {
+            r.ready = false;
+            return;
+        }
+        std::memcpy(residual, &scalars[1], sizeof(double));
+    }
+    void residentRelax() {
+        auto& r = resident;
+        require(r.ready, "Resident capillary relaxation out of order");
+        capres::relaxColor<<<residentGrid(cfg.cells), 256, 0, stream>>>(cfg.cells, r.colorBefore, r.color);
+        check(cudaGetLastError(), "kernel launch");
+        residentGeometry();
+    }
+    void residentCommit(ReactiveThermoState* states, double* color, double* energy, double* curvature) {
+        auto& r = resident;
+        const size_t n = cfg.cells;
+        require(r.ready && states && color && energy && curvature, "Resident capillary commit out of order");
+        // the closure is over: the seed buffer stages the states' download
+        capres::gatherStates<<<residentGrid(n), 256, 0, stream>>>(n, r.output, r.seed);
+        check(cudaGetLastError(), "kernel launch");
+        download(states, r.seed, n);
+        download(color, r.color, n);
+        download(energy, v.cEnergy, n);
+        download(curvature, v.cCurv, n);
+        finish();
+        capillaryProfile.geometryDownloadBytes += n * 2 * sizeof(double);
+        // the published geometry is exactly the build of `color`: a later
+        // identical host request reuses it
+        colorShadow.assign(color, color + n);
+        fixedColorShadow = r.fixedColor;
+        energyShadow.assign(energy, energy + n);
+        curvatureShadow.assign(curvature, curvature + n);
+        geometryShadowValid = true;
+        r.ready = false;
     }
     void installWale(const ReactiveWaleOptionsV1& options) {
         require(options.abiVersion == 1 && options.structBytes == sizeof(options), "Invalid WALE options ABI");

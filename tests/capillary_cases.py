@@ -169,3 +169,65 @@ def relative(a, b):
     a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
     return float(np.max(np.abs(a - b) / np.maximum(1e-300, np.maximum(np.abs(b), np.max(np.abs(b)) * 1e-3)),
                         initial=0))
+
+
+def drop_case(n=10, temperature=270.0, pressure=5e6, radius=.3, vapour=.6):
+    """A liquid N2O drop in air and N2O vapour on an n^3 box of the production
+    model's four species (N2, O2, N2O, isopropanol; nv = 9, the liquid inventory
+    at 8): color 0.5 (1 - tanh((r - R) / 1.5h)) with R = radius * edge; each cell
+    mixes, by that volume fraction, compressed liquid N2O and the gas (air with N2O
+    mass fraction `vapour`), both at (temperature, pressure), from the reference's
+    mixture evaluator; the states are their flash (the production model,
+    finite-difference Jacobian), the liquid inventory their liquid mass. Returns
+    the case dict, the model image and the states."""
+    from oracle import oracle
+    from spuma_multiphysics_b200 import cases, thermo_data as td
+    from spuma_multiphysics_b200.hem import GpuHem
+    ns, nv = 4, 9
+    image = td.model_bytes(td.production_model(analytic_jacobian=0))
+    lib = oracle.ref_flash_lib()
+
+    def props(Y, choice):
+        out = (C.c_double * (15 + ns))()
+        phase = C.c_int()
+        st = lib.ref_pr_mix_tp(image, 0, C.c_double(temperature), C.c_double(pressure), (C.c_double * ns)(*Y),
+                               choice, 0, out,
+                               C.byref(phase))
+        assert st == 0
+        return out[4], out[5]   # rho, e
+
+    rho_l, e_l = props([0, 0, 1, 0], 2)
+    y_gas = np.array([.767 * (1 - vapour), .233 * (1 - vapour), vapour, 0.0])
+    rho_g, e_g = props(y_gas, 1)
+    faces, volume = cases.box_faces((n, n, n), .08 / n)
+    h = .08 / n
+    x = (np.arange(n) + .5) * h
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    r = np.sqrt((X - .04) ** 2 + (Y - .04) ** 2 + (Z - .04) ** 2).transpose(2, 1, 0).ravel()  # x fastest
+    color = .5 * (1 - np.tanh((r - radius * .08) / (1.5 * h)))
+    nc = n ** 3
+    q = np.zeros((nc, nv))
+    q[:, :ns] = (color * rho_l)[:, None] * np.array([0, 0, 1.0, 0]) + ((1 - color) * rho_g)[:, None] * y_gas
+    energy = color * rho_l * e_l + (1 - color) * rho_g * e_g
+    q[:, ns + 3] = energy
+    guess = np.zeros(nc, dtype=A.THERMO_DTYPE)
+    guess["p"], guess["T"], guess["rho"] = pressure, temperature, q[:, :ns].sum(axis=1)
+    guess["liquidMass"][:, 0] = color * rho_l
+    hem = GpuHem(model=image, capacity=nc)
+    try:
+        states = guess.copy()
+        ok, _ = hem.run(np.ascontiguousarray(q[:, :ns]), energy, states)
+    finally:
+        hem.close()
+    assert ok.all(), int((ok == 0).sum())
+    q[:, ns + 4] = states["liquidMass"][:, 0]
+    fa = (A.Face * len(faces)).from_buffer_copy(np.ascontiguousarray(faces).tobytes())
+    cfg = A.Config(nc, ns, nv, len(faces), 0, 0.0, 0.0, 0.0, 1.1, 4e9, 0)
+    fixed_states = np.zeros(1, dtype=A.STATE_DTYPE)
+    case = dict(config=cfg, faces=fa, volume=np.ascontiguousarray(volume), q=q, states=None, y=None, h=None,
+                fixed_q=np.zeros((1, nv)), fixed_states=fixed_states,
+                fixed_states_ptr=C.cast(T.states_ptr(fixed_states), C.c_void_p), fixed_y=np.zeros((1, ns)),
+                fixed_h=np.zeros((1, ns)), ns=ns, nc=nc, nv=nv, mechanical=False, color=color, fixed_color=None,
+                species=2, name=f"drop{n}")
+    return case, image, states
+
