@@ -43,7 +43,11 @@ int reactive_gpu_hem_run_v1(void* hem, const double* q, const double* energy, si
  * run_resident_v1: device pointers indexed by global cell, order[0..count) names the cells, each
  * result (state, success) goes to output[cell] (reserved untouched), a failed cell returns its
  * seed; capillary may be NULL for the plain flash; synchronous, batch totals in *profile.
- * src/reactiveThermo/reactiveGpuHem.h:66-71 (primitive initialisation) returns 1 with a message. */
+ * initialize_tp_v1 (src/reactiveThermo/reactiveGpuHem.h:66-71, every record's equilibrium 0):
+ * at each seed's (p, T) and liquid mass, with the gas at p - color*jump and the liquid at
+ * p + (1 - color)*jump, the densities scaled so the phase volumes fill the cell; q, energy and
+ * state become the normalised densities, their energy and the state only if every cell succeeds
+ * (success per cell either way); on the same engine. */
 int reactive_gpu_hem_run_v2(void* hem, const double* q, const double* energy,
     const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* state, int* success,
     ReactiveGpuHemProfileV1* profile, char* error, size_t errorSize);

@@ -130,6 +130,9 @@ def ref_flash_lib():
                                                     C.POINTER(C.c_int), _v, C.POINTER(C.c_int),
                                                     C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.c_int]
         lib.ref_flash_recover_capillary.restype = C.c_int
+        lib.ref_flash_initialize_tp.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _d, _d, _v,
+                                                C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.ref_flash_initialize_tp.restype = C.c_int
         lib.ref_pr_evaluate_tp.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _d,
                                            C.POINTER(C.c_int)]
         lib.ref_pr_evaluate_trho.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, _d,
@@ -206,6 +209,25 @@ def ref_flash_recover_capillary(model_image, q, energy, guess, color, jump, equi
     if rc:
         raise RuntimeError("reference flash rejected the model image")
     return out, success, status, counters
+
+
+def ref_flash_initialize_tp(model_image, q, energy, guess, color, jump):
+    """The reference's capillary primitive initialisation on the host, per cell:
+    (normalised q, normalised energy, states, success, status); q and energy
+    keep their inputs where a cell fails."""
+    q = np.array(q, dtype=np.float64, order="C")
+    energy = np.array(energy, dtype=np.float64, order="C")
+    count = len(energy)
+    out = np.zeros(count, dtype=guess.dtype)
+    success = np.zeros(count, dtype=np.int32)
+    status = np.zeros(count, dtype=np.int32)
+    rc = ref_flash_lib().ref_flash_initialize_tp(
+        model_image, count, _p(q), _p(energy), guess.ctypes.data_as(_v),
+        _p(np.ascontiguousarray(color, dtype=np.float64)), _p(np.ascontiguousarray(jump, dtype=np.float64)),
+        out.ctypes.data_as(_v), success.ctypes.data_as(C.POINTER(C.c_int)), status.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc:
+        raise RuntimeError("reference flash rejected the model image")
+    return q, energy, out, success, status
 
 
 def cpu_threads():

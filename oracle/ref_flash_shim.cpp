@@ -15,6 +15,8 @@
 //   ref_flash_recover_capillary  ReactiveDeviceFlash::recoverCapillary per cell
 //                                (reactiveDeviceFlash.h:572-588): per-cell color,
 //                                pressure jump and equilibrium flag; status per cell
+//   ref_flash_initialize_tp      ReactiveDeviceFlash::initializeCapillaryTP per cell
+//                                (reactiveDeviceFlash.h:589-613)
 //   ref_pr_evaluate_tp / _trho   ReactiveDevicePR::evaluateTPTrusted / evaluateTrhoTrusted
 //                                (reactiveDevicePR.h:575, :474) for EOS unit checks
 //   ref_pr_mix_tp / _trho        the same for a mixture table with mass fractions Y
@@ -124,6 +126,40 @@ int ref_flash_recover_capillary(const void* image, size_t count, const double* q
         std::vector<std::thread> pool;
         for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
         for (auto& t : pool) t.join();
+    }
+    delete m;
+    return 0;
+}
+
+// The capillary primitive initialisation (initializeCapillaryTP,
+// reactiveDeviceFlash.h:589-613) per cell: q and energy are replaced by the
+// normalised densities where a cell succeeds; out receives the state.
+int ref_flash_initialize_tp(const void* image, size_t count, double* q, double* energy,
+                            const ReactiveThermoState* guess, const double* color, const double* jump,
+                            ReactiveThermoState* out, int* success, int* status) {
+    Model* m = new Model;
+    std::memcpy(m, image, sizeof(Model));
+    if (!ReactiveDeviceFlash::validModel(*m)) { delete m; return 1; }
+    Cache cache[2]{};
+    for (int i = 0; i < m->nl && i < 2; ++i)
+        ReactiveDevicePRPurePhaseCache::buildPureReportedPhaseCache(m->phase[i + 1], cache[i]);
+    const int ns = m->ns;
+    for (size_t c = 0; c < count; ++c) {
+        ReactiveDeviceFlash::Input in{};
+        for (int k = 0; k < ns; ++k) in.q[k] = q[c * ns + k];
+        in.energy = energy[c];
+        in.guess = guess[c];
+        double mass[ReactiveDeviceFlash::maxSpecies]{};
+        double e = energy[c];
+        const ReactiveDeviceFlash::Output o =
+            ReactiveDeviceFlash::initializeCapillaryTP(*m, in, color[c], jump[c], mass, e, cache);
+        out[c] = o.state;
+        success[c] = o.success;
+        status[c] = o.status;
+        if (o.success) {
+            for (int k = 0; k < ns; ++k) q[c * ns + k] = mass[k];
+            energy[c] = e;
+        }
     }
     delete m;
     return 0;

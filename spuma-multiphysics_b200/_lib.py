@@ -74,6 +74,8 @@ HEM = {
                C.c_int),
     "run_resident_v1": ([_v, _v, _v, _v, _v, _v, C.c_size_t, _v, C.POINTER(A.HemProfile), C.c_char_p, C.c_size_t],
                         C.c_int),
+    "initialize_tp_v1": ([_v, _d, _d, _v, C.c_size_t, _v, C.POINTER(C.c_int), C.POINTER(A.HemProfile), C.c_char_p,
+                          C.c_size_t], C.c_int),
     "device_bytes_v1": ([_v], C.c_size_t),
     "destroy_v1": ([_v], None),
     "run_v1": ([_v, _d, _d, C.c_size_t, _v, C.POINTER(C.c_int), C.POINTER(A.HemProfile), C.c_char_p, C.c_size_t],

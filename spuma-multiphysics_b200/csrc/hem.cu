@@ -1289,15 +1289,47 @@ int reactive_gpu_hem_run_v2(void* raw, const double* q, const double* energy,
     }
     return reactive_gpu_hem_run_v1(raw, q, energy, count, states, success, profile, error, size);
 }
-int reactive_gpu_hem_initialize_tp_v1(void*, double*, double*, const ReactiveGpuHemCapillaryInputV2*, size_t,
-                                      ReactiveThermoState*, int*, ReactiveGpuHemProfileV1*, char* error, size_t size) {
-    if (error && size) std::snprintf(error, size, "Capillary primitive initialisation is not part of this B200 build");
-    return 1;
+// src/reactiveTransport/reactiveGpuHem.cuh:403-408: the capillary primitive
+// initialisation (every record's equilibrium 0) on the multi-species engine.
+int reactive_gpu_hem_initialize_tp_v1(void* raw, double* q, double* energy,
+                                      const ReactiveGpuHemCapillaryInputV2* capillary, size_t count,
+                                      ReactiveThermoState* states, int* success, ReactiveGpuHemProfileV1* profile,
+                                      char* error, size_t size) {
+    try {
+        rb200::require(q && energy && capillary, "Null CUDA primitive input");
+        rb200::require(raw && states && success && profile && profile->abiVersion == 1
+                           && profile->structBytes == sizeof(*profile),
+                       "Invalid CUDA HEM batch arguments");
+        auto& d = *static_cast<HemDevice*>(raw);
+        for (size_t c = 0; c < count; ++c) {
+            const auto& in = capillary[c];
+            rb200::require(std::isfinite(in.color) && in.color >= 0 && in.color <= 1 && std::isfinite(in.pressureJump)
+                               && in.equilibrium == 0,
+                           "Invalid CUDA HEM capillary cell input");
+        }
+        std::lock_guard<std::mutex> lock(d.entry);
+        rb200::require(count && count <= d.capacity, "CUDA HEM batch exceeds capacity");
+        rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
+        rb200::MixtureFlash* engine = d.capillaryFlash();
+        rb200::require(engine, "Capillary primitive initialisation needs a model image with analyticJacobian = 0 on "
+                               "this build");
+        ReactiveGpuHemProfileV1 p{};
+        p.abiVersion = 1;
+        p.structBytes = sizeof(p);
+        rb200::mixtureInitialize(engine, q, energy, count, capillary, states, success, p);
+        *profile = p;
+        return 0;
+    } catch (const std::exception& e) {
+        if (error && size) std::snprintf(error, size, "%s", e.what());
+        return 1;
+    }
 }
-// The reference's device-resident batch (src/reactiveThermo/reactiveGpuHem.h:72-84)
-// for UV phase equilibrium without a pressure jump (capillary may be NULL, or
-// hold pressureJump = 0 and equilibrium = 1 for every named cell): gather the
-// named cells, the work-queue search, failed cells keep their seed, scatter to
+// The reference's device-resident batch (src/reactiveThermo/reactiveGpuHem.h:72-84).
+// With capillary records (or a multi-species handle) it runs on the
+// multi-species engine; a pure-fluid image outside that engine's scope takes
+// UV equilibrium without a pressure jump (capillary NULL, or pressureJump = 0
+// and equilibrium = 1 for every named cell) on its fast path: gather the named
+// cells, the work-queue search, failed cells keep their seed, scatter to
 // output[cell]. Synchronous on the handle's stream; only batch totals reach
 // the host.
 int reactive_gpu_hem_run_resident_v1(void* raw, const double* q, const double* energy, const ReactiveThermoState* seed,

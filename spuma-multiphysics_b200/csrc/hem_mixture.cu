@@ -36,6 +36,7 @@
 #include <chrono>
 #include <cstring>
 #include <memory>
+#include <vector>
 
 namespace rb200 {
 namespace {
@@ -806,6 +807,50 @@ __global__ void __launch_bounds__(kBlock) mixtureFlashKernel(const ReactiveB200H
     atomicAdd(totals + M_SUCCEEDED, succeeded);
 }
 
+// The capillary primitive initialisation (initializeCapillaryTP,
+// src/reactiveThermo/reactiveDeviceFlash.h:589-613), one thread per cell: at the
+// seed's (p, T) and liquid mass, with the gas at p - color*jump and the liquid
+// at p + (1 - color)*jump, scale the densities so the phase volumes fill the
+// cell; q and energy become the normalised densities and their energy where a
+// cell succeeds.
+__global__ void __launch_bounds__(kBlock) mixtureInitializeKernel(const ReactiveB200HemModel* __restrict__ model,
+                                                                 double* q, double* energy, size_t count,
+                                                                 const ReactiveThermoState* __restrict__ seed,
+                                                                 const ReactiveGpuHemCapillaryInputV2* capillary,
+                                                                 ReactiveThermoState* out, int* success,
+                                                                 unsigned long long* totals) {
+    const ReactiveB200HemModel& m = *model;
+    Tally n;
+    unsigned long long succeeded = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(blockDim.x) * gridDim.x) {
+        MixCell c{m, {0, 0, 0, 0}, energy[i], seed[i], false, n};
+        for (int k = 0; k < m.ns && k < kNs; ++k) c.q[k] = q[i * size_t(m.ns) + k];
+        c.color = capillary[i].color;
+        c.jump = capillary[i].pressureJump;
+        bool ok = m.nl == 1 && m.condensedKind[0] == 0 && fin(c.color) && c.color >= 0 && c.color <= 1 && fin(c.jump);
+        double liquid[kLiq] = {c.guess.liquidMass[0], 0};
+        MixEval unit, value;
+        if (ok) ok = evaluate(c, liquid, c.guess.p, c.guess.T, unit, false, nullptr) && fin(unit.volume)
+                     && unit.volume > 0;
+        if (ok) {
+            for (int k = 0; k < m.ns; ++k) c.q[k] /= unit.volume;
+            liquid[0] /= unit.volume;
+            ok = evaluate(c, liquid, c.guess.p, c.guess.T, value, false, nullptr) && fin(value.energy)
+                 && fabs(value.volume - 1) <= m.vtol;
+        }
+        if (ok) {
+            value.s.volumeResidual = fabs(value.volume - 1);
+            for (int k = 0; k < m.ns; ++k) q[i * size_t(m.ns) + k] = c.q[k];
+            energy[i] = value.energy;
+            out[i] = value.s;
+        } else out[i] = c.guess;
+        success[i] = ok ? 1 : 0;
+        succeeded += ok ? 1 : 0;
+    }
+    atomicAdd(totals + M_PHASES, n.phases);
+    atomicAdd(totals + M_SUCCEEDED, succeeded);
+}
+
 bool finiteHost(double x) { return x == x && std::fabs(x) <= 1.79769313486231570815e308; }
 
 // The scope this build's mixture flash covers, on top of the reference's model
@@ -951,6 +996,52 @@ void mixtureRun(MixtureFlash* f, const double* q, const double* energy, size_t c
     p.kernelSeconds = kernel / 1000.;
     p.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
     p.copySeconds = std::max(0.0, p.wallSeconds - p.kernelSeconds);
+}
+
+void mixtureInitialize(MixtureFlash* f, double* q, double* energy, size_t count,
+                       const ReactiveGpuHemCapillaryInputV2* capillary, ReactiveThermoState* states, int* success,
+                       ReactiveGpuHemProfileV1& p) {
+    require(count && count <= f->capacity, "CUDA HEM batch exceeds capacity");
+    check(cudaSetDevice(f->device), "cudaSetDevice");
+    const auto begin = std::chrono::steady_clock::now();
+    cudaStream_t s = f->stream;
+    if (!f->capillary) f->capillary = f->alloc<ReactiveGpuHemCapillaryInputV2>(f->capacity);
+    const size_t qBytes = count * size_t(f->ns) * sizeof(double);
+    check(cudaMemcpyAsync(f->q, q, qBytes, cudaMemcpyHostToDevice, s), "H2D q");
+    check(cudaMemcpyAsync(f->energy, energy, count * sizeof(double), cudaMemcpyHostToDevice, s), "H2D e");
+    check(cudaMemcpyAsync(f->seed, states, count * sizeof(ReactiveThermoState), cudaMemcpyHostToDevice, s), "H2D seed");
+    check(cudaMemcpyAsync(f->capillary, capillary, count * sizeof(ReactiveGpuHemCapillaryInputV2),
+                          cudaMemcpyHostToDevice, s),
+          "H2D capillary");
+    check(cudaMemsetAsync(f->totals, 0, M_COUNT * sizeof(unsigned long long), s), "memset");
+    mixtureInitializeKernel<<<gridFor(count, kBlock), kBlock, 0, s>>>(f->model, f->q, f->energy, count, f->seed,
+                                                                       f->capillary, f->out, f->success, f->totals);
+    check(cudaGetLastError(), "capillary initialisation");
+    std::vector<double> nq(count * size_t(f->ns)), ne(count);
+    std::vector<ReactiveThermoState> out(count);
+    check(cudaMemcpyAsync(nq.data(), f->q, qBytes, cudaMemcpyDeviceToHost, s), "D2H q");
+    check(cudaMemcpyAsync(ne.data(), f->energy, count * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H e");
+    check(cudaMemcpyAsync(out.data(), f->out, count * sizeof(ReactiveThermoState), cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(success, f->success, count * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H success");
+    unsigned long long t[M_COUNT] = {};
+    check(cudaMemcpyAsync(t, f->totals, sizeof(t), cudaMemcpyDeviceToHost, s), "D2H totals");
+    check(cudaStreamSynchronize(s), "sync");
+    p.batches = 1;
+    p.submitted = count;
+    p.succeeded = t[M_SUCCEEDED];
+    p.deviceFailures = count - p.succeeded;
+    p.phaseEvaluations = t[M_PHASES];
+    // the caller's arrays change only when every cell succeeded
+    if (!p.deviceFailures) {
+        std::memcpy(q, nq.data(), qBytes);
+        std::memcpy(energy, ne.data(), count * sizeof(double));
+        std::memcpy(states, out.data(), count * sizeof(ReactiveThermoState));
+    }
+    p.transferBytes = 2 * (qBytes + count * sizeof(double)) + count * (2 * sizeof(ReactiveThermoState) + sizeof(int)
+                                                                      + sizeof(ReactiveGpuHemCapillaryInputV2));
+    p.deviceBytes = f->bytes;
+    p.hostBytes = qBytes + count * (sizeof(double) + sizeof(ReactiveThermoState));
+    p.wallSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
 }
 
 void mixtureRunResident(MixtureFlash* f, const double* q, const double* energy, const ReactiveThermoState* seed,

@@ -23,6 +23,13 @@ size_t mixtureDeviceBytes(const MixtureFlash* flash);
 void mixtureRun(MixtureFlash* flash, const double* q, const double* energy, size_t count,
                 const ReactiveGpuHemCapillaryInputV2* capillary, ReactiveThermoState* states, int* success,
                 ReactiveGpuHemProfileV1& profile);
+// The reference's initialize_tp_v1 contract (capillary records with
+// equilibrium 0, already validated): q, energy and states become the
+// normalised densities, their energy and the states only if every cell
+// succeeds; success per cell either way.
+void mixtureInitialize(MixtureFlash* flash, double* q, double* energy, size_t count,
+                       const ReactiveGpuHemCapillaryInputV2* capillary, ReactiveThermoState* states, int* success,
+                       ReactiveGpuHemProfileV1& profile);
 // The reference's run_resident_v1 contract: DEVICE arrays indexed by cell,
 // order[0..count) names the cells, each result goes to output[cell] (a failed
 // cell gets its seed). Synchronous on the engine's stream; batch totals in profile.

@@ -84,6 +84,27 @@ class GpuHem:
             raise HemError(err.value.decode())
         return success, prof
 
+    def initialize_capillary(self, q, energy, capillary, states, success=None):
+        """The capillary primitive initialisation (reactive_gpu_hem_initialize_tp_v1)
+        on host arrays, in place: q (cell-major) and energy become the normalised
+        densities and their energy and states the initialised states, only if every
+        cell succeeds. Returns (success int32 array, profile)."""
+        assert q.dtype == np.float64 and q.flags.c_contiguous and energy.dtype == np.float64
+        capillary = np.ascontiguousarray(capillary, dtype=A.CAPILLARY_DTYPE)
+        n = len(energy)
+        if success is None:
+            success = np.zeros(n, dtype=np.int32)
+        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+        err = C.create_string_buffer(1024)
+        rc = self.lib.reactive_gpu_hem_initialize_tp_v1(self.handle, A.dptr(q), A.dptr(energy),
+                                                        capillary.ctypes.data_as(C.c_void_p), n,
+                                                        states.ctypes.data_as(C.c_void_p),
+                                                        success.ctypes.data_as(C.POINTER(C.c_int)), C.byref(prof),
+                                                        err, len(err))
+        if rc:
+            raise HemError(err.value.decode())
+        return success, prof
+
     def run_resident(self, q, energy, seed, capillary, order, count, output):
         """The device-resident batch (reactive_gpu_hem_run_resident_v1): device
         pointers or torch tensors indexed by cell; order[0..count) names the cells
