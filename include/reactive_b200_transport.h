@@ -129,24 +129,40 @@ int reactive_transport_set_capillary_v1(void* transport, const ReactiveCapillary
 int reactive_transport_capillary_geometry_v1(void* transport, const double* cellColor,
     const double* fixedColor, double* surfaceEnergy, double* curvature, double* normalXYZ);
 int reactive_transport_capillary_profile_v1(void* transport, ReactiveCapillaryProfileV1* profile);
-/* Entry points of the Cartesian implicit surface geometry and the WALE PR
- * properties, which the solver references statically (so that a solver linked
- * against this library resolves every symbol it names); each returns 1 with a
- * message, and the solver reaches them only with those options selected. Struct
- * arguments are opaque here.
+/* Entry points of the Cartesian implicit surface geometry, which the solver
+ * references statically (so that a solver linked against this library resolves
+ * every symbol it names); each returns 1 with a message, and the solver reaches
+ * them only with that option selected. Struct arguments are opaque here.
  * src/reactiveTransport/reactiveCartesianTransport.h:34-35 (Cartesian descriptor),
- * :44-49 (implicit geometry); reactiveTurbulence.h:69-81 (WALE PR properties). */
+ * :44-49 (implicit geometry). */
 int reactive_transport_install_cartesian_v1(void* transport, const void* mesh);
 int reactive_transport_cartesian_info_v1(void* transport, void* info);
 int reactive_transport_set_implicit_v1(void* transport, const void* options);
 int reactive_transport_implicit_coefficients_v1(void* transport, double* output, const double* restore,
     size_t count, size_t* required);
-int reactive_transport_set_wale_pr_model_v1(void* transport, const void* model);
-int reactive_transport_wale_pr_properties_v1(void* transport, const void* epoch, const double* q,
+/* The WALE Peng-Robinson scalar properties of the one-liquid capillary model
+ * (src/reactiveTransport/reactiveTurbulence.h:48-81, reactiveTransport.cpp:703-828):
+ * install once, before stepping, after set_capillary_v1 and set_wale_scalars_v1,
+ * with the model image (copied), the transport's physical model hash and the
+ * fixed cells' cp / species enthalpies; then each stage's (or CFL query's)
+ * properties from the accepted states: the state's cp and, with enthalpies, the
+ * effective species enthalpies (h_k = (gas_k hbar_k + [k condensable] m_l h_l) / q_k,
+ * hbar the gas mixture's partial molar enthalpies at p - c J, h_l the liquid's
+ * at p + (1 - c) J), every state checked against the phases it implies. The
+ * epoch names what the properties are for: the exact next RK input token of the
+ * stage, or a CFL query ({0,0,0} outside an attempt, {attempt, UINT64_MAX, 0}
+ * inside), the geometry build they were computed on, a thermo version that
+ * never decreases and boundary version 1; stage and CFL entries refuse
+ * properties of another epoch, a new geometry retires them, and host scalar
+ * uploads are refused once installed. A failing cell fails the call ("WALE PR
+ * GPU property cell N status S") and publishes nothing. v2: statesUnchanged != 0
+ * reuses the previous call's device copy of the states. */
+int reactive_transport_set_wale_pr_model_v1(void* transport, const ReactiveWalePrModelV1* model);
+int reactive_transport_wale_pr_properties_v1(void* transport, const ReactiveWalePrEpochV1* epoch, const double* q,
     size_t qStride, const ReactiveThermoState* state);
-int reactive_transport_wale_pr_properties_v2(void* transport, const void* epoch, const double* q,
+int reactive_transport_wale_pr_properties_v2(void* transport, const ReactiveWalePrEpochV1* epoch, const double* q,
     size_t qStride, const ReactiveThermoState* state, int statesUnchanged);
-int reactive_transport_wale_pr_profile_v1(void* transport, void* profile);
+int reactive_transport_wale_pr_profile_v1(void* transport, ReactiveWalePrProfileV1* profile);
 /* The resident capillary closure (src/reactiveTransport/reactiveCapillaryResident.h:26-41,
  * reactiveTransport.cpp:963-1127): the outer iteration between the capillary HEM
  * flash and the diffuse geometry with every per-cell array on the device; the

@@ -15,6 +15,7 @@
  *   ReactiveWaleScalarOptionsV1 / ProfileV1 src/reactiveTransport/reactiveTurbulence.h:28-35
  *   ReactiveCapillaryOptionsV1 / ProfileV1  src/reactiveTransport/reactiveTransport.h:38-47
  *   ReactiveCapillaryResidentViewV1         src/reactiveTransport/reactiveCapillaryResident.h:17-22
+ *   ReactiveWalePrModelV1 / EpochV1 / ProfileV1 src/reactiveTransport/reactiveTurbulence.h:48-68
  *   ReactiveGasThermoSpecies/Region/Partition src/reactiveThermo/reactiveGasThermo.h:12-21
  *   ReactiveThermoState                     src/reactiveThermo/reactiveThermo.h:11-19
  *   ReactiveGpuHemProfileV1                 src/reactiveThermo/reactiveGpuHem.h:14-21
@@ -128,6 +129,31 @@ typedef struct ReactiveCapillaryProfileV1 {
     uint64_t colorUploadBytes, geometryDownloadBytes, capillaryWorkspaceBytes;
 } ReactiveCapillaryProfileV1;
 
+/* The WALE Peng-Robinson scalar-property pass (src/reactiveTransport/reactiveTurbulence.h:48-68). */
+typedef struct ReactiveWalePrModelV1 {
+    uint32_t abiVersion, structBytes;
+    const void* modelImage;
+    size_t modelBytes;
+    char physicalModelHash[65];
+    const double* fixedCp;
+    const double* fixedSpeciesH;  /* fixed-cell-major, species values per cell */
+} ReactiveWalePrModelV1;
+
+typedef struct ReactiveWalePrEpochV1 {
+    uint32_t abiVersion, structBytes;
+    /* the exact next RK input of stage properties; a CFL-only cp query outside an
+     * attempt uses {0,0,0}, inside one {attemptId, UINT64_MAX, 0} */
+    ReactiveTransportToken nextConserved;
+    uint64_t thermoVersion, geometryVersion, boundaryVersion;
+    int enthalpies;  /* 0: cp only (CFL); 1: cp and the effective species enthalpies */
+} ReactiveWalePrEpochV1;
+
+typedef struct ReactiveWalePrProfileV1 {
+    uint32_t abiVersion, structBytes;
+    uint64_t builds, cells, kernels, failures, inputUploadBytes, scratchBytes;
+    double wallSeconds;
+} ReactiveWalePrProfileV1;
+
 typedef struct ReactiveGasThermoSpecies {
     uint64_t regionOffset, regionCount;
     double gasConstant;
@@ -232,6 +258,9 @@ static_assert(sizeof(ReactiveWaleScalarProfileV1) == 32, "WALE scalar profile la
 static_assert(sizeof(ReactiveCapillaryOptionsV1) == 40, "capillary options layout");
 static_assert(sizeof(ReactiveCapillaryProfileV1) == 64, "capillary profile layout");
 static_assert(sizeof(ReactiveCapillaryResidentViewV1) == 64, "resident capillary view layout");
+static_assert(sizeof(ReactiveWalePrModelV1) == 112, "WALE PR model layout");
+static_assert(sizeof(ReactiveWalePrEpochV1) == 64, "WALE PR epoch layout");
+static_assert(sizeof(ReactiveWalePrProfileV1) == 64, "WALE PR profile layout");
 static_assert(sizeof(ReactiveGpuHemOutputV1) == 184, "HEM output layout");
 static_assert(sizeof(ReactiveB200HemModel) == 47448, "HEM model image layout");
 static_assert(offsetof(ReactiveB200HemModel, stableGasPrune) == 45004, "HEM model image layout");

@@ -133,6 +133,9 @@ def ref_flash_lib():
         lib.ref_flash_initialize_tp.argtypes = [C.c_char_p, C.c_size_t, _d, _d, _v, _d, _d, _v,
                                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.ref_flash_initialize_tp.restype = C.c_int
+        lib.ref_wale_pr_evaluate.argtypes = [C.c_char_p, C.c_size_t, _d, _v, _d, _d, C.c_int, _d, _d,
+                                             C.POINTER(C.c_int)]
+        lib.ref_wale_pr_evaluate.restype = C.c_int
         lib.ref_pr_evaluate_tp.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _d,
                                            C.POINTER(C.c_int)]
         lib.ref_pr_evaluate_trho.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, _d,
@@ -228,6 +231,24 @@ def ref_flash_initialize_tp(model_image, q, energy, guess, color, jump):
     if rc:
         raise RuntimeError("reference flash rejected the model image")
     return q, energy, out, success, status
+
+
+def ref_wale_pr_evaluate(model_image, q, states, color, jump, enthalpies=True):
+    """The reference's WALE PR scalar properties per cell on the host:
+    (effective species enthalpies [count, ns], cp, status)."""
+    count = len(states)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    ns = q.shape[1]
+    effective = np.zeros((count, ns))
+    cp = np.zeros(count)
+    status = np.zeros(count, dtype=np.int32)
+    rc = ref_flash_lib().ref_wale_pr_evaluate(
+        model_image, count, _p(q), states.ctypes.data_as(_v), _p(np.ascontiguousarray(color, dtype=np.float64)),
+        _p(np.ascontiguousarray(jump, dtype=np.float64)), int(enthalpies), _p(effective), _p(cp),
+        status.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc:
+        raise RuntimeError("reference flash rejected the model image")
+    return effective, cp, status
 
 
 def cpu_threads():

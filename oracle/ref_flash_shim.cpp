@@ -17,10 +17,14 @@
 //                                pressure jump and equilibrium flag; status per cell
 //   ref_flash_initialize_tp      ReactiveDeviceFlash::initializeCapillaryTP per cell
 //                                (reactiveDeviceFlash.h:589-613)
+//   ref_wale_pr_evaluate         ReactiveDeviceWalePr::evaluate per cell
+//                                (reactiveDeviceWalePr.h:20-103): the phase-aware cp
+//                                and effective species enthalpies at accepted states
 //   ref_pr_evaluate_tp / _trho   ReactiveDevicePR::evaluateTPTrusted / evaluateTrhoTrusted
 //                                (reactiveDevicePR.h:575, :474) for EOS unit checks
 //   ref_pr_mix_tp / _trho        the same for a mixture table with mass fractions Y
 #include "reactiveDeviceFlash.h"
+#include "reactiveDeviceWalePr.h"
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -160,6 +164,28 @@ int ref_flash_initialize_tp(const void* image, size_t count, double* q, double* 
             for (int k = 0; k < ns; ++k) q[c * ns + k] = mass[k];
             energy[c] = e;
         }
+    }
+    delete m;
+    return 0;
+}
+
+// The WALE PR scalar properties per cell: total species densities q (ns per
+// cell), the accepted state, color and jump; effective (ns per cell) and cp out,
+// status[c] the reference's Status (0 success).
+int ref_wale_pr_evaluate(const void* image, size_t count, const double* q, const ReactiveThermoState* states,
+                         const double* color, const double* jump, int enthalpies, double* effective, double* cp,
+                         int* status) {
+    Model* m = new Model;
+    std::memcpy(m, image, sizeof(Model));
+    if (!ReactiveDeviceFlash::validModel(*m)) { delete m; return 1; }
+    const int ns = m->ns;
+    for (size_t c = 0; c < count; ++c) {
+        double local[ReactiveDeviceFlash::maxSpecies]{};
+        double candidate = 0;
+        status[c] = int(ReactiveDeviceWalePr::evaluate(*m, enthalpies ? q + c * ns : nullptr, states[c], color[c],
+                                                       jump[c], local, candidate, enthalpies != 0));
+        cp[c] = candidate;
+        for (int k = 0; k < ns; ++k) effective[c * ns + k] = local[k];
     }
     delete m;
     return 0;

@@ -99,6 +99,24 @@ class CapillaryResidentView(C.Structure):
         (n, C.c_void_p) for n in ("q", "energy", "seed", "capillary", "order", "output")] + [("count", C.c_size_t)]
 
 
+class WalePrModel(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32), ("modelImage", C.c_void_p),
+                ("modelBytes", C.c_size_t), ("physicalModelHash", C.c_char * 65), ("fixedCp", C.c_void_p),
+                ("fixedSpeciesH", C.c_void_p)]
+
+
+class WalePrEpoch(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32), ("nextConserved", Token),
+                ("thermoVersion", C.c_uint64), ("geometryVersion", C.c_uint64), ("boundaryVersion", C.c_uint64),
+                ("enthalpies", C.c_int)]
+
+
+class WalePrProfile(C.Structure):
+    _fields_ = [("abiVersion", C.c_uint32), ("structBytes", C.c_uint32)] + [
+        (n, C.c_uint64) for n in ("builds", "cells", "kernels", "failures", "inputUploadBytes", "scratchBytes")] + [
+        ("wallSeconds", C.c_double)]
+
+
 class ThermoState(C.Structure):
     _fields_ = [(k, C.c_double) for k in (
         "p", "T", "rho", "e", "entropy", "soundFrozen", "soundEquilibrium",

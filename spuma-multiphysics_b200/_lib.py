@@ -45,6 +45,10 @@ TRANSPORT = {
     "set_capillary_v1": ([_v, C.POINTER(A.CapillaryOptions)], C.c_int),
     "capillary_geometry_v1": ([_v, _d, _d, _d, _d, _d], C.c_int),
     "capillary_profile_v1": ([_v, C.POINTER(A.CapillaryProfile)], C.c_int),
+    "set_wale_pr_model_v1": ([_v, C.POINTER(A.WalePrModel)], C.c_int),
+    "wale_pr_properties_v1": ([_v, C.POINTER(A.WalePrEpoch), _d, C.c_size_t, _v], C.c_int),
+    "wale_pr_properties_v2": ([_v, C.POINTER(A.WalePrEpoch), _d, C.c_size_t, _v, C.c_int], C.c_int),
+    "wale_pr_profile_v1": ([_v, C.POINTER(A.WalePrProfile)], C.c_int),
     "capillary_resident_begin_v1": ([_v, C.c_size_t, _d, _d, _d, _v, _d, C.c_double, C.c_int, C.POINTER(C.c_int)],
                                     C.c_int),
     "capillary_resident_select_v1": ([_v, C.c_int, C.POINTER(A.CapillaryResidentView), C.POINTER(C.c_int)], C.c_int),

@@ -308,6 +308,52 @@ RB200_HD inline int trho(const ReactiveB200Table& t, double T, double rho, const
     return OK;
 }
 
+// Partial molar enthalpies [J/kmol] of the mixture of mass fractions Y at the
+// state s (from trho / tp on the chosen root): the ideal-gas reference h_k(T)
+// plus the Peng-Robinson departure at constant (T, p), h_k - T ds/dn_k terms
+// through dp/dn_k at constant (T, V), the a*alpha composition derivative
+// sum_i x_i a_ki sqrt(alpha_k alpha_i) and its T-derivative (the relations of
+// Cantera 3.2's PengRobinsonPhase::getPartialMolarEnthalpies, which the
+// reference's phasePartials restates, src/reactiveThermo/reactiveDeviceFlashJacobian.h:69-127).
+RB200_HD inline int partialEnthalpies(const ReactiveB200Table& t, double T, const double* Y, const Props& s,
+                                      double* hbar) {
+    double x[kMaxNs] = {}, W = 0;
+    if (const int st = moles(t, Y, x, W)) return st;
+    Mixing m;
+    if (const int st = mixing(t, T, x, m)) return st;
+    const double V = s.V, RT = kR * T, b = m.b;
+    const double vmb = V - b, den = V * V + 2.0 * V * b - b * b;
+    if (!(vmb > 0) || !(den > 0) || !(s.dpdV < 0)) return NONFINITE;
+    const double logRatio = log((V + (1.0 + kRt2) * b) / (V + (1.0 - kRt2) * b));
+    const double L = logRatio / (2.0 * kRt2 * b);
+    const double fac = T * m.da - m.aa, fac2 = V + T * s.dpdT / s.dpdV;
+    double dq[kMaxNs];
+    for (int i = 0; i < t.ns; ++i) {
+        const ReactiveB200Species& sp = t.species[i];
+        const double Tc = sp.a * kOmB / (sp.b * kOmA * kR), root = sqrt(T / Tc);
+        const double f = 1.0 + sp.kappa * (1.0 - root);
+        dq[i] = -(f > 0 ? 1.0 : -1.0) * sp.kappa / (2.0 * Tc * root);
+    }
+    for (int k = 0; k < t.ns; ++k) {
+        // a*alpha's composition derivative and its temperature derivative
+        double pp = 0, dpp = 0;
+        for (int i = 0; i < t.ns; ++i) {
+            const double pair = t.aBinary[k][i] * m.q[k] * m.q[i];
+            pp += x[i] * pair;
+            dpp += x[i] * pair * (2.0 * dq[i] / m.q[i] + 2.0 * dq[k] / m.q[k]);
+        }
+        double cpR, hRT, sR;
+        nasa(t.species[k], T, cpR, hRT, sR);
+        const double bk = t.species[k].b;
+        const double dpdn = RT / vmb + RT * bk / (vmb * vmb) - 2.0 * pp / den + 2.0 * vmb * m.aa * bk / (den * den);
+        const double departure = V * dpdn - RT - bk / (2.0 * kRt2 * b * b) * logRatio * fac
+                               + V * bk / (b * den) * fac + L * (T * dpp - 2.0 * pp);
+        hbar[k] = RT * hRT + departure - fac2 * dpdn;
+        if (!finiteD(hbar[k])) return NONFINITE;
+    }
+    return OK;
+}
+
 // Properties at (T, p, Y) on the chosen root (AUTO: the largest, as Cantera starts
 // gas-side), with the pressure postcondition |p(T, rho) - p| <= 1e-7 max(1, p)
 // and the reported phase consistent with a GAS / LIQUID choice.

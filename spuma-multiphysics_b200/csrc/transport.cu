@@ -8,10 +8,12 @@
 // backend 0 (the reference's serial CPU loop) is rejected, never emulated.
 #include "cartesian_kernels.cuh"
 #include "capillary_resident.cuh"
+#include "wale_pr.cuh"
 #include <cub/device/device_radix_sort.cuh>
 #include "../../include/reactive_b200_transport.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -45,6 +47,39 @@ struct DeviceArena {
     }
     ~DeviceArena() { for (void* p : blocks) cudaFree(p); }
 };
+
+// One thread per cell: the phase-aware cp and effective species enthalpies of
+// the accepted states (wale_pr.cuh); the first failing cell (lowest index) and
+// its status go to `failure` as (cell << 8) | status.
+__global__ void walePrProperties(const ReactiveB200HemModel* model, const double* q,
+                                 const ReactiveThermoState* states, const double* color, const double* curvature,
+                                 double sigma, size_t cells, size_t species, double* h, double* cp,
+                                 unsigned long long* failure, bool enthalpies) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < cells; c += size_t(blockDim.x) * gridDim.x) {
+        double local[mix::kMaxNs] = {};
+        double candidate = 0;
+        const int status = walepr::properties(*model, enthalpies ? q + c * species : nullptr, states[c], color[c],
+                                              sigma * curvature[c], local, candidate, enthalpies);
+        if (status != walepr::SUCCESS) {
+            atomicMin(failure, ((unsigned long long)c << 8) | unsigned(status));
+            continue;
+        }
+        cp[c] = candidate;
+        if (enthalpies)
+            for (size_t k = 0; k < species; ++k) h[c * species + k] = local[k];
+    }
+}
+
+// Publishes a successful property build into the WALE scalar fields.
+__global__ void walePrCommit(size_t cells, size_t species, size_t stride, const double* sourceH,
+                             const double* sourceCp, double* destinationH, double* destinationCp, bool enthalpies,
+                             bool heatFlux) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < cells; c += size_t(blockDim.x) * gridDim.x) {
+        if (heatFlux) destinationCp[c] = sourceCp[c];
+        if (enthalpies)
+            for (size_t k = 0; k < species; ++k) destinationH[k * stride + c] = sourceH[c * species + k];
+    }
+}
 
 struct Transport {
     std::mutex entry;
@@ -105,6 +140,16 @@ struct Transport {
         unsigned* flags = nullptr;
         std::vector<double> fixedColor;
     } resident;
+    // the WALE PR scalar-property pass (src/reactiveTransport/reactiveTransport.cpp:703-828)
+    bool walePrInstalled = false, walePrReady = false, walePrStatesCurrent = false;
+    ReactiveWalePrEpochV1 walePrEpoch{};
+    uint64_t walePrLastThermoVersion = 0;
+    ReactiveWalePrProfileV1 walePrProfile{1, sizeof(ReactiveWalePrProfileV1), 0, 0, 0, 0, 0, 0, 0.0};
+    ReactiveB200HemModel* walePrModel = nullptr;
+    ReactiveThermoState* walePrStates = nullptr;
+    double *walePrQ = nullptr, *walePrH = nullptr, *walePrCp = nullptr;
+    unsigned long long* walePrFailure = nullptr;
+    std::vector<double> walePrHostQ;
     std::string physicalHash;
     uint64_t attemptId = 0, lastAttempt = 0, tokenStage = 0;
     bool attemptOpen = false;
@@ -751,6 +796,7 @@ struct Transport {
     void prepareResident(const ReactiveTransportState* states, const double* gasY, const double* gasH, bool transport) {
         requireCapillaryGeometry();
         requireScalarFields(transport);
+        requireWalePrEpoch(transport);
         if (!structured) ensureGraphScalarWork();
         uploadState(states);
         if (transport && cfg.diffusivity > 0) {
@@ -921,6 +967,7 @@ struct Transport {
         require(firstFailure(cfg.cells, [&](size_t c) { return unit(cellColor[c]); }) == cfg.cells,
                 "Invalid material color");
         for (size_t c = 0; c < cfg.fixed; ++c) require(unit(fixedColor[c]), "Invalid fixed material color");
+        retireWalePr();
         const auto same = [](const std::vector<double>& shadow, const double* x, size_t n) {
             return shadow.size() == n && (n == 0 || std::memcmp(shadow.data(), x, n * sizeof(double)) == 0);
         };
@@ -962,6 +1009,156 @@ struct Transport {
         capillaryProfile.colorUploadBytes += (cfg.cells + cfg.fixed) * sizeof(double);
         capillaryProfile.geometryDownloadBytes +=
             cfg.cells * sizeof(double) * (1 + (curvature ? 1 : 0) + (normal ? 3 : 0));
+    }
+    // --------------------------------------------------- WALE PR properties
+    void installWalePr(const ReactiveWalePrModelV1& o) {
+        require(o.abiVersion == 1 && o.structBytes == sizeof(o) && o.modelImage
+                    && o.modelBytes == sizeof(ReactiveB200HemModel),
+                "Invalid WALE PR model ABI or image size");
+        require(o.physicalModelHash[64] == 0 && std::strlen(o.physicalModelHash) == 64
+                    && physicalHash == o.physicalModelHash,
+                "WALE PR model identity differs from transport physical model");
+        require(v.capillary && v.sgs && !walePrInstalled && !highestVersion && !stats.stages && !stats.stepQueries,
+                "WALE PR device model must be installed on CUDA before stepping");
+        ReactiveB200HemModel host;
+        std::memcpy(&host, o.modelImage, sizeof(host));
+        require(host.ns >= 1 && host.ns <= mix::kMaxNs && host.nl == 1 && host.condensedKind[0] == 0
+                    && size_t(host.ns) == cfg.species && v.capSpecies == size_t(host.condensable[0])
+                    && cfg.variables == cfg.species + 5 && host.phase[0].ns == host.ns && host.phase[1].ns == 1
+                    && std::isfinite(host.vtol) && host.vtol > 0,
+                "WALE PR model does not match the single-liquid capillary transport layout");
+        if (v.pr > 0) {
+            require(!cfg.fixed || o.fixedCp, "Missing fixed WALE heat capacities");
+            for (size_t c = 0; c < cfg.fixed; ++c)
+                require(std::isfinite(o.fixedCp[c]) && o.fixedCp[c] > 0, "Invalid fixed WALE heat capacity");
+        }
+        if (v.sc > 0) {
+            require(!cfg.fixed || o.fixedSpeciesH, "Missing fixed WALE species enthalpies");
+            for (size_t i = 0; i < cfg.fixed * cfg.species; ++i)
+                require(std::isfinite(o.fixedSpeciesH[i]), "Invalid fixed WALE species enthalpy");
+        }
+        const size_t n = cfg.cells, ns = cfg.species;
+        size_t bytes = sizeof(host) + sizeof(unsigned long long) + product(n, sizeof(ReactiveThermoState) + sizeof(double));
+        if (v.sc > 0) bytes += 2 * product(product(n, ns), sizeof(double));
+        require(double(arena.bytes) + double(bytes) <= arena.limit,
+                "WALE PR property scratch exceeds transport memory budget");
+        walePrModel = arena.get<ReactiveB200HemModel>(1);
+        walePrStates = arena.get<ReactiveThermoState>(n);
+        if (v.sc > 0) {
+            walePrQ = arena.get<double>(product(n, ns));
+            walePrH = arena.get<double>(product(n, ns));
+            walePrHostQ.resize(product(n, ns));
+        }
+        walePrCp = arena.get<double>(n);
+        walePrFailure = arena.get<unsigned long long>(1);
+        upload(walePrModel, &host, 1);
+        if (v.pr > 0) upload(const_cast<double*>(v.mixCp) + n, o.fixedCp, cfg.fixed);
+        if (v.sc > 0) packInto(const_cast<double*>(v.spH), o.fixedSpeciesH, cfg.fixed, ns, v.all, n);
+        finish();
+        // a prior host scalar upload is never a valid device PR property epoch
+        scalarCp = scalarH = false;
+        walePrReady = false;
+        walePrInstalled = true;
+        walePrProfile.scratchBytes = bytes;
+        walePrProfile.inputUploadBytes = sizeof(host) + cfg.fixed * (v.pr > 0 ? sizeof(double) : 0)
+                                       + cfg.fixed * ns * (v.sc > 0 ? sizeof(double) : 0);
+    }
+    void prepareWalePr(const ReactiveWalePrEpochV1& epoch, const double* hq, size_t stride,
+                       const ReactiveThermoState* states, bool statesUnchanged) {
+        const auto begin = std::chrono::steady_clock::now();
+        const bool reuse = statesUnchanged && walePrStatesCurrent;
+        // no failed request may publish old properties or promise a reusable upload
+        walePrStatesCurrent = false;
+        walePrReady = false;
+        scalarCp = scalarH = false;
+        require(epoch.abiVersion == 1 && epoch.structBytes == sizeof(epoch)
+                    && (epoch.enthalpies == 0 || epoch.enthalpies == 1) && epoch.thermoVersion > 0
+                    && epoch.thermoVersion >= walePrLastThermoVersion && epoch.boundaryVersion == 1,
+                "Invalid WALE PR property epoch");
+        require(walePrInstalled && colorReady && states && epoch.geometryVersion == capillaryProfile.geometryBuilds,
+                "WALE PR properties require installed model and current capillary geometry");
+        constexpr uint64_t kCflStage = std::numeric_limits<uint64_t>::max();
+        if (attemptOpen) {
+            if (epoch.nextConserved.stageId == kCflStage)
+                require(!epoch.enthalpies && epoch.nextConserved.attemptId == attemptId
+                            && !epoch.nextConserved.contentVersion,
+                        "Invalid WALE PR in-attempt CFL token");
+            else
+                require(epoch.nextConserved.attemptId == attemptId && epoch.nextConserved.stageId == tokenStage
+                            && epoch.nextConserved.contentVersion > highestVersion,
+                        "Stale WALE PR next-conserved token");
+        } else
+            require(!epoch.nextConserved.attemptId && !epoch.nextConserved.stageId
+                        && !epoch.nextConserved.contentVersion,
+                    "WALE PR CFL properties cannot claim an RK token");
+        if (epoch.enthalpies) {
+            require(v.sc > 0 && v.spH && walePrQ && walePrH, "WALE PR enthalpies require species mixing scratch");
+            require(hq && stride == cfg.variables, "WALE PR enthalpies need full conserved rows");
+            require(attemptOpen, "WALE PR enthalpies require an open RK attempt");
+        }
+        const size_t n = cfg.cells, ns = cfg.species;
+        if (epoch.enthalpies)
+            for (size_t c = 0; c < n; ++c)
+                for (size_t k = 0; k < ns; ++k) walePrHostQ[c * ns + k] = hq[c * stride + k];
+        const unsigned long long none = std::numeric_limits<unsigned long long>::max();
+        unsigned long long failure = none;
+        upload(walePrFailure, &none, 1);
+        if (!reuse) upload(walePrStates, states, n);
+        if (epoch.enthalpies) upload(walePrQ, walePrHostQ.data(), product(n, ns));
+        walePrProfile.inputUploadBytes += sizeof(none) + (reuse ? 0 : n * sizeof(ReactiveThermoState))
+                                        + (epoch.enthalpies ? product(n, ns) * sizeof(double) : 0);
+        const unsigned blocks = unsigned(std::min<size_t>((n + 127) / 128, 148 * 32));
+        walePrProperties<<<blocks, 128, 0, stream>>>(walePrModel, walePrQ, walePrStates, v.color, v.cCurv, v.sigma,
+                                                     n, ns, walePrH, walePrCp, walePrFailure, epoch.enthalpies != 0);
+        launched();
+        ++walePrProfile.kernels;
+        download(&failure, walePrFailure, 1);
+        finish();
+        walePrProfile.cells += n;
+        if (failure != none) {
+            ++walePrProfile.failures;
+            throw std::runtime_error("WALE PR GPU property cell " + std::to_string(failure >> 8) + " status "
+                                     + std::to_string(failure & 255));
+        }
+        walePrCommit<<<blocks, 128, 0, stream>>>(n, ns, v.all, walePrH, walePrCp, const_cast<double*>(v.spH),
+                                                 const_cast<double*>(v.mixCp), epoch.enthalpies != 0, v.pr > 0);
+        launched();
+        ++walePrProfile.kernels;
+        finish();
+        scalarCp = true;
+        scalarH = epoch.enthalpies != 0 || v.sc == 0;
+        walePrReady = true;
+        walePrEpoch = epoch;
+        walePrStatesCurrent = true;
+        walePrLastThermoVersion = epoch.thermoVersion;
+        ++walePrProfile.builds;
+        walePrProfile.wallSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+    }
+    // The published PR properties belong to the stage (transport) or the CFL
+    // query they were built for (src/reactiveTransport/reactiveTransport.cpp:1398-1430).
+    void requireWalePrEpoch(bool transport) const {
+        if (!walePrInstalled) return;
+        constexpr uint64_t kCflStage = std::numeric_limits<uint64_t>::max();
+        const ReactiveTransportToken& next = walePrEpoch.nextConserved;
+        if (transport)
+            require(walePrReady && next.attemptId == attemptId && next.stageId == tokenStage
+                        && next.contentVersion == residentVersion
+                        && walePrEpoch.geometryVersion == capillaryProfile.geometryBuilds
+                        && (v.sc == 0 || walePrEpoch.enthalpies == 1),
+                    "WALE PR properties have a stale conserved or geometry epoch");
+        else
+            require(walePrReady && walePrEpoch.geometryVersion == capillaryProfile.geometryBuilds
+                        && walePrEpoch.enthalpies == 0
+                        && (attemptOpen ? next.attemptId == attemptId && next.stageId == kCflStage
+                                              && !next.contentVersion
+                                        : !next.attemptId && !next.stageId && !next.contentVersion),
+                    "WALE PR CFL heat capacity has a stale geometry or attempt epoch");
+    }
+    // A new geometry retires the properties built on the old one.
+    void retireWalePr() {
+        if (!walePrInstalled) return;
+        walePrReady = false;
+        scalarCp = scalarH = false;
     }
     // ------------------------------------------- resident capillary closure
     // (src/reactiveTransport/reactiveTransport.cpp:963-1127)
@@ -1037,6 +1234,7 @@ struct Transport {
     void residentGeometry() {
         auto& r = resident;
         const size_t n = cfg.cells;
+        retireWalePr();
         geometryShadowValid = false;
         colorReady = false;
         check(cudaMemsetAsync(flags, 0, sizeof(unsigned), stream), "memset");
@@ -1227,6 +1425,7 @@ struct Transport {
     }
     void uploadWaleScalarFields(const double* cellCp, const double* cellH, const double* fixedCp,
                                 const double* fixedH) {
+        require(!walePrInstalled, "Host WALE scalar upload cannot replace installed PR device properties");
         require(v.sgs, "WALE scalar closure is not selected");
         const bool uploadH = cellH || fixedH;
         if (v.pr > 0) {
@@ -1265,6 +1464,7 @@ struct Transport {
     }
     void uploadWaleScalarFieldsDevice(const double* cellCp, const double* cellH, const double* fixedCp,
                                       const double* fixedH, size_t cpStride, size_t hStride, cudaStream_t s) {
+        require(!walePrInstalled, "Host WALE scalar upload cannot replace installed PR device properties");
         require(v.sgs, "WALE scalar closure is not selected");
         require(v.pr == 0 || cellCp, "Missing WALE mixture heat capacities");
         require((!cellCp || cpStride >= 1) && (!cellH || hStride >= cfg.species), "Invalid WALE scalar field strides");

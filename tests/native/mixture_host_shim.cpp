@@ -30,3 +30,20 @@ extern "C" int mix_tp(const ReactiveB200Table* t, double T, double p, const doub
     if (st == 0) pack(s, t->ns, out, phase);
     return st;
 }
+
+// The library's WALE PR scalar properties (wale_pr.cuh) for a batch of cells
+// with the model image `model`: effective (ns per cell), cp, status per cell.
+#include "wale_pr.cuh"
+extern "C" void wale_pr_properties(const ReactiveB200HemModel* model, size_t count, const double* q,
+                                   const ReactiveThermoState* states, const double* color, const double* jump,
+                                   int enthalpies, double* effective, double* cp, int* status) {
+    const int ns = model->ns;
+    for (size_t c = 0; c < count; ++c) {
+        double local[rb200::mix::kMaxNs] = {};
+        double candidate = 0;
+        status[c] = rb200::walepr::properties(*model, enthalpies ? q + c * ns : nullptr, states[c], color[c], jump[c],
+                                              local, candidate, enthalpies != 0);
+        cp[c] = candidate;
+        for (int k = 0; k < ns; ++k) effective[c * ns + k] = local[k];
+    }
+}
