@@ -38,8 +38,7 @@ int reactive_gpu_hem_run_v1(void* hem, const double* q, const double* energy, si
  * pure liquid (else the cell fails). run_v2 rejects the batch ("Invalid CUDA HEM capillary cell
  * input") for a color outside [0, 1], a non-finite jump or an equilibrium flag other than 0/1.
  * These run on the multi-species engine, one thread per cell (for a pure-fluid handle, one made
- * from the same image); a pure-fluid image with analyticJacobian = 1 takes only equilibrium batches
- * without a jump, on its fast path (the plain UV flash), and returns 1 with a message otherwise.
+ * from the same image, whose Newton Jacobian is always the bounded finite-difference one).
  * run_resident_v1: device pointers indexed by global cell, order[0..count) names the cells, each
  * result (state, success) goes to output[cell] (reserved untouched), a failed cell returns its
  * seed; capillary may be NULL for the plain flash; synchronous, batch totals in *profile.

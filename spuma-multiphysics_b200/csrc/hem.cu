@@ -714,7 +714,7 @@ struct HemDevice {
         if (!capillaryEngine && image) {
             std::string why;
             capillaryEngine = mixtureCreate(*image, capacity, device, why);
-            if (!capillaryEngine) image.reset();  // outside its scope (an analytic-Jacobian image)
+            if (!capillaryEngine) image.reset();  // outside its scope
             else bytes += mixtureDeviceBytes(capillaryEngine);
         }
         return capillaryEngine;
@@ -1246,9 +1246,9 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
 // the gas at p - color*jump, the liquid at p + (1 - color)*jump, UV equilibrium
 // with the boundary search, or the frozen partition at the seed's liquid masses.
 // It runs on the multi-species engine (hem_mixture.cu), for a pure-fluid handle
-// one made from the same image. A pure-fluid image with the analytic Jacobian
-// (outside that engine's scope) takes equilibrium batches without a jump on its
-// own fast path (the plain UV flash) and refuses the rest.
+// one made from the same image. A pure-fluid image outside that engine's scope
+// takes equilibrium batches without a jump on its own fast path (the plain UV
+// flash) and refuses the rest.
 int reactive_gpu_hem_run_v2(void* raw, const double* q, const double* energy,
                             const ReactiveGpuHemCapillaryInputV2* capillary, size_t count, ReactiveThermoState* states,
                             int* success, ReactiveGpuHemProfileV1* profile, char* error, size_t size) {
@@ -1281,8 +1281,8 @@ int reactive_gpu_hem_run_v2(void* raw, const double* q, const double* energy,
                 return 0;
             }
         }
-        rb200::require(plain, "Capillary pressure jumps and the frozen partition need a model image with "
-                              "analyticJacobian = 0 on this build");
+        rb200::require(plain, "Capillary pressure jumps and the frozen partition need a model image within the "
+                              "multi-species flash's scope");
     } catch (const std::exception& e) {
         if (error && size) std::snprintf(error, size, "%s", e.what());
         return 1;
@@ -1311,8 +1311,8 @@ int reactive_gpu_hem_initialize_tp_v1(void* raw, double* q, double* energy,
         rb200::require(count && count <= d.capacity, "CUDA HEM batch exceeds capacity");
         rb200::check(cudaSetDevice(d.device), "cudaSetDevice");
         rb200::MixtureFlash* engine = d.capillaryFlash();
-        rb200::require(engine, "Capillary primitive initialisation needs a model image with analyticJacobian = 0 on "
-                               "this build");
+        rb200::require(engine, "Capillary primitive initialisation needs a model image within the multi-species "
+                               "flash's scope");
         ReactiveGpuHemProfileV1 p{};
         p.abiVersion = 1;
         p.structBytes = sizeof(p);

@@ -3,8 +3,11 @@
 // isopropanol model of the reference's production case), one thread per cell.
 //
 // The search restates the reference device flash
-// (src/reactiveThermo/reactiveDeviceFlash.h) for models without solids, with the
-// finite-difference Jacobian (analyticJacobian 0), including its capillary form
+// (src/reactiveThermo/reactiveDeviceFlash.h) for models without solids, with its
+// bounded finite-difference Newton Jacobian (an image's analyticJacobian flag
+// selects the reference's analytic active-set Jacobian there, which is not
+// restated: such images run on the finite differences and converge to the same
+// solutions within the Newton tolerances), including its capillary form
 // (recoverCapillary, :572-588: the phases at their own pressures across a fixed
 // jump, the boundary search in every equilibrium batch, the frozen partition):
 //   * phase sums of one evaluation at (p, T) with given liquid masses, the gas
@@ -859,9 +862,6 @@ std::string mixtureScope(const ReactiveB200HemModel& m) {
     if (m.ns < 1 || m.ns > kNs || m.nl < 0 || m.nl > kLiq)
         return "HEM model outside the mixture flash's scope: 1 to 4 gas species and 0 to 2 pure liquids";
     if (m.condensedKind[0] != 0 || m.condensedKind[1] != 0) return "Solid condensed phases are not part of this build";
-    if (m.analyticJacobian != 0)
-        return "The mixture flash forms its Newton Jacobian by finite differences: export the image with "
-               "analyticJacobian = 0";
     if ((m.boundaryRecovery != 0 && m.boundaryRecovery != 1) || (m.scalarRecovery != 0 && m.scalarRecovery != 1)
         || (m.stableGasPrune != 0 && m.stableGasPrune != 1)
         || (m.stableGasPrune && m.nl != 1)
