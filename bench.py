@@ -184,8 +184,9 @@ class HostPath:
     :651-661, stableStep :798-812) on this library with host arrays: q and the
     thermo states cross PCIe every stage, exactly as the reference drop-in runs.
     The caller's arrays are pinned (page-locked) host memory and its own
-    bookkeeping (transport-state compaction, primitives, specific energy, state
-    copies) runs as multi-threaded torch CPU ops on views of those arrays."""
+    bookkeeping (transport-state compaction with the primitives, the flash
+    inputs, the step-start state copies) runs through the library's parallel
+    host helpers (reactive_b200_host_*_v3), as the solver's own parallel loops."""
 
     def __init__(self, pkg, faces, volume, flow, fixed_q):
         import torch
@@ -235,35 +236,24 @@ class HostPath:
         return t.numpy().view(dtype).reshape(shape)
 
     def _copy(self, dst, src):
-        """dst[:] = src for host arrays, as one multi-threaded torch copy."""
-        self.torch.from_numpy(dst.view(np.uint8)).copy_(self.torch.from_numpy(src.view(np.uint8)))
+        """dst[:] = src for host arrays (the library's parallel host copy)."""
+        assert self.lib.reactive_b200_host_copy_v3(dst.ctypes.data, src.ctypes.data, src.nbytes) == 0
         return dst
 
-    def _f64(self, arr, width):
-        return self.torch.from_numpy(arr.view(np.float64).reshape(len(arr), width))
-
     def _compact(self, states):
-        """Transport states (p, T, rho, cv, frozen sound, gas mass) of thermo states."""
-        src, dst = self._f64(states, 22), self._f64(self.tr, 7)
-        dst[:, 0:3] = src[:, 0:3]       # p, T, rho
-        dst[:, 3] = src[:, 20]          # cv
-        dst[:, 4] = src[:, 5]           # soundFrozen
-        dst[:, 5] = src[:, 18]          # gasMass
-        dst[:, 6] = 0.0
+        """Transport states (p, T, rho, cv, frozen sound, gas mass) of thermo
+        states and the primitives (rho, u) from them and q, in one parallel pass."""
+        assert self.lib.reactive_b200_host_transport_states_v3(
+            states.ctypes.data, self.cells, self.A.dptr(self.q), 5, 1, self.tr.ctypes.data,
+            self.prim.ctypes.data) == 0
         return self.tr
 
     def _primitives(self, tr):
-        """Primitives (rho, u) from the compacted transport states."""
-        src, q, prim = self._f64(tr, 7), self.torch.from_numpy(self.q), self.torch.from_numpy(self.prim)
-        prim[:, 0] = src[:, 2]
-        self.torch.div(q[:, 1:4], src[:, 2:3], out=prim[:, 1:])
         return self.prim
 
     def _energy(self):
-        q = self.torch.from_numpy(self.q)
-        kinetic = (q[:, 1:4] * q[:, 1:4]).sum(dim=1).div_(q[:, 0]).mul_(.5)
-        self.torch.sub(q[:, 4], kinetic, out=self.torch.from_numpy(self.e))
-        self.torch.from_numpy(self.rho).copy_(q[:, 0])
+        assert self.lib.reactive_b200_host_recovery_inputs_v3(self.A.dptr(self.q), self.cells, 5, 1,
+                                                             self.A.dptr(self.rho), self.A.dptr(self.e)) == 0
 
     def _check(self, rc):
         if rc:

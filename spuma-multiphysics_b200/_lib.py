@@ -114,6 +114,14 @@ MIXTURE = {
 }
 
 
+HOST = {
+    "threads_v3": ([], C.c_int),
+    "copy_v3": ([_v, _v, C.c_size_t], C.c_int),
+    "transport_states_v3": ([_v, C.c_size_t, _d, C.c_size_t, C.c_size_t, _v, _v], C.c_int),
+    "recovery_inputs_v3": ([_d, C.c_size_t, C.c_size_t, C.c_size_t, _d, _d], C.c_int),
+}
+
+
 def load():
     """The loaded library with typed entry points (raises if it is absent)."""
     global _lib
@@ -122,7 +130,8 @@ def load():
             raise RuntimeError(f"{LIB_PATH} is missing: run __graft_entry__.build() (the CUDA library is required)")
         lib = C.CDLL(str(LIB_PATH))
         for table, prefix in ((TRANSPORT, "reactive_transport_"), (HEM, "reactive_gpu_hem_"),
-                              (IDEAL, "reactive_ideal_gas_"), (MIXTURE, "reactive_b200_mixture_")):
+                              (IDEAL, "reactive_ideal_gas_"), (MIXTURE, "reactive_b200_mixture_"),
+                              (HOST, "reactive_b200_host_")):
             for name, (args, ret) in table.items():
                 fn = getattr(lib, prefix + name, None)
                 if fn is None:

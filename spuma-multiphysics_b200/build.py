@@ -21,7 +21,9 @@ SOURCES = {"transport.cu": ["--fmad=false"], "hem.cu": ["--fmad=true"],
            "hem_plain.cu": ["--fmad=true", "-DRB200_EOS_FN=inline", "-DRB200_FLASH_FN=inline"],
            "ideal.cu": ["--fmad=true"], "probe.cu": ["--fmad=true"], "mixture.cu": ["--fmad=true"],
            # the multi-species flash: separate rounding, as the reference's host build it is compared with
-           "hem_mixture.cu": ["--fmad=false"]}
+           "hem_mixture.cu": ["--fmad=false"],
+           # host-only helpers (no device code)
+           "host_tools.cpp": []}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--shared", "-Xptxas", "-warn-spills",
          "--expt-relaxed-constexpr"]
