@@ -228,6 +228,7 @@ class HostPath:
         self.version, self.attempt = 0, 0
         self.h2d = self.d2h = 0
         self.library_s = 0.0
+        self.library_calls = {}
 
     def _pinned(self, shape, dtype):
         dtype = np.dtype(dtype)
@@ -260,12 +261,15 @@ class HostPath:
             raise RuntimeError(self.lib.reactive_transport_error(self.t).decode())
 
     def _call(self, fn, *args):
-        """One library call, its wall time added to library_s."""
+        """One library call, its wall time added to library_s and to its entry's share."""
         t0 = time.perf_counter()
         try:
             return fn(*args)
         finally:
-            self.library_s += time.perf_counter() - t0
+            dt = time.perf_counter() - t0
+            self.library_s += dt
+            name = getattr(fn, "__name__", "call").replace("reactive_transport_", "").replace("reactive_gpu_hem_", "")
+            self.library_calls[name] = self.library_calls.get(name, 0.0) + dt
 
     def step(self, dt):
         A, lib, t, call = self.A, self.lib, self.t, self._call
@@ -522,6 +526,7 @@ def run_ours(args, rank, world):
         host.step(DT)  # warm-up
         host.h2d = host.d2h = 0
         host.library_s = 0.0
+        host.library_calls = {}
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
@@ -532,10 +537,13 @@ def run_ours(args, rank, world):
         e2e = {"value": world * cells / e2e_s / 1e6, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
                "h2d_bytes_per_step": host.h2d // args.e2e_steps, "d2h_bytes_per_step": host.d2h // args.e2e_steps,
                "library_ms_per_step": library_s * 1e3, "caller_ms_per_step": (e2e_s - library_s) * 1e3,
+               "library_calls_ms_per_step": {k: round(v * 1e3 / args.e2e_steps, 3)
+                                             for k, v in sorted(host.library_calls.items())},
                "path": "the reference solver's calls with host arrays: stable_step_primitives, upload_conserved, "
                        "2 x (advance_resident_v2, download_conserved, reactive_gpu_hem_run_v1); library = time "
                        "inside those calls (their PCIe copies included), caller = the caller's own host "
-                       "bookkeeping (state compaction, primitives, energy)"}
+                       "bookkeeping (state compaction, primitives, flash inputs, state copies) through the "
+                       "library's parallel host helpers"}
         host.close()
 
     # ---- the reference CPU arm's bounded sample, on the GPU: 40^3, same step window
