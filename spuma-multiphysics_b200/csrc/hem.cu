@@ -593,11 +593,20 @@ __global__ void hemStateVjp(const HemConst* __restrict__ Cp, const double* __res
 }
 
 // Failed cells get their seed state back, so one contiguous copy of the
-// results leaves them unchanged in the caller's array.
+// results leaves them unchanged in the caller's array; succeeded (optional)
+// counts the other cells.
 __global__ void keepFailed(const ReactiveThermoState* __restrict__ seed, const int* __restrict__ success,
-                           size_t count, ReactiveThermoState* __restrict__ out) {
-    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x)
+                           size_t count, ReactiveThermoState* __restrict__ out,
+                           unsigned long long* succeeded = nullptr) {
+    unsigned mine = 0;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < count; c += size_t(blockDim.x) * gridDim.x) {
         if (!success[c]) out[c] = seed[c];
+        else ++mine;
+    }
+    if (succeeded) {
+        mine = __reduce_add_sync(0xffffffffu, mine);
+        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(succeeded, (unsigned long long)mine);
+    }
 }
 
 __global__ void selectRestarts(const CandRecord* fb, size_t capacity, const unsigned* fallback,
@@ -1110,7 +1119,7 @@ std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C) {
     return "";
 }
 
-void readTotals(HemDevice& d, ReactiveGpuHemProfileV1& p, cudaStream_t s) {
+void readTotals(HemDevice& d, ReactiveGpuHemProfileV1& p, cudaStream_t s, unsigned long long* succeeded = nullptr) {
     unsigned long long t[NTOTALS] = {};
     unsigned ctr[NCOUNTERS] = {};
     check(cudaMemcpyAsync(t, d.totals, sizeof(t), cudaMemcpyDeviceToHost, s), "D2H totals");
@@ -1124,6 +1133,7 @@ void readTotals(HemDevice& d, ReactiveGpuHemProfileV1& p, cudaStream_t s) {
     p.analyticJacobians = t[T_ANALYTIC];
     p.finiteDifferenceJacobians = t[T_FD];
     p.deviceFailures = ctr[FAILED];
+    if (succeeded) *succeeded = t[T_SUCCEEDED];
 }
 
 }  // namespace
@@ -1166,11 +1176,12 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
         }
         d.ensureHostPath();
         const auto begin = std::chrono::steady_clock::now();
-        // Pipelined in chunks: the uploads of later chunks (copy stream up) and
-        // the downloads of finished ones (copy stream down) overlap the flash of
-        // the current chunk; the chunks' flashes run one after another on the
-        // handle's stream (they share the queue scratch).
-        const size_t chunks = count >= (size_t(1) << 20) ? 4 : 1;
+        // Pipelined in chunks of at least 256Ki cells (up to 16): the uploads of
+        // later chunks (copy stream up) and the downloads of finished ones (copy
+        // stream down) overlap the flash of the current chunk; the chunks'
+        // flashes run one after another on the handle's stream (they share the
+        // queue scratch).
+        const size_t chunks = std::min<size_t>(16, std::max<size_t>(1, count >> 18));
         const size_t per = (count + chunks - 1) / chunks;
         cudaStream_t s = d.stream;
         std::vector<cudaEvent_t> uploaded(chunks), computed(chunks);
@@ -1202,7 +1213,7 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
             d.launchSearch(n, d.dguess + off, d.dout + off, nullptr, d.dsuccess + off, s);
             // a failed cell leaves the caller's state unchanged: its seed goes back
             rb200::keepFailed<<<rb200::gridFor(n, 256), 256, 0, s>>>(d.dguess + off, d.dsuccess + off, n,
-                                                                     d.dout + off);
+                                                                     d.dout + off, d.totals + rb200::T_SUCCEEDED);
             rb200::check(cudaGetLastError(), "keepFailed");
             rb200::check(cudaEventRecord(computed[i], s), "event");
             if (i + 1 == chunks) rb200::check(cudaEventRecord(last, s), "event");
@@ -1217,7 +1228,8 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
         ReactiveGpuHemProfileV1 p{};
         p.abiVersion = 1;
         p.structBytes = sizeof(p);
-        rb200::readTotals(d, p, s);
+        unsigned long long succeeded = 0;
+        rb200::readTotals(d, p, s, &succeeded);
         float total = 0, kernel = 0;
         cudaEventElapsedTime(&total, start, end);
         cudaEventElapsedTime(&kernel, first, last);
@@ -1225,7 +1237,7 @@ int reactive_gpu_hem_run_v1(void* raw, const double* q, const double* energy, si
         for (size_t i = 0; i < chunks; ++i) { cudaEventDestroy(uploaded[i]); cudaEventDestroy(computed[i]); }
         p.batches = 1;
         p.submitted = count;
-        for (size_t c = 0; c < count; ++c) p.succeeded += success[c] != 0;
+        p.succeeded = succeeded;
         p.deviceFailures = count - p.succeeded;
         p.transferBytes = count * (2 * sizeof(double) + 2 * sizeof(ReactiveThermoState) + sizeof(int));
         p.deviceBytes = d.bytes;

@@ -7,7 +7,7 @@ namespace rb200 {
 namespace {
 
 enum Counter { Q_A = 0, Q_B, LIST, Q_C, FALLBACK, FAILED, NCOUNTERS = 8 };
-enum Total { T_PHASES = 0, T_RESIDUALS, T_CANDIDATES, T_STABLE, T_FAILURES, T_ANALYTIC, T_FD, NTOTALS = 8 };
+enum Total { T_PHASES = 0, T_RESIDUALS, T_CANDIDATES, T_STABLE, T_FAILURES, T_ANALYTIC, T_FD, T_SUCCEEDED, NTOTALS = 8 };
 
 // Work-queue kernels: 128 threads, at least four blocks per SM (<= 128
 // registers a thread). With the EOS routines out of line, sixteen resident warps

@@ -299,13 +299,71 @@ __device__ RB200_FLASH_FN bool solveSmall(double a[3][3], double b[3], int n, do
     return true;
 }
 
+// The gas root of the cubic at (g.t.T, p) and its properties into g (roots,
+// gas-root properties, chemical-potential intermediates): true when that root
+// is the density q the pressure came from (to 1e-8 of q). Out of line: the
+// probe and the completion of a deferred probe run the same instructions, so
+// a point's roots and properties carry the same bits on either path (inlined
+// copies could contract products into FMAs differently).
+__device__ RB200_FLASH_FN bool gasRootAt(const HemConst& C, double q, double p, GasPoint& g) {
+    if (cubicRootsBody(C.gas, g.t.T, p, g.t.aa, g.r) != EOS_OK) return false;
+    return rootPropsBody(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas, &g.chem) == EOS_OK
+           && !(fabs(g.gas.rho - q) > 1e-8 * q);
+}
+
+// The outcome of gasRootAt decided without solving the cubic: p = p(T, q), so
+// V0 = W/q is a root of the cubic at (T, p), which factors as
+// (V - V0)(V^2 + sV + t) and leaves the other two roots to a quadratic. 1: the
+// root solve would classify a gas root equal to V0 (to rounding) and accept it
+// on q's side of the reported-phase line; 0: it would not (another root is the
+// gas root, or the gas branch is missing there); -1: undecided, the root solve
+// decides. Every decision keeps margins orders of magnitude above rounding from
+// the root solve's own thresholds: its discriminant classes (|disc| >= 1e-10
+// against 1e-14, ||h| - |q|| >= 1e-8 against 1e-10), the other roots at least
+// 1e-6 of V0 away from V0 (so V0 is no near-double root and dp/dV stays off
+// zero there), and 1e-9 of V0 (or of the line's density) from the covolume,
+// the classification centre and the reported-phase line. `phase` is the
+// reported phase of the (T, q) evaluation.
+__device__ __forceinline__ int gasRootIsV0(const PureSpecies& sp, const TTerms& t, double p, double q, int phase) {
+    const double T = t.T, V0 = sp.W / q, ip = 1.0 / p;
+    const double b = sp.b, b2 = b * b, RTp = kGas * T * ip, aap = t.aa * ip, bn = b - RTp;
+    const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
+    const double center = -bn * kThird, delta2 = (bn * bn - 3.0 * cn) * (1.0 / 9.0);
+    const double qc = 2.0 * bn * bn * bn * (1.0 / 27.0) - bn * cn * kThird + dn;
+    const double delta = delta2 > 0 ? sqrt(delta2) : 0.0, h = 2.0 * delta * delta2;
+    const double disc = qc * qc - h * h, margin = 1e-9 * V0;
+    if (!(fabs(fabs(h) - fabs(qc)) >= 1e-8) || !(fabs(disc) >= 1e-10) || !(V0 - b > margin)) return -1;
+    bool single = disc > 0;  // one real root: V0
+    if (!single) {
+        const double s = bn + V0, tq = cn + V0 * s, d2 = s * s - 4.0 * tq;
+        if (!(d2 > 0)) return -1;
+        const double r = sqrt(d2), v1 = .5 * (-s + r), v2 = .5 * (-s - r);
+        if (v1 > V0 + 1e-6 * V0) return 0;  // the largest root, the gas root if any, is not V0
+        if (!(v1 < V0 - 1e-6 * V0) || !(fabs(v1 - b) > margin) || !(fabs(v2 - b) > margin)) return -1;
+        single = !(v1 > b);  // V0 the only root above the covolume
+    }
+    if (single && !(T > sp.Tc)) {
+        // a lone root is the gas root when it is not below the centre
+        if (!(fabs(V0 - center) > margin)) return -1;
+        if (V0 < center) return 0;
+    }
+    if (phase == -2) return 1;  // above the reported-phase line's temperature: no density test
+    const double rhoMid = sp.rhoC + (T - sp.tcLine) * sp.dRho / sp.dT;
+    if (q < rhoMid * (1 - 1e-9)) return phase == -1 ? 1 : -1;
+    if (q > rhoMid * (1 + 1e-9)) return phase == 0 ? 0 : -1;
+    return -1;
+}
+
 // Energy residual of the all-gas state at (T, rho) and the gas-root check: the
 // properties at (T, rho), then the gas root of the cubic at the resulting
 // pressure must be that density. One set of T-terms serves both (the same
 // values prTrho and gasPhase would each form); `g` receives them with the
-// roots and the gas root's properties at (p, T).
+// roots and the gas root's properties at (p, T). With `deferred`, a check that
+// gasRootIsV0 decides skips the root solve: *deferred is then true and g holds
+// the T-terms only, until gasRootAt completes it at the same (p, T) (the same
+// roots and properties the probe would have formed).
 __device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn, double T, double& F, double& cv, double& p,
-                                double& cp, GasPoint& g, Counts& n) {
+                                double& cp, GasPoint& g, Counts& n, bool* deferred = nullptr) {
     PhaseProps prop;
     int phase;
     ++n.phases;
@@ -314,11 +372,14 @@ __device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn,
         return false;
     p = prop.p;  // finite and positive
     if (!inBounds(C, p, T)) return false;
-    ++n.phases;
     if (C.enforceBounds && (T < C.gasTmin || T > C.gasTmax)) return false;
-    if (cubicRootsBody(C.gas, T, p, g.t.aa, g.r) != EOS_OK) return false;
-    if (rootPropsBody(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas, &g.chem) != EOS_OK || fabs(g.gas.rho - q) > 1e-8 * q)
-        return false;
+    const int decided = deferred ? gasRootIsV0(C.gas, g.t, p, q, phase) : -1;
+    if (decided == 0) return false;
+    if (decided < 0) {
+        ++n.phases;
+        if (!gasRootAt(C, q, p, g)) return false;
+    }
+    if (deferred) *deferred = decided > 0;
     F = q * prop.e - eIn;
     cv = q * prop.cv;
     cp = prop.cp;
@@ -333,12 +394,16 @@ struct CandidateOut {
 // Scalar T-Newton of the all-gas partition at fixed rho. `g` ends with the gas
 // table's terms at the converged (p, T): the probe that set them is the last
 // probe (a bracket search is always followed by a probe at the bracket end or
-// by at least one Newton probe, which rewrite `g`).
+// by at least one Newton probe, which rewrite `g`); when that probe's gas-root
+// check was decided without the root solve, the solve runs once at its point.
+// The probes' decisions are those of full root solves, so the iterates, the
+// final point and `g` are bit for bit those of probes that always solve.
 __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, GasPoint& g,
                                  Counts& n) {
     const double q = in.q;
     double T = clampd(in.gT, C.Tmin, C.Tmax), F, cv, p, cp;
-    if (!gasProbe(C, q, in.e, T, F, cv, p, cp, g, n)) return false;
+    bool deferred = false;  // the last probe's gas-root check skipped its root solve
+    if (!gasProbe(C, q, in.e, T, F, cv, p, cp, g, n, &deferred)) return false;
     const double scale = fmax(1e5 * q, q * cp * T);
     double lower = T, upper = T, fl = F, fh = F;
     if (fabs(F) > C.etol * scale) {
@@ -349,7 +414,7 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmax(C.Tmin, T - radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n)) { fl = val; lower = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n, &deferred)) { fl = val; lower = cand; found = true; }
                     else cand = .5 * (lower + cand);
                 }
                 if (!found) return false;
@@ -358,13 +423,13 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmin(C.Tmax, T + radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n)) { fh = val; upper = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n, &deferred)) { fh = val; upper = cand; found = true; }
                     else cand = .5 * (upper + cand);
                 }
                 if (!found) return false;
             }
-            if (fabs(fl) <= C.etol * scale) { T = lower; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false; break; }
-            if (fabs(fh) <= C.etol * scale) { T = upper; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false; break; }
+            if (fabs(fl) <= C.etol * scale) { T = lower; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n, &deferred)) return false; break; }
+            if (fabs(fh) <= C.etol * scale) { T = upper; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n, &deferred)) return false; break; }
             if (lower == C.Tmin && upper == C.Tmax) break;
         }
         if (!(fabs(F) <= C.etol * scale || (fl <= 0 && fh >= 0 && upper > lower))) return false;
@@ -375,9 +440,13 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
         const double next = T - F / cv;
         T = fin(next) && next > lower && next < upper ? next : .5 * (lower + upper);
         double d3;
-        if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false;
+        if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n, &deferred)) return false;
     }
     if (fabs(F) > C.etol * scale) return false;
+    if (deferred) {  // the last probe's roots and gas-root properties
+        ++n.phases;
+        if (!gasRootAt(C, q, p, g)) return false;
+    }
     if (!evaluate(C, q, 0.0, p, T, false, v, n, &g)) return false;
     o.vres = fabs(v.volume - 1);
     o.eres = fabs(v.energy - in.e) / energyScale(v, q);

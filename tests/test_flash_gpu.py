@@ -106,13 +106,18 @@ def test_cuda_flash_per_cell_form_matches_queue_form(prune):
         assert np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300)) <= 1e-10, field
 
 
-def test_cuda_flash_device_resident_matches_host_path():
+@pytest.mark.parametrize("n", [5000, 600000])
+def test_cuda_flash_device_resident_matches_host_path(n):
+    """The host-array batch (copies pipelined in chunks of 256Ki cells and more:
+    600,000 cells take two) equals the device-resident one bit for bit; a failed
+    cell keeps its seed; the profile counts the successes."""
     import torch
-    n = 5000
     q, e, guess = cases.flash_batch(n, seed=31337)
     hem = GpuHem(capacity=n)
     host = guess.copy()
-    ok, _ = hem.run(q, e, host)
+    ok, prof_host = hem.run(q, e, host)
+    assert prof_host.succeeded == int(np.count_nonzero(ok)) and prof_host.submitted == n
+    assert np.array_equal(host[ok == 0].view(np.uint8), guess[ok == 0].view(np.uint8))
     # conserved SoA rows: rho, m (zero velocity), E = e at rest
     cons = torch.zeros((5, n + 3), dtype=torch.float64, device="cuda")
     cons[0, :n] = torch.from_numpy(q).cuda()

@@ -1,8 +1,10 @@
 """GPU: the reference's device-resident HEM batch (reactive_gpu_hem_run_resident_v1)
-and host capillary batch (reactive_gpu_hem_run_v2) without a pressure jump: the
-same states and flags as the host batch (run_v1) on the same cells, results
-scattered to the named global cells, a failed cell returning its seed, and a
-pressure jump or the frozen partition refused with a message."""
+on a pure-fluid handle: with capillary inputs it is the capillary recovery
+(the multi-species engine made from the same image), bit for bit the host
+capillary batch (reactive_gpu_hem_run_v2) on the same cells, pressure jumps
+included; without them it is the plain batch, bit for bit run_v1. Results are
+scattered to the named global cells, a failed cell returns its seed, and cells
+the batch does not name are neither read nor written."""
 import ctypes as C
 
 import numpy as np
@@ -27,6 +29,18 @@ def batch(n, seed):
     return rho, e, np.concatenate([guess, g])
 
 
+def host_capillary(lib, hem, rho, e, cap, guess):
+    """The host capillary batch (run_v2) on copies of the seeds."""
+    n = len(rho)
+    states, ok = guess.copy(), np.zeros(n, dtype=np.int32)
+    prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+    err = C.create_string_buffer(1024)
+    assert lib.reactive_gpu_hem_run_v2(hem.handle, A.dptr(rho), A.dptr(e), cap.ctypes.data_as(C.c_void_p), n,
+                                       states.ctypes.data_as(C.c_void_p), ok.ctypes.data_as(C.POINTER(C.c_int)),
+                                       C.byref(prof), err, len(err)) == 0, err.value
+    return states, ok
+
+
 def test_resident_batch_matches_host_batch():
     rho, e, guess = batch(3000, 77)
     n = len(rho)
@@ -41,76 +55,47 @@ def test_resident_batch_matches_host_batch():
     cap["color"] = rng.uniform(0, 1, total)
     cap["equilibrium"] = 1
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
-    dq, de, dseed, dcap, dorder = dev(q_g), dev(e_g), dev(seed_g), dev(cap), dev(order)
+    dq, de, dseed, dorder = dev(q_g), dev(e_g), dev(seed_g), dev(order)
     out = torch.zeros(total * A.HEM_OUTPUT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     lib = _lib.load()
     hem = GpuHem(capacity=n, resident=True)
     host = GpuHem(capacity=n)
     err = C.create_string_buffer(1024)
+    prof = A.HemProfile(1, C.sizeof(A.HemProfile))
+
+    def resident(capillary):
+        out.zero_()
+        assert lib.reactive_gpu_hem_run_resident_v1(
+            hem.handle, dq.data_ptr(), de.data_ptr(), dseed.data_ptr(),
+            None if capillary is None else dev(capillary).data_ptr(), dorder.data_ptr(), n, out.data_ptr(),
+            C.byref(prof), err, len(err)) == 0, err.value
+        return out.cpu().numpy().view(A.HEM_OUTPUT_DTYPE).copy()
+
     try:
-        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
-        assert lib.reactive_gpu_hem_run_resident_v1(hem.handle, dq.data_ptr(), de.data_ptr(), dseed.data_ptr(),
-                                                    dcap.data_ptr(), dorder.data_ptr(), n, out.data_ptr(),
-                                                    C.byref(prof), err, len(err)) == 0, err.value
-        got = out.cpu().numpy().view(A.HEM_OUTPUT_DTYPE)
+        rest = np.setdiff1d(np.arange(total), order)
+        for jump in (False, True):
+            c = cap.copy()
+            if jump:  # jumps on named cells, and one on a cell the batch does not name
+                c["pressureJump"][order[::7]] = rng.uniform(0, 2e4, len(order[::7]))
+                c["pressureJump"][rest[0]] = 3.5e3
+            got = resident(c)
+            exp, ok = host_capillary(lib, host, rho, e, np.ascontiguousarray(c[order]), guess)
+            assert np.array_equal(got["success"][order], ok)
+            assert got["state"][order].tobytes() == exp.tobytes()
+            failed = ok == 0
+            assert got["state"][order][failed].tobytes() == guess[failed].tobytes()
+            assert not got[rest].view(np.uint8).any()
+            assert prof.submitted == n and prof.succeeded == int(ok.sum())
+            assert prof.phaseEvaluations > 0
+        # without capillary inputs: the plain batch
+        got = resident(None)
         exp = guess.copy()
         ok, _ = host.run(rho, e, exp)
         assert np.array_equal(got["success"][order], ok)
         assert got["state"][order].tobytes() == exp.tobytes()
         assert ok[-1] == 0 and got["state"][order[-1]].tobytes() == guess[-1:].tobytes()
-        rest = np.setdiff1d(np.arange(total), order)
         assert not got[rest].view(np.uint8).any()
         assert prof.submitted == n and prof.succeeded == int(ok.sum()) and prof.deviceFailures == n - int(ok.sum())
-        assert prof.phaseEvaluations > 0
-        # NULL capillary input is the same batch
-        out.zero_()
-        assert lib.reactive_gpu_hem_run_resident_v1(hem.handle, dq.data_ptr(), de.data_ptr(), dseed.data_ptr(), None,
-                                                    dorder.data_ptr(), n, out.data_ptr(), C.byref(prof), err,
-                                                    len(err)) == 0, err.value
-        assert out.cpu().numpy().view(A.HEM_OUTPUT_DTYPE)["state"][order].tobytes() == exp.tobytes()
-        # a pressure jump or the frozen partition on a named cell is refused
-        for field, value in (("pressureJump", 3.5e3), ("equilibrium", 0)):
-            bad = cap.copy()
-            bad[field][order[17]] = value
-            assert lib.reactive_gpu_hem_run_resident_v1(hem.handle, dq.data_ptr(), de.data_ptr(), dseed.data_ptr(),
-                                                        dev(bad).data_ptr(), dorder.data_ptr(), n, out.data_ptr(),
-                                                        C.byref(prof), err, len(err)) == 1
-            assert b"pressure jump" in err.value
-        # a jump on a cell the batch does not name is not read
-        other = cap.copy()
-        other["pressureJump"][rest[0]] = 3.5e3
-        assert lib.reactive_gpu_hem_run_resident_v1(hem.handle, dq.data_ptr(), de.data_ptr(), dseed.data_ptr(),
-                                                    dev(other).data_ptr(), dorder.data_ptr(), n, out.data_ptr(),
-                                                    C.byref(prof), err, len(err)) == 0, err.value
     finally:
         hem.close()
         host.close()
-
-
-def test_host_capillary_batch_without_jump_is_run_v1():
-    rho, e, guess = batch(800, 78)
-    n = len(rho)
-    cap = np.zeros(n, dtype=A.CAPILLARY_DTYPE)
-    cap["color"] = .3
-    cap["equilibrium"] = 1
-    lib = _lib.load()
-    hem = GpuHem(capacity=n)
-    err = C.create_string_buffer(1024)
-    try:
-        got = guess.copy()
-        ok2 = np.zeros(n, dtype=np.int32)
-        prof = A.HemProfile(1, C.sizeof(A.HemProfile))
-        assert lib.reactive_gpu_hem_run_v2(hem.handle, A.dptr(rho), A.dptr(e), cap.ctypes.data_as(C.c_void_p), n,
-                                           got.ctypes.data_as(C.c_void_p), ok2.ctypes.data_as(C.POINTER(C.c_int)),
-                                           C.byref(prof), err, len(err)) == 0, err.value
-        exp = guess.copy()
-        ok, _ = hem.run(rho, e, exp)
-        assert np.array_equal(ok2, ok) and got.tobytes() == exp.tobytes()
-        cap["pressureJump"][5] = 10.0
-        before = guess.copy()
-        assert lib.reactive_gpu_hem_run_v2(hem.handle, A.dptr(rho), A.dptr(e), cap.ctypes.data_as(C.c_void_p), n,
-                                           before.ctypes.data_as(C.c_void_p), ok2.ctypes.data_as(C.POINTER(C.c_int)),
-                                           C.byref(prof), err, len(err)) == 1
-        assert before.tobytes() == guess.tobytes()
-    finally:
-        hem.close()
