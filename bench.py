@@ -48,13 +48,14 @@ METRIC = "Mcell-steps/s at 160³, plain FP64 vs mixed/batched; adjoint/forward t
 UNIT = "Mcell-steps/s"
 # Per-unit figures of the dominant kernel (the flash: its one-thread-per-cell
 # single-phase pass, with the work queue for the cells the two-phase bound keeps),
-# each per PR phase evaluation (the device counter the flash reports), from ncu
-# captures of one recovery of the impingement flow: FP64 FLOPs = 2 DFMA + DADD +
-# DMUL thread instructions (40^3, steps 4-5; 516.8 at 80^3, steps 21-22), and DRAM
-# read+write bytes (80^3, steps 21-22: more cells than resident threads, as at
-# 160^3, so the pass's stack frames do not stay in L2).
-FLOPS_PER_PHASE_EVAL = 525.1
-DRAM_BYTES_PER_PHASE_EVAL = 166.2
+# each per PR phase evaluation (the device counter the flash reports; a gas
+# probe's root check decided without the root solve is not one), from ncu
+# captures of one recovery of the impingement flow at 80^3, steps 21-22: FP64
+# FLOPs = 2 DFMA + DADD + DMUL thread instructions, and DRAM read+write bytes
+# (more cells than resident threads, as at 160^3, so the pass's stack frames do
+# not stay in L2).
+FLOPS_PER_PHASE_EVAL = 580.5
+DRAM_BYTES_PER_PHASE_EVAL = 230.0
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
 REFERENCE_SAMPLE = 40  # cube size of the reference CPU arm's bounded sample
 
