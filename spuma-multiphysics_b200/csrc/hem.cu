@@ -645,11 +645,15 @@ std::string validateAndDerive(const ReactiveB200HemModel& m, HemConst& C);
 // largest cubic roots agree, by bisection in ln p (below it the liquid root has
 // the higher potential or only a vapour-like root exists; above it the reverse
 // or only a liquid-like root). out[5 i..5 i+4] = {valid, v_l, v_g, u_l, u_g}.
+// Per temperature: resolved flag, liquid and gas specific volumes, liquid and gas
+// specific internal energies, saturation pressure.
+constexpr int kSatFields = 6;
+
 __global__ void domeSaturation(const HemConst* __restrict__ Cp, int n, double T0, double dT, double* out) {
     const HemConst& C = *Cp;
     const PureSpecies& sp = C.gas;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x) {
-        double* o = out + 5 * size_t(i);
+        double* o = out + kSatFields * size_t(i);
         o[0] = 0;
         const double T = T0 + dT * i;
         TTerms t;
@@ -681,7 +685,7 @@ __global__ void domeSaturation(const HemConst* __restrict__ Cp, int n, double T0
             || prTrhoT(sp, t, sp.W / r.hi, true, G, ph) != EOS_OK)
             continue;
         if (!(fabs(L.mu - G.mu) <= 1e-9 * kGas * T) || !(G.rho < L.rho)) continue;
-        o[1] = 1 / L.rho; o[2] = 1 / G.rho; o[3] = L.e; o[4] = G.e;
+        o[1] = 1 / L.rho; o[2] = 1 / G.rho; o[3] = L.e; o[4] = G.e; o[5] = p;
         o[0] = 1;
     }
 }
@@ -810,7 +814,9 @@ struct HemDevice {
 // the largest latent energy plus ten energy tolerances, 1e-4 plus ten volume
 // tolerances in v. Not built (no bound) for two tables, a loose chemical
 // tolerance, a liquid range past the cubic's critical temperature, or any
-// unresolved temperature below the last resolved one.
+// unresolved temperature below the last resolved one. The same tie lines give
+// the saturation-pressure table of the all-gas stability shortcut
+// (gasStableBelowSaturation), which lives and switches with the bound.
 void buildDome(HemDevice& d) {
     HemConst& C = d.hostConst;
     C.domeN = 0;
@@ -821,11 +827,12 @@ void buildDome(HemDevice& d) {
     constexpr int nT = 4096, nV = 8192;
     const double dT = (T1 - T0) / (nT - 1);
     double* dev = nullptr;
-    check(cudaMalloc(&dev, sizeof(double) * 5 * nT), "cudaMalloc");
+    check(cudaMalloc(&dev, sizeof(double) * kSatFields * nT), "cudaMalloc");
     domeSaturation<<<nT / 128, 128, 0, d.stream>>>(d.cst, nT, T0, dT, dev);
-    std::vector<double> t(5 * nT);
+    std::vector<double> t(kSatFields * nT);
     cudaError_t e1 = cudaGetLastError();
-    cudaError_t e2 = cudaMemcpyAsync(t.data(), dev, sizeof(double) * 5 * nT, cudaMemcpyDeviceToHost, d.stream);
+    cudaError_t e2 = cudaMemcpyAsync(t.data(), dev, sizeof(double) * kSatFields * nT, cudaMemcpyDeviceToHost,
+                                     d.stream);
     cudaError_t e3 = cudaStreamSynchronize(d.stream);
     cudaFree(dev);
     check(e1, "domeSaturation");
@@ -833,16 +840,16 @@ void buildDome(HemDevice& d) {
     check(e3, "sync");
     int last = -1;
     for (int i = 0; i < nT; ++i)
-        if (t[5 * i] == 1) {
+        if (t[kSatFields * i] == 1) {
             if (last != i - 1) return;  // a gap below a resolved temperature
             last = i;
         }
     if (last < 1 || last < nT - 8) return;
     double vlo = HUGE_VAL, vhi = 0, latent = 0;
     for (int i = 0; i <= last; ++i) {
-        vlo = std::min(vlo, t[5 * i + 1]);
-        vhi = std::max(vhi, t[5 * i + 2]);
-        latent = std::max(latent, t[5 * i + 4] - t[5 * i + 3]);
+        vlo = std::min(vlo, t[kSatFields * i + 1]);
+        vhi = std::max(vhi, t[kSatFields * i + 2]);
+        latent = std::max(latent, t[kSatFields * i + 4] - t[kSatFields * i + 3]);
     }
     if (!(vlo > 0 && vhi > vlo && latent > 0)) return;
     const double lnV0 = std::log(vlo), step = std::log(vhi / vlo) / (nV - 1);
@@ -854,7 +861,8 @@ void buildDome(HemDevice& d) {
             if (k >= 0 && k < nV) { up[k] = std::max(up[k], u); lo[k] = std::min(lo[k], u); }
     };
     for (int i = 0; i <= last; ++i) {
-        const double vl = t[5 * i + 1], vg = t[5 * i + 2], ul = t[5 * i + 3], ug = t[5 * i + 4];
+        const double* ti = &t[kSatFields * i];
+        const double vl = ti[1], vg = ti[2], ul = ti[3], ug = ti[4];
         for (int j = std::max(0, index(vl)); j <= std::min(nV - 1, index(vg) + 1); ++j) {
             const double vj = vgrid[j];
             if (vj < vl || vj > vg) continue;
@@ -866,17 +874,25 @@ void buildDome(HemDevice& d) {
         touch(index(vg), ug);
     }
     {  // the critical end above the last resolved temperature
-        const double vl = t[5 * last + 1], vg = t[5 * last + 2], ul = t[5 * last + 3], ug = t[5 * last + 4];
+        const double* tl = &t[kSatFields * last];
+        const double vl = tl[1], vg = tl[2], ul = tl[3], ug = tl[4];
         for (int j = std::max(0, index(vl)); j <= std::min(nV - 1, index(vg) + 1); ++j) {
             up[j] = std::max(up[j], ug);
             lo[j] = std::min(lo[j], ul);
         }
     }
-    std::vector<double> packed(2 * nV);
+    std::vector<double> packed(2 * nV + nT, 0.0);
     std::copy(up.begin(), up.end(), packed.begin());
     std::copy(lo.begin(), lo.end(), packed.begin() + nV);
-    double* table = d.alloc<double>(2 * nV);
-    check(cudaMemcpyAsync(table, packed.data(), sizeof(double) * 2 * nV, cudaMemcpyHostToDevice, d.stream), "H2D dome");
+    // saturation pressures where the phases are well apart (Z_g - Z_l >= 0.05)
+    for (int i = 0; i <= last; ++i) {
+        const double T = T0 + dT * i, p = t[kSatFields * i + 5];
+        const double dz = p * sp.W * (t[kSatFields * i + 2] - t[kSatFields * i + 1]) / (kGas * T);
+        if (p > 0 && dz >= .05) packed[2 * nV + i] = p;
+    }
+    double* table = d.alloc<double>(2 * nV + nT);
+    check(cudaMemcpyAsync(table, packed.data(), sizeof(double) * (2 * nV + nT), cudaMemcpyHostToDevice, d.stream),
+          "H2D dome");
     C.domeUp = table;
     C.domeLo = table + nV;
     C.domeLnV0 = lnV0;
@@ -886,6 +902,10 @@ void buildDome(HemDevice& d) {
     C.domeMarginU = 1e-3 * latent + 10 * C.etol * std::max(1e5, 2000 * C.Tmax);
     C.domeMarginV = 1e-4 + 10 * C.vtol;
     C.domeN = nV;
+    C.satP = table + 2 * nV;
+    C.satN = nT;
+    C.satT0 = T0;
+    C.satInvStep = 1 / dT;
     d.domeBuilt = nV;
     check(cudaMemcpyAsync(d.cst, &C, sizeof(HemConst), cudaMemcpyHostToDevice, d.stream), "H2D constants");
     check(cudaStreamSynchronize(d.stream), "sync");

@@ -53,6 +53,12 @@ struct HemConst {
     const double* domeLo;
     int domeN;
     double domeLnV0, domeInvStep, domeVlo, domeVhi, domeMarginU, domeMarginV;
+    // Saturation pressure of the pure fluid at satN temperatures T_j = satT0 + j / satInvStep
+    // (built with the bound; satP[j] = 0 where unresolved or where the coexisting phases'
+    // compressibility factors lie within 0.05 of each other, near the critical end).
+    const double* satP;
+    int satN;
+    double satT0, satInvStep;
 };
 
 struct CellInput {
@@ -611,9 +617,35 @@ __device__ RB200_FLASH_FN bool twoPhaseSolve(const HemConst& C, const CellInput&
 
 // Stability of a converged candidate at (p, T) with liquid mass `mass`
 // (`known`: the gas table's terms at exactly (p, T), if the caller has them).
+// The stability test of an all-gas state at (p, T) with its gas point `g`
+// decided without evaluating the liquid root, where the outcome is provably
+// "stable": p lies 1e-6 of it below the saturation pressure tabulated at the
+// table temperature one below T's cell (the saturation pressure rises with T,
+// and the table's pressures, from a 160-step bisection to |mu_l - mu_g| <=
+// 1e-9 RT, are off by less than 1e-7 where the phases' Z differ by 0.05 or
+// more), so a liquid root has the larger chemical potential by far more than
+// rounding (the affinity is positive, above -mutol); and the liquid root, when
+// the cubic has one, lies at least 1e-6 of its volume below the middle root,
+// so its evaluation succeeds (dp/dV < 0 off the spinodal, cv > 0 with the PR
+// attraction term) or the root is not a liquid by the reported-phase line
+// (unavailable, also stable). T at or above the table's start is at or above
+// the liquid range's lower end, where the full test would fail the candidate.
+__device__ __forceinline__ bool gasStableBelowSaturation(const HemConst& C, double p, double T, const GasPoint& g) {
+    if (!C.domeN || C.satN < 2 || !(T >= C.satT0)) return false;
+    const double cell = floor((T - C.satT0) * C.satInvStep) - 1;
+    if (!(cell >= 0) || !(cell < C.satN)) return false;
+    const double ps = C.satP[int(cell)];
+    if (!(p < ps * (1 - 1e-6))) return false;
+    if (!g.r.liquid) return true;  // no liquid root: unavailable, stable
+    if (g.r.count != 3) return false;
+    const double mid = -(C.gas.b - kGas * T / p) - g.r.lo - g.r.hi;  // the roots sum to -bn
+    return mid - g.r.lo > 1e-6 * mid;
+}
+
 __device__ RB200_FLASH_FN bool stableAt(const HemConst& C, double q, double mass, double p, double T, Counts& n,
                                 const GasPoint* known = nullptr) {
     if (q - mass > 0) {
+        if (mass == 0 && known && gasStableBelowSaturation(C, p, T, *known)) return true;
         Eval cmp;
         if (!evaluate(C, q, mass, p, T, true, cmp, n, known)) return false;
         const double affinity = cmp.muL - cmp.muG;
