@@ -153,14 +153,21 @@ __device__ __forceinline__ int liquidFromShared(const HemConst& C, int shared, c
     return rootProps(C.liq, t, r, p, ROOT_LIQUID, chem, o);
 }
 
-// The gas table's T-terms, cubic roots and gas-root properties (without the
-// chemical potential) at one (p, T), each with status EOS_OK: what a gas probe
-// computed, handed to the evaluations that follow at the same point.
+// What an accepted gas probe at (p, T) hands to the evaluations that follow at
+// the same point: the gas table's T-terms, the gas phase's properties (without
+// the chemical potential) at the probe's density, which is the gas root of the
+// cubic at (p, T), with their chemical-potential intermediates, and the cubic's
+// roots when the probe solved it (`roots`; otherwise an evaluation that needs
+// them solves the cubic itself, through the same routine). `clear` (meaningful
+// without roots): the cubic has no liquid root, or one above the covolume and at
+// least 1e-6 of its volume below the middle root, both by margins far above
+// rounding.
 struct GasPoint {
     TTerms t;
     Roots r;
     PhaseProps gas;
-    ChemTerms chem;  // the gas root evaluation's chemical-potential intermediates
+    ChemTerms chem;
+    bool roots, clear;
 };
 
 // Phase sums at (p, T) for liquid mass `mass` out of total density q. With
@@ -168,10 +175,10 @@ struct GasPoint {
 // are formed (two-phase residual and stability test). When both branches are
 // needed and the tables hold one species, the T-terms and the cubic are formed
 // once for both roots (the same arithmetic as two separate evaluations).
-// `known` (optional) holds the gas table's terms at exactly (p, T): they replace
-// the T-terms and the cubic of the shared path and the gas root's properties,
-// with `virt` its chemical potential from the kept intermediates (the same values
-// those calls return).
+// `known` (optional) is an accepted gas probe's point at exactly (p, T): its
+// T-terms replace the shared path's, its gas properties the gas root's, with
+// `virt` its chemical potential from the kept intermediates; its roots, or the
+// cubic solved here through the same routine the probe uses, serve the liquid.
 __device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass, double p, double T, bool virt, Eval& v,
                                 Counts& n, const GasPoint* known = nullptr) {
     v.p = p; v.T = T;
@@ -195,7 +202,8 @@ __device__ RB200_FLASH_FN bool evaluate(const HemConst& C, double q, double mass
     int sharedStatus = EOS_OK;
     if (shared && known) {
         t = known->t;
-        r = known->r;
+        if (known->roots) r = known->r;
+        else sharedStatus = cubicRoots(C.gas, T, p, t.aa, r);
     } else if (shared) {
         sharedStatus = tTerms(C.gas, T, t);
         if (sharedStatus == EOS_OK) sharedStatus = cubicRoots(C.gas, T, p, t.aa, r);
@@ -305,16 +313,16 @@ __device__ RB200_FLASH_FN bool solveSmall(double a[3][3], double b[3], int n, do
     return true;
 }
 
-// The gas root of the cubic at (g.t.T, p) and its properties into g (roots,
-// gas-root properties, chemical-potential intermediates): true when that root
-// is the density q the pressure came from (to 1e-8 of q). Out of line: the
-// probe and the completion of a deferred probe run the same instructions, so
-// a point's roots and properties carry the same bits on either path (inlined
-// copies could contract products into FMAs differently).
+// The gas-root check by the root solve: the cubic's roots at (g.t.T, p) into
+// g.r (through the out-of-line cubicRoots, the routine every later evaluation
+// at this point uses, so the roots carry the same bits on every path), then the
+// gas root must pass the root-property checks and be the density q the
+// pressure came from (to 1e-8 of q).
 __device__ RB200_FLASH_FN bool gasRootAt(const HemConst& C, double q, double p, GasPoint& g) {
-    if (cubicRootsBody(C.gas, g.t.T, p, g.t.aa, g.r) != EOS_OK) return false;
-    return rootPropsBody(C.gas, g.t, g.r, p, ROOT_GAS, false, g.gas, &g.chem) == EOS_OK
-           && !(fabs(g.gas.rho - q) > 1e-8 * q);
+    if (cubicRoots(C.gas, g.t.T, p, g.t.aa, g.r) != EOS_OK) return false;
+    PhaseProps root;
+    return rootPropsBody(C.gas, g.t, g.r, p, ROOT_GAS, false, root, nullptr) == EOS_OK
+           && !(fabs(root.rho - q) > 1e-8 * q);
 }
 
 // The outcome of gasRootAt decided without solving the cubic: p = p(T, q), so
@@ -329,8 +337,9 @@ __device__ RB200_FLASH_FN bool gasRootAt(const HemConst& C, double q, double p, 
 // 1e-6 of V0 away from V0 (so V0 is no near-double root and dp/dV stays off
 // zero there), and 1e-9 of V0 (or of the line's density) from the covolume,
 // the classification centre and the reported-phase line. `phase` is the
-// reported phase of the (T, q) evaluation.
-__device__ __forceinline__ int gasRootIsV0(const PureSpecies& sp, const TTerms& t, double p, double q, int phase) {
+// reported phase of the (T, q) evaluation; `clear` as GasPoint::clear.
+__device__ __forceinline__ int gasRootIsV0(const PureSpecies& sp, const TTerms& t, double p, double q, int phase,
+                                           bool& clear) {
     const double T = t.T, V0 = sp.W / q, ip = 1.0 / p;
     const double b = sp.b, b2 = b * b, RTp = kGas * T * ip, aap = t.aa * ip, bn = b - RTp;
     const double cn = -(2.0 * RTp * b - aap + 3.0 * b2), dn = b2 * RTp + b2 * b - aap * b;
@@ -338,8 +347,10 @@ __device__ __forceinline__ int gasRootIsV0(const PureSpecies& sp, const TTerms& 
     const double qc = 2.0 * bn * bn * bn * (1.0 / 27.0) - bn * cn * kThird + dn;
     const double delta = delta2 > 0 ? sqrt(delta2) : 0.0, h = 2.0 * delta * delta2;
     const double disc = qc * qc - h * h, margin = 1e-9 * V0;
+    clear = false;
     if (!(fabs(fabs(h) - fabs(qc)) >= 1e-8) || !(fabs(disc) >= 1e-10) || !(V0 - b > margin)) return -1;
     bool single = disc > 0;  // one real root: V0
+    clear = single;
     if (!single) {
         const double s = bn + V0, tq = cn + V0 * s, d2 = s * s - 4.0 * tq;
         if (!(d2 > 0)) return -1;
@@ -347,6 +358,8 @@ __device__ __forceinline__ int gasRootIsV0(const PureSpecies& sp, const TTerms& 
         if (v1 > V0 + 1e-6 * V0) return 0;  // the largest root, the gas root if any, is not V0
         if (!(v1 < V0 - 1e-6 * V0) || !(fabs(v1 - b) > margin) || !(fabs(v2 - b) > margin)) return -1;
         single = !(v1 > b);  // V0 the only root above the covolume
+        // three physical roots with the liquid one off the spinodal, or V0 alone
+        clear = single || (v2 > b && v1 - v2 > 1e-6 * v1);
     }
     if (single && !(T > sp.Tc)) {
         // a lone root is the gas root when it is not below the centre
@@ -362,33 +375,30 @@ __device__ __forceinline__ int gasRootIsV0(const PureSpecies& sp, const TTerms& 
 
 // Energy residual of the all-gas state at (T, rho) and the gas-root check: the
 // properties at (T, rho), then the gas root of the cubic at the resulting
-// pressure must be that density. One set of T-terms serves both (the same
-// values prTrho and gasPhase would each form); `g` receives them with the
-// roots and the gas root's properties at (p, T). With `deferred`, a check that
-// gasRootIsV0 decides skips the root solve: *deferred is then true and g holds
-// the T-terms only, until gasRootAt completes it at the same (p, T) (the same
-// roots and properties the probe would have formed).
+// pressure must be that density: decided by gasRootIsV0 where its margins
+// allow, else by the root solve. `g` receives the point: the T-terms, the
+// properties at rho with their chemical-potential intermediates, and the roots
+// when they were solved.
 __device__ RB200_FLASH_FN bool gasProbe(const HemConst& C, double q, double eIn, double T, double& F, double& cv, double& p,
-                                double& cp, GasPoint& g, Counts& n, bool* deferred = nullptr) {
-    PhaseProps prop;
+                                double& cp, GasPoint& g, Counts& n) {
     int phase;
     ++n.phases;
     if (!fin(T) || !fin(q) || T <= 0 || q <= 0) return false;
-    if (tTermsBody(C.gas, T, g.t) != EOS_OK || prTrhoTBody(C.gas, g.t, q, false, prop, phase, nullptr) != EOS_OK)
+    if (tTermsBody(C.gas, T, g.t) != EOS_OK || prTrhoTBody(C.gas, g.t, q, false, g.gas, phase, &g.chem) != EOS_OK)
         return false;
-    p = prop.p;  // finite and positive
+    p = g.gas.p;  // finite and positive
     if (!inBounds(C, p, T)) return false;
     if (C.enforceBounds && (T < C.gasTmin || T > C.gasTmax)) return false;
-    const int decided = deferred ? gasRootIsV0(C.gas, g.t, p, q, phase) : -1;
+    const int decided = gasRootIsV0(C.gas, g.t, p, q, phase, g.clear);
     if (decided == 0) return false;
-    if (decided < 0) {
+    g.roots = decided < 0;
+    if (g.roots) {
         ++n.phases;
         if (!gasRootAt(C, q, p, g)) return false;
     }
-    if (deferred) *deferred = decided > 0;
-    F = q * prop.e - eIn;
-    cv = q * prop.cv;
-    cp = prop.cp;
+    F = q * g.gas.e - eIn;
+    cv = q * g.gas.cv;
+    cp = g.gas.cp;
     return fin(F) && fin(cv) && cv > 0;
 }
 
@@ -400,16 +410,14 @@ struct CandidateOut {
 // Scalar T-Newton of the all-gas partition at fixed rho. `g` ends with the gas
 // table's terms at the converged (p, T): the probe that set them is the last
 // probe (a bracket search is always followed by a probe at the bracket end or
-// by at least one Newton probe, which rewrite `g`); when that probe's gas-root
-// check was decided without the root solve, the solve runs once at its point.
-// The probes' decisions are those of full root solves, so the iterates, the
-// final point and `g` are bit for bit those of probes that always solve.
+// by at least one Newton probe, which rewrite `g`). The probes' gas-root
+// decisions are those of full root solves, so the iterates and the final
+// point are those of probes that always solve.
 __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in, Eval& v, CandidateOut& o, GasPoint& g,
                                  Counts& n) {
     const double q = in.q;
     double T = clampd(in.gT, C.Tmin, C.Tmax), F, cv, p, cp;
-    bool deferred = false;  // the last probe's gas-root check skipped its root solve
-    if (!gasProbe(C, q, in.e, T, F, cv, p, cp, g, n, &deferred)) return false;
+    if (!gasProbe(C, q, in.e, T, F, cv, p, cp, g, n)) return false;
     const double scale = fmax(1e5 * q, q * cp * T);
     double lower = T, upper = T, fl = F, fh = F;
     if (fabs(F) > C.etol * scale) {
@@ -420,7 +428,7 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmax(C.Tmin, T - radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n, &deferred)) { fl = val; lower = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n)) { fl = val; lower = cand; found = true; }
                     else cand = .5 * (lower + cand);
                 }
                 if (!found) return false;
@@ -429,13 +437,13 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
                 double cand = fmin(C.Tmax, T + radius);
                 bool found = false;
                 for (int r = 0; r < 8 && !found; ++r) {
-                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n, &deferred)) { fh = val; upper = cand; found = true; }
+                    if (gasProbe(C, q, in.e, cand, val, d1, d2, d3, g, n)) { fh = val; upper = cand; found = true; }
                     else cand = .5 * (upper + cand);
                 }
                 if (!found) return false;
             }
-            if (fabs(fl) <= C.etol * scale) { T = lower; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n, &deferred)) return false; break; }
-            if (fabs(fh) <= C.etol * scale) { T = upper; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n, &deferred)) return false; break; }
+            if (fabs(fl) <= C.etol * scale) { T = lower; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false; break; }
+            if (fabs(fh) <= C.etol * scale) { T = upper; if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false; break; }
             if (lower == C.Tmin && upper == C.Tmax) break;
         }
         if (!(fabs(F) <= C.etol * scale || (fl <= 0 && fh >= 0 && upper > lower))) return false;
@@ -446,13 +454,9 @@ __device__ RB200_FLASH_FN bool scalarGas(const HemConst& C, const CellInput& in,
         const double next = T - F / cv;
         T = fin(next) && next > lower && next < upper ? next : .5 * (lower + upper);
         double d3;
-        if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n, &deferred)) return false;
+        if (!gasProbe(C, q, in.e, T, F, cv, p, d3, g, n)) return false;
     }
     if (fabs(F) > C.etol * scale) return false;
-    if (deferred) {  // the last probe's roots and gas-root properties
-        ++n.phases;
-        if (!gasRootAt(C, q, p, g)) return false;
-    }
     if (!evaluate(C, q, 0.0, p, T, false, v, n, &g)) return false;
     o.vres = fabs(v.volume - 1);
     o.eres = fabs(v.energy - in.e) / energyScale(v, q);
@@ -636,6 +640,7 @@ __device__ __forceinline__ bool gasStableBelowSaturation(const HemConst& C, doub
     if (!(cell >= 0) || !(cell < C.satN)) return false;
     const double ps = C.satP[int(cell)];
     if (!(p < ps * (1 - 1e-6))) return false;
+    if (!g.roots) return g.clear;
     if (!g.r.liquid) return true;  // no liquid root: unavailable, stable
     if (g.r.count != 3) return false;
     const double mid = -(C.gas.b - kGas * T / p) - g.r.lo - g.r.hi;  // the roots sum to -bn
