@@ -54,8 +54,8 @@ UNIT = "Mcell-steps/s"
 # FLOPs = 2 DFMA + DADD + DMUL thread instructions, and DRAM read+write bytes
 # (more cells than resident threads, as at 160^3, so the pass's stack frames do
 # not stay in L2).
-FLOPS_PER_PHASE_EVAL = 580.5
-DRAM_BYTES_PER_PHASE_EVAL = 230.0
+FLOPS_PER_PHASE_EVAL = 617.9
+DRAM_BYTES_PER_PHASE_EVAL = 174.4
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
 REFERENCE_SAMPLE = 40  # cube size of the reference CPU arm's bounded sample
 
