@@ -517,6 +517,52 @@ __device__ inline bool vjpPoint(const HemConst& C, int kind, double q, double e,
     return fin(o.F[2]);
 }
 
+// The implicit-function adjoint of a single-phase cell in (T, rho) form. At the
+// cell's density q the phase's state is a function of T alone, fixed by the
+// energy residual F(T; q, e) = q e(T, q) - e = 0, so dT/de = 1/F_T and
+// dT/dq = -F_q/F_T; the outputs y = (p, T, cv, frozen sound, gas mass) are
+// those of the flash's evaluation of that phase at (T, q) (the (T, rho)
+// evaluation needs no cubic root). Central differences of 1e-6 relative in T,
+// and in q at fixed T. With lambda = sum(ybar y_T) / F_T: rhoBar +=
+// sum(ybar y_q) - lambda F_q and eBar = lambda. False where an evaluation
+// fails; the (ln p, ln T) form then runs.
+__device__ inline bool singlePhaseVjp(const HemConst& C, int kind, double q, double e, double T, const double ybar[5],
+                                      double& rhoBar, double& eBar) {
+    const PureSpecies& sp = kind == 0 ? C.gas : C.liq;
+    const double Tp = T * (1 + 1e-6), Tm = T * (1 - 1e-6), qp = q * (1 + 1e-6), qm = q * (1 - 1e-6);
+    double F[4], y[4][5];
+#pragma unroll 1
+    for (int i = 0; i < 4; ++i) {
+        const double Ti = i == 0 ? Tp : (i == 1 ? Tm : T), qi = i == 2 ? qp : (i == 3 ? qm : q);
+        PhaseProps s;
+        int phase;
+        if (prTrho(sp, Ti, qi, false, s, phase) != EOS_OK) return false;
+        // the flash's single-phase sums (mass qi at density qi: unit volume)
+        const double vp = -s.kappaT, vt = s.alpha, cpD = qi * s.cp;
+        const double cv = (cpD + Ti * vt * vt / vp) / qi;
+        const double specific = 1 / qi, adiabatic = vp / qi + Ti * (vt / qi) * (vt / qi) / s.cp;
+        F[i] = qi * s.e - e;
+        y[i][0] = s.p;
+        y[i][1] = Ti;
+        y[i][2] = cv;
+        y[i][3] = sqrt(-specific * specific / adiabatic);
+        y[i][4] = kind == 0 ? qi : 0.0;
+    }
+    const double hT = Tp - Tm, hq = qp - qm;
+    const double FT = (F[0] - F[1]) / hT, Fq = (F[2] - F[3]) / hq;
+    double dot = 0, dq = 0;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        dot += ybar[r] * (y[0][r] - y[1][r]) / hT;
+        dq += ybar[r] * (y[2][r] - y[3][r]) / hq;
+    }
+    const double lambda = dot / FT;
+    if (!fin(lambda) || !fin(dq) || !fin(Fq) || FT == 0) return false;
+    rhoBar += dq - lambda * Fq;
+    eBar = lambda;
+    return true;
+}
+
 __global__ void hemStateVjp(const HemConst* __restrict__ Cp, const double* __restrict__ cons, size_t stride,
                             size_t count, const ReactiveThermoState* __restrict__ state,
                             const ReactiveTransportState* __restrict__ bar, double* qBar, size_t barStride,
@@ -535,6 +581,17 @@ __global__ void hemStateVjp(const HemConst* __restrict__ Cp, const double* __res
         const int nx = kind == 2 ? 3 : 2;
         const double x[3] = {log(s.p), log(s.T), kind == 2 ? s.liquidMass[0] / q : 0.0};
         const double ybar[5] = {b.p, b.T, b.cv, b.sound, b.gasMass};
+        {
+            double rhoBar = b.rho, eBar = 0;
+            if (kind != 2 && singlePhaseVjp(C, kind, q, e, s.T, ybar, rhoBar, eBar)) {
+                qBar[c] += rhoBar + eBar * .5 * m2 / (q * q);
+                qBar[barStride + c] += -eBar * mx / q;
+                qBar[2 * barStride + c] += -eBar * my / q;
+                qBar[3 * barStride + c] += -eBar * mz / q;
+                qBar[4 * barStride + c] += eBar;
+                continue;
+            }
+        }
         double Fx[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, yx[5][3], Fq[3], yq[5];
         bool ok = true;
 #pragma unroll 1
