@@ -290,9 +290,11 @@ int reactive_transport_autotune_v3(void* transport, const double* q, const React
     void* stream, unsigned* chosen);
 /* Query (request NULL) or set the structured path's launch shapes {stage, gradient,
  * CFL} (no reference counterpart): stage 0 is the shared-memory tiled stage
- * kernel, 64/96/128 the per-cell kernel's block size; gradient and CFL block
- * sizes 64/128/256. Results do not depend on them. active (may be NULL)
- * receives the shapes in use. */
+ * kernel, 1 the split FP64 stage (each interior face's flux once into the face
+ * workspace, then the per-cell sums; 128 threads per cell in mixed precision or
+ * without the workspace), 64/96/128 the per-cell kernel's block size; gradient
+ * and CFL block sizes 64/128/256. Results do not depend on them. active (may be
+ * NULL) receives the shapes in use. */
 int reactive_transport_launch_shapes_v3(void* transport, const unsigned* request, unsigned* active);
 /* Device-resident refresh of the WALE scalar fields for the device stage
  * entries (no reference counterpart: the reference fills them from the host or

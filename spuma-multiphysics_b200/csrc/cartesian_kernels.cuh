@@ -50,6 +50,10 @@ struct CartView {
     // minimum and the boundary ledger cover them only (a z-slab's halo layers
     // are read as neighbours, and written by the halo exchange)
     size_t ownBegin, ownEnd;
+    // scratch of the split FP64 stage (cartFaceFluxes / cartRatesFromFaces): one
+    // flux per interior face and variable, SoA (axis, variable) x cells, indexed
+    // by the face's owner (the lower cell); null where the split is unavailable
+    double* faceFlux;
 };
 
 struct CellData {
@@ -475,6 +479,197 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
 #pragma unroll
         for (int kk = 0; kk < NS + 4; ++kk) {
             const double r = fp64 ? double(rate[kk]) : (double(rate[kk]) + double(comp[kk])) * iv;
+            const size_t o = size_t(kk) * outStride + c;
+            if (mode == 0) out[o] = r;
+            else if (mode == 1) out[o] = C.q[kk] + dt * r;
+            else out[o] = .5 * out[o] + .5 * (C.q[kk] + dt * r);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The FP64 stage split in two launches, each interior face's flux evaluated once
+// instead of once by each of its two cells. cartFaceFluxes: the owner (lower
+// cell) of every +x/+y/+z interior face with an own cell on either side
+// evaluates it in the owner orientation, exactly the call both cells' per-cell
+// evaluations make (faceFluxCart, the same inputs), into v.faceFlux.
+// cartRatesFromFaces and cartRatesBoxSides: every own cell sums its six faces
+// in its face-graph incidence order (-z, -y, -x, +x, +y, +z, then the box
+// sides, evaluated as cartRates does) with the same signs and scaling, and
+// applies the same update: the results are bitwise cartRates<NS, double>'s.
+template <int NS, bool SGS = false>
+__global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* __restrict__ q,
+                                                      const ReactiveTransportState* __restrict__ st,
+                                                      const double* __restrict__ grad,
+                                                      const double* __restrict__ nut, unsigned* error) {
+    constexpr int NQ = NS + 4;
+    const bool viscous = v.viscosity > 0 || v.wale;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        const bool ownC = c >= v.ownBegin && c < v.ownEnd;
+        bool any = false;
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const int s = 2 * axis + 1;
+            if (!hasNeighbour(v, s, i, j, k)) continue;
+            const size_t nb = neighbourOf(v, s, c);
+            any = any || ownC || (nb >= v.ownBegin && nb < v.ownEnd);
+        }
+        if (!any) continue;
+        CellData C;
+        loadCell<NS, SGS>(v, q, st, c, C, true);
+        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (viscous) {
+#pragma unroll
+            for (int jj = 0; jj < 9; ++jj) gC[jj] = grad[size_t(jj) * v.cells + c];
+        }
+        const double nutC = v.wale ? nut[c] : 0.0;
+        const CellT<double> cc = asCell<NS, double, SGS>(C);
+        bool bad = false, faceBad = false;
+#pragma unroll 1
+        for (int axis = 0; axis < 3; ++axis) {
+            const int s = 2 * axis + 1;
+            if (!hasNeighbour(v, s, i, j, k)) continue;
+            const size_t nb = neighbourOf(v, s, c);
+            if (!ownC && !(nb >= v.ownBegin && nb < v.ownEnd)) continue;
+            CellData N;
+            loadCell<NS, SGS>(v, q, st, nb, N, true);
+            double gN[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (viscous) {
+#pragma unroll
+                for (int jj = 0; jj < 9; ++jj) gN[jj] = grad[size_t(jj) * v.cells + nb];
+            }
+            const double nutN = v.wale ? nut[nb] : 0.0;
+            double F[NQ];
+            faceFluxCart<NS, double, SGS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc,
+                                          asCell<NS, double, SGS>(N), gC, gN, nutC, nutN, F, bad, faceBad);
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) v.faceFlux[(size_t(axis) * NQ + kk) * v.cells + c] = F[kk];
+        }
+        if (bad) atomicOr(error, 1u);
+        if (faceBad) atomicOr(error, 2u);
+    }
+}
+
+// Every own cell's interior faces in its incidence order (-z, -y, -x, +x, +y,
+// +z) from the face fluxes, and for a cell off the box sides the update. A
+// cell on a box side leaves its partial sums in the scratch after the face
+// fluxes (variable-major, stride cells) for cartRatesBoxSides, which adds its
+// box-side faces in cartRates' order and applies the update: the two kernels
+// together give cartRates' sums bit for bit, and this one stays light (no
+// boundary flux code, far fewer registers).
+template <int NS>
+__global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const double* __restrict__ q, double* out,
+                                                          size_t outStride, int mode, double dt) {
+    constexpr int NQ = NS + 4;
+    const double* __restrict__ flux = v.faceFlux;
+    double* partial = v.faceFlux + size_t(3) * NQ * v.cells;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
+        if (c < v.ownBegin || c >= v.ownEnd) continue;
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        const bool edge = i == 0 || i + 1 == v.nx || j == 0 || j + 1 == v.ny || k == 0 || k + 1 == v.nz;
+        const double iv = v.invV[c];
+        double rate[NQ];
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) rate[kk] = 0.0;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int s = sideOf(n);
+            if (!hasNeighbour(v, s, i, j, k)) continue;
+            const int axis = s >> 1;
+            const size_t owner = (s & 1) ? c : neighbourOf(v, s, c);
+            const double sign = (s & 1) ? -1 : 1;
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) rate[kk] += sign * flux[(size_t(axis) * NQ + kk) * v.cells + owner] * iv;
+        }
+        if (edge) {
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) partial[size_t(kk) * v.cells + c] = rate[kk];
+            continue;
+        }
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) {
+            const double r = rate[kk], qk = q[size_t(kk) * v.all + c];
+            const size_t o = size_t(kk) * outStride + c;
+            if (mode == 0) out[o] = r;
+            else if (mode == 1) out[o] = qk + dt * r;
+            else out[o] = .5 * out[o] + .5 * (qk + dt * r);
+        }
+    }
+}
+
+// Cells on the box's sides: the two end planes in z, then per inner plane its
+// rows j = 0 and j = ny - 1 and its columns i = 0 and i = nx - 1 between them
+// (every dimension at least 3).
+__device__ __forceinline__ size_t shellCells(const CartView& v) {
+    return 2 * size_t(v.nx) * v.ny + size_t(v.nz - 2) * (2 * size_t(v.nx) + 2 * size_t(v.ny - 2));
+}
+__device__ __forceinline__ size_t shellCell(const CartView& v, size_t e) {
+    const size_t nx = v.nx, ny = v.ny, plane = nx * ny;
+    if (e < 2 * plane) return e < plane ? e : e - plane + (size_t(v.nz) - 1) * plane;
+    e -= 2 * plane;
+    const size_t ring = 2 * nx + 2 * (ny - 2), k = 1 + e / ring, r = e % ring;
+    size_t i, j;
+    if (r < 2 * nx) {
+        j = r < nx ? 0 : ny - 1;
+        i = r < nx ? r : r - nx;
+    } else {
+        j = 1 + (r - 2 * nx) / 2;
+        i = ((r - 2 * nx) & 1) ? nx - 1 : 0;
+    }
+    return i + nx * (j + ny * k);
+}
+
+// The box-side faces of the own cells on the box's sides (after
+// cartRatesFromFaces), in cartRates' order, and their update: over the shell
+// of side cells, or over every cell when a dimension is below 3.
+template <int NS, bool SGS = false>
+__global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const double* __restrict__ q,
+                                                         const ReactiveTransportState* __restrict__ st,
+                                                         const double* __restrict__ grad,
+                                                         const double* __restrict__ nut, double* out,
+                                                         size_t outStride, int mode, double dt, unsigned* error) {
+    constexpr int NQ = NS + 4;
+    const bool viscous = v.viscosity > 0 || v.wale;
+    const double* partial = v.faceFlux + size_t(3) * NQ * v.cells;
+    const bool shell = v.nx >= 3 && v.ny >= 3 && v.nz >= 3;
+    const size_t items = shell ? shellCells(v) : v.cells;
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < items; e += size_t(blockDim.x) * gridDim.x) {
+        const size_t c = shell ? shellCell(v, e) : e;
+        if (c < v.ownBegin || c >= v.ownEnd) continue;
+        int i, j, k;
+        cellCoords(v, c, i, j, k);
+        if (!(i == 0 || i + 1 == v.nx || j == 0 || j + 1 == v.ny || k == 0 || k + 1 == v.nz)) continue;
+        CellData C;
+        loadCell<NS, SGS>(v, q, st, c, C, true);
+        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (viscous) {
+#pragma unroll
+            for (int jj = 0; jj < 9; ++jj) gC[jj] = grad[size_t(jj) * v.cells + c];
+        }
+        const double nutC = v.wale ? nut[c] : 0.0;
+        const double iv = v.invV[c];
+        double rate[NQ];
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) rate[kk] = partial[size_t(kk) * v.cells + c];
+        bool bad = false, faceBad = false;
+#pragma unroll
+        for (int n = 6; n < 12; ++n) {
+            const int s = sideOf(n);
+            if (hasNeighbour(v, s, i, j, k)) continue;
+            double F[NQ];
+            double sign;
+            sideFlux<NS, double, SGS>(v, q, st, grad, nut, c, s, false, i, j, k, C, gC, nutC, F, sign, bad, faceBad);
+#pragma unroll
+            for (int kk = 0; kk < NQ; ++kk) rate[kk] += sign * F[kk] * iv;
+        }
+        if (bad) atomicOr(error, 1u);
+        if (faceBad) atomicOr(error, 2u);
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) {
+            const double r = rate[kk];
             const size_t o = size_t(kk) * outStride + c;
             if (mode == 0) out[o] = r;
             else if (mode == 1) out[o] = C.q[kk] + dt * r;

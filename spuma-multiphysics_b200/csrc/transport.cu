@@ -561,6 +561,10 @@ struct Transport {
         b.sc = v.sc;
         b.mixCp = v.mixCp;
         b.spH = v.spH;
+        // the split stage's face fluxes live in the face graph's workspace, which
+        // the structured path leaves unused (capillary handles keep it for theirs)
+        const size_t need = product(product(4, cfg.variables), b.cells);  // face fluxes + box-side partial sums
+        b.faceFlux = v.work && !v.capillary && need <= product(v.faces, FW_FIELDS) ? v.work : nullptr;
         return b;
     }
     template <template <int> class K, class... Args> void bySpecies(Args&&... args) {
@@ -589,8 +593,9 @@ struct Transport {
         }
     };
     template <int NS> struct RatesK {
-        // block 0: the shared-memory tiled kernel; otherwise the per-cell kernel
-        // with that many threads a block (the two give the same bits)
+        // block 0: the shared-memory tiled kernel; 1: the split FP64 stage;
+        // otherwise the per-cell kernel with that many threads a block (all give
+        // the same bits)
         template <class R, bool SGS>
         static void tiled(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                           const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
@@ -614,6 +619,31 @@ struct Transport {
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                         const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
                         unsigned block, cudaStream_t s) {
+            // block 1: the split FP64 stage (face fluxes once, then the per-cell sums;
+            // the same bits); elsewhere, or without its scratch, 128 threads per cell
+            if (block == 1) {
+                if constexpr (sizeof(R) == sizeof(double)) {
+                    if (b.faceFlux) {
+                        const unsigned grid = gridFor(b.cells, 128);
+                        if (b.sgs) cartFaceFluxes<NS, true><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error);
+                        else cartFaceFluxes<NS><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error);
+                        cartRatesFromFaces<NS><<<gridFor(b.cells, 256), 256, 0, s>>>(b, q, out, stride, mode, dt);
+                        const bool shell = b.nx >= 3 && b.ny >= 3 && b.nz >= 3;
+                        const size_t sides = shell ? 2 * size_t(b.nx) * b.ny
+                                                         + size_t(b.nz - 2) * (2 * size_t(b.nx) + 2 * size_t(b.ny - 2))
+                                                   : b.cells;
+                        const unsigned sideGrid = gridFor(sides, 128);
+                        if (b.sgs)
+                            cartRatesBoxSides<NS, true><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode,
+                                                                                dt, error);
+                        else
+                            cartRatesBoxSides<NS><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt,
+                                                                          error);
+                        return;
+                    }
+                }
+                block = 128;
+            }
             if (block == 0) {
                 if (b.sgs) tiled<R, true>(b, q, st, grad, nut, out, stride, mode, dt, error, s);
                 else tiled<R, false>(b, q, st, grad, nut, out, stride, mode, dt, error, s);
@@ -774,7 +804,7 @@ struct Transport {
             if (mixed) launchBoxGradientsT(state, gradF, nutF, s);
             else launchBoxGradientsT(state, v.grad, v.nut, s);
         });
-        pick(launch.rates, {0u, 64u, 96u, 128u}, [&] { launchBoxStage(q, out, state, 1e-30, 0, nullptr, s); });
+        pick(launch.rates, {0u, 1u, 64u, 96u, 128u}, [&] { launchBoxStage(q, out, state, 1e-30, 0, nullptr, s); });
         pick(launch.steps, {64u, 128u, 256u}, [&] { launchBoxStep(state, .5, 1.0, reduceScratch + reduceBlocks, s); });
         check(cudaEventDestroy(a), "event");
         check(cudaEventDestroy(b), "event");

@@ -375,8 +375,10 @@ TILE_BOXES = BOXES + [
 def test_tiled_stage_kernel_equals_per_cell_kernel(spec, path):
     """The shared-memory tiled stage kernel (launch shape 0: each x and y face
     evaluated once per plane into shared memory, z faces carried down the
-    column) gives the per-cell kernel's stage results bit for bit: both stages,
-    the CFL step and the boundary ledger, across tiles and z-chunks."""
+    column) and the split FP64 stage (shape 1: each interior face's flux once,
+    then the per-cell sums; the per-cell kernel in mixed precision) give the
+    per-cell kernel's stage results bit for bit: both stages, the CFL step and
+    the boundary ledger, across tiles and z-chunks."""
     import torch
     L = _lib.load()
     lib = T.bind(L)
@@ -390,19 +392,21 @@ def test_tiled_stage_kernel_equals_per_cell_kernel(spec, path):
             assert L.reactive_transport_flux_v3(h, 1, None) == 0
         stream = torch.cuda.current_stream().cuda_stream
         runs = []
-        for stage_shape in (0, 128):
+        for stage_shape in (0, 1, 128):
             shapes = (C.c_uint * 3)(stage_shape, 256, 256)
             active = (C.c_uint * 3)()
             assert L.reactive_transport_launch_shapes_v3(h, shapes, active) == 0
             assert list(active) == [stage_shape, 256, 256]
             runs.append(_stage_pair(L, h, case, stream, torch))
-        tiled, per_cell = runs
-        assert tiled["status"] == per_cell["status"]
-        assert tiled["dt"] == per_cell["dt"]
-        assert np.array_equal(tiled["q1"], per_cell["q1"])
-        assert np.array_equal(tiled["qn"], per_cell["qn"])
-        assert np.array_equal(tiled["br0"], per_cell["br0"]) and np.array_equal(tiled["br1"], per_cell["br1"])
-        assert tiled["tail"] and per_cell["tail"]
+        per_cell = runs[-1]
+        for other in runs[:-1]:
+            assert other["status"] == per_cell["status"]
+            assert other["dt"] == per_cell["dt"]
+            assert np.array_equal(other["q1"], per_cell["q1"])
+            assert np.array_equal(other["qn"], per_cell["qn"])
+            assert np.array_equal(other["br0"], per_cell["br0"]) and np.array_equal(other["br1"], per_cell["br1"])
+            assert other["tail"]
+        assert per_cell["tail"]
         bad = (C.c_uint * 3)(32, 256, 256)
         assert L.reactive_transport_launch_shapes_v3(h, bad, None) == 1
     finally:
