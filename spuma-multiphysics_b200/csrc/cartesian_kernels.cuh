@@ -497,11 +497,54 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
 // in its face-graph incidence order (-z, -y, -x, +x, +y, +z, then the box
 // sides, evaluated as cartRates does) with the same signs and scaling, and
 // applies the same update: the results are bitwise cartRates<NS, double>'s.
+// (defined with the CFL kernels below)
+template <bool SGS = false>
+__device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, double sgn, double dist, double w,
+                                                int kind, const CellData& L, const CellData& R, double nutL,
+                                                double nutR);
+
+// The split stage's scratch in v.faceFlux, in doubles: the face fluxes
+// (3 NQ cells), the box-side cells' partial sums (NQ cells), with the CFL pass
+// the +x/+y/+z face speeds (3 cells), the box-side cells' partial
+// denominators (cells) and the per-block step minima of both kernels.
+constexpr size_t kSplitStepPartials = 2 * size_t(kSmCount) * 8 * 16;
+__host__ __device__ inline size_t splitSpeedOffset(int nq, size_t cells) { return 4 * size_t(nq) * cells; }
+__host__ __device__ inline size_t splitDenominatorOffset(int nq, size_t cells) { return (4 * size_t(nq) + 3) * cells; }
+__host__ __device__ inline size_t splitStepOffset(int nq, size_t cells) { return (4 * size_t(nq) + 4) * cells; }
+__host__ __device__ inline size_t splitScratchDoubles(int nq, size_t cells, bool cflPass) {
+    return cflPass ? splitStepOffset(nq, cells) + kSplitStepPartials : 4 * size_t(nq) * cells;
+}
+
+// One block's minimum of m into partial[block] (all threads of the block).
+__device__ __forceinline__ void blockMinimum(double m, double* partial) {
+    __shared__ double warpValues[32];
+    m = warpMin(m);
+    if ((threadIdx.x & 31) == 0) warpValues[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? warpValues[threadIdx.x] : HUGE_VAL;
+        m = warpMin(m);
+        if (threadIdx.x == 0) partial[blockIdx.x] = m;
+    }
+}
+
+// A cell's CFL step from its face-speed denominator, as cartSteps forms it.
+__device__ __forceinline__ double cellStep(const CartView& v, size_t c, double denominator, bool bad, double cfl,
+                                           double maximumStep) {
+    double step = denominator > 0 ? dmin(maximumStep, cfl / (v.invV[c] * denominator)) : maximumStep;
+    if (bad || !isfinite(denominator) || denominator < 0) step = -1;
+    return isfinite(step) && step > 0 ? step : -1.0;
+}
+
+// With `cfl` > 0 the split stage also forms the CFL step of the same state
+// (cartSteps' per-cell steps from the same face speeds, each face's speed
+// evaluated once): the minimum over both kernels' block minima
+// (minimumReduce) is bitwise cartSteps'.
 template <int NS, bool SGS = false>
 __global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* __restrict__ q,
                                                       const ReactiveTransportState* __restrict__ st,
                                                       const double* __restrict__ grad,
-                                                      const double* __restrict__ nut, unsigned* error) {
+                                                      const double* __restrict__ nut, unsigned* error, bool cflPass) {
     constexpr int NQ = NS + 4;
     const bool viscous = v.viscosity > 0 || v.wale;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
@@ -546,6 +589,9 @@ __global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* 
                                           asCell<NS, double, SGS>(N), gC, gN, nutC, nutN, F, bad, faceBad);
 #pragma unroll
             for (int kk = 0; kk < NQ; ++kk) v.faceFlux[(size_t(axis) * NQ + kk) * v.cells + c] = F[kk];
+            if (cflPass)
+                v.faceFlux[splitSpeedOffset(NQ, v.cells) + size_t(axis) * v.cells + c] =
+                    faceSpeedCart<SGS>(v, axis, 1.0, v.dist[axis], .5, 0, C, N, nutC, nutN);
         }
         if (bad) atomicOr(error, 1u);
         if (faceBad) atomicOr(error, 2u);
@@ -561,10 +607,15 @@ __global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* 
 // boundary flux code, far fewer registers).
 template <int NS>
 __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const double* __restrict__ q, double* out,
-                                                          size_t outStride, int mode, double dt) {
+                                                          size_t outStride, int mode, double dt, double cfl,
+                                                          double maximumStep) {
     constexpr int NQ = NS + 4;
     const double* __restrict__ flux = v.faceFlux;
     double* partial = v.faceFlux + size_t(3) * NQ * v.cells;
+    const double* speed = v.faceFlux + splitSpeedOffset(NQ, v.cells);
+    double* denominators = v.faceFlux + splitDenominatorOffset(NQ, v.cells);
+    const bool cflPass = cfl > 0;
+    double m = maximumStep;  // as cartSteps starts its minimum
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         if (c < v.ownBegin || c >= v.ownEnd) continue;
         int i, j, k;
@@ -584,6 +635,23 @@ __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const doub
 #pragma unroll
             for (int kk = 0; kk < NQ; ++kk) rate[kk] += sign * flux[(size_t(axis) * NQ + kk) * v.cells + owner] * iv;
         }
+        if (cflPass) {
+            // cartSteps' denominator over the interior faces, in the same order
+            double denominator = 0;
+            bool bad = false;
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                const int s = sideOf(n);
+                if (!hasNeighbour(v, s, i, j, k)) continue;
+                const int axis = s >> 1;
+                const size_t owner = (s & 1) ? c : neighbourOf(v, s, c);
+                const double sp = speed[size_t(axis) * v.cells + owner];
+                if (!isfinite(sp) || sp < 0) bad = true;
+                else if (!bad) denominator += v.area[axis] * sp;
+            }
+            if (edge) denominators[c] = bad ? NAN : denominator;
+            else m = fmin(m, cellStep(v, c, denominator, bad, cfl, maximumStep));
+        }
         if (edge) {
 #pragma unroll
             for (int kk = 0; kk < NQ; ++kk) partial[size_t(kk) * v.cells + c] = rate[kk];
@@ -598,6 +666,7 @@ __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const doub
             else out[o] = .5 * out[o] + .5 * (qk + dt * r);
         }
     }
+    if (cflPass) blockMinimum(m, v.faceFlux + splitStepOffset(NQ, v.cells));
 }
 
 // Cells on the box's sides: the two end planes in z, then per inner plane its
@@ -630,10 +699,14 @@ __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const doubl
                                                          const ReactiveTransportState* __restrict__ st,
                                                          const double* __restrict__ grad,
                                                          const double* __restrict__ nut, double* out,
-                                                         size_t outStride, int mode, double dt, unsigned* error) {
+                                                         size_t outStride, int mode, double dt, unsigned* error,
+                                                         double cfl, double maximumStep, unsigned stepBase) {
     constexpr int NQ = NS + 4;
     const bool viscous = v.viscosity > 0 || v.wale;
     const double* partial = v.faceFlux + size_t(3) * NQ * v.cells;
+    const double* denominators = v.faceFlux + splitDenominatorOffset(NQ, v.cells);
+    const bool cflPass = cfl > 0;
+    double m = maximumStep;
     const bool shell = v.nx >= 3 && v.ny >= 3 && v.nz >= 3;
     const size_t items = shell ? shellCells(v) : v.cells;
     for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < items; e += size_t(blockDim.x) * gridDim.x) {
@@ -667,6 +740,25 @@ __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const doubl
         }
         if (bad) atomicOr(error, 1u);
         if (faceBad) atomicOr(error, 2u);
+        if (cflPass) {
+            // the box sides' speeds after the interior faces', as cartSteps adds them
+            double denominator = denominators[c];
+            bool badSpeed = isnan(denominator);
+#pragma unroll
+            for (int n = 6; n < 12; ++n) {
+                const int s = sideOf(n);
+                if (hasNeighbour(v, s, i, j, k) || badSpeed) continue;
+                const int axis = s >> 1;
+                const ReactiveTransportFace& f = sideFace(v, s, i, j, k);
+                CellData Rt;
+                boundaryRight<NS, SGS>(v, nullptr, st, f, axis, C, Rt, false);
+                const double sp = faceSpeedCart<SGS>(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight,
+                                                     f.kind, C, Rt, nutC, nutC);
+                if (!isfinite(sp) || sp < 0) badSpeed = true;
+                else denominator += f.area * sp;
+            }
+            m = fmin(m, cellStep(v, c, denominator, badSpeed, cfl, maximumStep));
+        }
 #pragma unroll
         for (int kk = 0; kk < NQ; ++kk) {
             const double r = rate[kk];
@@ -676,6 +768,7 @@ __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const doubl
             else out[o] = .5 * out[o] + .5 * (C.q[kk] + dt * r);
         }
     }
+    if (cflPass) blockMinimum(m, v.faceFlux + splitStepOffset(NQ, v.cells) + stepBase);
 }
 
 // ---------------------------------------------------------------------------
@@ -935,7 +1028,7 @@ __global__ void __launch_bounds__(kTileX * kTileY, RB200_TILE_MINBLOCKS) cartRat
 }
 
 // Wave/diffusion speed of one face (faceSpeeds of the face graph); -1 when invalid.
-template <bool SGS = false>
+template <bool SGS>
 __device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, double sgn, double dist, double w,
                                                 int kind, const CellData& L, const CellData& R, double nutL,
                                                 double nutR) {

@@ -563,7 +563,7 @@ struct Transport {
         b.spH = v.spH;
         // the split stage's face fluxes live in the face graph's workspace, which
         // the structured path leaves unused (capillary handles keep it for theirs)
-        const size_t need = product(product(4, cfg.variables), b.cells);  // face fluxes + box-side partial sums
+        const size_t need = splitScratchDoubles(int(cfg.variables), b.cells, true);
         b.faceFlux = v.work && !v.capillary && need <= product(v.faces, FW_FIELDS) ? v.work : nullptr;
         return b;
     }
@@ -593,6 +593,33 @@ struct Transport {
         }
     };
     template <int NS> struct RatesK {
+        // The split FP64 stage (cartFaceFluxes, cartRatesFromFaces,
+        // cartRatesBoxSides); with cfl > 0 also the CFL step of the same state
+        // into *result (cartSteps' minimum, from the same face speeds).
+        static void split(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
+                          const double* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
+                          double cfl, double maximumStep, double* result, cudaStream_t s) {
+            const bool cflPass = cfl > 0;
+            const unsigned grid = gridFor(b.cells, 128), cellGrid = gridFor(b.cells, 256);
+            if (b.sgs) cartFaceFluxes<NS, true><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error, cflPass);
+            else cartFaceFluxes<NS><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error, cflPass);
+            cartRatesFromFaces<NS><<<cellGrid, 256, 0, s>>>(b, q, out, stride, mode, dt, cfl, maximumStep);
+            const bool shell = b.nx >= 3 && b.ny >= 3 && b.nz >= 3;
+            const size_t sides = shell ? 2 * size_t(b.nx) * b.ny
+                                             + size_t(b.nz - 2) * (2 * size_t(b.nx) + 2 * size_t(b.ny - 2))
+                                       : b.cells;
+            const unsigned sideGrid = gridFor(sides, 128);
+            if (b.sgs)
+                cartRatesBoxSides<NS, true><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error,
+                                                                    cfl, maximumStep, cellGrid);
+            else
+                cartRatesBoxSides<NS><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error, cfl,
+                                                              maximumStep, cellGrid);
+            if (cflPass)
+                minimumReduce<<<1, 1024, 0, s>>>(b.faceFlux + splitStepOffset(NQ, b.cells), size_t(cellGrid) + sideGrid,
+                                                 result);
+        }
+        static constexpr int NQ = NS + 4;
         // block 0: the shared-memory tiled kernel; 1: the split FP64 stage;
         // otherwise the per-cell kernel with that many threads a block (all give
         // the same bits)
@@ -624,21 +651,7 @@ struct Transport {
             if (block == 1) {
                 if constexpr (sizeof(R) == sizeof(double)) {
                     if (b.faceFlux) {
-                        const unsigned grid = gridFor(b.cells, 128);
-                        if (b.sgs) cartFaceFluxes<NS, true><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error);
-                        else cartFaceFluxes<NS><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error);
-                        cartRatesFromFaces<NS><<<gridFor(b.cells, 256), 256, 0, s>>>(b, q, out, stride, mode, dt);
-                        const bool shell = b.nx >= 3 && b.ny >= 3 && b.nz >= 3;
-                        const size_t sides = shell ? 2 * size_t(b.nx) * b.ny
-                                                         + size_t(b.nz - 2) * (2 * size_t(b.nx) + 2 * size_t(b.ny - 2))
-                                                   : b.cells;
-                        const unsigned sideGrid = gridFor(sides, 128);
-                        if (b.sgs)
-                            cartRatesBoxSides<NS, true><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode,
-                                                                                dt, error);
-                        else
-                            cartRatesBoxSides<NS><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt,
-                                                                          error);
+                        split(b, q, st, grad, nut, out, stride, mode, dt, error, 0.0, 0.0, nullptr, s);
                         return;
                     }
                 }
@@ -655,6 +668,13 @@ struct Transport {
             else
                 cartRates<NS, R><<<gridFor(b.cells, block), block, 0, s>>>(b, q, st, grad, nut, out, stride, mode,
                                                                          dt, error);
+        }
+    };
+    template <int NS> struct SplitK {
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
+                        const double* nut, double* out, size_t stride, int mode, double dt, unsigned* error, double cfl,
+                        double maximumStep, double* result, cudaStream_t s) {
+            RatesK<NS>::split(b, q, st, grad, nut, out, stride, mode, dt, error, cfl, maximumStep, result, s);
         }
     };
     template <int NS> struct StepsK {
@@ -720,6 +740,25 @@ struct Transport {
     // gradients and eddy viscosities when WALE is on, and the stage reuses them.
     void launchBoxStepStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt,
                             int stage, double* rate, double cfl, double maximumStep, double* result, cudaStream_t s) {
+        if (!mixed && launch.rates == 1) {
+            const CartView b = boxView();
+            if (b.faceFlux) {
+                // the split stage forms the CFL step of the same state with its fluxes
+                launchBoxGradientsT(state, v.grad, v.nut, s);
+                if (rate) {
+                    bySpecies<LedgerK>(b, qIn, state, static_cast<const double*>(v.grad),
+                                       static_cast<const double*>(v.nut), ledgerPartial, ledgerBlocks, s);
+                    foldPartials<<<1, 32 * unsigned(cfg.variables), 0, s>>>(ledgerPartial, int(ledgerBlocks),
+                                                                            int(cfg.variables), rate);
+                    launched();
+                }
+                bySpecies<SplitK>(b, qIn, state, static_cast<const double*>(v.grad), static_cast<const double*>(v.nut),
+                                  qOut, v.all, stage == 0 ? 1 : 2, dt, flags, cfl, maximumStep, result, s);
+                ++deviceProfile.cflFaceLaunches;
+                ++deviceProfile.transportFaceLaunches;
+                return;
+            }
+        }
         launchBoxStep(state, cfl, maximumStep, result, s);
         if (mixed) launchBoxStageT(qIn, qOut, state, dt, stage, rate, gradF, nutF, s, v.wale);
         else launchBoxStageT(qIn, qOut, state, dt, stage, rate, v.grad, v.nut, s, v.wale);

@@ -411,3 +411,67 @@ def test_tiled_stage_kernel_equals_per_cell_kernel(spec, path):
         assert L.reactive_transport_launch_shapes_v3(h, bad, None) == 1
     finally:
         lib.reactive_transport_destroy(h)
+
+
+def _stage_cfl_pair(L, h, case, stream, torch):
+    """Both stages through the combined CFL + stage entry (stage_cfl_device_v3)."""
+    nc, nv, ns = case["nc"], case["nv"], case["ns"]
+    cells, fixed, nvar, nsp = (C.c_size_t() for _ in range(4))
+    assert L.reactive_transport_layout_v3(h, C.byref(cells), C.byref(fixed), C.byref(nvar), C.byref(nsp)) == 0
+    all_ = nc + fixed.value
+    q0 = torch.zeros((nv, all_), dtype=torch.float64, device="cuda")
+    q0[:, :nc] = torch.from_numpy(case["q"].T.copy()).cuda()
+    st = torch.zeros((all_, 7), dtype=torch.float64, device="cuda")
+    st[:nc] = torch.from_numpy(case["states"].view(np.float64).reshape(nc, 7)).cuda()
+    assert L.reactive_transport_fill_fixed_v3(h, q0.data_ptr(), st.data_ptr(), stream) == 0
+    dt = torch.zeros(2, dtype=torch.float64, device="cuda")
+    assert L.reactive_transport_stable_step_device_v3(h, q0.data_ptr(), st.data_ptr(), .23, .1, dt.data_ptr(),
+                                                      stream) == 0
+    torch.cuda.synchronize()
+    step = .1 * dt[0].item()
+    q1, qn = q0.clone(), q0.clone()
+    br = torch.zeros((2, nv), dtype=torch.float64, device="cuda")
+    assert L.reactive_transport_stage_cfl_device_v3(h, q0.data_ptr(), q1.data_ptr(), st.data_ptr(), step, 0,
+                                                    br[0].data_ptr(), .23, .1, dt[0:].data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    got1 = np.ascontiguousarray(q1[:, :nc].cpu().numpy().T)
+    st1, _, _ = T.ideal_states(got1, ns)
+    st[:nc] = torch.from_numpy(st1.view(np.float64).reshape(nc, 7)).cuda()
+    assert L.reactive_transport_stage_cfl_device_v3(h, q1.data_ptr(), qn.data_ptr(), st.data_ptr(), step, 1,
+                                                    br[1].data_ptr(), .23, .1, dt[1:].data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    status = C.c_uint()
+    assert L.reactive_transport_status_v3(h, C.byref(status), 1, stream) == 0
+    return dict(dt=dt.cpu().numpy(), q1=got1, qn=qn[:, :nc].cpu().numpy().T, br=br.cpu().numpy(),
+                status=status.value)
+
+
+@pytest.mark.parametrize("path", ["fp64", "hllc"])
+@pytest.mark.parametrize("spec", TILE_BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
+def test_split_stage_with_its_cfl_step_equals_per_cell_kernels(spec, path):
+    """The combined CFL + stage entry with the split FP64 stage (launch shape 1:
+    the CFL step formed from the face speeds the face pass evaluates once,
+    beside the fluxes) gives the per-cell kernels' CFL steps, stages and
+    boundary ledgers bit for bit, on both stages."""
+    import torch
+    L = _lib.load()
+    lib = T.bind(L)
+    kinds = mixed_kinds(spec["dims"], 17) if spec["kinds"] == "mixed" else spec["kinds"]
+    case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
+    h = T.create(lib, 1, case, wale_cw=spec.get("wale"))
+    try:
+        if path == "hllc":
+            assert L.reactive_transport_flux_v3(h, 1, None) == 0
+        stream = torch.cuda.current_stream().cuda_stream
+        runs = []
+        for stage_shape in (1, 128):
+            shapes = (C.c_uint * 3)(stage_shape, 256, 256)
+            assert L.reactive_transport_launch_shapes_v3(h, shapes, None) == 0
+            runs.append(_stage_cfl_pair(L, h, case, stream, torch))
+        split, per_cell = runs
+        assert split["status"] == per_cell["status"]
+        assert np.array_equal(split["dt"], per_cell["dt"]) and (split["dt"] > 0).all()
+        assert np.array_equal(split["q1"], per_cell["q1"]) and np.array_equal(split["qn"], per_cell["qn"])
+        assert np.array_equal(split["br"], per_cell["br"])
+    finally:
+        lib.reactive_transport_destroy(h)
