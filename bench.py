@@ -452,6 +452,12 @@ def run_ours(args, rank, world):
     lib.reactive_transport_stats(flow.transport, C.byref(stats1))
     launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
     tuned = {"fp64": flow.autotune(), "mixed": mixed.autotune()}
+    if args.stage_shape is not None:  # a fixed stage launch shape (e.g. for a profile of one stage kernel)
+        for form, f in (("fp64", flow), ("mixed", mixed)):
+            shapes = (C.c_uint * 3)(args.stage_shape, tuned[form]["gradient_block"], tuned[form]["cfl_block"])
+            assert f.lib.reactive_transport_launch_shapes_v3(f.transport, shapes, None) == 0
+            f.graph = None
+            tuned[form]["stage_block"] = args.stage_shape
     start = []
     graph_ms, clocks = timed_graph_steps(flow, True, start)
     mixed_ms, _ = timed_graph_steps(mixed, False)
@@ -932,6 +938,9 @@ def main():
                    help="run the ideal-gas blast box adjoint check on this cube size")
     p.add_argument("--adjoint-steps", type=int, default=50)
     p.add_argument("--skip-adjoint", action="store_true")
+    p.add_argument("--stage-shape", type=int, choices=(0, 1, 64, 96, 128), default=None,
+                   help="fix the structured stage's launch shape after autotuning (0 tiled, 1 split FP64 stage, "
+                        "64/96/128 per-cell block sizes); results do not depend on it")
     p.add_argument("--decompose", choices=("auto", "replicas", "slab"), default="auto",
                    help="N > 1: the case split into z-slabs with a halo exchange (strong scaling; the default) "
                         "or independent replicas (weak scaling); N = 1 runs the undivided case")
