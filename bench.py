@@ -939,7 +939,7 @@ def main():
     p.add_argument("--adjoint-steps", type=int, default=50)
     p.add_argument("--skip-adjoint", action="store_true")
     p.add_argument("--stage-shape", type=int, choices=(0, 1, 64, 96, 128), default=None,
-                   help="fix the structured stage's launch shape after autotuning (0 tiled, 1 split FP64 stage, "
+                   help="fix the structured stage's launch shape after autotuning (0 tiled, 1 split stage, "
                         "64/96/128 per-cell block sizes); results do not depend on it")
     p.add_argument("--decompose", choices=("auto", "replicas", "slab"), default="auto",
                    help="N > 1: the case split into z-slabs with a halo exchange (strong scaling; the default) "

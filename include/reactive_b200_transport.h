@@ -290,9 +290,9 @@ int reactive_transport_autotune_v3(void* transport, const double* q, const React
     void* stream, unsigned* chosen);
 /* Query (request NULL) or set the structured path's launch shapes {stage, gradient,
  * CFL} (no reference counterpart): stage 0 is the shared-memory tiled stage
- * kernel, 1 the split FP64 stage (each interior face's flux once into the face
- * workspace, then the per-cell sums; 128 threads per cell in mixed precision or
- * without the workspace), 64/96/128 the per-cell kernel's block size; gradient
+ * kernel, 1 the split stage (each interior face's flux once into the face
+ * workspace, then the per-cell sums; 128 threads per cell without the
+ * workspace), 64/96/128 the per-cell kernel's block size; gradient
  * and CFL block sizes 64/128/256. Results do not depend on them. active (may be
  * NULL) receives the shapes in use. */
 int reactive_transport_launch_shapes_v3(void* transport, const unsigned* request, unsigned* active);

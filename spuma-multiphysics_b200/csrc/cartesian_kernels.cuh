@@ -50,9 +50,10 @@ struct CartView {
     // minimum and the boundary ledger cover them only (a z-slab's halo layers
     // are read as neighbours, and written by the halo exchange)
     size_t ownBegin, ownEnd;
-    // scratch of the split FP64 stage (cartFaceFluxes / cartRatesFromFaces): one
-    // flux per interior face and variable, SoA (axis, variable) x cells, indexed
-    // by the face's owner (the lower cell); null where the split is unavailable
+    // scratch of the split stage (cartFaceFluxes / cartRatesFromFaces /
+    // cartRatesBoxSides): one flux per interior face and variable, SoA (axis,
+    // variable) x cells, indexed by the face's owner (the lower cell), and the
+    // layout below; null where the split is unavailable
     double* faceFlux;
 };
 
@@ -488,7 +489,7 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
 }
 
 // ---------------------------------------------------------------------------
-// The FP64 stage split in two launches, each interior face's flux evaluated once
+// The stage split in three launches, each interior face's flux evaluated once
 // instead of once by each of its two cells. cartFaceFluxes: the owner (lower
 // cell) of every +x/+y/+z interior face with an own cell on either side
 // evaluates it in the owner orientation, exactly the call both cells' per-cell
@@ -496,7 +497,8 @@ __global__ void __launch_bounds__(128) cartRates(CartView v, const double* __res
 // cartRatesFromFaces and cartRatesBoxSides: every own cell sums its six faces
 // in its face-graph incidence order (-z, -y, -x, +x, +y, +z, then the box
 // sides, evaluated as cartRates does) with the same signs and scaling, and
-// applies the same update: the results are bitwise cartRates<NS, double>'s.
+// applies the same update: the results are bitwise cartRates<NS, R>'s (FP64,
+// and FP32 faces with the compensated sums continued in the same order).
 // (defined with the CFL kernels below)
 template <bool SGS = false>
 __device__ __forceinline__ double faceSpeedCart(const CartView& v, int axis, double sgn, double dist, double w,
@@ -540,13 +542,14 @@ __device__ __forceinline__ double cellStep(const CartView& v, size_t c, double d
 // (cartSteps' per-cell steps from the same face speeds, each face's speed
 // evaluated once): the minimum over both kernels' block minima
 // (minimumReduce) is bitwise cartSteps'.
-template <int NS, bool SGS = false>
+template <int NS, class R, bool SGS = false>
 __global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* __restrict__ q,
                                                       const ReactiveTransportState* __restrict__ st,
-                                                      const double* __restrict__ grad,
-                                                      const double* __restrict__ nut, unsigned* error, bool cflPass) {
+                                                      const R* __restrict__ grad, const R* __restrict__ nut,
+                                                      unsigned* error, bool cflPass) {
     constexpr int NQ = NS + 4;
     const bool viscous = v.viscosity > 0 || v.wale;
+    R* flux = reinterpret_cast<R*>(v.faceFlux);
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         int i, j, k;
         cellCoords(v, c, i, j, k);
@@ -562,13 +565,13 @@ __global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* 
         if (!any) continue;
         CellData C;
         loadCell<NS, SGS>(v, q, st, c, C, true);
-        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        R gC[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
             for (int jj = 0; jj < 9; ++jj) gC[jj] = grad[size_t(jj) * v.cells + c];
         }
-        const double nutC = v.wale ? nut[c] : 0.0;
-        const CellT<double> cc = asCell<NS, double, SGS>(C);
+        const R nutC = v.wale ? nut[c] : R(0);
+        const CellT<R> cc = asCell<NS, R, SGS>(C);
         bool bad = false, faceBad = false;
 #pragma unroll 1
         for (int axis = 0; axis < 3; ++axis) {
@@ -578,40 +581,55 @@ __global__ void __launch_bounds__(128) cartFaceFluxes(CartView v, const double* 
             if (!ownC && !(nb >= v.ownBegin && nb < v.ownEnd)) continue;
             CellData N;
             loadCell<NS, SGS>(v, q, st, nb, N, true);
-            double gN[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            R gN[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
             if (viscous) {
 #pragma unroll
                 for (int jj = 0; jj < 9; ++jj) gN[jj] = grad[size_t(jj) * v.cells + nb];
             }
-            const double nutN = v.wale ? nut[nb] : 0.0;
-            double F[NQ];
-            faceFluxCart<NS, double, SGS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc,
-                                          asCell<NS, double, SGS>(N), gC, gN, nutC, nutN, F, bad, faceBad);
+            const R nutN = v.wale ? nut[nb] : R(0);
+            R F[NQ];
+            faceFluxCart<NS, R, SGS>(v, axis, 1.0, v.area[axis], v.dist[axis], .5, 0, true, cc,
+                                     asCell<NS, R, SGS>(N), gC, gN, nutC, nutN, F, bad, faceBad);
 #pragma unroll
-            for (int kk = 0; kk < NQ; ++kk) v.faceFlux[(size_t(axis) * NQ + kk) * v.cells + c] = F[kk];
+            for (int kk = 0; kk < NQ; ++kk) flux[(size_t(axis) * NQ + kk) * v.cells + c] = F[kk];
             if (cflPass)
                 v.faceFlux[splitSpeedOffset(NQ, v.cells) + size_t(axis) * v.cells + c] =
-                    faceSpeedCart<SGS>(v, axis, 1.0, v.dist[axis], .5, 0, C, N, nutC, nutN);
+                    faceSpeedCart<SGS>(v, axis, 1.0, v.dist[axis], .5, 0, C, N, double(nutC), double(nutN));
         }
         if (bad) atomicOr(error, 1u);
         if (faceBad) atomicOr(error, 2u);
     }
 }
 
+// A cell's sums over its faces, as cartRates forms them: FP64 adds each face's
+// sign * F / V; FP32 (mixed) keeps the Neumaier pair (sum, error) of the signed
+// fluxes and divides by the volume at the end in FP64.
+template <class R> struct FaceSums {
+    R rate, comp;
+    __device__ __forceinline__ void add(double sign, R F, double iv) {
+        if constexpr (sizeof(R) == sizeof(double)) rate += sign * F * iv;
+        else twoSum(rate, comp, sign > 0 ? F : -F);
+    }
+    __device__ __forceinline__ double value(double iv) const {
+        if constexpr (sizeof(R) == sizeof(double)) return double(rate);
+        else return (double(rate) + double(comp)) * iv;
+    }
+};
+
 // Every own cell's interior faces in its incidence order (-z, -y, -x, +x, +y,
 // +z) from the face fluxes, and for a cell off the box sides the update. A
 // cell on a box side leaves its partial sums in the scratch after the face
-// fluxes (variable-major, stride cells) for cartRatesBoxSides, which adds its
-// box-side faces in cartRates' order and applies the update: the two kernels
-// together give cartRates' sums bit for bit, and this one stays light (no
-// boundary flux code, far fewer registers).
-template <int NS>
+// fluxes (variable-major, stride cells; FP32: the sums then their errors) for
+// cartRatesBoxSides, which adds its box-side faces in cartRates' order and
+// applies the update: the two kernels together give cartRates' sums bit for
+// bit, and this one stays light (no boundary flux code, far fewer registers).
+template <int NS, class R>
 __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const double* __restrict__ q, double* out,
                                                           size_t outStride, int mode, double dt, double cfl,
                                                           double maximumStep) {
     constexpr int NQ = NS + 4;
-    const double* __restrict__ flux = v.faceFlux;
-    double* partial = v.faceFlux + size_t(3) * NQ * v.cells;
+    const R* __restrict__ flux = reinterpret_cast<const R*>(v.faceFlux);
+    R* partial = reinterpret_cast<R*>(v.faceFlux + size_t(3) * NQ * v.cells);
     const double* speed = v.faceFlux + splitSpeedOffset(NQ, v.cells);
     double* denominators = v.faceFlux + splitDenominatorOffset(NQ, v.cells);
     const bool cflPass = cfl > 0;
@@ -622,9 +640,9 @@ __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const doub
         cellCoords(v, c, i, j, k);
         const bool edge = i == 0 || i + 1 == v.nx || j == 0 || j + 1 == v.ny || k == 0 || k + 1 == v.nz;
         const double iv = v.invV[c];
-        double rate[NQ];
+        FaceSums<R> sum[NQ];
 #pragma unroll
-        for (int kk = 0; kk < NQ; ++kk) rate[kk] = 0.0;
+        for (int kk = 0; kk < NQ; ++kk) sum[kk] = FaceSums<R>{R(0), R(0)};
 #pragma unroll
         for (int n = 0; n < 6; ++n) {
             const int s = sideOf(n);
@@ -633,7 +651,7 @@ __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const doub
             const size_t owner = (s & 1) ? c : neighbourOf(v, s, c);
             const double sign = (s & 1) ? -1 : 1;
 #pragma unroll
-            for (int kk = 0; kk < NQ; ++kk) rate[kk] += sign * flux[(size_t(axis) * NQ + kk) * v.cells + owner] * iv;
+            for (int kk = 0; kk < NQ; ++kk) sum[kk].add(sign, flux[(size_t(axis) * NQ + kk) * v.cells + owner], iv);
         }
         if (cflPass) {
             // cartSteps' denominator over the interior faces, in the same order
@@ -654,12 +672,15 @@ __global__ void __launch_bounds__(256) cartRatesFromFaces(CartView v, const doub
         }
         if (edge) {
 #pragma unroll
-            for (int kk = 0; kk < NQ; ++kk) partial[size_t(kk) * v.cells + c] = rate[kk];
+            for (int kk = 0; kk < NQ; ++kk) {
+                partial[size_t(kk) * v.cells + c] = sum[kk].rate;
+                if constexpr (sizeof(R) != sizeof(double)) partial[size_t(NQ + kk) * v.cells + c] = sum[kk].comp;
+            }
             continue;
         }
 #pragma unroll
         for (int kk = 0; kk < NQ; ++kk) {
-            const double r = rate[kk], qk = q[size_t(kk) * v.all + c];
+            const double r = sum[kk].value(iv), qk = q[size_t(kk) * v.all + c];
             const size_t o = size_t(kk) * outStride + c;
             if (mode == 0) out[o] = r;
             else if (mode == 1) out[o] = qk + dt * r;
@@ -694,16 +715,16 @@ __device__ __forceinline__ size_t shellCell(const CartView& v, size_t e) {
 // The box-side faces of the own cells on the box's sides (after
 // cartRatesFromFaces), in cartRates' order, and their update: over the shell
 // of side cells, or over every cell when a dimension is below 3.
-template <int NS, bool SGS = false>
+template <int NS, class R, bool SGS = false>
 __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const double* __restrict__ q,
                                                          const ReactiveTransportState* __restrict__ st,
-                                                         const double* __restrict__ grad,
-                                                         const double* __restrict__ nut, double* out,
-                                                         size_t outStride, int mode, double dt, unsigned* error,
-                                                         double cfl, double maximumStep, unsigned stepBase) {
+                                                         const R* __restrict__ grad, const R* __restrict__ nut,
+                                                         double* out, size_t outStride, int mode, double dt,
+                                                         unsigned* error, double cfl, double maximumStep,
+                                                         unsigned stepBase) {
     constexpr int NQ = NS + 4;
     const bool viscous = v.viscosity > 0 || v.wale;
-    const double* partial = v.faceFlux + size_t(3) * NQ * v.cells;
+    const R* partial = reinterpret_cast<const R*>(v.faceFlux + size_t(3) * NQ * v.cells);
     const double* denominators = v.faceFlux + splitDenominatorOffset(NQ, v.cells);
     const bool cflPass = cfl > 0;
     double m = maximumStep;
@@ -717,26 +738,29 @@ __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const doubl
         if (!(i == 0 || i + 1 == v.nx || j == 0 || j + 1 == v.ny || k == 0 || k + 1 == v.nz)) continue;
         CellData C;
         loadCell<NS, SGS>(v, q, st, c, C, true);
-        double gC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        R gC[9] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
         if (viscous) {
 #pragma unroll
             for (int jj = 0; jj < 9; ++jj) gC[jj] = grad[size_t(jj) * v.cells + c];
         }
-        const double nutC = v.wale ? nut[c] : 0.0;
+        const R nutC = v.wale ? nut[c] : R(0);
         const double iv = v.invV[c];
-        double rate[NQ];
+        FaceSums<R> sum[NQ];
 #pragma unroll
-        for (int kk = 0; kk < NQ; ++kk) rate[kk] = partial[size_t(kk) * v.cells + c];
+        for (int kk = 0; kk < NQ; ++kk) {
+            sum[kk].rate = partial[size_t(kk) * v.cells + c];
+            sum[kk].comp = sizeof(R) == sizeof(double) ? R(0) : partial[size_t(NQ + kk) * v.cells + c];
+        }
         bool bad = false, faceBad = false;
 #pragma unroll
         for (int n = 6; n < 12; ++n) {
             const int s = sideOf(n);
             if (hasNeighbour(v, s, i, j, k)) continue;
-            double F[NQ];
+            R F[NQ];
             double sign;
-            sideFlux<NS, double, SGS>(v, q, st, grad, nut, c, s, false, i, j, k, C, gC, nutC, F, sign, bad, faceBad);
+            sideFlux<NS, R, SGS>(v, q, st, grad, nut, c, s, false, i, j, k, C, gC, nutC, F, sign, bad, faceBad);
 #pragma unroll
-            for (int kk = 0; kk < NQ; ++kk) rate[kk] += sign * F[kk] * iv;
+            for (int kk = 0; kk < NQ; ++kk) sum[kk].add(sign, F[kk], iv);
         }
         if (bad) atomicOr(error, 1u);
         if (faceBad) atomicOr(error, 2u);
@@ -753,7 +777,7 @@ __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const doubl
                 CellData Rt;
                 boundaryRight<NS, SGS>(v, nullptr, st, f, axis, C, Rt, false);
                 const double sp = faceSpeedCart<SGS>(v, axis, (s & 1) ? 1.0 : -1.0, f.distance, f.ownerWeight,
-                                                     f.kind, C, Rt, nutC, nutC);
+                                                     f.kind, C, Rt, double(nutC), double(nutC));
                 if (!isfinite(sp) || sp < 0) badSpeed = true;
                 else denominator += f.area * sp;
             }
@@ -761,7 +785,7 @@ __global__ void __launch_bounds__(128) cartRatesBoxSides(CartView v, const doubl
         }
 #pragma unroll
         for (int kk = 0; kk < NQ; ++kk) {
-            const double r = rate[kk];
+            const double r = sum[kk].value(iv);
             const size_t o = size_t(kk) * outStride + c;
             if (mode == 0) out[o] = r;
             else if (mode == 1) out[o] = C.q[kk] + dt * r;

@@ -593,34 +593,35 @@ struct Transport {
         }
     };
     template <int NS> struct RatesK {
-        // The split FP64 stage (cartFaceFluxes, cartRatesFromFaces,
-        // cartRatesBoxSides); with cfl > 0 also the CFL step of the same state
+        // The split stage (cartFaceFluxes, cartRatesFromFaces, cartRatesBoxSides)
+        // in arithmetic type R; with cfl > 0 also the CFL step of the same state
         // into *result (cartSteps' minimum, from the same face speeds).
-        static void split(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
-                          const double* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
-                          double cfl, double maximumStep, double* result, cudaStream_t s) {
+        template <class R>
+        static void split(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
+                          const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error, double cfl,
+                          double maximumStep, double* result, cudaStream_t s) {
             const bool cflPass = cfl > 0;
             const unsigned grid = gridFor(b.cells, 128), cellGrid = gridFor(b.cells, 256);
-            if (b.sgs) cartFaceFluxes<NS, true><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error, cflPass);
-            else cartFaceFluxes<NS><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error, cflPass);
-            cartRatesFromFaces<NS><<<cellGrid, 256, 0, s>>>(b, q, out, stride, mode, dt, cfl, maximumStep);
+            if (b.sgs) cartFaceFluxes<NS, R, true><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error, cflPass);
+            else cartFaceFluxes<NS, R><<<grid, 128, 0, s>>>(b, q, st, grad, nut, error, cflPass);
+            cartRatesFromFaces<NS, R><<<cellGrid, 256, 0, s>>>(b, q, out, stride, mode, dt, cfl, maximumStep);
             const bool shell = b.nx >= 3 && b.ny >= 3 && b.nz >= 3;
             const size_t sides = shell ? 2 * size_t(b.nx) * b.ny
                                              + size_t(b.nz - 2) * (2 * size_t(b.nx) + 2 * size_t(b.ny - 2))
                                        : b.cells;
             const unsigned sideGrid = gridFor(sides, 128);
             if (b.sgs)
-                cartRatesBoxSides<NS, true><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error,
-                                                                    cfl, maximumStep, cellGrid);
+                cartRatesBoxSides<NS, R, true><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt,
+                                                                       error, cfl, maximumStep, cellGrid);
             else
-                cartRatesBoxSides<NS><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error, cfl,
-                                                              maximumStep, cellGrid);
+                cartRatesBoxSides<NS, R><<<sideGrid, 128, 0, s>>>(b, q, st, grad, nut, out, stride, mode, dt, error,
+                                                                 cfl, maximumStep, cellGrid);
             if (cflPass)
                 minimumReduce<<<1, 1024, 0, s>>>(b.faceFlux + splitStepOffset(NQ, b.cells), size_t(cellGrid) + sideGrid,
                                                  result);
         }
         static constexpr int NQ = NS + 4;
-        // block 0: the shared-memory tiled kernel; 1: the split FP64 stage;
+        // block 0: the shared-memory tiled kernel; 1: the split stage;
         // otherwise the per-cell kernel with that many threads a block (all give
         // the same bits)
         template <class R, bool SGS>
@@ -646,14 +647,12 @@ struct Transport {
         static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
                         const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error,
                         unsigned block, cudaStream_t s) {
-            // block 1: the split FP64 stage (face fluxes once, then the per-cell sums;
-            // the same bits); elsewhere, or without its scratch, 128 threads per cell
+            // block 1: the split stage (face fluxes once, then the per-cell sums; the
+            // same bits); without its scratch, 128 threads per cell
             if (block == 1) {
-                if constexpr (sizeof(R) == sizeof(double)) {
-                    if (b.faceFlux) {
-                        split(b, q, st, grad, nut, out, stride, mode, dt, error, 0.0, 0.0, nullptr, s);
-                        return;
-                    }
+                if (b.faceFlux) {
+                    split<R>(b, q, st, grad, nut, out, stride, mode, dt, error, 0.0, 0.0, nullptr, s);
+                    return;
                 }
                 block = 128;
             }
@@ -671,10 +670,12 @@ struct Transport {
         }
     };
     template <int NS> struct SplitK {
-        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const double* grad,
-                        const double* nut, double* out, size_t stride, int mode, double dt, unsigned* error, double cfl,
+        template <class R>
+        static void run(const CartView& b, const double* q, const ReactiveTransportState* st, const R* grad,
+                        const R* nut, double* out, size_t stride, int mode, double dt, unsigned* error, double cfl,
                         double maximumStep, double* result, cudaStream_t s) {
-            RatesK<NS>::split(b, q, st, grad, nut, out, stride, mode, dt, error, cfl, maximumStep, result, s);
+            RatesK<NS>::template split<R>(b, q, st, grad, nut, out, stride, mode, dt, error, cfl, maximumStep, result,
+                                          s);
         }
     };
     template <int NS> struct StepsK {
@@ -740,28 +741,33 @@ struct Transport {
     // gradients and eddy viscosities when WALE is on, and the stage reuses them.
     void launchBoxStepStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt,
                             int stage, double* rate, double cfl, double maximumStep, double* result, cudaStream_t s) {
-        if (!mixed && launch.rates == 1) {
-            const CartView b = boxView();
-            if (b.faceFlux) {
-                // the split stage forms the CFL step of the same state with its fluxes
-                launchBoxGradientsT(state, v.grad, v.nut, s);
-                if (rate) {
-                    bySpecies<LedgerK>(b, qIn, state, static_cast<const double*>(v.grad),
-                                       static_cast<const double*>(v.nut), ledgerPartial, ledgerBlocks, s);
-                    foldPartials<<<1, 32 * unsigned(cfg.variables), 0, s>>>(ledgerPartial, int(ledgerBlocks),
-                                                                            int(cfg.variables), rate);
-                    launched();
-                }
-                bySpecies<SplitK>(b, qIn, state, static_cast<const double*>(v.grad), static_cast<const double*>(v.nut),
-                                  qOut, v.all, stage == 0 ? 1 : 2, dt, flags, cfl, maximumStep, result, s);
-                ++deviceProfile.cflFaceLaunches;
-                ++deviceProfile.transportFaceLaunches;
-                return;
-            }
+        if (launch.rates == 1 && boxView().faceFlux) {
+            // the split stage forms the CFL step of the same state with its fluxes
+            if (mixed) launchSplitStepStage(qIn, qOut, state, dt, stage, rate, cfl, maximumStep, result, gradF, nutF, s);
+            else launchSplitStepStage(qIn, qOut, state, dt, stage, rate, cfl, maximumStep, result, v.grad, v.nut, s);
+            return;
         }
         launchBoxStep(state, cfl, maximumStep, result, s);
         if (mixed) launchBoxStageT(qIn, qOut, state, dt, stage, rate, gradF, nutF, s, v.wale);
         else launchBoxStageT(qIn, qOut, state, dt, stage, rate, v.grad, v.nut, s, v.wale);
+    }
+    template <class R>
+    void launchSplitStepStage(const double* qIn, double* qOut, const ReactiveTransportState* state, double dt,
+                              int stage, double* rate, double cfl, double maximumStep, double* result, R* grad,
+                              R* nut, cudaStream_t s) {
+        const CartView b = boxView();
+        launchBoxGradientsT(state, grad, nut, s);
+        if (rate) {
+            bySpecies<LedgerK>(b, qIn, state, static_cast<const R*>(grad), static_cast<const R*>(nut), ledgerPartial,
+                               ledgerBlocks, s);
+            foldPartials<<<1, 32 * unsigned(cfg.variables), 0, s>>>(ledgerPartial, int(ledgerBlocks),
+                                                                    int(cfg.variables), rate);
+            launched();
+        }
+        bySpecies<SplitK>(b, qIn, state, static_cast<const R*>(grad), static_cast<const R*>(nut), qOut, v.all,
+                          stage == 0 ? 1 : 2, dt, flags, cfl, maximumStep, result, s);
+        ++deviceProfile.cflFaceLaunches;
+        ++deviceProfile.transportFaceLaunches;
     }
     void launchBoxStep(const ReactiveTransportState* state, double cfl, double maximumStep, double* result,
                        cudaStream_t s) {

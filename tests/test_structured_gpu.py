@@ -375,8 +375,9 @@ TILE_BOXES = BOXES + [
 def test_tiled_stage_kernel_equals_per_cell_kernel(spec, path):
     """The shared-memory tiled stage kernel (launch shape 0: each x and y face
     evaluated once per plane into shared memory, z faces carried down the
-    column) and the split FP64 stage (shape 1: each interior face's flux once,
-    then the per-cell sums; the per-cell kernel in mixed precision) give the
+    column) and the split stage (shape 1: each interior face's flux once, then
+    the per-cell sums, in mixed precision the compensated sums continued in the
+    same order) give the
     per-cell kernel's stage results bit for bit: both stages, the CFL step and
     the boundary ledger, across tiles and z-chunks."""
     import torch
@@ -446,10 +447,10 @@ def _stage_cfl_pair(L, h, case, stream, torch):
                 status=status.value)
 
 
-@pytest.mark.parametrize("path", ["fp64", "hllc"])
+@pytest.mark.parametrize("path", ["fp64", "mixed", "hllc"])
 @pytest.mark.parametrize("spec", TILE_BOXES, ids=lambda s: "x".join(map(str, s["dims"])) + f"-ns{s['ns']}")
 def test_split_stage_with_its_cfl_step_equals_per_cell_kernels(spec, path):
-    """The combined CFL + stage entry with the split FP64 stage (launch shape 1:
+    """The combined CFL + stage entry with the split stage (launch shape 1:
     the CFL step formed from the face speeds the face pass evaluates once,
     beside the fluxes) gives the per-cell kernels' CFL steps, stages and
     boundary ledgers bit for bit, on both stages."""
@@ -460,7 +461,9 @@ def test_split_stage_with_its_cfl_step_equals_per_cell_kernels(spec, path):
     case = box_case(spec["dims"], spec["ns"], kinds, spec.get("viscous", False), spec.get("conduction", False))
     h = T.create(lib, 1, case, wale_cw=spec.get("wale"))
     try:
-        if path == "hllc":
+        if path == "mixed":
+            assert L.reactive_transport_precision_v3(h, 1, None) == 0
+        elif path == "hllc":
             assert L.reactive_transport_flux_v3(h, 1, None) == 0
         stream = torch.cuda.current_stream().cuda_stream
         runs = []
