@@ -580,10 +580,11 @@ struct Transport {
     // times the candidates on the handle's own problem and keeps the fastest;
     // the results do not depend on them).
     struct BoxLaunch {
-        // rates 0 selects the shared-memory tiled stage kernel; the per-cell kernel
-        // with 96 threads a block is the default (the faster of the two on the
-        // 160^3 box on B200, FP64 and mixed; the autotuner times both)
-        unsigned rates = 96, gradients = 256, steps = 256;
+        // rates 0 selects the shared-memory tiled stage kernel, 1 the split stage
+        // (the default: the fastest on the 160^3 box on B200, FP64 and mixed; it
+        // runs the per-cell kernel where the face workspace cannot hold its
+        // scratch), 64/96/128 the per-cell kernel; the autotuner times them all
+        unsigned rates = 1, gradients = 128, steps = 256;
     } launch;
     template <int NS> struct GradientsK {
         template <class R>
