@@ -55,6 +55,7 @@ UNIT = "Mcell-steps/s"
 # (more cells than resident threads, as at 160^3, so the pass's stack frames do
 # not stay in L2).
 FLOPS_PER_PHASE_EVAL = 617.9
+FLASH_BYTES_PER_CELL = 40 + 24 + 184 + 56
 DRAM_BYTES_PER_PHASE_EVAL = 174.4
 VISCOSITY, CONDUCTIVITY, WALE_CW, DT = 1.821e-5, 0.02587, 0.325, 1e-8
 REFERENCE_SAMPLE = 40  # cube size of the reference CPU arm's bounded sample
@@ -581,7 +582,13 @@ def run_ours(args, rank, world):
                     "traffic_note": "DRAM bytes per launch, ncu per-phase-evaluation figure x this launch's "
                                     "phase evaluations",
                     "ms_per_launch": flash_ms, "phase_evaluations_per_launch": flash_phase_evals,
-                    "flops_per_phase_evaluation": flops_per_eval}
+                    "flops_per_phase_evaluation": flops_per_eval,
+                    # a recovery's own bytes: the conserved row (40 B) and the seed's p, T and
+                    # liquid mass (24 B) read, the thermo state (184 B) and transport state
+                    # (56 B) written
+                    "algorithmic_bytes_per_launch": FLASH_BYTES_PER_CELL * cells,
+                    "traffic_over_algorithmic": args.dram_bytes_per_phase_eval * flash_phase_evals
+                    / (FLASH_BYTES_PER_CELL * cells)}
     # HBM roofline of the whole step (algorithmic bytes per cell-step, FP64, nv=5, 4 transport thermo fields)
     bytes_per_cell_step = 8 * (5 * 5 + 2 * 4) + 2 * (8 * 5 + 80)
     hbm = peaks.get("hbm_gbs", 6650.0)
