@@ -1701,51 +1701,66 @@ __global__ void __launch_bounds__(128) cartViscousGradVjp(CartView v, const doub
 }
 
 // gBar += nutBar * d nu_t / d g per cell (the WALE eddy viscosity of the cell's
-// gradient, the Nicoud-Ducros relation of wale.cuh written for duals:
+// gradient, the Nicoud-Ducros relation of wale.cuh:
 // nu_t = (Cw Delta)^2 |g|_max (Sd:Sd)^(3/2) / ((S:S)^(5/2) + (Sd:Sd)^(5/4))
-// with the invariants of g / |g|_max; zero where the forward gives zero).
+// with the invariants of g / |g|_max; zero where the forward gives zero), by a
+// reverse pass derived by hand.
 __global__ void cartWaleVjp(CartView v, const double* __restrict__ grad, const double* __restrict__ nutBar,
                             double* __restrict__ gBar) {
-    using D = Dual<9>;
+    // nu_t = (Cw Delta)^2 |g|_max ratio(g / |g|_max) and ratio is homogeneous of
+    // degree one, so d nu_t / d g = (Cw Delta)^2 d ratio / d h at h = g / |g|_max
+    // (the normalisation's own derivative cancels). With ratio = dd^(3/2) /
+    // (ss^(5/2) + dd^(5/4)), ss = S:S (S = sym h), dd = D:D (D = dev sym(h h)):
+    // d ss / d h = 2 S and d dd / d h = G h^T + h^T G with G = 2 D.
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < v.cells; c += size_t(blockDim.x) * gridDim.x) {
         const double nb = nutBar[c];
         if (nb == 0) continue;
-        D g[9];
-        int largest = 0;
+        double g[9], scale = 0;
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
-            g[t] = D::seed(grad[size_t(t) * v.cells + c], t);
-            if (::fabs(g[t].v) > ::fabs(g[largest].v)) largest = t;
+            g[t] = grad[size_t(t) * v.cells + c];
+            scale = fmax(scale, ::fabs(g[t]));
         }
         const double delta = cbrt(1 / v.invV[c]);
-        if (g[largest].v == 0 || v.cw == 0 || delta == 0) continue;
-        D scale = fabs(g[largest]);
-        D h[9];
+        if (scale == 0 || v.cw == 0 || delta == 0) continue;
+        double h[9];
 #pragma unroll
         for (int t = 0; t < 9; ++t) h[t] = g[t] / scale;
-        D sq[9];
+        double sq[9];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) sq[3 * a + b] = h[3 * a] * h[b] + h[3 * a + 1] * h[3 + b] + h[3 * a + 2] * h[6 + b];
-        const D trace = sq[0] + sq[4] + sq[8];
-        D ss(0.0), dd(0.0);
+        const double trace = sq[0] + sq[4] + sq[8];
+        double S[9], G[9], ss = 0, dd = 0;
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                const D sab = D(.5) * (h[3 * a + b] + h[3 * b + a]);
-                D dab = D(.5) * (sq[3 * a + b] + sq[3 * b + a]);
-                if (a == b) dab = dab - trace / D(3.0);
+                const double sab = .5 * (h[3 * a + b] + h[3 * b + a]);
+                double dab = .5 * (sq[3 * a + b] + sq[3 * b + a]);
+                if (a == b) dab -= trace / 3.0;
+                S[3 * a + b] = sab;
+                G[3 * a + b] = 2 * dab;
                 ss += sab * sab;
                 dd += dab * dab;
             }
-        if (!(dd.v > 0)) continue;
-        const D rootD = sqrt(dd);
-        const D ratio = dd * rootD / (ss * ss * sqrt(ss) + dd * sqrt(rootD));
-        const D nutD = D(v.cw * delta * v.cw * delta) * scale * ratio;
+        if (!(dd > 0)) continue;
+        const double rootD = sqrt(dd), quarter = sqrt(rootD), rootS = sqrt(ss);
+        const double numerator = dd * rootD, denominator = ss * ss * rootS + dd * quarter;
+        const double den2 = denominator * denominator;
+        const double rDd = (1.5 * rootD * denominator - numerator * 1.25 * quarter) / den2;
+        const double rSs = -numerator * 2.5 * ss * rootS / den2;
+        const double weight = nb * (v.cw * delta * v.cw * delta);
 #pragma unroll
-        for (int t = 0; t < 9; ++t) gBar[size_t(t) * v.cells + c] += nb * nutD.d[t];
+        for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int w = 0; w < 3; ++w) {
+                double dDd = 0;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) dDd += G[3 * u + k] * h[3 * w + k] + G[3 * k + w] * h[3 * k + u];
+                gBar[size_t(3 * u + w) * v.cells + c] += weight * (rDd * dDd + rSs * 2 * S[3 * u + w]);
+            }
     }
 }
 

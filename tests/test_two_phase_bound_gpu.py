@@ -93,6 +93,36 @@ def test_bound_keeps_states_at_the_dome_edge_bitwise():
     assert_same(on, off)
 
 
+def test_bound_keeps_states_near_the_critical_point_and_the_table_ends_bitwise():
+    """Single-phase states on both branches at pressures from 1e-9 to 1e-2 of
+    the saturation pressure on either side, at temperatures up to 0.1 K below
+    the critical point (305-309.4 K, where the tie lines collapse) and at the
+    saturation table's cold end (the liquid range's lower end, 148 K, and just
+    above it), seeded at their own (p, T): with the bound on (and with it the
+    saturation-table stability shortcut) every bit equals the exhaustive
+    search's."""
+    fluid = PureFluid(N2O)
+    T = np.concatenate([[148.0, 148.0 + 1e-6, 148.01, 148.5, 150.0], np.linspace(305.0, 309.4, 12)])
+    ps, _, _ = fluid.saturation(T)
+    ps = np.where(T > 308.0, 7.2446e6, ps)  # above 308 K: about the critical pressure
+    offsets = np.concatenate([-np.logspace(-9, -2, 8), [0.0], np.logspace(-9, -2, 8)])
+    rho, e, seeds = [], [], []
+    for root in ("gas", "liquid"):
+        for d in offsets:
+            p = ps * (1 + d)
+            props = fluid.tp(T, p, root=root)
+            ok = np.isfinite(props["rho"]) & np.isfinite(props["e"]) & (props["rho"] > 0)
+            rho.append(props["rho"][ok])
+            e.append(props["rho"][ok] * props["e"][ok])
+            g = np.zeros(int(ok.sum()), dtype=A.THERMO_DTYPE)
+            g["p"], g["T"], g["rho"] = p[ok], T[ok], props["rho"][ok]
+            seeds.append(g)
+    rho, e, guess = np.concatenate(rho), np.concatenate(e), np.concatenate(seeds)
+    assert len(rho) > 400
+    on, off = both(rho, e, guess)
+    assert_same(on, off)
+
+
 def test_bound_keeps_the_impingement_flash_bitwise():
     from spuma_multiphysics_b200.flow import Flow
     n = 24
