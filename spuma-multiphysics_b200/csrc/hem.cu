@@ -350,12 +350,14 @@ __device__ __forceinline__ void appendTo(unsigned* list, unsigned* counter, bool
 // FROM_CONSERVED: the pass forms each cell's inputs itself from the SoA conserved
 // rows and the seeds (as inputsFromConserved does) and stores them in `in` only
 // for the cells it hands to the work queue or the restart search, the two later
-// readers of `in`; the cells it decides never write their inputs.
+// readers of `in`; the cells it decides never write their inputs. `seed` may be
+// `state` (an in-place recovery): a thread reads its own cell's seed before it
+// writes that cell's state and touches no other cell's.
 template <bool FROM_CONSERVED>
 __global__ void __launch_bounds__(kPassThreads, RB200_PASS_MINBLOCKS) passSinglePhase(const HemConst* __restrict__ Cp,
                                                                 CellInput* __restrict__ in,
                                                                 const double* __restrict__ cons, size_t stride,
-                                                                const ReactiveThermoState* __restrict__ seed,
+                                                                const ReactiveThermoState* seed,
                                                                 size_t count, ReactiveThermoState* state,
                                                                 ReactiveTransportState* transport, int* success,
                                                                 unsigned* list, unsigned* fallback, unsigned* counters,
