@@ -74,6 +74,34 @@ def load_package():
     return sys.modules[name]
 
 
+def step_kernels(stream, launch):
+    """Kernels one step launches: `launch` (the step's launches, as a step graph
+    records them) captured into a throwaway CUDA graph that is never replayed,
+    and its kernel nodes counted through the driver API. None when that fails."""
+    import torch
+    try:
+        cuda = C.CDLL("libcuda.so.1")
+        g = torch.cuda.CUDAGraph(keep_graph=True)
+        with torch.cuda.graph(g, stream=stream):
+            launch()
+        handle = C.c_void_p(g.raw_cuda_graph())
+        count = C.c_size_t(0)
+        if cuda.cuGraphGetNodes(handle, None, C.byref(count)):
+            return None
+        nodes = (C.c_void_p * count.value)()
+        if count.value and cuda.cuGraphGetNodes(handle, nodes, C.byref(count)):
+            return None
+        kind, total = C.c_int(), 0
+        for node in nodes[:count.value]:
+            if cuda.cuGraphNodeGetType(C.c_void_p(node), C.byref(kind)):
+                return None
+            total += kind.value == 0  # CU_GRAPH_NODE_TYPE_KERNEL
+        del g
+        return total
+    except (OSError, AttributeError, RuntimeError, TypeError):
+        return None
+
+
 def workload(n, precision="FP64 (state, transport and flash)"):
     q_mb = 5 * 8 * n ** 3 / 1e6
     return {"workload": f"N2O impingement {n}^3 ({n ** 3:,} cells), 40 bar ambient, 2 liquid inlets, "
@@ -353,7 +381,8 @@ def run_slab(args, rank, world):
     stats1 = pkg._abi.Stats()
     f.lib.reactive_transport_stats(f.transport, C.byref(stats1))
     # transport launches counted by the handle while capturing both half steps,
-    # plus five per flash (inputs, queue, select, restart queue, restart select)
+    # plus five per flash (single-phase pass, queue, selection, restart queue,
+    # restart selection)
     launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
 
     def barrier():
@@ -445,14 +474,16 @@ def run_ours(args, rank, world):
         f.check(DT)
         return max_over_ranks_(a.elapsed_time(b) / steps), clocks_
 
-    # kernels launched per step: transport launches counted by the handle, plus
-    # five per flash (inputs, queue, select, restart queue, restart select)
+    # kernels launched per step: the kernel nodes of the step's launches captured
+    # once more (else the transport's call count plus five per flash:
+    # single-phase pass, queue, selection, restart queue, restart selection)
     stats0 = pkg._abi.Stats()
     lib.reactive_transport_stats(flow.transport, C.byref(stats0))
     flow.capture(DT)
     stats1 = pkg._abi.Stats()
     lib.reactive_transport_stats(flow.transport, C.byref(stats1))
-    launches_per_step = int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5
+    launches_per_step = (step_kernels(flow.stream, lambda: flow._launch_step(DT))
+                         or int(stats1.kernelLaunches - stats0.kernelLaunches) + 2 * 5)
     tuned = {"fp64": flow.autotune(), "mixed": mixed.autotune()}
     if args.stage_shape is not None:  # a fixed stage launch shape (e.g. for a profile of one stage kernel)
         for form, f in (("fp64", flow), ("mixed", mixed)):
