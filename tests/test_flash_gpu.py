@@ -139,6 +139,40 @@ def test_cuda_flash_device_resident_matches_host_path(n):
     assert prof.flashCandidates > 0
 
 
+def test_cuda_flash_in_place_recovery_equals_separate_output():
+    """A device recovery whose seed array is also its output array (the step
+    driver's second recovery of a step) gives the same bits as one into a
+    separate array: the single-phase pass reads each cell's seed before it
+    writes that cell's state and touches no other cell's, and the work queue
+    and the restart search take their inputs from the records the pass stored.
+    The batch mixes cells outside the two-phase bound (decided in the pass) and
+    two-phase cells (the queue); a failed cell's output is its seed either way."""
+    import torch
+    n = 20000
+    q, e, guess = cases.flash_batch(n, seed=9090)
+    hem = GpuHem(capacity=n)
+    cons = torch.zeros((5, n), dtype=torch.float64, device="cuda")
+    cons[0] = torch.from_numpy(q).cuda()
+    cons[4] = torch.from_numpy(e).cuda()
+    seed = torch.from_numpy(guess.view(np.uint8).copy()).cuda()
+    stream = torch.cuda.current_stream().cuda_stream
+    out = torch.zeros_like(seed)
+    tr_out = torch.zeros((n, 7), dtype=torch.float64, device="cuda")
+    ok_out = torch.zeros(n, dtype=torch.int32, device="cuda")
+    hem.run_device(cons, n, n, 5, seed, out, tr_out, ok_out, stream)
+    same = seed.clone()
+    tr_same = torch.zeros_like(tr_out)
+    ok_same = torch.zeros_like(ok_out)
+    hem.run_device(cons, n, n, 5, same, same, tr_same, ok_same, stream)
+    torch.cuda.synchronize()
+    ok = ok_out.cpu().numpy()
+    assert 0 < np.count_nonzero(ok) and np.array_equal(ok, ok_same.cpu().numpy())
+    assert np.array_equal(out.cpu().numpy(), same.cpu().numpy())
+    assert np.array_equal(tr_out.cpu().numpy(), tr_same.cpu().numpy())
+    labels = cases.phase_label(out.cpu().numpy().view(A.THERMO_DTYPE)[ok != 0])
+    assert len(np.unique(labels)) > 1  # single-phase and two-phase cells both present
+
+
 def test_cuda_flash_labels_match_reference_on_large_batch_sample():
     """Config-3 style batch (60% saturated two-phase states on 65,536
     temperature levels, 40% single phase), 40,000 cells: success flags and
